@@ -1,0 +1,99 @@
+/*
+ * pi_b200 -- exact big-integer multiplication on one NVIDIA B200 (sm_100a).
+ *
+ * C ABI of libpigpu.so, the drop-in boundary for the multiply hot path of
+ * f97johan/pi-compute. The reference's boundary is the C++ strategy interface
+ *
+ *     class pi::Multiplier {                                   (src/arithmetic/multiplier.h:16-39)
+ *       virtual void multiply(mpz_t result, const mpz_t a, const mpz_t b) = 0;    (:26)
+ *       virtual void square(mpz_t result, const mpz_t a) { multiply(result,a,a); } (:36-38)
+ *     };
+ *
+ * whose CUDA implementations are GpuNttMultiplier (src/arithmetic/gpu_ntt_multiplier.cpp:144-214)
+ * and IntNttMultiplier (src/arithmetic/int_ntt_multiplier.cpp:115-163), each a GMP <-> device
+ * bridge over an engine (src/gpu/ntt_engine.cu:109-158, src/gpu/int_ntt.cu:301-380).
+ * This header replaces those engines' entry points with plain pointers and sizes: magnitudes
+ * are little-endian arrays of 64-bit limbs, exactly the layout of mpz_limbs_read(); signs,
+ * zero and mpz_t reallocation stay in the C++ adaptor (B200Multiplier, host/b200_multiplier.h).
+ *
+ * Errors are integer status codes (the reference throws std::runtime_error from CUDA_CHECK,
+ * src/gpu/int_ntt.cu:20-26). There is no CPU fallback: a product outside the proven exact
+ * range returns PG_ERR_TOO_LARGE instead of silently computing on the host (the reference's
+ * IntNttMultiplier falls back to mpz_mul, src/arithmetic/int_ntt_multiplier.cpp:146-151).
+ *
+ * Thread safety: every call on one context is serialised by an internal lock (the reference
+ * locks one mutex per GPU, src/arithmetic/gpu_ntt_multiplier.cpp:179-188).
+ */
+#ifndef PI_B200_H
+#define PI_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pg_status;
+#define PG_OK 0
+#define PG_ERR_OOM 1          /* device allocation failed */
+#define PG_ERR_TOO_LARGE 2    /* product outside the proven exact range of the transform */
+#define PG_ERR_BAD_ARG 3      /* null pointer, output too small, bad device index */
+#define PG_ERR_DEVICE 4       /* CUDA runtime error (message in pg_last_error) */
+#define PG_ERR_TIMEOUT 5      /* a bounded device-side wait ran out (carry look-back) */
+#define PG_ERR_INTERNAL 6     /* device consistency check failed (carry out of the top word) */
+
+typedef struct pg_ctx pg_ctx;
+
+/* Library version, (major << 16) | (minor << 8) | patch. */
+int pg_version(void);
+
+/* Create a context on CUDA device `device`: builds the twiddle tables and a stream.
+ * Replaces the engine constructors (ntt_engine.cu NttEngine::NttEngine, int_ntt.cu
+ * IntNttEngine::IntNttEngine, int_ntt.h:49). */
+pg_status pg_create(int device, pg_ctx** out);
+void pg_destroy(pg_ctx* ctx);
+
+/* Message for the last non-OK status on this context ("" if none). */
+const char* pg_last_error(const pg_ctx* ctx);
+
+/* Largest na + nb (in 64-bit limbs) that pg_mul accepts: transforms of up to 2^26
+ * points of 32-bit coefficients over three 31-bit primes. */
+size_t pg_mul_max_limbs(void);
+
+/* out = a * b for magnitudes in HOST memory (little-endian 64-bit limbs).
+ * out must have room for na + nb limbs (out_cap >= na + nb); *out_len receives the
+ * product's length without leading zero limbs (0 if either operand is empty).
+ * out may alias a or b: both are read completely before out is written.
+ * Replaces GpuNttMultiplier::multiply / IntNttMultiplier::multiply
+ * (gpu_ntt_multiplier.cpp:144-210, int_ntt_multiplier.cpp:115-159). */
+pg_status pg_mul(pg_ctx* ctx, const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                 size_t out_cap, size_t* out_len);
+
+/* out = a * a (two forward transforms fewer than pg_mul). Replaces the square()
+ * overrides, which call multiply(a, a) (gpu_ntt_multiplier.cpp:212-214, int_ntt_multiplier.cpp:161-163). */
+pg_status pg_sqr(pg_ctx* ctx, const uint64_t* a, size_t na, uint64_t* out, size_t out_cap, size_t* out_len);
+
+/* Device-resident forms: d_a, d_b, d_out are device addresses (16-byte aligned) on the
+ * context's device; d_out receives exactly na + nb limbs (leading zeros kept). The work is
+ * queued on the context's stream and the call returns without waiting; pg_sync waits and
+ * reports device-side errors. d_out must not overlap d_a or d_b.
+ * Replaces the device part of IntNttEngine::multiply (int_ntt.cu:301-380), which round-trips
+ * every operand through host memory. */
+pg_status pg_mul_device(pg_ctx* ctx, const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
+                        uint64_t* d_out);
+pg_status pg_sqr_device(pg_ctx* ctx, const uint64_t* d_a, size_t na, uint64_t* d_out);
+pg_status pg_sync(pg_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own work after it. */
+void* pg_stream(pg_ctx* ctx);
+
+/* Number of kernels this context has launched so far (diagnostics and benchmarks; the
+ * reference keeps per-multiplier call counters, gpu_ntt_multiplier.h:83-90). */
+uint64_t pg_launch_count(const pg_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PI_B200_H */

@@ -1,0 +1,189 @@
+"""pi-compute_b200: exact big-integer products on one B200 behind the pi::Multiplier boundary.
+
+Python side of the package: a ctypes binding of the C ABI in include/pi_b200.h
+(libpigpu.so) used by tests, smoke checks and the benchmark, plus operand
+helpers. The product path is native; nothing here computes a product on the CPU.
+If the shared library is missing the import of :class:`Engine` fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+LIBPIGPU = os.path.join(HERE, "libpigpu.so")
+LIBPIB200 = os.path.join(HERE, "libpib200.so")
+PI_B200_BIN = os.path.join(HERE, "pi_b200")
+HEADERS = [os.path.join(ROOT, "include", "pi_b200.h")]
+
+PG_OK = 0
+PG_ERR_OOM = 1
+PG_ERR_TOO_LARGE = 2
+PG_ERR_BAD_ARG = 3
+PG_ERR_DEVICE = 4
+PG_ERR_TIMEOUT = 5
+PG_ERR_INTERNAL = 6
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_sizep = ctypes.POINTER(ctypes.c_size_t)
+
+
+class PgError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"pg status {status}: {msg}")
+        self.status = status
+
+
+_lib: Optional[ctypes.CDLL] = None
+
+
+def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
+    """Load libpigpu.so and declare the C ABI signatures. Raises if the library is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"{path} not built: run `python pi-compute_b200/build.py`")
+    lib = ctypes.CDLL(path)
+    lib.pg_version.restype = ctypes.c_int
+    lib.pg_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    lib.pg_create.restype = ctypes.c_int
+    lib.pg_destroy.argtypes = [ctypes.c_void_p]
+    lib.pg_destroy.restype = None
+    lib.pg_last_error.argtypes = [ctypes.c_void_p]
+    lib.pg_last_error.restype = ctypes.c_char_p
+    lib.pg_mul_max_limbs.restype = ctypes.c_size_t
+    lib.pg_mul.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, _u64p,
+                           ctypes.c_size_t, _sizep]
+    lib.pg_mul.restype = ctypes.c_int
+    lib.pg_sqr.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_size_t, _sizep]
+    lib.pg_sqr.restype = ctypes.c_int
+    lib.pg_mul_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                                  ctypes.c_size_t, ctypes.c_void_p]
+    lib.pg_mul_device.restype = ctypes.c_int
+    lib.pg_sqr_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+    lib.pg_sqr_device.restype = ctypes.c_int
+    lib.pg_sync.argtypes = [ctypes.c_void_p]
+    lib.pg_sync.restype = ctypes.c_int
+    lib.pg_stream.argtypes = [ctypes.c_void_p]
+    lib.pg_stream.restype = ctypes.c_void_p
+    lib.pg_launch_count.argtypes = [ctypes.c_void_p]
+    lib.pg_launch_count.restype = ctypes.c_uint64
+    _lib = lib
+    return lib
+
+
+def declared_symbols() -> list[str]:
+    """Every function name declared in include/*.h (the C ABI the library must export)."""
+    import re
+
+    names = []
+    for h in HEADERS:
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(pg_\w+)\s*\(", text, flags=re.M):
+            names.append(m.group(1))
+    return sorted(set(names))
+
+
+# ------------------------------------------------------------------ limb helpers
+def int_to_limbs(x: int) -> np.ndarray:
+    """Magnitude of x as little-endian uint64 limbs (empty for 0)."""
+    x = abs(int(x))
+    n = (x.bit_length() + 63) // 64
+    if n == 0:
+        return np.zeros(0, dtype=np.uint64)
+    return np.frombuffer(x.to_bytes(8 * n, "little"), dtype="<u8").astype(np.uint64)
+
+
+def limbs_to_int(a: np.ndarray) -> int:
+    a = np.ascontiguousarray(a, dtype="<u8")
+    return int.from_bytes(a.tobytes(), "little")
+
+
+def splitmix64(seed: int, n: int) -> np.ndarray:
+    """n outputs of the splitmix64 generator started at `seed` (vectorised)."""
+    with np.errstate(over="ignore"):
+        idx = np.arange(1, n + 1, dtype=np.uint64)
+        z = np.uint64(seed) + idx * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return z
+
+
+def random_operand(n: int, seed: int) -> np.ndarray:
+    """Uniform random n-limb operand with the top limb's most significant bit set (exact length)."""
+    a = splitmix64(seed, n)
+    if n:
+        a[-1] |= np.uint64(1 << 63)
+    return a
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_u64p)
+
+
+class Engine:
+    """One pg_ctx (device context, twiddle tables, workspace) on a CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load_library()
+        ctx = ctypes.c_void_p()
+        st = self.lib.pg_create(device, ctypes.byref(ctx))
+        if st != PG_OK:
+            raise PgError(st, f"pg_create(device={device}) failed")
+        self.ctx = ctx
+
+    def close(self) -> None:
+        if self.ctx:
+            self.lib.pg_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self) -> str:
+        return self.lib.pg_last_error(self.ctx).decode()
+
+    def _check(self, st: int) -> None:
+        if st != PG_OK:
+            raise PgError(st, self.last_error())
+
+    def mul_limbs(self, a: np.ndarray, b: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        b = np.ascontiguousarray(b, dtype=np.uint64)
+        out = np.zeros(max(len(a) + len(b), 1), dtype=np.uint64)
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.pg_mul(self.ctx, _ptr(a), len(a), _ptr(b), len(b), _ptr(out), len(out),
+                                    ctypes.byref(n)))
+        return out[: n.value]
+
+    def sqr_limbs(self, a: np.ndarray) -> np.ndarray:
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        out = np.zeros(max(2 * len(a), 1), dtype=np.uint64)
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.pg_sqr(self.ctx, _ptr(a), len(a), _ptr(out), len(out), ctypes.byref(n)))
+        return out[: n.value]
+
+    def mul(self, a: int, b: int) -> int:
+        """Signed product like GmpMultiplier::multiply: sign handled here, magnitudes on the GPU."""
+        sign = (-1 if a < 0 else 1) * (-1 if b < 0 else 1)
+        r = limbs_to_int(self.mul_limbs(int_to_limbs(a), int_to_limbs(b)))
+        return -r if sign < 0 else r
+
+    def sqr(self, a: int) -> int:
+        return limbs_to_int(self.sqr_limbs(int_to_limbs(a)))

@@ -1,0 +1,240 @@
+// Exact CRT recombination of the three inverse-transformed residue arrays and
+// the carry-propagation scan that turns the convolution into product limbs.
+//
+// Coefficient i of the (w = 32) convolution is x_i < p0*p1*p2 < 2^91, rebuilt
+// by Garner's method with all constants precomputed (scale L^-1 * 2^32 for the
+// unnormalised inverse transform and the Montgomery pointwise product folded
+// into them). Output 32-bit word j receives
+//     W_j = x_j[0] + x_{j-1}[1] + x_{j-2}[2]      (x[k] = 32-bit word k of x)
+// so W_j < 2^33 + 2^27 and every carry between words is 0, 1 or 2.
+//
+// The scan: each thread owns 16 consecutive words; its carry behaviour is the
+// transfer function f: {0,1,2} -> {0,1,2} (carry in -> carry out), packed in 6
+// bits. Functions compose associatively, so a warp scan, a block scan and a
+// decoupled look-back across blocks (single pass, CTA order fixed by an atomic
+// ticket so every predecessor is resident) give each thread its exact carry in.
+// Every spin in the look-back has an iteration limit; running out sets an error
+// word the host checks, and the kernel finishes without hanging.
+#pragma once
+#include <cstdint>
+
+#include "modarith.cuh"
+#include "types.cuh"
+
+namespace pg {
+
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+struct X3 {
+    uint32_t w0, w1, w2;
+};
+
+__device__ __forceinline__ X3 crt3(uint32_t r0, uint32_t r1, uint32_t r2, const CrtConsts& k) {
+    const uint32_t p0 = kPrime(0), p1 = kPrime(1), p2 = kPrime(2);
+    uint32_t x0 = mul_shoup(r0, k.c00, k.c00p, p0);
+    uint32_t y1 = sub_mod(mul_shoup(r1, k.c11, k.c11p, p1), mul_shoup(x0, k.k01, k.k01p, p1), p1);
+    uint32_t t1 = mul_shoup(r2, k.c22, k.c22p, p2);
+    uint32_t t2 = mul_shoup(x0, k.k02, k.k02p, p2);
+    uint32_t t3 = mul_shoup(y1, k.k12, k.k12p, p2);
+    uint32_t y2 = sub_mod(sub_mod(t1, t2, p2), t3, p2);
+    uint64_t lo = (uint64_t)x0 + (uint64_t)p0 * y1;  // < 2^63
+    uint64_t plo = k.p01 * (uint64_t)y2;
+    uint64_t phi = __umul64hi(k.p01, (uint64_t)y2);
+    uint64_t s = lo + plo;
+    phi += (s < lo);
+    X3 r;
+    r.w0 = (uint32_t)s;
+    r.w1 = (uint32_t)(s >> 32);
+    r.w2 = (uint32_t)phi;
+    return r;
+}
+
+// f packed as f(0) | f(1) << 2 | f(2) << 4.  compose(g, f) = g o f (apply f first).
+__device__ __forceinline__ uint32_t fapply(uint32_t f, uint32_t c) { return (f >> (2 * c)) & 3u; }
+__device__ __forceinline__ uint32_t fcompose(uint32_t g, uint32_t f) {
+    return fapply(g, fapply(f, 0)) | (fapply(g, fapply(f, 1)) << 2) | (fapply(g, fapply(f, 2)) << 4);
+}
+constexpr uint32_t kFIdentity = 0u | (1u << 2) | (2u << 4);
+
+enum : uint32_t { kStNone = 0, kStAgg = 1, kStIncl = 2 };
+
+__global__ void __launch_bounds__(kCrtThreads) crt_carry_kernel(CrtParams P) {
+    __shared__ uint32_t s_tail[kCrtThreads / 32][3];
+    __shared__ uint32_t s_wagg[kCrtThreads / 32];
+    __shared__ uint32_t s_bid;
+    __shared__ uint32_t s_carry_in;
+
+    if (threadIdx.x == 0) s_bid = atomicAdd(P.ticket, 1u);
+    __syncthreads();
+    const uint32_t bid = s_bid;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t j0 = ((uint64_t)bid * kCrtThreads + threadIdx.x) * kCrtWords;
+
+    const uint32_t* r0 = P.res;
+    const uint32_t* r1 = P.res + P.L;
+    const uint32_t* r2 = P.res + 2 * P.L;
+
+    uint32_t a0[kCrtWords], a1[kCrtWords], a2[kCrtWords];
+    if (j0 + kCrtWords <= P.L) {
+#pragma unroll
+        for (int u = 0; u < kCrtWords; u += 4) {
+            uint4 v0 = *reinterpret_cast<const uint4*>(r0 + j0 + u);
+            uint4 v1 = *reinterpret_cast<const uint4*>(r1 + j0 + u);
+            uint4 v2 = *reinterpret_cast<const uint4*>(r2 + j0 + u);
+            X3 x;
+            x = crt3(v0.x, v1.x, v2.x, P.k); a0[u] = x.w0; a1[u] = x.w1; a2[u] = x.w2;
+            x = crt3(v0.y, v1.y, v2.y, P.k); a0[u + 1] = x.w0; a1[u + 1] = x.w1; a2[u + 1] = x.w2;
+            x = crt3(v0.z, v1.z, v2.z, P.k); a0[u + 2] = x.w0; a1[u + 2] = x.w1; a2[u + 2] = x.w2;
+            x = crt3(v0.w, v1.w, v2.w, P.k); a0[u + 3] = x.w0; a1[u + 3] = x.w1; a2[u + 3] = x.w2;
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u) {
+            uint64_t i = j0 + u;
+            if (i < P.L) {
+                X3 x = crt3(r0[i], r1[i], r2[i], P.k);
+                a0[u] = x.w0; a1[u] = x.w1; a2[u] = x.w2;
+            } else {
+                a0[u] = a1[u] = a2[u] = 0;
+            }
+        }
+    }
+
+    // Words 1 and 2 of the two coefficients just below j0 (from the previous thread).
+    uint32_t pw1 = __shfl_up_sync(0xffffffffu, a1[kCrtWords - 1], 1);
+    uint32_t pw2a = __shfl_up_sync(0xffffffffu, a2[kCrtWords - 1], 1);
+    uint32_t pw2b = __shfl_up_sync(0xffffffffu, a2[kCrtWords - 2], 1);
+    if (lane == 31) {
+        s_tail[warp][0] = a1[kCrtWords - 1];
+        s_tail[warp][1] = a2[kCrtWords - 1];
+        s_tail[warp][2] = a2[kCrtWords - 2];
+    }
+    __syncthreads();
+    if (lane == 0) {
+        if (warp > 0) {
+            pw1 = s_tail[warp - 1][0];
+            pw2a = s_tail[warp - 1][1];
+            pw2b = s_tail[warp - 1][2];
+        } else if (j0 >= 2) {
+            // first thread of the CTA: rebuild the two coefficients below its range
+            X3 xm1 = {0, 0, 0}, xm2 = {0, 0, 0};
+            if (j0 - 1 < P.L) xm1 = crt3(r0[j0 - 1], r1[j0 - 1], r2[j0 - 1], P.k);
+            if (j0 - 2 < P.L) xm2 = crt3(r0[j0 - 2], r1[j0 - 2], r2[j0 - 2], P.k);
+            pw1 = xm1.w1; pw2a = xm1.w2; pw2b = xm2.w2;
+        } else {
+            pw1 = pw2a = pw2b = 0;
+        }
+    }
+
+    // Raw word sums and the carry-in-0 pass.
+    uint64_t W[kCrtWords];
+#pragma unroll
+    for (int u = 0; u < kCrtWords; ++u) {
+        uint64_t w = a0[u];
+        w += (u >= 1) ? a1[u - 1] : pw1;
+        w += (u >= 2) ? a2[u - 2] : (u == 1 ? pw2a : pw2b);
+        W[u] = w;
+    }
+    uint32_t f;
+    {
+        uint64_t acc = 0;
+        bool allones_hi = true;
+        uint32_t low0 = 0;
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u) {
+            acc += W[u];
+            uint32_t o = (uint32_t)acc;
+            if (u == 0) low0 = o; else allones_hi &= (o == 0xffffffffu);
+            acc >>= 32;
+        }
+        uint32_t c0 = (uint32_t)acc;
+        uint32_t c1 = c0 + ((allones_hi && low0 == 0xffffffffu) ? 1u : 0u);
+        uint32_t c2 = c0 + ((allones_hi && low0 >= 0xfffffffeu) ? 1u : 0u);
+        f = c0 | (c1 << 2) | (c2 << 4);
+    }
+
+    // Warp inclusive scan of transfer functions (lane order = word order).
+    uint32_t incl = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = fcompose(incl, o);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = kFIdentity;
+    if (lane == 31) s_wagg[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // Block aggregate and each warp's exclusive prefix.
+        uint32_t acc = kFIdentity;
+        for (int w = 0; w < kCrtThreads / 32; ++w) {
+            uint32_t a = s_wagg[w];
+            s_wagg[w] = acc;
+            acc = fcompose(a, acc);
+        }
+        uint32_t blk = acc;
+        uint32_t carry_in = 0;
+        volatile uint32_t* st = P.status;
+        if (bid == 0) {
+            st[0] = (kStIncl) | (fapply(blk, 0) << 8);
+        } else {
+            __threadfence();
+            st[bid] = kStAgg | (blk << 8);
+            uint32_t look = kFIdentity;
+            int64_t jb = (int64_t)bid - 1;
+            uint32_t spins = 0;
+            while (true) {
+                uint32_t v = st[jb];
+                uint32_t s = v & 0xffu;
+                if (s == kStNone) {
+                    if (++spins > kSpinLimit) {
+                        atomicExch(P.error, 1u);
+                        carry_in = 0;
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                __threadfence();
+                uint32_t pay = (v >> 8) & 0xffu;
+                if (s == kStIncl) {
+                    carry_in = fapply(look, pay);
+                    break;
+                }
+                look = fcompose(look, pay);
+                --jb;
+            }
+            __threadfence();
+            st[bid] = kStIncl | (fapply(blk, carry_in) << 8);
+        }
+        s_carry_in = carry_in;
+        if ((uint64_t)(bid + 1) * kCrtThreads * kCrtWords >= P.nwords && fapply(blk, carry_in) != 0) {
+            atomicExch(P.error, 2u);  // product overflowed its limb count: cannot happen for valid inputs
+        }
+    }
+    __syncthreads();
+    uint32_t c = fapply(excl, fapply(s_wagg[warp], s_carry_in));
+
+    // Final words.
+    uint32_t o[kCrtWords];
+    {
+        uint64_t acc = c;
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u) {
+            acc += W[u];
+            o[u] = (uint32_t)acc;
+            acc >>= 32;
+        }
+    }
+    if (j0 + kCrtWords <= P.nwords) {
+#pragma unroll
+        for (int u = 0; u < kCrtWords; u += 4)
+            *reinterpret_cast<uint4*>(P.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u)
+            if (j0 + u < P.nwords) P.out[j0 + u] = o[u];
+    }
+}
+
+}  // namespace pg

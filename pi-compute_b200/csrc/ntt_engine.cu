@@ -1,0 +1,314 @@
+// Device engine implementation: twiddle tables, pass dispatch, CRT constants and
+// the per-product launch sequence.
+#include <cstring>
+#include <vector>
+
+#include "crt_carry.cuh"
+#include "ntt_engine.cuh"
+#include "ntt_pass.cuh"
+
+namespace pg {
+
+// ---------------------------------------------------------------- host modular helpers
+uint32_t pow_mod(uint32_t b, uint64_t e, uint32_t p) {
+    uint64_t r = 1, x = b % p;
+    while (e) {
+        if (e & 1) r = r * x % p;
+        x = x * x % p;
+        e >>= 1;
+    }
+    return (uint32_t)r;
+}
+uint32_t inv_mod(uint32_t a, uint32_t p) { return pow_mod(a, p - 2, p); }
+uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
+
+// ---------------------------------------------------------------- tables
+// Layout of the single table allocation, in uint2 entries:
+//   [dir][prime] stage  : 2^13 each
+//   [dir][prime] fs_lo  : 2^13 each
+//   [dir][prime] fs_hi  : 2^13 each
+cudaError_t DeviceTables::build(int device) {
+    (void)device;
+    constexpr size_t kEnt = 1u << 13;
+    constexpr size_t kTables = 3 * 2 * kNumPrimes;
+    std::vector<uint2> h(kTables * kEnt);
+    for (int dir = 0; dir < 2; ++dir) {
+        for (int j = 0; j < kNumPrimes; ++j) {
+            const uint32_t p = kPrime(j);
+            uint32_t w26 = pow_mod(kGenerator(j), (uint64_t)(p - 1) >> kMaxLogL, p);  // primitive 2^26-th root
+            if (dir == 1) w26 = inv_mod(w26, p);
+            const uint32_t w14 = pow_mod(w26, 1ull << (kMaxLogL - kStageLog), p);
+            const uint32_t w26hi = pow_mod(w26, 1ull << kFsLog, p);
+            uint2* st = h.data() + ((0 * 2 + dir) * kNumPrimes + j) * kEnt;
+            uint2* lo = h.data() + ((1 * 2 + dir) * kNumPrimes + j) * kEnt;
+            uint2* hi = h.data() + ((2 * 2 + dir) * kNumPrimes + j) * kEnt;
+            uint64_t a = 1, b = 1, c = 1;
+            for (size_t i = 0; i < kEnt; ++i) {
+                st[i] = make_uint2((uint32_t)a, shoup_companion((uint32_t)a, p));
+                lo[i] = make_uint2((uint32_t)b, shoup_companion((uint32_t)b, p));
+                hi[i] = make_uint2((uint32_t)c, shoup_companion((uint32_t)c, p));
+                a = a * w14 % p;
+                b = b * w26 % p;
+                c = c * w26hi % p;
+            }
+        }
+    }
+    cudaError_t e = cudaMalloc(&base, h.size() * sizeof(uint2));
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpy(base, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return e;
+    for (int dir = 0; dir < 2; ++dir)
+        for (int j = 0; j < kNumPrimes; ++j) {
+            tw.stage[dir][j] = base + ((0 * 2 + dir) * kNumPrimes + j) * kEnt;
+            tw.fs_lo[dir][j] = base + ((1 * 2 + dir) * kNumPrimes + j) * kEnt;
+            tw.fs_hi[dir][j] = base + ((2 * 2 + dir) * kNumPrimes + j) * kEnt;
+        }
+    return cudaSuccess;
+}
+
+void DeviceTables::release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+}
+
+// ---------------------------------------------------------------- workspace
+static cudaError_t grow(void** ptr, uint64_t bytes) {
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    return cudaMalloc(ptr, bytes);
+}
+
+cudaError_t Workspace::ensure_res(uint64_t n) {
+    if (n <= res_cap) return cudaSuccess;
+    cudaError_t e = grow((void**)&a_res, n * 4);
+    if (e == cudaSuccess) e = grow((void**)&b_res, n * 4);
+    res_cap = (e == cudaSuccess) ? n : 0;
+    return e;
+}
+
+cudaError_t Workspace::ensure_limbs(uint64_t n) {
+    if (n <= limb_cap) return cudaSuccess;
+    n = n < 1024 ? 1024 : n;
+    cudaError_t e = grow((void**)&in_a, n * 8);
+    if (e == cudaSuccess) e = grow((void**)&in_b, n * 8);
+    if (e == cudaSuccess) e = grow((void**)&outl, n * 8);
+    if (e == cudaSuccess) {
+        if (pinned) cudaFreeHost(pinned);
+        pinned = nullptr;
+        e = cudaMallocHost((void**)&pinned, 3 * n * 8);
+    }
+    limb_cap = (e == cudaSuccess) ? n : 0;
+    return e;
+}
+
+cudaError_t Workspace::ensure_sync(uint64_t nblocks) {
+    if (nblocks + 2 <= sync_cap) return cudaSuccess;
+    uint64_t n = nblocks + 2 < 4096 ? 4096 : nblocks + 2;
+    cudaError_t e = grow((void**)&sync, n * 4);
+    if (e == cudaSuccess) e = cudaMemset(sync, 0, n * 4);
+    sync_cap = (e == cudaSuccess) ? n : 0;
+    return e;
+}
+
+void Workspace::release() {
+    if (a_res) cudaFree(a_res);
+    if (b_res) cudaFree(b_res);
+    if (in_a) cudaFree(in_a);
+    if (in_b) cudaFree(in_b);
+    if (outl) cudaFree(outl);
+    if (sync) cudaFree(sync);
+    if (pinned) cudaFreeHost(pinned);
+    *this = Workspace{};
+}
+
+// ---------------------------------------------------------------- pass dispatch
+template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
+static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, uint64_t L, cudaStream_t st) {
+    constexpr int LOGE = kTileLog;
+    auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
+    const size_t smem = (size_t)4 << LOGE;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        configured = true;
+    }
+    uint64_t tiles = L >> LOGE;
+    if (tiles == 0) tiles = 1;
+    dim3 grid((unsigned)tiles, kNumPrimes);
+    kern<<<grid, kPassThreads, smem, st>>>(prm, tw);
+    return cudaGetLastError();
+}
+
+#define PG_CONTIG_CASE(N)                                                                                    \
+    case N:                                                                                                  \
+        if (src == Source::Limbs) {                                                                          \
+            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::None>(prm, tw, L, st); \
+            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::MulInverse>(prm, tw, L, st); \
+            return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::SqrInverse>(prm, tw, L, st);     \
+        } else {                                                                                             \
+            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::None>(prm, tw, L, st); \
+            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::MulInverse>(prm, tw, L, st); \
+            return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::SqrInverse>(prm, tw, L, st);  \
+        }
+
+#define PG_STRIDED_CASE(N)                                                                                   \
+    case N:                                                                                                  \
+        if (inverse) return run_pass<Layout::Strided, N, true, Source::Residues, Fuse::None>(prm, tw, L, st); \
+        if (src == Source::Limbs) return run_pass<Layout::Strided, N, false, Source::Limbs, Fuse::None>(prm, tw, L, st); \
+        return run_pass<Layout::Strided, N, false, Source::Residues, Fuse::None>(prm, tw, L, st);
+
+cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm,
+                        const TwiddleTables& tw, cudaStream_t st) {
+    const uint64_t L = 1ull << plan.logL;
+    const int logN = plan.logN[pass];
+    const bool contig = (pass == plan.npass - 1);
+    if (contig) {
+        if (inverse) return cudaErrorInvalidValue;  // contiguous inverse runs fused with the pointwise product
+        switch (logN) {
+            PG_CONTIG_CASE(6)
+            PG_CONTIG_CASE(7)
+            PG_CONTIG_CASE(8)
+            PG_CONTIG_CASE(9)
+            PG_CONTIG_CASE(10)
+            PG_CONTIG_CASE(11)
+            PG_CONTIG_CASE(12)
+            PG_CONTIG_CASE(13)
+            default:
+                return cudaErrorInvalidValue;
+        }
+    } else {
+        switch (logN) {
+            PG_STRIDED_CASE(5)
+            PG_STRIDED_CASE(6)
+            PG_STRIDED_CASE(7)
+            PG_STRIDED_CASE(8)
+            PG_STRIDED_CASE(9)
+            PG_STRIDED_CASE(10)
+            default:
+                return cudaErrorInvalidValue;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- CRT constants
+static void shoup_pair(uint32_t v, uint32_t p, uint32_t& w, uint32_t& wp) {
+    w = v % p;
+    wp = shoup_companion(w, p);
+}
+
+CrtConsts make_crt_consts(int logL) {
+    const uint32_t p0 = kPrime(0), p1 = kPrime(1), p2 = kPrime(2);
+    // scale f_j = L^-1 * 2^32 mod p_j (unnormalised inverse + Montgomery pointwise factor)
+    auto scale = [&](uint32_t p) {
+        uint64_t linv = inv_mod(pow_mod(2, (uint64_t)logL, p), p);
+        uint64_t r32 = pow_mod(2, 32, p);
+        return (uint32_t)(linv * r32 % p);
+    };
+    const uint64_t f0 = scale(p0), f1 = scale(p1), f2 = scale(p2);
+    const uint64_t i01 = inv_mod(p0 % p1, p1);          // p0^-1 mod p1
+    const uint64_t i02 = inv_mod(p0 % p2, p2);          // p0^-1 mod p2
+    const uint64_t i12 = inv_mod(p1 % p2, p2);          // p1^-1 mod p2
+    CrtConsts k;
+    shoup_pair((uint32_t)f0, p0, k.c00, k.c00p);
+    shoup_pair((uint32_t)(f1 * i01 % p1), p1, k.c11, k.c11p);
+    shoup_pair((uint32_t)i01, p1, k.k01, k.k01p);
+    shoup_pair((uint32_t)(f2 * i02 % p2 * i12 % p2), p2, k.c22, k.c22p);
+    shoup_pair((uint32_t)(i02 * i12 % p2), p2, k.k02, k.k02p);
+    shoup_pair((uint32_t)i12, p2, k.k12, k.k12p);
+    k.p01 = (uint64_t)p0 * p1;
+    return k;
+}
+
+// ---------------------------------------------------------------- one product
+cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                            const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
+                            uint64_t* launches) {
+    const bool square = (d_b == nullptr);
+    if (square) nb = na;
+    const int logL = product_logL(na, nb);
+    const Plan plan = make_plan(logL);
+    const uint64_t L = 1ull << logL;
+    cudaError_t e = W.ensure_res(3 * L);
+    if (e != cudaSuccess) return e;
+    const uint64_t nwords = 2ull * (na + nb);
+    const uint64_t crt_blocks = (nwords + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+    e = W.ensure_sync(crt_blocks);
+    if (e != cudaSuccess) return e;
+
+    auto base = [&](uint32_t* data, const uint64_t* limbs, uint64_t ncoef) {
+        PassParams p{};
+        p.data = data;
+        p.out = data;
+        p.other = nullptr;
+        p.words = reinterpret_cast<const uint32_t*>(limbs);
+        p.ncoef = ncoef;
+        p.L = L;
+        p.nrows = 1;
+        return p;
+    };
+    auto set_pass = [&](PassParams& p, int i) {
+        p.logS = plan.logS[i];
+        p.logNp = plan.logN[i] + plan.logS[i];
+        p.nrows = (uint32_t)(L >> plan.logN[i]);
+    };
+
+    const int last = plan.npass - 1;
+    // Operand a: full forward transform (all but the last pass when squaring).
+    {
+        PassParams p = base(W.a_res, d_a, 2ull * na);
+        const int upto = square ? last : plan.npass;
+        for (int i = 0; i < upto; ++i) {
+            set_pass(p, i);
+            Fuse f = Fuse::None;
+            e = launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, f, p, T.tw, st);
+            if (e != cudaSuccess) return e;
+        }
+        if (square) {
+            set_pass(p, last);
+            e = launch_pass(plan, last, false, last == 0 ? Source::Limbs : Source::Residues, Fuse::SqrInverse, p,
+                            T.tw, st);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    uint32_t* prod = W.a_res;
+    if (!square) {
+        PassParams p = base(W.b_res, d_b, 2ull * nb);
+        for (int i = 0; i < last; ++i) {
+            set_pass(p, i);
+            e = launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, Fuse::None, p, T.tw, st);
+            if (e != cudaSuccess) return e;
+        }
+        set_pass(p, last);
+        p.other = W.a_res;
+        e = launch_pass(plan, last, false, last == 0 ? Source::Limbs : Source::Residues, Fuse::MulInverse, p, T.tw,
+                        st);
+        if (e != cudaSuccess) return e;
+        prod = W.b_res;
+    }
+    // Inverse strided passes, last strided pass first.
+    {
+        PassParams p = base(prod, nullptr, 0);
+        for (int i = last - 1; i >= 0; --i) {
+            set_pass(p, i);
+            e = launch_pass(plan, i, true, Source::Residues, Fuse::None, p, T.tw, st);
+            if (e != cudaSuccess) return e;
+        }
+    }
+    // CRT + carry.
+    e = cudaMemsetAsync(W.sync + 1, 0, (crt_blocks + 1) * 4, st);
+    if (e != cudaSuccess) return e;
+    CrtParams c{};
+    c.res = prod;
+    c.L = L;
+    c.nwords = nwords;
+    c.out = reinterpret_cast<uint32_t*>(d_out);
+    c.ticket = W.sync + 1;
+    c.status = W.sync + 2;
+    c.error = W.sync;
+    c.k = make_crt_consts(logL);
+    crt_carry_kernel<<<(unsigned)crt_blocks, kCrtThreads, 0, st>>>(c);
+    if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + 1;
+    return cudaGetLastError();
+}
+
+}  // namespace pg

@@ -1,0 +1,188 @@
+// C ABI of libpigpu.so (declarations and reference citations in include/pi_b200.h).
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/pi_b200.h"
+#include "ntt_engine.cuh"
+
+struct pg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    pg::DeviceTables tables;
+    pg::Workspace ws;
+    std::string last_error;
+    uint64_t launches = 0;
+};
+
+namespace {
+
+pg_status fail(pg_ctx* c, pg_status s, const std::string& msg) {
+    if (c) c->last_error = msg;
+    return s;
+}
+
+pg_status cuda_fail(pg_ctx* c, cudaError_t e, const char* where) {
+    cudaGetLastError();  // clear a sticky launch error so the context stays usable
+    if (e == cudaErrorMemoryAllocation) return fail(c, PG_ERR_OOM, std::string(where) + ": out of device memory");
+    return fail(c, PG_ERR_DEVICE, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+size_t trimmed(const uint64_t* x, size_t n) {
+    while (n > 0 && x[n - 1] == 0) --n;
+    return n;
+}
+
+// Read and clear the device error word; map it to a status.
+pg_status check_device_error(pg_ctx* c) {
+    uint32_t err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, c->ws.sync, 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "pg_sync");
+    if (err != 0) {
+        cudaMemsetAsync(c->ws.sync, 0, 4, c->stream);
+        cudaStreamSynchronize(c->stream);
+        if (err == 1) return fail(c, PG_ERR_TIMEOUT, "carry look-back wait ran out of iterations");
+        return fail(c, PG_ERR_INTERNAL, "carry out of the most significant word");
+    }
+    return PG_OK;
+}
+
+pg_status host_product(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* b, size_t nb, bool square,
+                       uint64_t* out, size_t out_cap, size_t* out_len) {
+    if (!c || !out_len || (na && !a) || (!square && nb && !b)) return fail(c, PG_ERR_BAD_ARG, "null argument");
+    if (square) nb = na, b = a;
+    // Reject by buffer length before reading the operands.
+    if (na + nb > pg_mul_max_limbs()) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
+    na = trimmed(a, na);
+    nb = trimmed(b, nb);
+    if (na == 0 || nb == 0) {
+        *out_len = 0;
+        return PG_OK;
+    }
+    if (!out || out_cap < na + nb) return fail(c, PG_ERR_BAD_ARG, "output buffer smaller than na + nb limbs");
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    e = c->ws.ensure_limbs(na + nb);
+    if (e != cudaSuccess) return cuda_fail(c, e, "workspace");
+    // Stage through pinned memory so the copies run at full PCIe/C2C speed and stay async.
+    uint64_t* pin = c->ws.pinned;
+    std::memcpy(pin, a, na * 8);
+    e = cudaMemcpyAsync(c->ws.in_a, pin, na * 8, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess && !square) {
+        std::memcpy(pin + c->ws.limb_cap, b, nb * 8);
+        e = cudaMemcpyAsync(c->ws.in_b, pin + c->ws.limb_cap, nb * 8, cudaMemcpyHostToDevice, c->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(c, e, "host to device copy");
+    e = pg::enqueue_product(c->tables, c->ws, c->ws.in_a, na, square ? nullptr : c->ws.in_b, nb, c->ws.outl,
+                            c->stream, &c->launches);
+    if (e != cudaSuccess) return cuda_fail(c, e, "product launch");
+    uint64_t* pout = pin + 2 * c->ws.limb_cap;
+    e = cudaMemcpyAsync(pout, c->ws.outl, (na + nb) * 8, cudaMemcpyDeviceToHost, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "device to host copy");
+    pg_status s = check_device_error(c);
+    if (s != PG_OK) return s;
+    std::memcpy(out, pout, (na + nb) * 8);
+    *out_len = trimmed(out, na + nb);
+    return PG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int pg_version(void) { return (0 << 16) | (1 << 8) | 0; }
+
+size_t pg_mul_max_limbs(void) { return (size_t)1 << (pg::kMaxLogL - 1); }
+
+pg_status pg_create(int device, pg_ctx** out) {
+    if (!out) return PG_ERR_BAD_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return PG_ERR_BAD_ARG;
+    }
+    pg_ctx* c = new (std::nothrow) pg_ctx;
+    if (!c) return PG_ERR_OOM;
+    c->device = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = c->tables.build(device);
+    if (e == cudaSuccess) e = c->ws.ensure_sync(1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        pg_destroy(c);
+        return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
+    }
+    *out = c;
+    return PG_OK;
+}
+
+void pg_destroy(pg_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    c->ws.release();
+    c->tables.release();
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* pg_last_error(const pg_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+pg_status pg_mul(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out,
+                 size_t out_cap, size_t* out_len) {
+    return host_product(c, a, na, b, nb, false, out, out_cap, out_len);
+}
+
+pg_status pg_sqr(pg_ctx* c, const uint64_t* a, size_t na, uint64_t* out, size_t out_cap, size_t* out_len) {
+    return host_product(c, a, na, nullptr, 0, true, out, out_cap, out_len);
+}
+
+pg_status pg_mul_device(pg_ctx* c, const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
+                        uint64_t* d_out) {
+    if (!c || !d_out || (na && !d_a) || (nb && !d_b)) return fail(c, PG_ERR_BAD_ARG, "null argument");
+    if (((uintptr_t)d_a | (uintptr_t)d_b | (uintptr_t)d_out) & 15)
+        return fail(c, PG_ERR_BAD_ARG, "device pointers must be 16-byte aligned");
+    if (na + nb > pg_mul_max_limbs()) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    if (na == 0 || nb == 0) {
+        e = cudaMemsetAsync(d_out, 0, (na + nb) * 8, c->stream);
+        return e == cudaSuccess ? PG_OK : cuda_fail(c, e, "memset");
+    }
+    e = pg::enqueue_product(c->tables, c->ws, d_a, na, d_b, nb, d_out, c->stream, &c->launches);
+    return e == cudaSuccess ? PG_OK : cuda_fail(c, e, "product launch");
+}
+
+pg_status pg_sqr_device(pg_ctx* c, const uint64_t* d_a, size_t na, uint64_t* d_out) {
+    if (!c || !d_out || (na && !d_a)) return fail(c, PG_ERR_BAD_ARG, "null argument");
+    if (((uintptr_t)d_a | (uintptr_t)d_out) & 15) return fail(c, PG_ERR_BAD_ARG, "device pointers must be 16-byte aligned");
+    if (2 * na > pg_mul_max_limbs()) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    if (na == 0) return PG_OK;
+    e = pg::enqueue_product(c->tables, c->ws, d_a, na, nullptr, na, d_out, c->stream, &c->launches);
+    return e == cudaSuccess ? PG_OK : cuda_fail(c, e, "product launch");
+}
+
+pg_status pg_sync(pg_ctx* c) {
+    if (!c) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(c->mu);
+    cudaSetDevice(c->device);
+    return check_device_error(c);
+}
+
+void* pg_stream(pg_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+uint64_t pg_launch_count(const pg_ctx* c) { return c ? c->launches : 0; }
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// Host-side transform planning and constant generation (no CUDA types).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+
+namespace pg {
+
+constexpr int kTileLog = 13;        // E = 2^13 residues per CTA tile (32 KB of shared memory)
+constexpr int kMinLogL = 6;         // smallest transform (64 points)
+constexpr int kMaxStridedLog = 10;  // strided passes keep >= 8 adjacent columns per tile
+
+struct Plan {
+    int logL = 0;
+    int npass = 0;
+    int logN[3] = {0, 0, 0};   // sub-transform length of each pass, first = largest stride
+    int logS[3] = {0, 0, 0};   // element stride of each pass
+};
+
+// Pass split for L = 2^logL: one contiguous pass up to 2^13, two passes up to 2^23, three to 2^26.
+inline Plan make_plan(int logL) {
+    Plan p;
+    p.logL = logL;
+    if (logL <= kTileLog) {
+        p.npass = 1;
+        p.logN[0] = logL;
+    } else if (logL <= 20) {
+        p.npass = 2;
+        p.logN[0] = logL / 2;
+        p.logN[1] = logL - logL / 2;
+    } else if (logL <= kTileLog + kMaxStridedLog) {
+        p.npass = 2;
+        p.logN[0] = logL - kTileLog;
+        p.logN[1] = kTileLog;
+    } else {
+        p.npass = 3;
+        int rest = logL - kTileLog;
+        p.logN[0] = rest / 2;
+        p.logN[1] = rest - rest / 2;
+        p.logN[2] = kTileLog;
+    }
+    int s = logL;
+    for (int i = 0; i < p.npass; ++i) {
+        s -= p.logN[i];
+        p.logS[i] = s;
+    }
+    return p;
+}
+
+inline int ceil_log2(uint64_t x) {
+    int l = 0;
+    while ((1ull << l) < x) ++l;
+    return l;
+}
+
+// Transform length for an na x nb limb product with 32-bit coefficients.
+inline int product_logL(size_t na, size_t nb) {
+    uint64_t conv = 2ull * (na + nb) - 1;  // coefficients of the linear convolution
+    int l = ceil_log2(conv);
+    return l < kMinLogL ? kMinLogL : l;
+}
+
+uint32_t pow_mod(uint32_t b, uint64_t e, uint32_t p);
+uint32_t inv_mod(uint32_t a, uint32_t p);
+uint32_t shoup_companion(uint32_t w, uint32_t p);
+
+}  // namespace pg

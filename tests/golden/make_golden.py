@@ -1,0 +1,97 @@
+"""Regenerate the golden fixtures in tests/golden/ from the reference build and the oracle.
+
+Run from the repository root after `make -C oracle` (needs the reference sources mounted
+for the reference build; the fixtures it writes are committed and used on machines
+without them):
+
+    python tests/golden/make_golden.py
+
+Outputs
+  pi_1000.txt        "3." + 1000 digits from the reference program (checked byte-for-byte
+                     against the reference's own tests/data/pi_1000.txt when it is mounted)
+  pi_golden.json     sha256 / head / tail of the reference program's 1M and 10M digit files
+  bs_golden.json     P, Q, R (hex) of the reference's BinarySplitting for small ranges, and
+                     sha256 of P/Q/R for the 1M-digit term range
+  products.json      sha256 of seeded random products computed by libgmp's mpz_mul
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+from helpers import oracle, pkg  # noqa: E402
+
+REF_DATA = "/root/reference/tests/data/pi_1000.txt"
+
+
+def run_ref(digits: int, threads: int) -> bytes:
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "pi.txt")
+        subprocess.run([oracle.PI_COMPUTE_REF, "--digits", str(digits), "--threads", str(threads), "--output", out],
+                       check=True, stdout=subprocess.DEVNULL)
+        return open(out, "rb").read()
+
+
+def limb_hash(a) -> str:
+    return hashlib.sha256(a.astype("<u8").tobytes()).hexdigest()
+
+
+# Seeded product cases: (na, nb, seed). Shapes follow the multiply sweep: balanced,
+# 1:4, 1:16 and squares, at sizes around transform-length boundaries.
+PRODUCT_CASES = []
+for n in [1, 2, 3, 7, 16, 31, 32, 33, 100, 1000, 1024, 1536, 4096, 6144, 16384, 65536, 98304, 262144, 1048576]:
+    PRODUCT_CASES.append((n, n, 1000 + n))
+    if n >= 4:
+        PRODUCT_CASES.append((n, n // 4, 2000 + n))
+    if n >= 16:
+        PRODUCT_CASES.append((n, n // 16, 3000 + n))
+    PRODUCT_CASES.append((n, 0, 4000 + n))  # nb == 0 encodes a square
+
+
+def main() -> None:
+    oracle.build()
+    os.makedirs(HERE, exist_ok=True)
+
+    pi1000 = run_ref(1000, 1)
+    if os.path.exists(REF_DATA):
+        assert pi1000 == open(REF_DATA, "rb").read().rstrip(b"\r\n "), "reference build disagrees with pi_1000.txt"
+    open(os.path.join(HERE, "pi_1000.txt"), "wb").write(pi1000)
+
+    pig = {}
+    for d in (1_000_000, 10_000_000):
+        s = run_ref(d, os.cpu_count() or 1)
+        pig[str(d)] = {"sha256": hashlib.sha256(s).hexdigest(), "bytes": len(s), "head": s[:66].decode(),
+                       "tail": s[-64:].decode()}
+    json.dump(pig, open(os.path.join(HERE, "pi_golden.json"), "w"), indent=1)
+
+    bsg = {"ranges": {}, "hash_ranges": {}}
+    for a, b in [(0, 1), (1, 2), (2, 3), (0, 2), (0, 8), (3, 11), (0, 79), (100, 357), (0, 1000)]:
+        P, Q, R = oracle.ref_bs(a, b, 1)
+        bsg["ranges"][f"{a},{b}"] = [hex(P), hex(Q), hex(R)]
+    for a, b in [(0, 70522), (1000, 9000)]:
+        P, Q, R = oracle.ref_bs(a, b, 1)
+        bsg["hash_ranges"][f"{a},{b}"] = [hashlib.sha256(hex(v).encode()).hexdigest() for v in (P, Q, R)]
+    json.dump(bsg, open(os.path.join(HERE, "bs_golden.json"), "w"), indent=1)
+
+    prods = []
+    for na, nb, seed in PRODUCT_CASES:
+        a = pkg.random_operand(na, seed)
+        if nb == 0:
+            r = oracle.mul_gmp(a, a)
+        else:
+            b = pkg.random_operand(nb, seed + 7)
+            r = oracle.mul_gmp(a, b)
+        prods.append({"na": na, "nb": nb, "seed": seed, "len": int(len(r)), "sha256": limb_hash(r)})
+    json.dump(prods, open(os.path.join(HERE, "products.json"), "w"), indent=1)
+    print("golden fixtures written to", HERE)
+
+
+if __name__ == "__main__":
+    main()
