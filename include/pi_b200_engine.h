@@ -1,0 +1,45 @@
+/*
+ * pi_b200 engine -- C entry points of libpib200.so, the C++17 host library that runs the
+ * reference's pi pipeline (binary splitting -> final formula -> decimal string) with its
+ * products on the B200 (B200Multiplier over libpigpu.so).
+ *
+ * The reference has no C API for its engine; its CLI (src/main.cpp:57-211) drives
+ * pi::PiEngine::compute (src/engine/pi_engine.cpp:207-603). These entry points expose the
+ * same computation to non-C++ callers (tests, benchmarks, FFI bindings).
+ */
+#ifndef PI_B200_ENGINE_H
+#define PI_B200_ENGINE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Binary-splitting modes. */
+#define PIB_MODE_GMP 0        /* products through GMP's mpz_mul (the reference's GmpMultiplier) */
+#define PIB_MODE_PER_CALL 1   /* products >= threshold limbs through B200Multiplier, one call at a time */
+#define PIB_MODE_BATCHED 2    /* level-batched, device-resident binary splitting */
+
+/* Compute pi to `digits` decimals; writes "3." + digits (no terminator) into out, which must
+ * have room for digits + 2 bytes. threads = host threads issuing per-call products;
+ * threshold = min limbs of the smaller operand for the GPU path (PIB_MODE_PER_CALL).
+ * times (may be NULL) receives 4 doubles: binary splitting, final formula, conversion, total
+ * seconds. Returns 0 on success, non-zero on error (message via pib_last_error). */
+int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int device, char* out, size_t out_cap,
+           double* times);
+
+/* P(a,b), Q(a,b), R(a,b) of the Chudnovsky series as signed little-endian limb arrays.
+ * Each output buffer needs `cap` limbs; lengths and signs are written to len[3] and sign[3]. */
+int pib_bs(unsigned long a, unsigned long b, int mode, size_t threshold, int device, uint64_t* P, uint64_t* Q,
+           uint64_t* R, size_t cap, size_t* len, int* sign);
+
+/* Message of the last failing call in this thread. */
+const char* pib_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PI_B200_ENGINE_H */

@@ -19,6 +19,9 @@ LIBPIGPU = os.path.join(HERE, "libpigpu.so")
 LIBPIB200 = os.path.join(HERE, "libpib200.so")
 PI_B200_BIN = os.path.join(HERE, "pi_b200")
 HEADERS = [os.path.join(ROOT, "include", "pi_b200.h")]
+# header -> library that must export every function it declares
+ABI = {os.path.join(ROOT, "include", "pi_b200.h"): LIBPIGPU,
+       os.path.join(ROOT, "include", "pi_b200_engine.h"): LIBPIB200}
 
 PG_OK = 0
 PG_ERR_OOM = 1
@@ -77,16 +80,14 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     return lib
 
 
-def declared_symbols() -> list[str]:
-    """Every function name declared in include/*.h (the C ABI the library must export)."""
+def declared_symbols(header: str = HEADERS[0]) -> list[str]:
+    """Every function name declared in one of include/*.h (the C ABI its library must export)."""
     import re
 
-    names = []
-    for h in HEADERS:
-        text = open(h).read()
-        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(pg_\w+)\s*\(", text, flags=re.M):
-            names.append(m.group(1))
+    text = open(header).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    names = [m.group(1) for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b((?:pg|pib)_\w+)\s*\(", text,
+                                             flags=re.M)]
     return sorted(set(names))
 
 

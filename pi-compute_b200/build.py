@@ -71,13 +71,16 @@ def build_host() -> str:
         return ""
     lib_srcs = [s for s in srcs if os.path.basename(s) != "main.cpp"]
     hdr = sorted(glob.glob(os.path.join(HOST, "*.h")) + glob.glob(os.path.join(INCLUDE, "*.h")))
-    flags = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-Wall", "-I", HOST, "-I", INCLUDE]
+    cuda_inc = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "include")
+    cuda_lib = os.path.join(os.path.dirname(os.path.dirname(NVCC)), "lib64")
+    flags = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-Wall", "-I", HOST, "-I", INCLUDE, "-I", cuda_inc]
     rpath = ["-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.dirname(GMP_SO)]
     if _newer(LIBPIB200, lib_srcs + hdr + [LIBPIGPU]):
-        _run([CXX, *flags, "-shared", "-o", LIBPIB200, *lib_srcs, LIBPIGPU, GMP_SO, *rpath])
+        _run([CXX, *flags, "-shared", "-o", LIBPIB200, *lib_srcs, LIBPIGPU, GMP_SO, "-L", cuda_lib, "-lcudart",
+              *rpath])
     main = os.path.join(HOST, "main.cpp")
     if os.path.exists(main) and _newer(PI_B200, [main, LIBPIB200] + hdr):
-        _run([CXX, *flags, "-o", PI_B200, main, LIBPIB200, LIBPIGPU, GMP_SO, *rpath])
+        _run([CXX, *flags, "-o", PI_B200, main, LIBPIB200, LIBPIGPU, GMP_SO, "-L", cuda_lib, "-lcudart", *rpath])
     return LIBPIB200
 
 

@@ -1,0 +1,78 @@
+// C entry points of libpib200.so (declarations in include/pi_b200_engine.h).
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "b200_multiplier.h"
+#include "binary_splitting.h"
+#include "pi_b200_engine.h"
+#include "pi_engine.h"
+
+namespace {
+thread_local std::string g_err;
+
+std::unique_ptr<pi::Multiplier> make_multiplier(int mode, size_t threshold, int device) {
+    if (mode == PIB_MODE_GMP) return std::make_unique<pi::GmpMultiplier>();
+    if (mode == PIB_MODE_PER_CALL) return std::make_unique<pi::B200Multiplier>(threshold, device);
+    throw std::invalid_argument("unknown binary-splitting mode " + std::to_string(mode));
+}
+
+void export_signed(const mpz_t v, uint64_t* out, size_t cap, size_t* len, int* sign) {
+    size_t n = mpz_size(v);
+    if (n > cap) throw std::length_error("output buffer too small");
+    if (n) std::memcpy(out, mpz_limbs_read(v), n * 8);
+    *len = n;
+    *sign = mpz_sgn(v);
+}
+}  // namespace
+
+extern "C" {
+
+int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int device, char* out, size_t out_cap,
+           double* times) {
+    try {
+        if (!out || out_cap < digits + 2) throw std::invalid_argument("output buffer smaller than digits + 2");
+        pi::PiConfig cfg;
+        cfg.digits = digits;
+        cfg.num_threads = threads ? threads : 1;
+        cfg.device = device;
+        cfg.mode = (mode == PIB_MODE_BATCHED) ? pi::BSMode::Batched : pi::BSMode::PerCall;
+        std::unique_ptr<pi::Multiplier> m = make_multiplier(mode == PIB_MODE_BATCHED ? PIB_MODE_GMP : mode,
+                                                            threshold, device);
+        pi::PiEngine eng(*m);
+        pi::PiResult r = eng.compute(cfg);
+        std::memcpy(out, r.digits.data(), r.digits.size());
+        if (times) {
+            times[0] = r.t.bs;
+            times[1] = r.t.final;
+            times[2] = r.t.convert;
+            times[3] = r.t.total;
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+int pib_bs(unsigned long a, unsigned long b, int mode, size_t threshold, int device, uint64_t* P, uint64_t* Q,
+           uint64_t* R, size_t cap, size_t* len, int* sign) {
+    try {
+        if (b <= a) throw std::invalid_argument("empty range");
+        std::unique_ptr<pi::Multiplier> m = make_multiplier(mode, threshold, device);
+        pi::BinarySplitting bs(*m, 1);
+        pi::BSResult r = bs.compute(a, b);
+        export_signed(r.P, P, cap, &len[0], &sign[0]);
+        export_signed(r.Q, Q, cap, &len[1], &sign[1]);
+        export_signed(r.R, R, cap, &len[2], &sign[2]);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
+const char* pib_last_error(void) { return g_err.c_str(); }
+
+}  // extern "C"

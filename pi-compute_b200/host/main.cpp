@@ -1,0 +1,88 @@
+// pi_b200 -- command-line program with the reference's pi_compute flags (src/main.cpp:25-105)
+// plus the B200 modes.
+//
+//   pi_b200 --digits N [--output FILE] [--threads T] [--verbose]
+//           [--gpu | --b200]           products >= --gpu-threshold limbs on the B200, per call
+//           [--batched]                level-batched device-resident binary splitting
+//           [--gpu-threshold N]        (default 10000 like the reference)
+//           [--device D]
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+
+#include "b200_multiplier.h"
+#include "pi_engine.h"
+
+static void usage() {
+    std::puts(
+        "pi_b200 - pi digits with exact big-integer products on one B200\n\n"
+        "USAGE: pi_b200 --digits <N> [--output FILE] [--threads T] [--gpu|--b200] [--batched]\n"
+        "               [--gpu-threshold N] [--device D] [--verbose]\n");
+}
+
+int main(int argc, char** argv) {
+    pi::PiConfig cfg;
+    bool has_digits = false, gpu = false;
+    size_t threshold = 10000;
+    std::string output = "pi_digits.txt";
+    for (int i = 1; i < argc; ++i) {
+        std::string a = argv[i];
+        if (a == "--help" || a == "-h") {
+            usage();
+            return 0;
+        } else if (a == "--digits" && i + 1 < argc) {
+            cfg.digits = std::stoul(argv[++i]);
+            has_digits = true;
+        } else if (a == "--output" && i + 1 < argc) {
+            output = argv[++i];
+        } else if (a == "--threads" && i + 1 < argc) {
+            cfg.num_threads = std::stoul(argv[++i]);
+        } else if (a == "--gpu" || a == "--b200" || a == "--ntt") {
+            gpu = true;
+        } else if (a == "--batched") {
+            cfg.mode = pi::BSMode::Batched;
+        } else if (a == "--gpu-threshold" && i + 1 < argc) {
+            threshold = std::stoul(argv[++i]);
+        } else if (a == "--device" && i + 1 < argc) {
+            cfg.device = std::stoi(argv[++i]);
+        } else if (a == "--verbose" || a == "-v") {
+            cfg.verbose = true;
+        } else {
+            std::fprintf(stderr, "Unknown option: %s\n", a.c_str());
+            usage();
+            return 1;
+        }
+    }
+    if (!has_digits || cfg.digits == 0) {
+        std::fprintf(stderr, "Error: --digits <N> (N > 0) is required\n");
+        return 1;
+    }
+    try {
+        std::unique_ptr<pi::Multiplier> mult;
+        const char* mode = "CPU";
+        if (gpu && cfg.mode == pi::BSMode::PerCall) {
+            mult = std::make_unique<pi::B200Multiplier>(threshold, cfg.device);
+            mode = "B200 per-call";
+        } else {
+            mult = std::make_unique<pi::GmpMultiplier>();
+            if (cfg.mode == pi::BSMode::Batched) mode = "B200 batched";
+        }
+        pi::PiEngine eng(*mult);
+        pi::PiResult r = eng.compute(cfg);
+        FILE* f = std::fopen(output.c_str(), "wb");
+        if (!f) throw std::runtime_error("cannot open " + output);
+        std::fwrite(r.digits.data(), 1, r.digits.size(), f);
+        std::fclose(f);
+        std::printf("Computed %zu digits of pi in %g seconds (%lu terms, %s).\nOutput written to: %s\n", cfg.digits,
+                    r.elapsed_seconds, r.terms_used, mode, output.c_str());
+        if (auto* b = dynamic_cast<pi::B200Multiplier*>(mult.get())) {
+            if (cfg.verbose) b->print_stats();
+        }
+        return 0;
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "Error: %s\n", e.what());
+        return 1;
+    }
+}

@@ -1,0 +1,108 @@
+#include "pi_engine.h"
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <stdexcept>
+
+#include "binary_splitting.h"
+
+namespace pi {
+
+using Clock = std::chrono::steady_clock;
+static double secs(Clock::time_point a, Clock::time_point b) { return std::chrono::duration<double>(b - a).count(); }
+
+PiEngine::PiEngine(Multiplier& m) : mult_(m) {}
+
+void final_formula_mpf(mpz_t pi_int, const mpz_t Q, const mpz_t R, size_t digits) {
+    const size_t precision = digits + 100;
+    const mp_bitcnt_t bits = static_cast<mp_bitcnt_t>(precision * 3.3219281) + 64;
+    mpf_t s, num, den, pv, scale;
+    mpf_init2(s, bits);
+    mpf_set_prec(s, bits);
+    mpf_set_ui(s, 10005);
+    mpf_sqrt(s, s);
+    mpz_t t;
+    mpz_init(t);
+    mpz_mul_ui(t, Q, 426880);
+    mpf_init2(num, bits);
+    mpf_init2(den, bits);
+    mpf_init2(pv, bits);
+    mpf_set_z(num, t);
+    mpf_set_z(den, R);
+    mpf_mul(pv, num, s);
+    mpf_div(pv, pv, den);
+    mpz_ui_pow_ui(t, 10, digits);
+    mpf_init2(scale, bits);
+    mpf_set_z(scale, t);
+    mpf_mul(pv, pv, scale);
+    mpz_set_f(pi_int, pv);
+    mpz_clear(t);
+    mpf_clear(s);
+    mpf_clear(num);
+    mpf_clear(den);
+    mpf_clear(pv);
+    mpf_clear(scale);
+}
+
+std::string format_digits(const mpz_t pi_int, size_t digits) {
+    void (*freefunc)(void*, size_t) = nullptr;
+    mp_get_memory_functions(nullptr, nullptr, &freefunc);
+    char* s = mpz_get_str(nullptr, 10, pi_int);
+    size_t n = std::strlen(s);
+    std::string out;
+    out.reserve(digits + 2);
+    out.push_back(s[0]);
+    out.push_back('.');
+    out.append(s + 1, std::min(n - 1, digits));
+    freefunc(s, n + 1);
+    return out;
+}
+
+PiResult PiEngine::compute(const PiConfig& cfg) {
+    auto t0 = Clock::now();
+    PiResult res;
+    const size_t precision = cfg.digits + 100;
+    const unsigned long terms = BinarySplitting::terms_needed(precision);
+    res.terms_used = terms;
+    mpz_t Q, R, pi_int;
+    mpz_init(Q);
+    mpz_init(R);
+    mpz_init(pi_int);
+    if (cfg.mode == BSMode::Batched) {
+        throw std::runtime_error("level-batched binary splitting is not available in this build");
+    } else {
+        BinarySplitting bs(mult_, cfg.num_threads);
+        BSResult r = bs.compute(0, terms);
+        mpz_swap(Q, r.Q);
+        mpz_swap(R, r.R);
+    }
+    auto t1 = Clock::now();
+    final_formula_mpf(pi_int, Q, R, cfg.digits);
+    auto t2 = Clock::now();
+    res.digits = format_digits(pi_int, cfg.digits);
+    auto t3 = Clock::now();
+    res.t.bs = secs(t0, t1);
+    res.t.final = secs(t1, t2);
+    res.t.convert = secs(t2, t3);
+    res.t.total = secs(t0, t3);
+    res.elapsed_seconds = res.t.total;
+    if (cfg.verbose) {
+        std::printf("  Terms: %lu\n  Binary splitting: %.3fs\n  Final computation: %.3fs\n"
+                    "  String conversion: %.3fs\n  Total: %.3fs\n",
+                    terms, res.t.bs, res.t.final, res.t.convert, res.t.total);
+    }
+    mpz_clear(Q);
+    mpz_clear(R);
+    mpz_clear(pi_int);
+    return res;
+}
+
+std::string PiEngine::compute_digits(size_t digits) {
+    PiConfig c;
+    c.digits = digits;
+    return compute(c).digits;
+}
+
+}  // namespace pi

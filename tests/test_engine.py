@@ -1,0 +1,109 @@
+"""Tests of the host engine (libpib200.so): binary splitting and pi digits.
+
+CPU cases use GMP products (PIB_MODE_GMP) and check the engine against the reference's
+known answers (tests/test_binary_splitting.cpp, tests/test_validation.cpp, tests/data/pi_1000.txt)
+and the reference build's golden hashes. GPU cases route products through B200Multiplier
+(PIB_MODE_PER_CALL, the per-call drop-in) and must give byte-identical digits.
+"""
+import ctypes
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN, oracle, pkg
+
+GMP, PER_CALL, BATCHED = 0, 1, 2
+
+
+@pytest.fixture(scope="module")
+def lib():
+    L = ctypes.CDLL(pkg.LIBPIB200)
+    L.pib_pi.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_uint, ctypes.c_size_t, ctypes.c_int,
+                         ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
+    L.pib_pi.restype = ctypes.c_int
+    P = ctypes.POINTER(ctypes.c_uint64)
+    L.pib_bs.argtypes = [ctypes.c_ulong, ctypes.c_ulong, ctypes.c_int, ctypes.c_size_t, ctypes.c_int, P, P, P,
+                         ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
+    L.pib_bs.restype = ctypes.c_int
+    L.pib_last_error.restype = ctypes.c_char_p
+    return L
+
+
+def pi_digits(lib, digits, mode, threshold=1024, threads=1):
+    buf = ctypes.create_string_buffer(digits + 2)
+    t = (ctypes.c_double * 4)()
+    st = lib.pib_pi(digits, mode, threads, threshold, 0, buf, digits + 2, t)
+    assert st == 0, lib.pib_last_error()
+    return buf.raw[: digits + 2].decode(), list(t)
+
+
+def bs(lib, a, b, mode, threshold=1):
+    cap = 64 + 2 * (b - a) * 3
+    bufs = [np.zeros(cap, dtype=np.uint64) for _ in range(3)]
+    ln = (ctypes.c_size_t * 3)()
+    sg = (ctypes.c_int * 3)()
+    P = ctypes.POINTER(ctypes.c_uint64)
+    st = lib.pib_bs(a, b, mode, threshold, 0, *(x.ctypes.data_as(P) for x in bufs), cap, ln, sg)
+    assert st == 0, lib.pib_last_error()
+    return tuple(sg[i] * pkg.limbs_to_int(bufs[i][: ln[i]]) for i in range(3))
+
+
+def test_engine_leaves_and_merges_gmp(lib):
+    assert bs(lib, 0, 1, GMP) == (1, 1, 13591409)
+    assert bs(lib, 1, 2, GMP) == (-5, 10939058860032000, -2793657715)
+    assert bs(lib, 2, 3, GMP)[:2] == (-231, 87512470880256000)
+    g = json.load(open(os.path.join(GOLDEN, "bs_golden.json")))
+    for key, (P, Q, R) in g["ranges"].items():
+        a, b = map(int, key.split(","))
+        assert bs(lib, a, b, GMP) == (int(P, 16), int(Q, 16), int(R, 16)), key
+
+
+def test_engine_digits_gmp(lib):
+    # test_validation.cpp:29-89 and the reference program's 1000-digit file
+    s50, _ = pi_digits(lib, 50, GMP)
+    assert s50 == "3.14159265358979323846264338327950288419716939937510"
+    s1000, t = pi_digits(lib, 1000, GMP)
+    assert s1000 == open(os.path.join(GOLDEN, "pi_1000.txt")).read()
+    assert t[3] > 0
+    s100, _ = pi_digits(lib, 100, GMP)
+    s500, _ = pi_digits(lib, 500, GMP)
+    assert s1000.startswith(s500) and s500.startswith(s100)
+
+
+def test_engine_1m_gmp_matches_reference_hash(lib):
+    s, _ = pi_digits(lib, 1_000_000, GMP, threads=4)
+    g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
+    assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
+
+
+def test_bad_mode_reports_error(lib):
+    buf = ctypes.create_string_buffer(20)
+    assert lib.pib_pi(10, 7, 1, 1, 0, buf, 20, None) != 0
+    assert b"mode" in lib.pib_last_error()
+    assert lib.pib_pi(10, GMP, 1, 1, 0, buf, 5, None) != 0
+
+
+# ---------------------------------------------------------------- GPU: per-call drop-in
+@pytest.mark.gpu
+def test_per_call_bs_matches_oracle_with_every_product_on_gpu(lib):
+    for a, b in [(0, 2), (0, 8), (3, 11), (0, 79), (100, 357), (0, 1000), (1000, 9000)]:
+        assert bs(lib, a, b, PER_CALL, threshold=1) == oracle.bs(a, b), (a, b)
+
+
+@pytest.mark.gpu
+def test_per_call_digits_small_all_gpu(lib):
+    s, _ = pi_digits(lib, 1000, PER_CALL, threshold=1)
+    assert s == open(os.path.join(GOLDEN, "pi_1000.txt")).read()
+    s, _ = pi_digits(lib, 10000, PER_CALL, threshold=1, threads=4)   # test_gpu_ntt_multiplier.cpp:159-166
+    assert s.startswith("3.14159") and len(s) == 10002
+
+
+@pytest.mark.gpu
+def test_per_call_1m_digits_byte_identical(lib):
+    # configuration 1: every product whose smaller operand has >= 2^10 limbs on the GPU, one call at a time
+    s, t = pi_digits(lib, 1_000_000, PER_CALL, threshold=1024)
+    g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
+    assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
