@@ -92,6 +92,27 @@ void* pg_stream(pg_ctx* ctx);
  * reference keeps per-multiplier call counters, gpu_ntt_multiplier.h:83-90). */
 uint64_t pg_launch_count(const pg_ctx* ctx);
 
+/* d_out = d_a * d_b without allocating any device memory. This entry point has no
+ * counterpart in the reference.
+ *
+ * It is for callers that cannot call cudaMalloc, for example code running while another
+ * framework owns the device allocator, or a plugin callback where allocating (and the device
+ * synchronisation an allocation can imply) is not allowed. It needs no pg_ctx: the scratch
+ * residues and the twiddle tables live in fixed-size device arrays inside libpigpu.so
+ * (about 1.9 MB, held on every GPU that loads the library until the process exits).
+ *
+ * Limit: na + nb <= 16384 limbs; larger products return PG_ERR_TOO_LARGE without touching
+ * any memory. Pointers are device addresses on the CURRENT device, 16-byte aligned; d_out
+ * receives exactly na + nb limbs and must not overlap d_a or d_b (d_a == d_b is allowed).
+ * `stream` is a cudaStream_t (NULL = the legacy default stream); the call returns after the
+ * product is complete and reports device-side errors like pg_sync.
+ *
+ * The first call on a device sets that device up (looks up the arrays and fills the tables,
+ * waiting for it); make it before any stream capture. All calls share the same arrays, so
+ * calls whose GPU work overlaps (from several host threads or streams) race: serialise them. */
+pg_status pg_mul_noalloc(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb, uint64_t* d_out,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif
