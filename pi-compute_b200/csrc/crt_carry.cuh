@@ -12,7 +12,8 @@
 // transfer function f: {0,1,2} -> {0,1,2} (carry in -> carry out), packed in 6
 // bits. Functions compose associatively, so a warp scan, a block scan and a
 // decoupled look-back across blocks (single pass, CTA order fixed by an atomic
-// ticket so every predecessor is resident) give each thread its exact carry in.
+// ticket so every predecessor is resident; one warp inspects 32 predecessors per
+// step) give each thread its exact carry in.
 // Every spin in the look-back has an iteration limit; running out sets an error
 // word the host checks, and the kernel finishes without hanging.
 #pragma once
@@ -58,7 +59,7 @@ constexpr uint32_t kFIdentity = 0u | (1u << 2) | (2u << 4);
 
 enum : uint32_t { kStNone = 0, kStAgg = 1, kStIncl = 2 };
 
-__global__ void __launch_bounds__(kCrtThreads) crt_carry_kernel(CrtParams P) {
+__global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) {
     __shared__ uint32_t s_tail[kCrtThreads / 32][3];
     __shared__ uint32_t s_wagg[kCrtThreads / 32];
     __shared__ uint32_t s_bid;
@@ -164,52 +165,78 @@ __global__ void __launch_bounds__(kCrtThreads) crt_carry_kernel(CrtParams P) {
     if (lane == 0) excl = kFIdentity;
     if (lane == 31) s_wagg[warp] = incl;
     __syncthreads();
-    if (threadIdx.x == 0) {
-        // Block aggregate and each warp's exclusive prefix.
-        uint32_t acc = kFIdentity;
-        for (int w = 0; w < kCrtThreads / 32; ++w) {
-            uint32_t a = s_wagg[w];
-            s_wagg[w] = acc;
-            acc = fcompose(a, acc);
+    if (warp == 0) {
+        // Exclusive prefix over the block's warps (lanes 0..7), block aggregate in lane 7.
+        constexpr int NW = kCrtThreads / 32;
+        uint32_t wf = (lane < NW) ? s_wagg[lane] : kFIdentity;
+        uint32_t wincl = wf;
+#pragma unroll
+        for (int off = 1; off < NW; off <<= 1) {
+            uint32_t o = __shfl_up_sync(0xffffffffu, wincl, off);
+            if (lane >= off) wincl = fcompose(wincl, o);
         }
-        uint32_t blk = acc;
-        uint32_t carry_in = 0;
+        uint32_t wexcl = __shfl_up_sync(0xffffffffu, wincl, 1);
+        if (lane == 0) wexcl = kFIdentity;
+        const uint32_t blk = __shfl_sync(0xffffffffu, wincl, NW - 1);
+        __syncwarp();
+        if (lane < NW) s_wagg[lane] = wexcl;
+
+        // Decoupled look-back, one window of 32 predecessors per step (lane l reads block
+        // base - l). The window's functions compose into one; the nearest block that already
+        // knows its carry out ends the walk.
         volatile uint32_t* st = P.status;
+        uint32_t carry_in = 0;
         if (bid == 0) {
-            st[0] = (kStIncl) | (fapply(blk, 0) << 8);
+            if (lane == 0) st[0] = kStIncl | (fapply(blk, 0) << 8);
         } else {
-            __threadfence();
-            st[bid] = kStAgg | (blk << 8);
+            if (lane == 0) {
+                __threadfence();
+                st[bid] = kStAgg | (blk << 8);
+            }
             uint32_t look = kFIdentity;
-            int64_t jb = (int64_t)bid - 1;
+            int64_t base = (int64_t)bid - 1;
             uint32_t spins = 0;
             while (true) {
-                uint32_t v = st[jb];
-                uint32_t s = v & 0xffu;
-                if (s == kStNone) {
+                const int64_t jb = base - lane;
+                const uint32_t v = (jb >= 0) ? st[jb] : (uint32_t)kStIncl;  // before block 0: carry 0
+                const uint32_t sv = v & 0xffu;
+                const unsigned incl_mask = __ballot_sync(0xffffffffu, sv == kStIncl);
+                const unsigned none_mask = __ballot_sync(0xffffffffu, sv == kStNone);
+                const int first = incl_mask ? (__ffs(incl_mask) - 1) : 32;
+                const unsigned upto = (first >= 31) ? 0xffffffffu : ((2u << first) - 1u);
+                if (none_mask & upto) {
                     if (++spins > kSpinLimit) {
-                        atomicExch(P.error, 1u);
-                        carry_in = 0;
+                        if (lane == 0) atomicExch(P.error, 1u);
                         break;
                     }
-                    __nanosleep(32);
+                    __nanosleep(64);
                     continue;
                 }
                 __threadfence();
-                uint32_t pay = (v >> 8) & 0xffu;
-                if (s == kStIncl) {
-                    carry_in = fapply(look, pay);
+                const uint32_t pay = (v >> 8) & 0xffu;
+                uint32_t g = (lane < first) ? pay : (lane == first ? (pay | (pay << 2) | (pay << 4)) : kFIdentity);
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    uint32_t o = __shfl_down_sync(0xffffffffu, g, off);
+                    if (lane + off < 32) g = fcompose(g, o);
+                }
+                g = __shfl_sync(0xffffffffu, g, 0);
+                look = fcompose(look, g);
+                if (first < 32) {
+                    carry_in = fapply(look, 0);
                     break;
                 }
-                look = fcompose(look, pay);
-                --jb;
+                base -= 32;
             }
-            __threadfence();
-            st[bid] = kStIncl | (fapply(blk, carry_in) << 8);
+            if (lane == 0) {
+                __threadfence();
+                st[bid] = kStIncl | (fapply(blk, carry_in) << 8);
+            }
         }
-        s_carry_in = carry_in;
-        if ((uint64_t)(bid + 1) * kCrtThreads * kCrtWords >= P.nwords && fapply(blk, carry_in) != 0) {
-            atomicExch(P.error, 2u);  // product overflowed its limb count: cannot happen for valid inputs
+        if (lane == 0) {
+            s_carry_in = carry_in;
+            if ((uint64_t)(bid + 1) * kCrtThreads * kCrtWords >= P.nwords && fapply(blk, carry_in) != 0)
+                atomicExch(P.error, 2u);  // product overflowed its limb count: cannot happen for valid inputs
         }
     }
     __syncthreads();

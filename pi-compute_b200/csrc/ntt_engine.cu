@@ -24,7 +24,7 @@ uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)
 
 // ---------------------------------------------------------------- tables
 // Layout of the single table allocation, in uint2 entries:
-//   [dir][prime] stage  : 2^13 each
+//   [dir][prime] stage  : 2^13 each, entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
 //   [dir][prime] fs_lo  : 2^13 each
 //   [dir][prime] fs_hi  : 2^13 each
 cudaError_t DeviceTables::build(int device) {
@@ -42,12 +42,12 @@ cudaError_t DeviceTables::build(int device) {
             uint2* st = h.data() + ((0 * 2 + dir) * kNumPrimes + j) * kEnt;
             uint2* lo = h.data() + ((1 * 2 + dir) * kNumPrimes + j) * kEnt;
             uint2* hi = h.data() + ((2 * 2 + dir) * kNumPrimes + j) * kEnt;
-            uint64_t a = 1, b = 1, c = 1;
+            uint64_t b = 1, c = 1;
             for (size_t i = 0; i < kEnt; ++i) {
-                st[i] = make_uint2((uint32_t)a, shoup_companion((uint32_t)a, p));
+                const uint32_t a = pow_mod(w14, stage_exponent((uint32_t)i), p);
+                st[i] = make_uint2(a, shoup_companion(a, p));
                 lo[i] = make_uint2((uint32_t)b, shoup_companion((uint32_t)b, p));
                 hi[i] = make_uint2((uint32_t)c, shoup_companion((uint32_t)c, p));
-                a = a * w14 % p;
                 b = b * w26 % p;
                 c = c * w26hi % p;
             }

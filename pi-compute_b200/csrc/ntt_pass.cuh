@@ -33,14 +33,32 @@ __device__ __forceinline__ uint32_t bitrev_n(uint32_t x, int logn) {
     return logn == 0 ? 0u : (__brev(x) >> (32 - logn));
 }
 
-// Four-step twiddle w_{N'}^e (e < N') applied to x: w_{2^26}^(e * 2^(26 - logNp)).
-__device__ __forceinline__ uint32_t fourstep_twiddle(uint32_t x, uint64_t e, int logNp, const uint2* lo,
-                                                     const uint2* hi, uint32_t p) {
-    uint32_t E = (uint32_t)((e << (kMaxLogL - logNp)) & ((1u << kMaxLogL) - 1));
-    uint2 a = __ldg(lo + (E & ((1u << kFsLog) - 1)));
-    uint2 b = __ldg(hi + (E >> kFsLog));
-    x = mul_shoup(x, a.x, a.y, p);
-    return mul_shoup(x, b.x, b.y, p);
+// Four-step twiddles for four consecutive columns t..t+3 of one row (output index k):
+// x.x *= w, x.y *= w*s, x.z *= w*s^2, x.w *= w*s^3 with w = w_{N'}^{t k}, s = w_{N'}^k.
+// Only w and s come from the tables (s is the same for a whole row, so its loads broadcast
+// across the warp); the other three twiddles follow by Montgomery products in registers.
+// r32 = 2^32 mod p with Shoup companion r32p (conversion into Montgomery form).
+__device__ __forceinline__ void fourstep_twiddle4(uint4& x, uint64_t t, uint64_t k, int logNp, const uint2* lo,
+                                                  const uint2* hi, uint32_t p, uint32_t pinv, uint32_t r32,
+                                                  uint32_t r32p) {
+    const uint32_t mask26 = (1u << kMaxLogL) - 1, mask13 = (1u << kFsLog) - 1;
+    const uint32_t E0 = (uint32_t)(((t * k) << (kMaxLogL - logNp)) & mask26);
+    const uint32_t Es = (uint32_t)((k << (kMaxLogL - logNp)) & mask26);
+    const uint2 a = __ldg(lo + (E0 & mask13));
+    const uint2 b = __ldg(hi + (E0 >> kFsLog));
+    const uint2 c = __ldg(lo + (Es & mask13));
+    const uint2 d = __ldg(hi + (Es >> kFsLog));
+    const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
+    const uint32_t st = mul_shoup(c.x, d.x, d.y, p);
+    uint32_t wm = mul_shoup(w, r32, r32p, p);   // w * 2^32  (Montgomery form)
+    const uint32_t sm = mul_shoup(st, r32, r32p, p);
+    x.x = mul_mont(x.x, wm, p, pinv);
+    wm = mul_mont(wm, sm, p, pinv);
+    x.y = mul_mont(x.y, wm, p, pinv);
+    wm = mul_mont(wm, sm, p, pinv);
+    x.z = mul_mont(x.z, wm, p, pinv);
+    wm = mul_mont(wm, sm, p, pinv);
+    x.w = mul_mont(x.w, wm, p, pinv);
 }
 
 // One decimation-in-frequency round of radix R = 2^LR on v[0..R), the group's
@@ -54,13 +72,12 @@ __device__ __forceinline__ void dif_round(uint32_t (&v)[1 << LR], uint32_t tp, i
     for (int k = 0; k < LR; ++k) {
         const int half = 1 << (LR - 1 - k);     // pair distance in q
         const int logh = logs + (LR - 1 - k);   // log2 of stage half size h
-        const int shift = (kStageLog - 1) - logh;
 #pragma unroll
         for (int q = 0; q < (1 << LR); ++q) {
             if (q & half) continue;
             uint32_t a = v[q], b = v[q + half];
             uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
-            uint2 w = __ldg(stw + (x << shift));
+            uint2 w = __ldg(stw + ((1u << logh) + x));
             v[q] = add_mod(a, b, p);
             v[q + half] = mul_shoup(a - b + p, w.x, w.y, p);
         }
@@ -76,12 +93,11 @@ __device__ __forceinline__ void dit_round(uint32_t (&v)[1 << LR], uint32_t tp, i
     for (int k = 0; k < LR; ++k) {
         const int half = 1 << k;
         const int logh = logs + k;
-        const int shift = (kStageLog - 1) - logh;
 #pragma unroll
         for (int q = 0; q < (1 << LR); ++q) {
             if (q & half) continue;
             uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
-            uint2 w = __ldg(stw + (x << shift));
+            uint2 w = __ldg(stw + ((1u << logh) + x));
             uint32_t a = v[q];
             uint32_t b = mul_shoup(v[q + half], w.x, w.y, p);
             v[q] = add_mod(a, b, p);
@@ -90,13 +106,19 @@ __device__ __forceinline__ void dit_round(uint32_t (&v)[1 << LR], uint32_t tp, i
     }
 }
 
+// Shared-memory address of linear tile index x: 16-byte chunks are permuted inside each
+// 128-byte line by bits of the line index (x >> 5) and (x >> 8), so the strided access
+// patterns of the radix rounds (strides of 16 and 256 words across lanes) and the 16-byte
+// vector accesses of the global<->shared copies all fall on distinct banks.
+__device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ ((((x >> 5) ^ (x >> 8)) & 7u) << 2); }
+
 // Shared-memory address of tile element (m, c).
 template <Layout LAY, int LOGN, int LOGE>
 __device__ __forceinline__ uint32_t sidx(uint32_t m, uint32_t c) {
     if constexpr (LAY == Layout::Strided) {
-        return (m << (LOGE - LOGN)) + c;
+        return swz((m << (LOGE - LOGN)) + c);
     } else {
-        return (c << LOGN) + m;
+        return swz((c << LOGN) + m);
     }
 }
 
@@ -105,7 +127,9 @@ __device__ __forceinline__ uint32_t sidx(uint32_t m, uint32_t c) {
 template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV>
 __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, uint32_t p) {
     constexpr int LOGC = LOGE - LOGN;
-    // Radix schedule: rounds of 4 stages, the remainder (LOGN % 4) as one smaller round.
+    // Radix schedule: the remainder (LOGN % 4 stages) is the top round (largest stride), then
+    // radix-16 rounds at strides 2^(4k), down to the round at stride 1. Every radix-16 round
+    // therefore has stride 1, 16 or >= 256, the strides the swizzle makes conflict-free.
     constexpr int NFULL = LOGN / 4;
     constexpr int REM = LOGN % 4;
     constexpr int NROUND = NFULL + (REM ? 1 : 0);
@@ -113,11 +137,10 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
     for (int rr = 0; rr < NROUND; ++rr) {
         // DIF: the first rounds take the highest stages. DIT: reversed order.
         const int r = INV ? (NROUND - 1 - rr) : rr;
-        // Round r covers stages with log-half-size in [lo, lo + LR): rounds 0..NFULL-1 are radix 16
-        // taken from the top, the remainder round sits at the bottom (smallest strides).
-        const bool is_rem = (REM != 0) && (r == NROUND - 1);
+        const bool is_rem = (REM != 0) && (r == 0);
         const int LRr = is_rem ? REM : 4;
-        const int logs = is_rem ? 0 : (LOGN - 4 * (r + 1));
+        // round r (r >= 1 when REM != 0) covers log-half-sizes [logs, logs + 4)
+        const int logs = is_rem ? (LOGN - REM) : (LOGN - REM - 4 * (r - (REM ? 1 : 0) + 1));
         // groups: E / R
         if (LRr == 4) {
             constexpr int R = 16;
@@ -148,29 +171,29 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                 for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)] = v[q];
             }
         } else {
-            // remainder round at logs = 0
+            // remainder round: the top LRX stages, stride s = 2^(LOGN - LRX), one block
             constexpr int LRX = (REM == 0) ? 1 : REM;
             constexpr int R = 1 << LRX;
             constexpr int NG = (1 << LOGE) / R;
+            constexpr int LOGSR = LOGN - LRX;
             for (int g = threadIdx.x; g < NG; g += NTHREADS) {
-                uint32_t c, blk;
+                uint32_t c, tp;
                 if constexpr (LAY == Layout::Strided) {
                     c = g & ((1u << LOGC) - 1);
-                    blk = g >> LOGC;
+                    tp = g >> LOGC;
                 } else {
-                    blk = g & ((1u << (LOGN - LRX)) - 1);
-                    c = g >> (LOGN - LRX);
+                    tp = g & ((1u << LOGSR) - 1);
+                    c = g >> LOGSR;
                 }
-                uint32_t m0 = blk * R;
                 uint32_t v[R];
 #pragma unroll
-                for (int q = 0; q < R; ++q) v[q] = sm[sidx<LAY, LOGN, LOGE>(m0 + q, c)];
+                for (int q = 0; q < R; ++q) v[q] = sm[sidx<LAY, LOGN, LOGE>(tp + ((uint32_t)q << LOGSR), c)];
                 if (INV)
-                    dit_round<LRX>(v, 0, 0, stw, p);
+                    dit_round<LRX>(v, tp, LOGSR, stw, p);
                 else
-                    dif_round<LRX>(v, 0, 0, stw, p);
+                    dif_round<LRX>(v, tp, LOGSR, stw, p);
 #pragma unroll
-                for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(m0 + q, c)] = v[q];
+                for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(tp + ((uint32_t)q << LOGSR), c)] = v[q];
             }
         }
         __syncthreads();
@@ -217,6 +240,9 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
     uint32_t* data = P.data + (uint64_t)j * P.L;
     uint32_t* out = P.out + (uint64_t)j * P.L;
     const int dir = INV ? 1 : 0;
+    const uint32_t pinv = inv_mod_2_32(p);
+    const uint32_t r32 = (uint32_t)(0x100000000ull % p);
+    const uint32_t r32p = (uint32_t)(((uint64_t)r32 << 32) / p);
 
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
     for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
@@ -232,7 +258,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
         if constexpr (LAY == Layout::Contig) {
             if (((tile << LOGC) + c) >= P.nrows) {
                 x = make_uint4(0, 0, 0, 0);
-                *reinterpret_cast<uint4*>(sm + e4) = x;
+                *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
                 continue;
             }
         }
@@ -256,12 +282,9 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
             // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m))
             uint32_t t = tcol<LAY, LOGN, LOGE>(tile, c, P.logS);
             uint64_t k = bitrev_n(m, LOGN);
-            x.x = fourstep_twiddle(x.x, (uint64_t)(t + 0) * k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p);
-            x.y = fourstep_twiddle(x.y, (uint64_t)(t + 1) * k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p);
-            x.z = fourstep_twiddle(x.z, (uint64_t)(t + 2) * k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p);
-            x.w = fourstep_twiddle(x.w, (uint64_t)(t + 3) * k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p);
+            fourstep_twiddle4(x, t, k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p, pinv, r32, r32p);
         }
-        *reinterpret_cast<uint4*>(sm + e4) = x;
+        *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
     }
     __syncthreads();
 
@@ -269,13 +292,12 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
 
     if constexpr (FUSE != Fuse::None) {
         static_assert(LAY == Layout::Contig && !INV, "pointwise fusion happens in the last forward pass");
-        const uint32_t pinv = inv_mod_2_32(p);
         const uint32_t* oth = P.other + (uint64_t)j * P.L;
         for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
             uint32_t c = e4 >> LOGN, m = e4 & ((1u << LOGN) - 1);
             if (((tile << LOGC) + c) >= P.nrows) continue;
             uint64_t g = gidx<LAY, LOGN, LOGE>(tile, m, c, 0);
-            uint4 a = *reinterpret_cast<uint4*>(sm + e4);
+            uint4 a = *reinterpret_cast<uint4*>(sm + swz(e4));
             uint4 b;
             if constexpr (FUSE == Fuse::MulInverse) {
                 b = *reinterpret_cast<const uint4*>(oth + g);
@@ -286,7 +308,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
             a.y = mul_mont(a.y, b.y, p, pinv);
             a.z = mul_mont(a.z, b.z, p, pinv);
             a.w = mul_mont(a.w, b.w, p, pinv);
-            *reinterpret_cast<uint4*>(sm + e4) = a;
+            *reinterpret_cast<uint4*>(sm + swz(e4)) = a;
         }
         __syncthreads();
         tile_transform<LAY, LOGN, LOGE, NTHREADS, true>(sm, T.stage[1][j], p);
@@ -303,14 +325,11 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
             m = e4 & ((1u << LOGN) - 1);
             if (((tile << LOGC) + c) >= P.nrows) continue;
         }
-        uint4 x = *reinterpret_cast<uint4*>(sm + e4);
+        uint4 x = *reinterpret_cast<uint4*>(sm + swz(e4));
         if constexpr (!INV && LAY == Layout::Strided) {
             uint32_t t = tcol<LAY, LOGN, LOGE>(tile, c, P.logS);
             uint64_t k = bitrev_n(m, LOGN);
-            x.x = fourstep_twiddle(x.x, (uint64_t)(t + 0) * k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p);
-            x.y = fourstep_twiddle(x.y, (uint64_t)(t + 1) * k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p);
-            x.z = fourstep_twiddle(x.z, (uint64_t)(t + 2) * k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p);
-            x.w = fourstep_twiddle(x.w, (uint64_t)(t + 3) * k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p);
+            fourstep_twiddle4(x, t, k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p, pinv, r32, r32p);
         }
         uint64_t g = gidx<LAY, LOGN, LOGE>(tile, m, c, P.logS);
         *reinterpret_cast<uint4*>(out + g) = x;

@@ -82,7 +82,7 @@ __global__ void fill_tables_kernel(uint2* t, uint32_t r0f, uint32_t r1f, uint32_
     const uint32_t root = dir == 0 ? (j == 0 ? r0f : j == 1 ? r1f : r2f) : (j == 0 ? r0i : j == 1 ? r1i : r2i);
     uint64_t e;
     if (type == 0)
-        e = (uint64_t)i << (pg::kMaxLogL - pg::kStageLog);  // w_{2^14}^i
+        e = (uint64_t)pg::stage_exponent(i) << (pg::kMaxLogL - pg::kStageLog);  // entry h + x = w_{2h}^x
     else if (type == 1)
         e = i;                                                // w_{2^26}^i
     else

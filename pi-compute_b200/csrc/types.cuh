@@ -8,12 +8,27 @@
 
 namespace pg {
 
+__host__ __device__ inline int __builtin_clz_portable(uint32_t x) {
+#ifdef __CUDA_ARCH__
+    return __clz(x);
+#else
+    return __builtin_clz(x);
+#endif
+}
+
 constexpr int kStageLog = 14;  // stage twiddles come from w_{2^14}: sub-transforms up to 2^13 points
 constexpr int kFsLog = 13;     // four-step twiddles: w_{2^26}^e = lo[e & 8191] * hi[e >> 13]
 
+// Exponent of w_{2^14} stored at stage-table entry i = h + x (h = 2^k <= i < 2h): w_{2h}^x.
+__host__ __device__ inline uint32_t stage_exponent(uint32_t i) {
+    if (i == 0) return 0;
+    int k = 31 - __builtin_clz_portable(i);
+    return (i - (1u << k)) << (kStageLog - 1 - k);
+}
+
 struct TwiddleTables {
     // (w, w') Shoup pairs, [dir][prime]; dir 0 = forward (w), 1 = inverse (w^-1).
-    const uint2* stage[2][kNumPrimes];  // w_{2^14}^j,           j < 2^13
+    const uint2* stage[2][kNumPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), 2^13 entries
     const uint2* fs_lo[2][kNumPrimes];  // w_{2^26}^j,           j < 2^13
     const uint2* fs_hi[2][kNumPrimes];  // w_{2^26}^(2^13 * i),  i < 2^13
 };
