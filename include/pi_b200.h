@@ -92,6 +92,17 @@ void* pg_stream(pg_ctx* ctx);
  * reference keeps per-multiplier call counters, gpu_ntt_multiplier.h:83-90). */
 uint64_t pg_launch_count(const pg_ctx* ctx);
 
+/* Level-batched, device-resident Chudnovsky binary splitting of the term range [a, b):
+ * P(a,b), Q(a,b), R(a,b) as magnitudes in HOST buffers of `cap` limbs each (P may be NULL
+ * when it is not needed, as for the root of a pi computation), their lengths in len[3] and
+ * signs in sign[3]. Same series, leaves and split point as the reference's BinarySplitting
+ * (src/engine/binary_splitting.cpp:137-159, 161-293, 295-348), so the values are identical;
+ * every depth of the tree runs as a few launches over all of its merges, with operands kept
+ * in device memory from the leaves to the root. Replaces BinarySplitting::compute
+ * (binary_splitting.cpp:605-644) with its per-merge Multiplier calls. */
+pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R, size_t cap,
+                size_t* len, int* sign);
+
 /* d_out = d_a * d_b without allocating any device memory. This entry point has no
  * counterpart in the reference.
  *

@@ -1,0 +1,674 @@
+// Level-batched, device-resident Chudnovsky binary splitting.
+//
+// Replaces the reference's recursive BinarySplitting (src/engine/binary_splitting.cpp:295-394,
+// 605-644) for the GPU: the same tree (range [a, b) split at m = a + (b - a)/2, so every
+// P/Q/R equals the reference's) is evaluated bottom-up one depth at a time, every merge of a
+// depth in the same launches, with all operands resident in HBM:
+//
+//   depth D-1 (D = ceil(log2(b - a)))   nodes of 1 or 2 terms: one thread each, leaf formulas
+//                                       (binary_splitting.cpp:137-159) and one merge in registers
+//   small depths                        one warp per merge, schoolbook products in shared memory
+//   larger depths                       batched NTT: forward transforms of Pl Ql Rl Pr Qr Rr for every
+//                                       merge, one pointwise pass producing P^ = Pl^Pr^, Q^ = Ql^Qr^ and
+//                                       R^ = Qr^Rl^ + s Pl^Rr^, three inverse transforms, one CRT+carry
+//                                       launch for all outputs (signed lift for R when s = -1)
+//
+// Node i of depth d merges nodes 2i and 2i+1 of depth d+1 (every depth above D-1 is full).
+// Magnitudes only are stored; signs follow from the node range (see merge_r_sign).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pi_b200.h"
+#include "ntt_engine.cuh"
+#include "series.cuh"
+
+namespace pg {
+
+// ------------------------------------------------------------------ small multi-limb helpers
+typedef unsigned __int128 u128;
+
+// out[0 .. nx+ny) = x * y (schoolbook, 64-bit limbs).
+__device__ __forceinline__ void sb_mul(const uint64_t* x, int nx, const uint64_t* y, int ny, uint64_t* out) {
+    for (int i = 0; i < nx + ny; ++i) out[i] = 0;
+    for (int i = 0; i < nx; ++i) {
+        uint64_t carry = 0;
+        for (int k = 0; k < ny; ++k) {
+            u128 t = (u128)x[i] * y[k] + out[i + k] + carry;
+            out[i + k] = (uint64_t)t;
+            carry = (uint64_t)(t >> 64);
+        }
+        out[i + ny] = carry;
+    }
+}
+
+__device__ __forceinline__ int sb_len(const uint64_t* x, int n) {
+    while (n > 0 && x[n - 1] == 0) --n;
+    return n;
+}
+
+// x[0..n) += s * y[0..ny) (s = +1 or -1); for s = -1 the result must be non-negative.
+__device__ __forceinline__ void sb_addsub(uint64_t* x, int n, const uint64_t* y, int ny, int s) {
+    if (s > 0) {
+        uint64_t c = 0;
+        for (int i = 0; i < n; ++i) {
+            u128 t = (u128)x[i] + (i < ny ? y[i] : 0) + c;
+            x[i] = (uint64_t)t;
+            c = (uint64_t)(t >> 64);
+        }
+    } else {
+        uint64_t br = 0;
+        for (int i = 0; i < n; ++i) {
+            const uint64_t yi = i < ny ? y[i] : 0;
+            const uint64_t d = x[i] - yi - br;
+            br = (x[i] < yi) || (x[i] - yi < br);
+            x[i] = d;
+        }
+    }
+}
+
+// Leaf magnitudes of term k (binary_splitting.cpp:137-159): |P| = (6k-5)(2k-1)(6k-1),
+// Q = k^3 * 640320^3/24, |R| = |P| * (13591409 + 545140134 k); k = 0: 1, 1, 13591409.
+__device__ void leaf_values(uint64_t k, uint64_t P[2], int& nP, uint64_t Q[3], int& nQ, uint64_t R[3], int& nR) {
+    if (k == 0) {
+        P[0] = 1; P[1] = 0; nP = 1;
+        Q[0] = 1; Q[1] = Q[2] = 0; nQ = 1;
+        R[0] = 13591409; R[1] = R[2] = 0; nR = 1;
+        return;
+    }
+    const u128 p = (u128)(6 * k - 5) * (2 * k - 1) * (6 * k - 1);   // < 2^100 for k < 2^32
+    P[0] = (uint64_t)p; P[1] = (uint64_t)(p >> 64);
+    nP = sb_len(P, 2);
+    const u128 k3 = (u128)k * k * k;                                   // < 2^96
+    const uint64_t C = 10939058860032000ull;                           // 640320^3 / 24
+    const u128 lo = (u128)(uint64_t)k3 * C;
+    const u128 hi = (u128)(uint64_t)(k3 >> 64) * C + (uint64_t)(lo >> 64);
+    Q[0] = (uint64_t)lo; Q[1] = (uint64_t)hi; Q[2] = (uint64_t)(hi >> 64);
+    nQ = sb_len(Q, 3);
+    const uint64_t lin = 13591409ull + 545140134ull * k;               // < 2^62
+    const u128 r0 = (u128)P[0] * lin;
+    const u128 r1 = (u128)P[1] * lin + (uint64_t)(r0 >> 64);
+    R[0] = (uint64_t)r0; R[1] = (uint64_t)r1; R[2] = (uint64_t)(r1 >> 64);
+    nR = sb_len(R, 3);
+}
+
+struct LevelView {
+    uint64_t* X[3];    // P, Q, R slot arrays
+    uint32_t cap[3];   // limbs per slot
+    uint32_t* len;     // len[3 i + k]
+};
+
+// Depth D-1: node i covers 1 or 2 terms. Caps: P 4, Q 6, R 8 limbs (7 needed, kept even).
+__global__ void bs_pair_kernel(LevelView out, uint64_t nodes, uint64_t a0, uint64_t b0, int depth) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nodes) return;
+    uint64_t a, b;
+    node_range(a0, b0, depth, i, a, b);
+    uint64_t* P = out.X[0] + i * out.cap[0];
+    uint64_t* Q = out.X[1] + i * out.cap[1];
+    uint64_t* R = out.X[2] + i * out.cap[2];
+    uint64_t Pl[2], Ql[3], Rl[3];
+    int nPl, nQl, nRl;
+    leaf_values(a, Pl, nPl, Ql, nQl, Rl, nRl);
+    int nP, nQ, nR;
+    if (b - a == 1) {
+        for (int t = 0; t < 2; ++t) P[t] = Pl[t];
+        for (int t = 0; t < 3; ++t) Q[t] = Ql[t], R[t] = Rl[t];
+        nP = nPl; nQ = nQl; nR = nRl;
+    } else {
+        uint64_t Pr[2], Qr[3], Rr[3];
+        int nPr, nQr, nRr;
+        leaf_values(a + 1, Pr, nPr, Qr, nQr, Rr, nRr);
+        uint64_t x[7], y[7];
+        sb_mul(Pl, nPl, Pr, nPr, x);
+        nP = sb_len(x, nPl + nPr);
+        for (int t = 0; t < 4; ++t) P[t] = t < nPl + nPr ? x[t] : 0;
+        sb_mul(Ql, nQl, Qr, nQr, x);
+        nQ = sb_len(x, nQl + nQr);
+        for (int t = 0; t < 6; ++t) Q[t] = t < nQl + nQr ? x[t] : 0;
+        for (int t = 0; t < 7; ++t) x[t] = y[t] = 0;
+        sb_mul(Qr, nQr, Rl, nRl, x);
+        sb_mul(Pl, nPl, Rr, nRr, y);
+        sb_addsub(x, 7, y, 7, merge_r_sign(a, b));
+        nR = sb_len(x, 7);
+        for (int t = 0; t < 7; ++t) R[t] = x[t];
+    }
+    out.len[3 * i + 0] = nP;
+    out.len[3 * i + 1] = nQ;
+    out.len[3 * i + 2] = nR;
+}
+
+// One warp per merge with operands of at most MAXC limbs (shared memory schoolbook).
+// Column sums are computed in parallel by the lanes; lane 0 propagates carries.
+template <int MAXC>
+__global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelView out, uint64_t merges,
+                                                            uint64_t a0, uint64_t b0, int depth) {
+    constexpr int W = 4;  // warps per block
+    __shared__ uint64_t s_op[W][6][MAXC];
+    __shared__ uint64_t s_col[W][3][2 * MAXC];  // 192-bit column sums: lo, mid, hi
+    __shared__ uint64_t s_res[W][2][2 * MAXC + 1];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t m = (uint64_t)blockIdx.x * W + warp;
+    if (m >= merges) return;
+    // load Pl Ql Rl Pr Qr Rr
+    int n[6];
+    for (int o = 0; o < 6; ++o) {
+        const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
+        const int k = o % 3;
+        n[o] = (int)in.len[3 * child + k];
+        const uint64_t* src = in.X[k] + child * in.cap[k];
+        for (int t = lane; t < MAXC; t += 32) s_op[warp][o][t] = t < n[o] ? src[t] : 0;
+    }
+    __syncwarp();
+    uint64_t a, b;
+    node_range(a0, b0, depth, m, a, b);
+    const int sgn = merge_r_sign(a, b);
+
+    // product helper: column sums then lane-0 carry pass into dst (nx + ny limbs)
+    auto product = [&](int ox, int oy, uint64_t* dst) -> int {
+        const int nx = n[ox], ny = n[oy];
+        const uint64_t* x = s_op[warp][ox];
+        const uint64_t* y = s_op[warp][oy];
+        const int ncol = nx + ny - 1;
+        for (int c = lane; c < ncol; c += 32) {
+            uint64_t lo = 0, mid = 0, hi = 0;
+            const int i0 = c - ny + 1 > 0 ? c - ny + 1 : 0;
+            const int i1 = c < nx - 1 ? c : nx - 1;
+            for (int i = i0; i <= i1; ++i) {
+                const u128 t = (u128)x[i] * y[c - i];
+                const u128 s = (u128)lo + (uint64_t)t;
+                lo = (uint64_t)s;
+                const u128 s2 = (u128)mid + (uint64_t)(t >> 64) + (uint64_t)(s >> 64);
+                mid = (uint64_t)s2;
+                hi += (uint64_t)(s2 >> 64);
+            }
+            s_col[warp][0][c] = lo;
+            s_col[warp][1][c] = mid;
+            s_col[warp][2][c] = hi;
+        }
+        __syncwarp();
+        int len = 0;
+        if (lane == 0) {
+            u128 carry = 0;  // < 2^129 never happens: column sums < MAXC * 2^128 << 2^192
+            uint64_t carry_hi = 0;
+            for (int c = 0; c < nx + ny; ++c) {
+                uint64_t lo = c < ncol ? s_col[warp][0][c] : 0;
+                uint64_t mid = c < ncol ? s_col[warp][1][c] : 0;
+                uint64_t hi = c < ncol ? s_col[warp][2][c] : 0;
+                const u128 t0 = (u128)lo + (uint64_t)carry;
+                dst[c] = (uint64_t)t0;
+                const u128 t1 = (u128)mid + (uint64_t)(carry >> 64) + (uint64_t)(t0 >> 64);
+                const uint64_t nh = hi + carry_hi + (uint64_t)(t1 >> 64);
+                carry = ((u128)nh << 64) | (uint64_t)t1;
+                carry_hi = 0;
+            }
+            len = sb_len(dst, nx + ny);
+        }
+        __syncwarp();
+        return __shfl_sync(0xffffffffu, len, 0);
+    };
+
+    // P = Pl * Pr
+    {
+        uint64_t* dst = out.X[0] + m * out.cap[0];
+        int l = (n[0] && n[3]) ? product(0, 3, s_res[warp][0]) : 0;
+        for (int t = lane; t < (int)out.cap[0]; t += 32) dst[t] = t < l ? s_res[warp][0][t] : 0;
+        if (lane == 0) out.len[3 * m + 0] = l;
+        __syncwarp();
+    }
+    // Q = Ql * Qr
+    {
+        uint64_t* dst = out.X[1] + m * out.cap[1];
+        int l = product(1, 4, s_res[warp][0]);
+        for (int t = lane; t < (int)out.cap[1]; t += 32) dst[t] = t < l ? s_res[warp][0][t] : 0;
+        if (lane == 0) out.len[3 * m + 1] = l;
+        __syncwarp();
+    }
+    // R = Qr * Rl + s * Pl * Rr
+    {
+        const int lx = product(4, 2, s_res[warp][0]);
+        const int ly = product(0, 5, s_res[warp][1]);
+        const int nmax = 2 * MAXC + 1;
+        if (lane == 0) {
+            uint64_t* x = s_res[warp][0];
+            for (int t = lx; t < nmax; ++t) x[t] = 0;
+            sb_addsub(x, nmax, s_res[warp][1], ly, sgn);
+        }
+        __syncwarp();
+        uint64_t* dst = out.X[2] + m * out.cap[2];
+        for (int t = lane; t < (int)out.cap[2]; t += 32) dst[t] = t < nmax ? s_res[warp][0][t] : 0;
+        if (lane == 0) out.len[3 * m + 2] = sb_len(s_res[warp][0], nmax < (int)out.cap[2] ? nmax : out.cap[2]);
+        __syncwarp();
+    }
+}
+
+// Pointwise combination for every merge of an NTT level: operands at base + (6m + o) * stride
+// (o = Pl Ql Rl Pr Qr Rr); writes P^ -> slot 3, Q^ -> slot 4, R^ -> slot 5.
+__global__ void bs_combine_kernel(uint32_t* base, uint64_t stride, uint64_t L, uint64_t merges, uint64_t a0,
+                                  uint64_t b0, int depth) {
+    const uint64_t m = blockIdx.y + (uint64_t)blockIdx.z * 65535;
+    if (m >= merges) return;
+    uint64_t a, b;
+    node_range(a0, b0, depth, m, a, b);
+    const int sgn = merge_r_sign(a, b);
+    uint32_t* g = base + 6 * m * stride;
+    for (uint64_t e = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; e < 3 * L;
+         e += (uint64_t)gridDim.x * blockDim.x * 4) {
+        const int j = (int)(e / L);
+        const uint32_t p = kPrime(j), pinv = inv_mod_2_32(p);
+        const uint4 pl = *reinterpret_cast<const uint4*>(g + 0 * stride + e);
+        const uint4 ql = *reinterpret_cast<const uint4*>(g + 1 * stride + e);
+        const uint4 rl = *reinterpret_cast<const uint4*>(g + 2 * stride + e);
+        const uint4 pr = *reinterpret_cast<const uint4*>(g + 3 * stride + e);
+        const uint4 qr = *reinterpret_cast<const uint4*>(g + 4 * stride + e);
+        const uint4 rr = *reinterpret_cast<const uint4*>(g + 5 * stride + e);
+        uint4 P, Q, R;
+#define PG_COMB(f)                                                             \
+    P.f = mul_mont(pl.f, pr.f, p, pinv);                                       \
+    Q.f = mul_mont(ql.f, qr.f, p, pinv);                                       \
+    {                                                                          \
+        const uint32_t u = mul_mont(qr.f, rl.f, p, pinv);                      \
+        const uint32_t v = mul_mont(pl.f, rr.f, p, pinv);                      \
+        R.f = sgn > 0 ? add_mod(u, v, p) : sub_mod(u, v, p);                   \
+    }
+        PG_COMB(x) PG_COMB(y) PG_COMB(z) PG_COMB(w)
+#undef PG_COMB
+        *reinterpret_cast<uint4*>(g + 3 * stride + e) = P;
+        *reinterpret_cast<uint4*>(g + 4 * stride + e) = Q;
+        *reinterpret_cast<uint4*>(g + 5 * stride + e) = R;
+    }
+}
+
+// ------------------------------------------------------------------ host side
+namespace {
+
+int bitlen128(u128 x) {
+    int n = 0;
+    while (x) {
+        ++n;
+        x >>= 1;
+    }
+    return n;
+}
+
+// Exact bit lengths of the leaf magnitudes of term k.
+void leaf_bits(uint64_t k, int& bp, int& bq, int& br) {
+    if (k == 0) {
+        bp = 1;
+        bq = 1;
+        br = 24;
+        return;
+    }
+    const u128 p = (u128)(6 * k - 5) * (2 * k - 1) * (6 * k - 1);
+    bp = bitlen128(p);
+    const u128 k3 = (u128)k * k * k;
+    const u128 lo = (u128)(uint64_t)k3 * 10939058860032000ull;
+    const u128 hi = (u128)(uint64_t)(k3 >> 64) * 10939058860032000ull + (uint64_t)(lo >> 64);
+    bq = hi ? 64 + bitlen128(hi) : bitlen128(lo);
+    const u128 lin = 13591409ull + (u128)545140134ull * k;
+    br = bp + bitlen128(lin);  // upper bound
+}
+
+struct DepthPlan {
+    uint64_t nodes;
+    uint32_t cap[3];  // limbs
+    int kind;         // 0 pair, 1 warp schoolbook, 2 ntt
+    int logL;         // ntt
+};
+
+constexpr uint32_t kWarpMaxC = 64;
+
+}  // namespace
+
+struct DeviceBS {
+    const DeviceTables* T = nullptr;
+    cudaStream_t st = nullptr;
+    uint64_t* launches = nullptr;
+    // owned buffers
+    uint64_t* lev[2][3] = {{nullptr}};
+    uint64_t lev_cap[2][3] = {{0}};
+    uint32_t* lev_len[2] = {nullptr, nullptr};
+    uint64_t lev_len_cap[2] = {0, 0};
+    uint32_t* res = nullptr;
+    uint64_t res_cap = 0;
+    uint32_t* sync = nullptr;
+    uint64_t sync_cap = 0;
+
+    ~DeviceBS() { release(); }
+    void release() {
+        for (int s = 0; s < 2; ++s) {
+            for (int k = 0; k < 3; ++k)
+                if (lev[s][k]) cudaFree(lev[s][k]), lev[s][k] = nullptr, lev_cap[s][k] = 0;
+            if (lev_len[s]) cudaFree(lev_len[s]), lev_len[s] = nullptr, lev_len_cap[s] = 0;
+        }
+        if (res) cudaFree(res), res = nullptr, res_cap = 0;
+        if (sync) cudaFree(sync), sync = nullptr, sync_cap = 0;
+    }
+    static cudaError_t grow(void** p, uint64_t& cap, uint64_t need) {
+        if (need <= cap) return cudaSuccess;
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaMalloc(p, need);
+        if (e == cudaSuccess) cap = need;
+        return e;
+    }
+
+    std::vector<DepthPlan> plan(uint64_t a0, uint64_t b0, int& D, std::string& err) {
+        std::vector<DepthPlan> dp;
+        const uint64_t n = b0 - a0;
+        D = 0;
+        while ((1ull << D) < n) ++D;
+        // rightmost node at each depth: [b0 - s_d, b0)
+        std::vector<uint64_t> s(D + 1);
+        {
+            uint64_t lo = a0, hi = b0;
+            for (int d = 0; d <= D; ++d) {
+                s[d] = hi - lo;
+                if (hi - lo > 1) lo = lo + (hi - lo) / 2;
+            }
+        }
+        // bit sums over the rightmost node of each depth
+        std::vector<uint64_t> sp(D + 1), sq(D + 1);
+        for (int d = 0; d <= D; ++d) {
+            uint64_t bp = 0, bq = 0;
+            for (uint64_t k = b0 - s[d]; k < b0; ++k) {
+                int p, q, r;
+                leaf_bits(k, p, q, r);
+                bp += p;
+                bq += q;
+            }
+            sp[d] = bp;
+            sq[d] = bq;
+        }
+        dp.resize(D);
+        // depth D-1: pair nodes
+        if (D >= 1) {
+            dp[D - 1].nodes = 1ull << (D - 1);
+            dp[D - 1].cap[0] = 4;
+            dp[D - 1].cap[1] = 6;
+            dp[D - 1].cap[2] = 8;  // 7 limbs rounded up to even
+            dp[D - 1].kind = 0;
+        }
+        uint64_t rbits = 0;  // running R bound (bits) of the child depth
+        {
+            int p, q, r;
+            leaf_bits(b0 - 1, p, q, r);
+            // pair level R bound: max(q + r, p + r) + 1 over two leaves of the largest terms
+            rbits = (uint64_t)(q + r + 1);
+        }
+        for (int d = D - 2; d >= 0; --d) {
+            DepthPlan& P = dp[d];
+            P.nodes = 1ull << d;
+            const uint64_t pb = sp[d], qb = sq[d];
+            // children's bounds (depth d + 1)
+            const uint64_t cqb = sq[d + 1], cpb = sp[d + 1];
+            const uint64_t rb = std::max(cqb + rbits, cpb + rbits) + 1;
+            // limbs, +1 spare, rounded up to even so every slot starts on a 16-byte boundary
+            P.cap[0] = (uint32_t)(((pb + 63) / 64 + 2) & ~1ull);
+            P.cap[1] = (uint32_t)(((qb + 63) / 64 + 2) & ~1ull);
+            P.cap[2] = (uint32_t)(((rb + 63) / 64 + 2) & ~1ull);
+            rbits = rb;
+            const DepthPlan& C = dp[d + 1];
+            const uint32_t cmax = std::max({C.cap[0], C.cap[1], C.cap[2]});
+            if (cmax <= kWarpMaxC) {
+                P.kind = 1;
+                P.logL = 0;
+            } else {
+                P.kind = 2;
+                const uint64_t conv =
+                    2ull * std::max({C.cap[1] + C.cap[1], C.cap[1] + C.cap[2], C.cap[0] + C.cap[2], C.cap[0] + C.cap[0]});
+                int l = 0;
+                while ((1ull << l) < conv) ++l;
+                P.logL = std::max(l, kMinLogL);
+                if (P.logL > kMaxLogL) {
+                    err = "binary-splitting product exceeds the transform range";
+                    return {};
+                }
+                // CRT exactness: R^ sums two convolutions, lifted to (-P/2, P/2]:
+                // (min(2capQ, 2capR) + min(2capP, 2capR)) * (2^32 - 1)^2 < p0 p1 p2 / 2
+                const double bound = (double)(2.0 * std::min(C.cap[1], C.cap[2]) + 2.0 * std::min(C.cap[0], C.cap[2])) *
+                                     18446744065119617025.0;
+                const double half = 2013265921.0 * 1811939329.0 * 469762049.0 / 2.0;
+                if (bound >= half) {
+                    err = "binary-splitting merge exceeds the proven CRT bound";
+                    return {};
+                }
+            }
+        }
+        return dp;
+    }
+
+    cudaError_t launch_ntt_level(const DepthPlan& P, const DepthPlan& C, const LevelView& in, const LevelView& out,
+                                 uint64_t a0, uint64_t b0, int depth) {
+        const Plan plan = make_plan(P.logL);
+        const uint64_t L = 1ull << P.logL;
+        const uint64_t M = P.nodes;
+        const uint64_t stride = 3 * L;
+        cudaError_t e = grow((void**)&res, res_cap, 6 * M * stride * 4);
+        if (e != cudaSuccess) return e;
+        // forward transforms of all 6M operands
+        PassParams p{};
+        p.data = res;
+        p.out = res;
+        p.L = L;
+        p.logL = P.logL;
+        p.job_stride = stride;
+        p.njobs = (uint32_t)(6 * M);
+        p.merge = 1;
+        for (int k = 0; k < 3; ++k) {
+            p.ms.X[k] = in.X[k];
+            p.ms.cap[k] = in.cap[k];
+        }
+        p.ms.len = in.len;
+        for (int i = 0; i < plan.npass; ++i) {
+            set_pass(p, plan, i);
+            e = launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, Fuse::None, p, T->tw, st);
+            if (e != cudaSuccess) return e;
+            if (launches) ++*launches;
+        }
+        // pointwise combination
+        {
+            const uint64_t per = std::max<uint64_t>(1, std::min<uint64_t>((3 * L / 4 + 255) / 256, 64));
+            dim3 grid((unsigned)per, (unsigned)std::min<uint64_t>(M, 65535), (unsigned)((M + 65534) / 65535));
+            bs_combine_kernel<<<grid, 256, 0, st>>>(res, stride, L, M, a0, b0, depth);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            if (launches) ++*launches;
+        }
+        // inverse transforms of the 3M outputs (slots 3..5 of every merge): as a batch of
+        // 2M jobs of stride 3*stride starting at slot 3 would skip slots; run them as 6M jobs
+        // over the whole workspace instead would transform inputs too. Use jobs with stride
+        // `stride` over slots [3, 6) of each merge: three launches of M jobs each.
+        for (int k = 0; k < 3; ++k) {
+            PassParams q{};
+            q.data = res + (3 + k) * stride;
+            q.out = q.data;
+            q.L = L;
+            q.logL = P.logL;
+            q.job_stride = 6 * stride;
+            q.njobs = (uint32_t)M;
+            q.merge = 0;
+            for (int i = plan.npass - 1; i >= 0; --i) {
+                set_pass(q, plan, i);
+                e = launch_pass(plan, i, true, Source::Residues, Fuse::None, q, T->tw, st);
+                if (e != cudaSuccess) return e;
+                if (launches) ++*launches;
+            }
+        }
+        // CRT + carry for all 3M outputs
+        uint64_t maxw = 2ull * std::max({out.cap[0], out.cap[1], out.cap[2]});
+        const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+        const uint64_t jobs = 3 * M;
+        e = grow((void**)&sync, sync_cap, (1 + jobs + jobs * bpj) * 4);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(sync + 1, 0, (jobs + jobs * bpj) * 4, st);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(out.len, 0, 3 * M * 4, st);
+        if (e != cudaSuccess) return e;
+        CrtParams c{};
+        c.L = L;
+        c.error = sync;
+        c.ticket = sync + 1;
+        c.status = sync + 1 + jobs;
+        c.blocks_per_job = bpj;
+        c.k = make_crt_consts(P.logL);
+        c.merge = 1;
+        c.res = res;
+        c.res_stride = stride;
+        for (int k = 0; k < 3; ++k) {
+            c.dst[k] = out.X[k];
+            c.dcap[k] = out.cap[k];
+        }
+        c.dlen = out.len;
+        c.a0 = a0;
+        c.b0 = b0;
+        c.depth = depth;
+        e = launch_crt(c, jobs * bpj, st);
+        if (launches) ++*launches;
+        (void)C;
+        return e;
+    }
+
+    // Computes P, Q, R of [a0, b0); results stay in the final level buffers (root = node 0).
+    cudaError_t run(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
+        int D = 0;
+        std::vector<DepthPlan> dp = plan(a0, b0, D, err);
+        if (!err.empty()) return cudaErrorInvalidValue;
+        cudaError_t e = grow((void**)&sync, sync_cap, 4096 * 4);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(sync, 0, 4, st);
+        if (e != cudaSuccess) return e;
+        if (D == 0) {
+            // single term: the root is a leaf; treat it as a "pair level" of one node of size 1
+            dp.resize(1);
+            dp[0].nodes = 1;
+            dp[0].cap[0] = 4;
+            dp[0].cap[1] = 6;
+            dp[0].cap[2] = 8;
+            dp[0].kind = 0;
+            D = 1;
+        }
+        auto view = [&](int slot, const DepthPlan& P) {
+            LevelView v;
+            for (int k = 0; k < 3; ++k) {
+                v.X[k] = lev[slot][k];
+                v.cap[k] = P.cap[k];
+            }
+            v.len = lev_len[slot];
+            return v;
+        };
+        auto alloc = [&](int slot, const DepthPlan& P) -> cudaError_t {
+            for (int k = 0; k < 3; ++k) {
+                cudaError_t r = grow((void**)&lev[slot][k], lev_cap[slot][k], P.nodes * P.cap[k] * 8);
+                if (r != cudaSuccess) return r;
+            }
+            return grow((void**)&lev_len[slot], lev_len_cap[slot], P.nodes * 3 * 4);
+        };
+        int slot = 0;
+        // depth D-1
+        {
+            const DepthPlan& P = dp[D - 1];
+            e = alloc(slot, P);
+            if (e != cudaSuccess) return e;
+            LevelView v = view(slot, P);
+            const int depth = (b0 - a0 == 1) ? 0 : D - 1;
+            bs_pair_kernel<<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(v, P.nodes, a0, b0, depth);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            if (launches) ++*launches;
+        }
+        for (int d = D - 2; d >= 0; --d) {
+            const DepthPlan& C = dp[d + 1];
+            const DepthPlan& P = dp[d];
+            const int oslot = slot ^ 1;
+            e = alloc(oslot, P);
+            if (e != cudaSuccess) return e;
+            LevelView in = view(slot, C), out = view(oslot, P);
+            if (P.kind == 1) {
+                bs_warp_merge_kernel<kWarpMaxC><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes, a0,
+                                                                                              b0, d);
+                e = cudaGetLastError();
+                if (launches) ++*launches;
+            } else {
+                e = launch_ntt_level(P, C, in, out, a0, b0, d);
+            }
+            if (e != cudaSuccess) return e;
+            slot = oslot;
+        }
+        root = view(slot, dp[0]);
+        return cudaSuccess;
+    }
+};
+
+}  // namespace pg
+
+// ------------------------------------------------------------------ C ABI
+struct pg_ctx;
+namespace pg {
+// defined in pg_api.cu
+const DeviceTables& ctx_tables(pg_ctx* c);
+cudaStream_t ctx_stream(pg_ctx* c);
+std::mutex& ctx_mutex(pg_ctx* c);
+uint64_t* ctx_launches(pg_ctx* c);
+void ctx_set_error(pg_ctx* c, const std::string& msg);
+int ctx_device(pg_ctx* c);
+}  // namespace pg
+
+extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R,
+                           size_t cap, size_t* len, int* sign) {
+    if (!ctx || !Q || !R || !len || !sign || b <= a) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    pg::DeviceBS bs;
+    bs.T = &pg::ctx_tables(ctx);
+    bs.st = pg::ctx_stream(ctx);
+    bs.launches = pg::ctx_launches(ctx);
+    pg::LevelView root;
+    std::string err;
+    cudaError_t e = bs.run(a, b, root, err);
+    if (!err.empty()) {
+        pg::ctx_set_error(ctx, err);
+        return PG_ERR_TOO_LARGE;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        pg::ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
+    }
+    uint32_t hl[3] = {0, 0, 0};
+    uint32_t herr = 0;
+    e = cudaMemcpyAsync(hl, root.len, 12, cudaMemcpyDeviceToHost, bs.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, bs.sync, 4, cudaMemcpyDeviceToHost, bs.st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(bs.st);
+    if (e != cudaSuccess) {
+        pg::ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
+        return PG_ERR_DEVICE;
+    }
+    if (herr) {
+        pg::ctx_set_error(ctx, herr == 1 ? "carry look-back wait ran out of iterations" : "carry out of the top word");
+        return herr == 1 ? PG_ERR_TIMEOUT : PG_ERR_INTERNAL;
+    }
+    if (hl[1] > cap || hl[2] > cap || (P && hl[0] > cap)) {
+        pg::ctx_set_error(ctx, "output buffers smaller than the result");
+        return PG_ERR_BAD_ARG;
+    }
+    uint64_t* dsts[3] = {P, Q, R};
+    for (int k = 0; k < 3; ++k) {
+        len[k] = hl[k];
+        if (dsts[k] && hl[k]) cudaMemcpyAsync(dsts[k], root.X[k], hl[k] * 8, cudaMemcpyDeviceToHost, bs.st);
+    }
+    e = cudaStreamSynchronize(bs.st);
+    if (e != cudaSuccess) return PG_ERR_DEVICE;
+    // signs over the series: P(a,b) = (-1)^(#k >= 1), Q > 0, R(a,b) has the sign of R(a, a+1)
+    const unsigned long neg_terms = (b - a) - (a == 0 ? 1 : 0);
+    sign[0] = hl[0] ? ((neg_terms & 1) ? -1 : 1) : 0;
+    sign[1] = hl[1] ? 1 : 0;
+    sign[2] = hl[2] ? (a == 0 ? 1 : -1) : 0;
+    return PG_OK;
+}

@@ -1,25 +1,31 @@
 // Exact CRT recombination of the three inverse-transformed residue arrays and
 // the carry-propagation scan that turns the convolution into product limbs.
 //
-// Coefficient i of the (w = 32) convolution is x_i < p0*p1*p2 < 2^91, rebuilt
-// by Garner's method with all constants precomputed (scale L^-1 * 2^32 for the
-// unnormalised inverse transform and the Montgomery pointwise product folded
-// into them). Output 32-bit word j receives
-//     W_j = x_j[0] + x_{j-1}[1] + x_{j-2}[2]      (x[k] = 32-bit word k of x)
-// so W_j < 2^33 + 2^27 and every carry between words is 0, 1 or 2.
+// Coefficient i of the (w = 32) convolution is x_i, rebuilt by Garner's method with all
+// constants precomputed (the scale L^-1 * 2^32 for the unnormalised inverse transform and
+// the Montgomery pointwise product are folded into them). For a plain product x_i lies in
+// [0, p0*p1*p2) and is < 2^91. For a signed combination (the binary-splitting R = Qr*Rl -
+// Pl*Rr done in the transform domain) coefficients may be negative: the CRT value is lifted
+// to (-p0p1p2/2, p0p1p2/2] and held as a 96-bit two's-complement number.
 //
-// The scan: each thread owns 16 consecutive words; its carry behaviour is the
-// transfer function f: {0,1,2} -> {0,1,2} (carry in -> carry out), packed in 6
-// bits. Functions compose associatively, so a warp scan, a block scan and a
-// decoupled look-back across blocks (single pass, CTA order fixed by an atomic
-// ticket so every predecessor is resident; one warp inspects 32 predecessors per
-// step) give each thread its exact carry in.
-// Every spin in the look-back has an iteration limit; running out sets an error
-// word the host checks, and the kernel finishes without hanging.
+// Output 32-bit word j receives W_j = x_j[0] + x_{j-1}[1] + x_{j-2}[2] (x[2] signed), so
+// W_j lies in (-2^31, 2^33 + 2^31) and every carry between words is in {-1, 0, 1, 2}.
+//
+// The scan: each thread owns 16 consecutive words; its carry behaviour is the transfer
+// function f: {-1,0,1,2} -> {-1,0,1,2} (carry in -> carry out), stored as 4 two-bit
+// entries of (carry + 1). Functions compose associatively, so a warp scan, a block scan
+// and a decoupled look-back across blocks (single pass, CTA order fixed by an atomic
+// ticket so every predecessor is resident; one warp inspects 32 predecessors per step)
+// give each thread its exact carry in. Every spin in the look-back has an iteration limit;
+// running out sets an error word the host checks, and the kernel finishes without hanging.
+//
+// One launch can recombine many products (the three outputs of every merge of a
+// binary-splitting level); each has its own ticket and status words.
 #pragma once
 #include <cstdint>
 
 #include "modarith.cuh"
+#include "series.cuh"
 #include "types.cuh"
 
 namespace pg {
@@ -30,7 +36,7 @@ struct X3 {
     uint32_t w0, w1, w2;
 };
 
-__device__ __forceinline__ X3 crt3(uint32_t r0, uint32_t r1, uint32_t r2, const CrtConsts& k) {
+__device__ __forceinline__ X3 crt3(uint32_t r0, uint32_t r1, uint32_t r2, const CrtConsts& k, bool centred) {
     const uint32_t p0 = kPrime(0), p1 = kPrime(1), p2 = kPrime(2);
     uint32_t x0 = mul_shoup(r0, k.c00, k.c00p, p0);
     uint32_t y1 = sub_mod(mul_shoup(r1, k.c11, k.c11p, p1), mul_shoup(x0, k.k01, k.k01p, p1), p1);
@@ -43,6 +49,15 @@ __device__ __forceinline__ X3 crt3(uint32_t r0, uint32_t r1, uint32_t r2, const 
     uint64_t phi = __umul64hi(k.p01, (uint64_t)y2);
     uint64_t s = lo + plo;
     phi += (s < lo);
+    if (centred) {
+        // x > P/2  <=>  Garner digits (y2, y1, x0) > those of floor(P/2), compared lexicographically
+        const bool neg = (y2 > k.h2) || (y2 == k.h2 && (y1 > k.h1 || (y1 == k.h1 && x0 > k.h0)));
+        if (neg) {  // x - P as a 96-bit two's-complement number
+            const uint64_t b0 = s - k.P_lo;
+            phi = phi - k.P_hi - (s < k.P_lo ? 1 : 0);
+            s = b0;
+        }
+    }
     X3 r;
     r.w0 = (uint32_t)s;
     r.w1 = (uint32_t)(s >> 32);
@@ -50,14 +65,50 @@ __device__ __forceinline__ X3 crt3(uint32_t r0, uint32_t r1, uint32_t r2, const 
     return r;
 }
 
-// f packed as f(0) | f(1) << 2 | f(2) << 4.  compose(g, f) = g o f (apply f first).
-__device__ __forceinline__ uint32_t fapply(uint32_t f, uint32_t c) { return (f >> (2 * c)) & 3u; }
-__device__ __forceinline__ uint32_t fcompose(uint32_t g, uint32_t f) {
-    return fapply(g, fapply(f, 0)) | (fapply(g, fapply(f, 1)) << 2) | (fapply(g, fapply(f, 2)) << 4);
+// f packed as (f(-1)+1) | (f(0)+1) << 2 | (f(1)+1) << 4 | (f(2)+1) << 6, indexed by u = carry + 1.
+__device__ __forceinline__ uint32_t fapply(uint32_t f, uint32_t u) { return (f >> (2 * u)) & 3u; }
+__device__ __forceinline__ uint32_t fcompose(uint32_t g, uint32_t f) {  // g o f (apply f first)
+    return fapply(g, fapply(f, 0)) | (fapply(g, fapply(f, 1)) << 2) | (fapply(g, fapply(f, 2)) << 4) |
+           (fapply(g, fapply(f, 3)) << 6);
 }
-constexpr uint32_t kFIdentity = 0u | (1u << 2) | (2u << 4);
+constexpr uint32_t kFIdentity = 0u | (1u << 2) | (2u << 4) | (3u << 6);
+__device__ __forceinline__ uint32_t fconst(uint32_t u) { return u | (u << 2) | (u << 4) | (u << 6); }
 
 enum : uint32_t { kStNone = 0, kStAgg = 1, kStIncl = 2 };
+
+// Job description resolved per block: where the residues are, where the words go.
+struct CrtJob {
+    const uint32_t* res;
+    uint32_t* out;
+    uint64_t nwords;
+    uint32_t* len;     // if non-null: receives the product's length in limbs (atomicMax)
+    bool centred;
+};
+
+__device__ __forceinline__ CrtJob crt_job(const CrtParams& P, uint64_t job) {
+    CrtJob J;
+    if (!P.merge) {
+        J.res = P.res;
+        J.out = P.out;
+        J.nwords = P.nwords;
+        J.len = nullptr;
+        J.centred = false;
+        return J;
+    }
+    const uint64_t m = job / 3;
+    const int which = (int)(job % 3);
+    J.res = P.res + (6 * m + 3 + which) * P.res_stride;
+    J.out = reinterpret_cast<uint32_t*>(P.dst[which] + m * P.dcap[which]);
+    J.nwords = 2ull * P.dcap[which];
+    J.len = P.dlen + 3 * m + which;
+    J.centred = false;
+    if (which == 2) {
+        uint64_t a, b;
+        node_range(P.a0, P.b0, P.depth, m, a, b);
+        J.centred = merge_r_sign(a, b) < 0;
+    }
+    return J;
+}
 
 __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) {
     __shared__ uint32_t s_tail[kCrtThreads / 32][3];
@@ -65,15 +116,23 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
     __shared__ uint32_t s_bid;
     __shared__ uint32_t s_carry_in;
 
-    if (threadIdx.x == 0) s_bid = atomicAdd(P.ticket, 1u);
+    const uint64_t job = blockIdx.x / P.blocks_per_job;
+    const CrtJob J = crt_job(P, job);
+    const uint64_t nblocks = (J.nwords + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+    if (blockIdx.x % P.blocks_per_job >= nblocks) return;  // this job needs fewer blocks
+    uint32_t* ticket = P.ticket + job;
+    volatile uint32_t* st = P.status + job * P.blocks_per_job;
+
+    if (threadIdx.x == 0) s_bid = atomicAdd(ticket, 1u);
     __syncthreads();
     const uint32_t bid = s_bid;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t j0 = ((uint64_t)bid * kCrtThreads + threadIdx.x) * kCrtWords;
 
-    const uint32_t* r0 = P.res;
-    const uint32_t* r1 = P.res + P.L;
-    const uint32_t* r2 = P.res + 2 * P.L;
+    const uint32_t* r0 = J.res;
+    const uint32_t* r1 = J.res + P.L;
+    const uint32_t* r2 = J.res + 2 * P.L;
+    const bool cen = J.centred;
 
     uint32_t a0[kCrtWords], a1[kCrtWords], a2[kCrtWords];
     if (j0 + kCrtWords <= P.L) {
@@ -83,17 +142,17 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
             uint4 v1 = *reinterpret_cast<const uint4*>(r1 + j0 + u);
             uint4 v2 = *reinterpret_cast<const uint4*>(r2 + j0 + u);
             X3 x;
-            x = crt3(v0.x, v1.x, v2.x, P.k); a0[u] = x.w0; a1[u] = x.w1; a2[u] = x.w2;
-            x = crt3(v0.y, v1.y, v2.y, P.k); a0[u + 1] = x.w0; a1[u + 1] = x.w1; a2[u + 1] = x.w2;
-            x = crt3(v0.z, v1.z, v2.z, P.k); a0[u + 2] = x.w0; a1[u + 2] = x.w1; a2[u + 2] = x.w2;
-            x = crt3(v0.w, v1.w, v2.w, P.k); a0[u + 3] = x.w0; a1[u + 3] = x.w1; a2[u + 3] = x.w2;
+            x = crt3(v0.x, v1.x, v2.x, P.k, cen); a0[u] = x.w0; a1[u] = x.w1; a2[u] = x.w2;
+            x = crt3(v0.y, v1.y, v2.y, P.k, cen); a0[u + 1] = x.w0; a1[u + 1] = x.w1; a2[u + 1] = x.w2;
+            x = crt3(v0.z, v1.z, v2.z, P.k, cen); a0[u + 2] = x.w0; a1[u + 2] = x.w1; a2[u + 2] = x.w2;
+            x = crt3(v0.w, v1.w, v2.w, P.k, cen); a0[u + 3] = x.w0; a1[u + 3] = x.w1; a2[u + 3] = x.w2;
         }
     } else {
 #pragma unroll
         for (int u = 0; u < kCrtWords; ++u) {
             uint64_t i = j0 + u;
             if (i < P.L) {
-                X3 x = crt3(r0[i], r1[i], r2[i], P.k);
+                X3 x = crt3(r0[i], r1[i], r2[i], P.k, cen);
                 a0[u] = x.w0; a1[u] = x.w1; a2[u] = x.w2;
             } else {
                 a0[u] = a1[u] = a2[u] = 0;
@@ -119,39 +178,45 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
         } else if (j0 >= 2) {
             // first thread of the CTA: rebuild the two coefficients below its range
             X3 xm1 = {0, 0, 0}, xm2 = {0, 0, 0};
-            if (j0 - 1 < P.L) xm1 = crt3(r0[j0 - 1], r1[j0 - 1], r2[j0 - 1], P.k);
-            if (j0 - 2 < P.L) xm2 = crt3(r0[j0 - 2], r1[j0 - 2], r2[j0 - 2], P.k);
+            if (j0 - 1 < P.L) xm1 = crt3(r0[j0 - 1], r1[j0 - 1], r2[j0 - 1], P.k, cen);
+            if (j0 - 2 < P.L) xm2 = crt3(r0[j0 - 2], r1[j0 - 2], r2[j0 - 2], P.k, cen);
             pw1 = xm1.w1; pw2a = xm1.w2; pw2b = xm2.w2;
         } else {
             pw1 = pw2a = pw2b = 0;
         }
     }
 
-    // Raw word sums and the carry-in-0 pass.
-    uint64_t W[kCrtWords];
+    // Raw word sums (signed) and the carry-in-0 pass.
+    int64_t W[kCrtWords];
 #pragma unroll
     for (int u = 0; u < kCrtWords; ++u) {
-        uint64_t w = a0[u];
-        w += (u >= 1) ? a1[u - 1] : pw1;
-        w += (u >= 2) ? a2[u - 2] : (u == 1 ? pw2a : pw2b);
+        int64_t w = (int64_t)a0[u];
+        w += (int64_t)((u >= 1) ? a1[u - 1] : pw1);
+        w += (int64_t)(int32_t)((u >= 2) ? a2[u - 2] : (u == 1 ? pw2a : pw2b));
         W[u] = w;
     }
     uint32_t f;
     {
-        uint64_t acc = 0;
-        bool allones_hi = true;
+        int64_t acc = 0;
+        bool ones_hi = true, zero_hi = true;
         uint32_t low0 = 0;
 #pragma unroll
         for (int u = 0; u < kCrtWords; ++u) {
             acc += W[u];
             uint32_t o = (uint32_t)acc;
-            if (u == 0) low0 = o; else allones_hi &= (o == 0xffffffffu);
-            acc >>= 32;
+            if (u == 0) {
+                low0 = o;
+            } else {
+                ones_hi &= (o == 0xffffffffu);
+                zero_hi &= (o == 0u);
+            }
+            acc >>= 32;  // arithmetic: floor division by 2^32
         }
-        uint32_t c0 = (uint32_t)acc;
-        uint32_t c1 = c0 + ((allones_hi && low0 == 0xffffffffu) ? 1u : 0u);
-        uint32_t c2 = c0 + ((allones_hi && low0 >= 0xfffffffeu) ? 1u : 0u);
-        f = c0 | (c1 << 2) | (c2 << 4);
+        const int c0 = (int)acc;
+        const int fm1 = c0 - ((zero_hi && low0 == 0u) ? 1 : 0);
+        const int f1 = c0 + ((ones_hi && low0 == 0xffffffffu) ? 1 : 0);
+        const int f2 = c0 + ((ones_hi && low0 >= 0xfffffffeu) ? 1 : 0);
+        f = (uint32_t)(fm1 + 1) | ((uint32_t)(c0 + 1) << 2) | ((uint32_t)(f1 + 1) << 4) | ((uint32_t)(f2 + 1) << 6);
     }
 
     // Warp inclusive scan of transfer functions (lane order = word order).
@@ -183,11 +248,10 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
 
         // Decoupled look-back, one window of 32 predecessors per step (lane l reads block
         // base - l). The window's functions compose into one; the nearest block that already
-        // knows its carry out ends the walk.
-        volatile uint32_t* st = P.status;
-        uint32_t carry_in = 0;
+        // knows its carry out ends the walk. Carries are stored as u = carry + 1.
+        uint32_t u_in = 1;
         if (bid == 0) {
-            if (lane == 0) st[0] = kStIncl | (fapply(blk, 0) << 8);
+            if (lane == 0) st[0] = kStIncl | (fapply(blk, 1) << 8);
         } else {
             if (lane == 0) {
                 __threadfence();
@@ -198,7 +262,7 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
             uint32_t spins = 0;
             while (true) {
                 const int64_t jb = base - lane;
-                const uint32_t v = (jb >= 0) ? st[jb] : (uint32_t)kStIncl;  // before block 0: carry 0
+                const uint32_t v = (jb >= 0) ? st[jb] : (uint32_t)(kStIncl | (1u << 8));  // before block 0: carry 0
                 const uint32_t sv = v & 0xffu;
                 const unsigned incl_mask = __ballot_sync(0xffffffffu, sv == kStIncl);
                 const unsigned none_mask = __ballot_sync(0xffffffffu, sv == kStNone);
@@ -214,7 +278,7 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
                 }
                 __threadfence();
                 const uint32_t pay = (v >> 8) & 0xffu;
-                uint32_t g = (lane < first) ? pay : (lane == first ? (pay | (pay << 2) | (pay << 4)) : kFIdentity);
+                uint32_t g = (lane < first) ? pay : (lane == first ? fconst(pay) : kFIdentity);
 #pragma unroll
                 for (int off = 1; off < 32; off <<= 1) {
                     uint32_t o = __shfl_down_sync(0xffffffffu, g, off);
@@ -223,44 +287,53 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
                 g = __shfl_sync(0xffffffffu, g, 0);
                 look = fcompose(look, g);
                 if (first < 32) {
-                    carry_in = fapply(look, 0);
+                    u_in = fapply(look, 1);
                     break;
                 }
                 base -= 32;
             }
             if (lane == 0) {
                 __threadfence();
-                st[bid] = kStIncl | (fapply(blk, carry_in) << 8);
+                st[bid] = kStIncl | (fapply(blk, u_in) << 8);
             }
         }
         if (lane == 0) {
-            s_carry_in = carry_in;
-            if ((uint64_t)(bid + 1) * kCrtThreads * kCrtWords >= P.nwords && fapply(blk, carry_in) != 0)
-                atomicExch(P.error, 2u);  // product overflowed its limb count: cannot happen for valid inputs
+            s_carry_in = u_in;
+            if ((uint64_t)(bid + 1) * kCrtThreads * kCrtWords >= J.nwords && fapply(blk, u_in) != 1)
+                atomicExch(P.error, 2u);  // carry out of the top word: the result does not fit
         }
     }
     __syncthreads();
-    uint32_t c = fapply(excl, fapply(s_wagg[warp], s_carry_in));
+    const int c = (int)fapply(excl, fapply(s_wagg[warp], s_carry_in)) - 1;
 
     // Final words.
     uint32_t o[kCrtWords];
+    int top = -1;
     {
-        uint64_t acc = c;
+        int64_t acc = c;
 #pragma unroll
         for (int u = 0; u < kCrtWords; ++u) {
             acc += W[u];
             o[u] = (uint32_t)acc;
+            if (o[u] != 0 && j0 + u < J.nwords) top = u;
             acc >>= 32;
         }
     }
-    if (j0 + kCrtWords <= P.nwords) {
+    if (j0 + kCrtWords <= J.nwords) {
 #pragma unroll
         for (int u = 0; u < kCrtWords; u += 4)
-            *reinterpret_cast<uint4*>(P.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
+            *reinterpret_cast<uint4*>(J.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
     } else {
 #pragma unroll
         for (int u = 0; u < kCrtWords; ++u)
-            if (j0 + u < P.nwords) P.out[j0 + u] = o[u];
+            if (j0 + u < J.nwords) J.out[j0 + u] = o[u];
+    }
+    if (J.len) {
+        // length in limbs = (index of the highest non-zero word) / 2 + 1
+        uint32_t lim = top >= 0 ? (uint32_t)((j0 + top) / 2 + 1) : 0u;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lim = max(lim, __shfl_xor_sync(0xffffffffu, lim, off));
+        if (lane == 0 && lim) atomicMax(J.len, lim);
     }
 }
 

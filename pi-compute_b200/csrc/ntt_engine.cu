@@ -123,17 +123,18 @@ void Workspace::release() {
 
 // ---------------------------------------------------------------- pass dispatch
 template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
-static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, uint64_t L, cudaStream_t st) {
+static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cudaStream_t st) {
     constexpr int LOGE = kTileLog;
     auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
     const size_t smem = (size_t)4 << LOGE;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        configured = true;
+    uint64_t tiles;
+    if constexpr (LAY == Layout::Strided) {
+        tiles = (uint64_t)prm.njobs << (prm.logL - LOGE);
+    } else {
+        const uint64_t rows = (uint64_t)prm.njobs << (prm.logL - LOGN);
+        const uint64_t per = 1ull << (LOGE - LOGN);
+        tiles = (rows + per - 1) / per;
     }
-    uint64_t tiles = L >> LOGE;
-    if (tiles == 0) tiles = 1;
     dim3 grid((unsigned)tiles, kNumPrimes);
     kern<<<grid, kPassThreads, smem, st>>>(prm, tw);
     return cudaGetLastError();
@@ -141,29 +142,29 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, uint
 
 #define PG_CONTIG_CASE(N)                                                                                    \
     case N:                                                                                                  \
+        if (inverse) return run_pass<Layout::Contig, N, true, Source::Residues, Fuse::None>(prm, tw, st);   \
         if (src == Source::Limbs) {                                                                          \
-            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::None>(prm, tw, L, st); \
-            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::MulInverse>(prm, tw, L, st); \
-            return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::SqrInverse>(prm, tw, L, st);     \
+            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::None>(prm, tw, st); \
+            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::MulInverse>(prm, tw, st); \
+            return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::SqrInverse>(prm, tw, st);        \
         } else {                                                                                             \
-            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::None>(prm, tw, L, st); \
-            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::MulInverse>(prm, tw, L, st); \
-            return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::SqrInverse>(prm, tw, L, st);  \
+            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::None>(prm, tw, st); \
+            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::MulInverse>(prm, tw, st); \
+            return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::SqrInverse>(prm, tw, st);     \
         }
 
 #define PG_STRIDED_CASE(N)                                                                                   \
     case N:                                                                                                  \
-        if (inverse) return run_pass<Layout::Strided, N, true, Source::Residues, Fuse::None>(prm, tw, L, st); \
-        if (src == Source::Limbs) return run_pass<Layout::Strided, N, false, Source::Limbs, Fuse::None>(prm, tw, L, st); \
-        return run_pass<Layout::Strided, N, false, Source::Residues, Fuse::None>(prm, tw, L, st);
+        if (inverse) return run_pass<Layout::Strided, N, true, Source::Residues, Fuse::None>(prm, tw, st);  \
+        if (src == Source::Limbs) return run_pass<Layout::Strided, N, false, Source::Limbs, Fuse::None>(prm, tw, st); \
+        return run_pass<Layout::Strided, N, false, Source::Residues, Fuse::None>(prm, tw, st);
 
 cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm,
                         const TwiddleTables& tw, cudaStream_t st) {
-    const uint64_t L = 1ull << plan.logL;
     const int logN = plan.logN[pass];
     const bool contig = (pass == plan.npass - 1);
     if (contig) {
-        if (inverse) return cudaErrorInvalidValue;  // contiguous inverse runs fused with the pointwise product
+        if (inverse && (src != Source::Residues || fuse != Fuse::None)) return cudaErrorInvalidValue;
         switch (logN) {
             PG_CONTIG_CASE(6)
             PG_CONTIG_CASE(7)
@@ -188,6 +189,16 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
                 return cudaErrorInvalidValue;
         }
     }
+}
+
+cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st) {
+    crt_carry_kernel<<<(unsigned)blocks, kCrtThreads, 0, st>>>(c);
+    return cudaGetLastError();
+}
+
+void set_pass(PassParams& p, const Plan& plan, int i) {
+    p.logS = plan.logS[i];
+    p.logNp = plan.logN[i] + plan.logS[i];
 }
 
 // ---------------------------------------------------------------- CRT constants
@@ -216,6 +227,14 @@ CrtConsts make_crt_consts(int logL) {
     shoup_pair((uint32_t)(i02 * i12 % p2), p2, k.k02, k.k02p);
     shoup_pair((uint32_t)i12, p2, k.k12, k.k12p);
     k.p01 = (uint64_t)p0 * p1;
+    // floor(P/2) in Garner digits: P/2 = (p0 p1 p2 - 1)/2; digits by repeated division
+    const unsigned __int128 P = (unsigned __int128)p0 * p1 * p2;
+    const unsigned __int128 H = P / 2;
+    k.h0 = (uint32_t)(H % p0);
+    k.h1 = (uint32_t)((H / p0) % p1);
+    k.h2 = (uint32_t)(H / ((unsigned __int128)p0 * p1));
+    k.P_lo = (uint64_t)P;
+    k.P_hi = (uint64_t)(P >> 64);
     return k;
 }
 
@@ -243,14 +262,13 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
         p.words = reinterpret_cast<const uint32_t*>(limbs);
         p.ncoef = ncoef;
         p.L = L;
-        p.nrows = 1;
+        p.logL = logL;
+        p.job_stride = 3 * L;
+        p.njobs = 1;
+        p.merge = 0;
         return p;
     };
-    auto set_pass = [&](PassParams& p, int i) {
-        p.logS = plan.logS[i];
-        p.logNp = plan.logN[i] + plan.logS[i];
-        p.nrows = (uint32_t)(L >> plan.logN[i]);
-    };
+    auto set_pass = [&](PassParams& p, int i) { pg::set_pass(p, plan, i); };
 
     const int last = plan.npass - 1;
     // Operand a: full forward transform (all but the last pass when squaring).
@@ -305,6 +323,8 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
     c.ticket = W.sync + 1;
     c.status = W.sync + 2;
     c.error = W.sync;
+    c.blocks_per_job = crt_blocks;
+    c.merge = 0;
     c.k = make_crt_consts(logL);
     crt_carry_kernel<<<(unsigned)crt_blocks, kCrtThreads, 0, st>>>(c);
     if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + 1;

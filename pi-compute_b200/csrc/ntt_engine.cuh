@@ -19,6 +19,12 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
 
 CrtConsts make_crt_consts(int logL);
 
+// Launch the CRT + carry kernel over `blocks` blocks.
+cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st);
+
+// Stride and four-step block size of pass i.
+void set_pass(PassParams& p, const Plan& plan, int i);
+
 struct DeviceTables {
     uint2* base = nullptr;  // one allocation holding every table
     TwiddleTables tw{};

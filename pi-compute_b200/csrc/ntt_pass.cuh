@@ -200,7 +200,8 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
     }
 }
 
-// Global index of tile element (m, c) for this CTA.
+// Global index of tile element (m, c) within its job's array. For Strided tiles `tile` is the
+// tile index inside the job; for Contig tiles `row` is the row index inside the job.
 template <Layout LAY, int LOGN, int LOGE>
 __device__ __forceinline__ uint64_t gidx(uint64_t tile, uint32_t m, uint32_t c, int logS) {
     constexpr int LOGC = LOGE - LOGN;
@@ -211,7 +212,7 @@ __device__ __forceinline__ uint64_t gidx(uint64_t tile, uint32_t m, uint32_t c, 
         uint64_t t0 = (tile & ((1ull << logTpb) - 1)) << LOGC;
         return (blk << (LOGN + logS)) + t0 + c + ((uint64_t)m << logS);
     } else {
-        return (((tile << LOGC) + c) << LOGN) + m;
+        return (tile << LOGN) + m;  // here `tile` is the row inside the job
     }
 }
 
@@ -219,16 +220,28 @@ __device__ __forceinline__ uint64_t gidx(uint64_t tile, uint32_t m, uint32_t c, 
 template <Layout LAY, int LOGN, int LOGE>
 __device__ __forceinline__ uint32_t tcol(uint64_t tile, uint32_t c, int logS) {
     constexpr int LOGC = LOGE - LOGN;
-    if constexpr (LAY == Layout::Strided) {
-        const int logTpb = logS - LOGC;
-        return (uint32_t)(((tile & ((1ull << logTpb) - 1)) << LOGC) + c);
+    const int logTpb = logS - LOGC;
+    return (uint32_t)(((tile & ((1ull << logTpb) - 1)) << LOGC) + c);
+}
+
+// Source limbs of job `job` (first forward pass).
+__device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, const uint32_t*& words,
+                                           uint64_t& ncoef) {
+    if (P.merge) {
+        const uint64_t m = job / 6, o = job % 6;
+        const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
+        const int which = (int)(o % 3);
+        words = reinterpret_cast<const uint32_t*>(P.ms.X[which] + child * P.ms.cap[which]);
+        ncoef = 2ull * P.ms.len[3 * child + which];
     } else {
-        return 0;
+        words = P.words;
+        ncoef = P.ncoef;
     }
 }
 
-// The pass kernel. grid = (tiles, primes). Tile contents are loaded with 16-byte
-// vector accesses along the contiguous dimension.
+// The pass kernel. grid = (tiles over all jobs, primes). Tile contents move with 16-byte
+// vector accesses along the contiguous dimension. Job j's residues are the array at
+// data + j * job_stride (prime i at + i * L).
 template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE>
 __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, TwiddleTables T) {
     extern __shared__ uint32_t sm[];
@@ -236,51 +249,64 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
     constexpr uint32_t E = 1u << LOGE;
     const int j = blockIdx.y;
     const uint32_t p = kPrime(j);
-    const uint64_t tile = blockIdx.x;
-    uint32_t* data = P.data + (uint64_t)j * P.L;
-    uint32_t* out = P.out + (uint64_t)j * P.L;
     const int dir = INV ? 1 : 0;
     const uint32_t pinv = inv_mod_2_32(p);
     const uint32_t r32 = (uint32_t)(0x100000000ull % p);
     const uint32_t r32p = (uint32_t)(((uint64_t)r32 << 32) / p);
+    const uint64_t prime_off = (uint64_t)j * P.L;
+
+    // Strided: one job per tile. Contig: row c of the tile is global row R = tile*C + c.
+    uint64_t sjob = 0, stile = 0;
+    if constexpr (LAY == Layout::Strided) {
+        const int logTpj = P.logL - LOGE;
+        sjob = (uint64_t)blockIdx.x >> logTpj;
+        stile = (uint64_t)blockIdx.x & ((1ull << logTpj) - 1);
+    }
+    const uint64_t total_rows = (uint64_t)P.njobs << (P.logL - LOGN);
+    const int logRows = P.logL - LOGN;
 
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
     for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
         uint32_t m, c;
+        uint64_t job, g;
         if constexpr (LAY == Layout::Strided) {
             m = e4 >> LOGC;
             c = e4 & ((1u << LOGC) - 1);
+            job = sjob;
+            g = gidx<LAY, LOGN, LOGE>(stile, m, c, P.logS);
         } else {
             c = e4 >> LOGN;
             m = e4 & ((1u << LOGN) - 1);
-        }
-        uint4 x;
-        if constexpr (LAY == Layout::Contig) {
-            if (((tile << LOGC) + c) >= P.nrows) {
-                x = make_uint4(0, 0, 0, 0);
-                *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
+            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            if (R >= total_rows) {
+                *reinterpret_cast<uint4*>(sm + swz(e4)) = make_uint4(0, 0, 0, 0);
                 continue;
             }
+            job = R >> logRows;
+            g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);
         }
-        uint64_t g = gidx<LAY, LOGN, LOGE>(tile, m, c, P.logS);
+        uint4 x;
         if constexpr (SRC == Source::Limbs) {
+            const uint32_t* words;
+            uint64_t ncoef;
+            job_source(P, job, words, ncoef);
             const uint32_t one_p = (uint32_t)(0x100000000ull / p);
             uint32_t w[4];
-            if (g + 4 <= P.ncoef) {
-                uint4 raw = __ldg(reinterpret_cast<const uint4*>(P.words + g));
+            if (g + 4 <= ncoef) {
+                uint4 raw = __ldg(reinterpret_cast<const uint4*>(words + g));
                 w[0] = raw.x; w[1] = raw.y; w[2] = raw.z; w[3] = raw.w;
             } else {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) w[u] = (g + u < P.ncoef) ? __ldg(P.words + g + u) : 0u;
+                for (int u = 0; u < 4; ++u) w[u] = (g + u < ncoef) ? __ldg(words + g + u) : 0u;
             }
             x = make_uint4(reduce_u32(w[0], p, one_p), reduce_u32(w[1], p, one_p), reduce_u32(w[2], p, one_p),
                            reduce_u32(w[3], p, one_p));
         } else {
-            x = *reinterpret_cast<const uint4*>(data + g);
+            x = *reinterpret_cast<const uint4*>(P.data + job * P.job_stride + prime_off + g);
         }
         if constexpr (INV && LAY == Layout::Strided) {
             // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m))
-            uint32_t t = tcol<LAY, LOGN, LOGE>(tile, c, P.logS);
+            uint32_t t = tcol<LAY, LOGN, LOGE>(stile, c, P.logS);
             uint64_t k = bitrev_n(m, LOGN);
             fourstep_twiddle4(x, t, k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p, pinv, r32, r32p);
         }
@@ -292,15 +318,16 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
 
     if constexpr (FUSE != Fuse::None) {
         static_assert(LAY == Layout::Contig && !INV, "pointwise fusion happens in the last forward pass");
-        const uint32_t* oth = P.other + (uint64_t)j * P.L;
         for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
             uint32_t c = e4 >> LOGN, m = e4 & ((1u << LOGN) - 1);
-            if (((tile << LOGC) + c) >= P.nrows) continue;
-            uint64_t g = gidx<LAY, LOGN, LOGE>(tile, m, c, 0);
+            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            if (R >= total_rows) continue;
+            const uint64_t job = R >> logRows;
+            uint64_t g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);
             uint4 a = *reinterpret_cast<uint4*>(sm + swz(e4));
             uint4 b;
             if constexpr (FUSE == Fuse::MulInverse) {
-                b = *reinterpret_cast<const uint4*>(oth + g);
+                b = *reinterpret_cast<const uint4*>(P.other + job * P.job_stride + prime_off + g);
             } else {
                 b = a;
             }
@@ -317,22 +344,27 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
     // ---- store
     for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
         uint32_t m, c;
+        uint64_t job, g;
         if constexpr (LAY == Layout::Strided) {
             m = e4 >> LOGC;
             c = e4 & ((1u << LOGC) - 1);
+            job = sjob;
+            g = gidx<LAY, LOGN, LOGE>(stile, m, c, P.logS);
         } else {
             c = e4 >> LOGN;
             m = e4 & ((1u << LOGN) - 1);
-            if (((tile << LOGC) + c) >= P.nrows) continue;
+            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            if (R >= total_rows) continue;
+            job = R >> logRows;
+            g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);
         }
         uint4 x = *reinterpret_cast<uint4*>(sm + swz(e4));
         if constexpr (!INV && LAY == Layout::Strided) {
-            uint32_t t = tcol<LAY, LOGN, LOGE>(tile, c, P.logS);
+            uint32_t t = tcol<LAY, LOGN, LOGE>(stile, c, P.logS);
             uint64_t k = bitrev_n(m, LOGN);
             fourstep_twiddle4(x, t, k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p, pinv, r32, r32p);
         }
-        uint64_t g = gidx<LAY, LOGN, LOGE>(tile, m, c, P.logS);
-        *reinterpret_cast<uint4*>(out + g) = x;
+        *reinterpret_cast<uint4*>(P.out + job * P.job_stride + prime_off + g) = x;
     }
 }
 

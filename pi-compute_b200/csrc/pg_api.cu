@@ -94,6 +94,16 @@ pg_status host_product(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* 
 
 }  // namespace
 
+// Accessors used by the binary-splitting module (bs_device.cu).
+namespace pg {
+const DeviceTables& ctx_tables(pg_ctx* c) { return c->tables; }
+cudaStream_t ctx_stream(pg_ctx* c) { return c->stream; }
+std::mutex& ctx_mutex(pg_ctx* c) { return c->mu; }
+uint64_t* ctx_launches(pg_ctx* c) { return &c->launches; }
+void ctx_set_error(pg_ctx* c, const std::string& msg) { c->last_error = msg; }
+int ctx_device(pg_ctx* c) { return c->device; }
+}  // namespace pg
+
 extern "C" {
 
 int pg_version(void) { return (0 << 16) | (1 << 8) | 0; }

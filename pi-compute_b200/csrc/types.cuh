@@ -37,16 +37,28 @@ enum class Layout : int { Strided = 0, Contig = 1 };
 enum class Source : int { Residues = 0, Limbs = 1 };
 enum class Fuse : int { None = 0, MulInverse = 1, SqrInverse = 2 };
 
+// Child level of a merge batch: node i's P/Q/R limbs at X[k] + i * cap[k] (k = 0, 1, 2),
+// lengths (limbs) at len[3 * i + k].
+struct MergeSrc {
+    const uint64_t* X[3];
+    uint32_t cap[3];
+    const uint32_t* len;
+};
+
 struct PassParams {
-    uint32_t* data;          // residue array of this operand: prime j at data + j*L
+    uint32_t* data;          // residues of job 0: prime i at data + i*L; job j at data + j*job_stride
     const uint32_t* other;   // Fuse::MulInverse: fully transformed other operand (same layout)
-    uint32_t* out;           // where the tile is written (== data for in-place passes)
-    const uint32_t* words;   // Source::Limbs: operand as 32-bit words (little-endian)
-    uint64_t ncoef;          // Source::Limbs: number of valid 32-bit coefficients
+    uint32_t* out;           // where tiles are written (== data for in-place passes)
+    const uint32_t* words;   // Source::Limbs, single job: operand as 32-bit words (little-endian)
+    uint64_t ncoef;          // Source::Limbs, single job: number of valid 32-bit coefficients
     uint64_t L;              // transform length (elements per prime)
+    uint64_t job_stride;     // residue words between consecutive jobs (>= 3*L)
+    uint32_t njobs;          // number of transforms in this launch
+    int logL;
     int logS;                // log2 of the element stride of this pass (0 for Contig)
     int logNp;               // log2 of the block size N' = N * S (four-step twiddle)
-    uint32_t nrows;          // Contig: number of valid rows (blocks of N) in the array
+    int merge;               // Source::Limbs resolved per job from `ms` (job = 6*merge + operand)
+    MergeSrc ms;
 };
 
 struct CrtConsts {
@@ -58,17 +70,31 @@ struct CrtConsts {
     uint32_t k02, k02p;   // p0^-1 * p1^-1            mod p2
     uint32_t k12, k12p;   // p1^-1                    mod p2
     uint64_t p01;         // p0 * p1
+    // centred lift: Garner digits of floor(P/2) and P = p0*p1*p2 as (P_hi << 64) + P_lo
+    uint32_t h0, h1, h2;
+    uint64_t P_lo, P_hi;
 };
 
 struct CrtParams {
-    const uint32_t* res;     // residues: prime j at res + j*L, natural order
+    const uint32_t* res;     // single product: residues, prime j at res + j*L, natural order
     uint64_t L;
-    uint64_t nwords;         // output words (2 * output limbs)
-    uint32_t* out;           // output words
-    uint32_t* status;        // one word per CTA, zeroed before launch
-    uint32_t* ticket;        // zeroed before launch
+    uint64_t nwords;         // single product: output words (2 * output limbs)
+    uint32_t* out;           // single product: output words
+    uint32_t* status;        // blocks_per_job words per job, zeroed before launch
+    uint32_t* ticket;        // one per job, zeroed before launch
     uint32_t* error;         // set non-zero on a look-back timeout or a final carry
+    uint64_t blocks_per_job; // grid = jobs * blocks_per_job
     CrtConsts k;
+    // merge batch: job = 3 * merge + {P, Q, R}; residues of merge m, output k (0..2) at
+    // res + (6m + 3 + k) * res_stride; the words go to dst[k] + m * dcap[k] (limbs), the
+    // length to dlen[3m + k]; node ranges of the level come from [a0, b0) and depth.
+    int merge;
+    uint64_t res_stride;
+    uint64_t* dst[3];
+    uint32_t dcap[3];
+    uint32_t* dlen;
+    uint64_t a0, b0;
+    int depth;
 };
 
 constexpr int kCrtThreads = 256;

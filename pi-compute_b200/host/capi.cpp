@@ -6,6 +6,7 @@
 
 #include "b200_multiplier.h"
 #include "binary_splitting.h"
+#include "device_bs.h"
 #include "pi_b200_engine.h"
 #include "pi_engine.h"
 
@@ -60,9 +61,15 @@ int pib_bs(unsigned long a, unsigned long b, int mode, size_t threshold, int dev
            uint64_t* R, size_t cap, size_t* len, int* sign) {
     try {
         if (b <= a) throw std::invalid_argument("empty range");
-        std::unique_ptr<pi::Multiplier> m = make_multiplier(mode, threshold, device);
-        pi::BinarySplitting bs(*m, 1);
-        pi::BSResult r = bs.compute(a, b);
+        pi::BSResult r;
+        if (mode == PIB_MODE_BATCHED) {
+            pi::DeviceBinarySplitting dbs(device);
+            dbs.compute(a, b, r.P, r.Q, r.R);
+        } else {
+            std::unique_ptr<pi::Multiplier> m = make_multiplier(mode, threshold, device);
+            pi::BinarySplitting bs(*m, 1);
+            r = bs.compute(a, b);
+        }
         export_signed(r.P, P, cap, &len[0], &sign[0]);
         export_signed(r.Q, Q, cap, &len[1], &sign[1]);
         export_signed(r.R, R, cap, &len[2], &sign[2]);

@@ -7,6 +7,7 @@
 #include <stdexcept>
 
 #include "binary_splitting.h"
+#include "device_bs.h"
 
 namespace pi {
 
@@ -71,7 +72,8 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
     mpz_init(R);
     mpz_init(pi_int);
     if (cfg.mode == BSMode::Batched) {
-        throw std::runtime_error("level-batched binary splitting is not available in this build");
+        DeviceBinarySplitting dbs(cfg.device);
+        dbs.compute(0, terms, nullptr, Q, R);  // P(0, N) is not needed (pi_engine.cpp:257-258)
     } else {
         BinarySplitting bs(mult_, cfg.num_threads);
         BSResult r = bs.compute(0, terms);

@@ -41,7 +41,7 @@ def pi_digits(lib, digits, mode, threshold=1024, threads=1):
 
 
 def bs(lib, a, b, mode, threshold=1):
-    cap = 64 + 2 * (b - a) * 3
+    cap = 64 + 2 * (b - a) * 3 + 4 * (b - a)
     bufs = [np.zeros(cap, dtype=np.uint64) for _ in range(3)]
     ln = (ctypes.c_size_t * 3)()
     sg = (ctypes.c_int * 3)()
@@ -106,4 +106,61 @@ def test_per_call_1m_digits_byte_identical(lib):
     # configuration 1: every product whose smaller operand has >= 2^10 limbs on the GPU, one call at a time
     s, t = pi_digits(lib, 1_000_000, PER_CALL, threshold=1024)
     g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
+    assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
+
+
+# ---------------------------------------------------------------- sign rule used by the device merges
+def test_series_sign_rule_holds():
+    # The device stores magnitudes: sgn P(a,b) = (-1)^(#terms k >= 1), Q > 0, sgn R(a,b) = sgn R(a,a+1),
+    # and R = Qr*Rl + s*Pl*Rr with |Qr*Rl| > |Pl*Rr| (so the magnitude never changes sign).
+    import random
+
+    rnd = random.Random(5)
+    ranges = [(0, 2), (0, 3), (1, 3), (0, 50), (7, 300)] + [(a, a + rnd.randint(2, 400)) for a in
+                                                              (rnd.randint(0, 5000) for _ in range(30))]
+    for a, b in ranges:
+        m = a + (b - a) // 2
+        Pl, Ql, Rl = oracle.bs(a, m)
+        Pr, Qr, Rr = oracle.bs(m, b)
+        P, Q, R = oracle.bs(a, b)
+        neg = (b - a) - (1 if a == 0 else 0)
+        assert (P < 0) == (neg % 2 == 1) and Q > 0
+        assert (R > 0) == (a == 0)
+        assert abs(Qr * Rl) > abs(Pl * Rr)
+        s = (-1 if Rl < 0 else 1) * (-1 if Pl < 0 else 1) * (-1 if Rr < 0 else 1)
+        e = (m - a) if a >= 1 else m
+        assert s == (-1 if e % 2 else 1)
+        assert abs(R) == abs(Qr * Rl) + s * abs(Pl * Rr)
+
+
+# ---------------------------------------------------------------- GPU: level-batched device binary splitting
+@pytest.mark.gpu
+@pytest.mark.parametrize("a,b", [(0, 1), (1, 2), (5, 6), (0, 2), (0, 3), (1, 4), (0, 8), (3, 11), (0, 79),
+                                 (100, 357), (0, 1000), (1000, 9000), (0, 4097), (12345, 31000)])
+def test_batched_bs_matches_oracle(lib, a, b):
+    assert bs(lib, a, b, BATCHED) == oracle.bs(a, b), (a, b)
+
+
+@pytest.mark.gpu
+def test_batched_bs_golden_hash_1m_terms(lib):
+    g = json.load(open(os.path.join(GOLDEN, "bs_golden.json")))
+    for key, hs in g["hash_ranges"].items():
+        a, b = map(int, key.split(","))
+        vals = bs(lib, a, b, BATCHED)
+        assert [hashlib.sha256(hex(v).encode()).hexdigest() for v in vals] == hs, key
+
+
+@pytest.mark.gpu
+def test_batched_digits_1000_and_1m(lib):
+    s, _ = pi_digits(lib, 1000, BATCHED)
+    assert s == open(os.path.join(GOLDEN, "pi_1000.txt")).read()
+    s, _ = pi_digits(lib, 1_000_000, BATCHED)
+    g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
+    assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
+
+
+@pytest.mark.gpu
+def test_batched_digits_10m(lib):
+    s, t = pi_digits(lib, 10_000_000, BATCHED)
+    g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["10000000"]
     assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
