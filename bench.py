@@ -1,40 +1,48 @@
 #!/usr/bin/env python
-"""Benchmark of the multiply hot path (one JSON line on rank 0).
+"""Benchmark: pi digits/s at 100M digits on one B200, plus the multiply's HBM roofline.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload mul]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--digits D]
 
-Workload "mul" (default): the standalone multiply at its headline size, one balanced
-2^24 x 2^24-limb product per step (seeded splitmix64 operands, top bit set), the size at
-which the 50%-of-HBM-roofline target is stated. `value` is the algorithmic GB/s of the
-device-resident product (B_mul = 400 * (na + nb) bytes per product, operands already in
-HBM); `e2e` is the same metric through the host C ABI call pg_mul (host buffers, copies in
-the timed region). Every product moves ~2.5 GB through HBM, far above the 126 MB L2, so no
-explicit flush is needed between steps.
+Step (workload "pi", the default): one complete computation of pi to D = 100,000,000 digits
+through the engine's C entry point pib_pi in level-batched mode: device-resident binary
+splitting of 7,051,375 terms, integer Newton reciprocal and sqrt(10005) with the final exact
+correction, divide-and-conquer decimal conversion (large products on the B200), the digit
+string in host memory. The digits of the first step are checked against the reference
+program's sha256 (tests/golden/pi_golden.json). `value` = D / wall seconds per step (the
+pipeline is host-orchestrated around device work, so the clock is the host clock with the
+device synchronised on both sides); `e2e` = the same through the command-line program
+(process start, CUDA context, output file), end to end like the reference's pi_compute.
 
---impl reference times the reference's own CPU product, pi::GmpMultiplier::multiply
-(compiled unchanged from its sources into oracle/_ref/libpiref.so), on a bounded sample:
-one 2^22 x 2^22-limb product per thread on every host core.
+`roofline` is measured live in the same run on the hot path's unit, one balanced
+2^24 x 2^24-limb product (operands in HBM, CUDA events on the library's stream), against the
+fixed algorithmic bytes B_mul = 400 * (na + nb) and the measured HBM copy bandwidth.
 
-Multi-GPU (torchrun): the products are independent, so each rank runs its own replica
-("replicas only", no collective on the data path); value = total work / max rank time.
+`cpu_baseline` = the reference's own program (oracle/_ref/pi_compute_ref, compiled unchanged
+from its sources) on every host core, bounded sample: pi to 10M digits. `--impl reference`
+runs that program at the full D digits once (about a minute on 16 cores) and reports digits/s.
+
+Multi-GPU (torchrun): each rank computes pi independently (replicas only: the north star is
+one GPU and the path has no exchange step); value = total digits / max rank time.
 """
 from __future__ import annotations
 
 import argparse
 import ctypes
+import hashlib
 import json
 import os
 import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "pi digits/s at 100M (batched vs per-call GPU, bit-exact); mul GB/s vs HBM"
+PIB_MODE_BATCHED = 2
+PI_COMPUTE_REF = os.path.join(ROOT, "oracle", "_ref", "pi_compute_ref")
 
 
 def load_pkg():
@@ -47,16 +55,6 @@ def load_pkg():
     return mod
 
 
-def load_oracle():
-    import importlib.util
-
-    spec = importlib.util.spec_from_file_location("pi_oracle", os.path.join(ROOT, "oracle", "oracle.py"))
-    mod = importlib.util.module_from_spec(spec)
-    sys.modules["pi_oracle"] = mod
-    spec.loader.exec_module(mod)
-    return mod
-
-
 def measured_peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -65,9 +63,10 @@ def measured_peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def b_mul(na: int, nb: int) -> int:
-    """Algorithmic bytes of one product (fixed formula: 16(na+nb) I/O + 3 transforms x 128(na+nb))."""
-    return 400 * (na + nb)
+def golden_sha(digits: int):
+    g = json.load(open(os.path.join(ROOT, "tests", "golden", "pi_golden.json")))
+    e = g.get(str(digits))
+    return e["sha256"] if e else None
 
 
 class ClockSampler:
@@ -98,23 +97,27 @@ class ClockSampler:
         time.sleep(0.25)
         self.proc.terminate()
         self.proc.wait()
-        sm, smax, reasons = [], None, set()
+        sm, busy, smax, reasons = [], [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
             try:
-                sm.append(float(f[1]))
+                v = float(f[1])
+                sm.append(v)
                 smax = float(f[2])
+                if float(f[3]) > 250:  # under load
+                    busy.append(v)
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
+            for n, val in zip(names, f[5:9]):
+                if val.lower().startswith("active"):
                     reasons.add(n)
         os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        med = statistics.median(busy or sm) if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "samples_under_load": len(busy)}
 
 
 def dist_setup():
@@ -124,58 +127,95 @@ def dist_setup():
     return world, rank, local
 
 
-def cpu_gmp_sample(n: int = 1 << 22, threads: int = 0, seconds: float = 10.0) -> dict:
-    """Reference CPU product throughput: GmpMultiplier::multiply on every core, bounded sample."""
-    orc = load_oracle()
-    pkg = sys.modules.get("pi_compute_b200") or load_pkg()
-    threads = threads or (os.cpu_count() or 1)
-    a = pkg.random_operand(n, 11)
-    b = pkg.random_operand(n, 12)
-    done = [0] * threads
-    stop = time.perf_counter() + seconds
-    use_ref = orc.ref_available()
+def run_reference_program(digits: int, threads: int) -> tuple[float, str]:
+    """Wall seconds of the reference's pi_compute (unchanged sources) and the sha256 of its output."""
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "pi.txt")
+        t0 = time.perf_counter()
+        subprocess.run([PI_COMPUTE_REF, "--digits", str(digits), "--threads", str(threads), "--output", out],
+                       check=True, stdout=subprocess.DEVNULL, cwd=td)
+        dt = time.perf_counter() - t0
+        sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
+    return dt, sha
 
-    def work(i):
-        while True:
-            (orc.ref_mul if use_ref else orc.mul_gmp)(a, b)
-            done[i] += 1
-            if time.perf_counter() >= stop:
-                break
 
-    t0 = time.perf_counter()
-    ts = [threading.Thread(target=work, args=(i,)) for i in range(threads)]
-    for t in ts:
-        t.start()
-    for t in ts:
-        t.join()
-    dt = time.perf_counter() - t0
-    total = sum(done)
-    return {"value": round(b_mul(n, n) * total / dt / 1e9, 4), "unit": "GB/s", "cores": threads,
-            "kind": "reference" if use_ref else "port",
-            "sample": f"{total} products of {n}x{n} limbs (pi::GmpMultiplier::multiply -> mpz_mul, "
-                      f"one per thread, {threads} threads) in {dt:.1f} s"}
+def cpu_baseline(digits: int = 10_000_000) -> dict:
+    threads = os.cpu_count() or 1
+    if not os.path.exists(PI_COMPUTE_REF):
+        return {"value": None, "unit": "digits/s", "cores": threads, "kind": "reference",
+                "sample": "reference program not built"}
+    dt, sha = run_reference_program(digits, threads)
+    return {"value": round(digits / dt, 1), "unit": "digits/s", "cores": threads, "kind": "reference",
+            "sample": f"reference pi_compute (GmpMultiplier, mpf finish) to {digits:,} digits with --threads "
+                      f"{threads}: {dt:.2f} s; sha256 {sha[:16]}"}
 
 
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    steps = []
-    for _ in range(args.warmup):
-        pass  # CPU runs need no warm-up; the sample below is timed as is
-    for _ in range(max(1, args.steps)):
-        steps.append(cpu_gmp_sample(seconds=max(3.0, 20.0 / max(1, args.steps))))
-    v = statistics.median(s["value"] for s in steps)
-    cb = dict(steps[0])
-    cb["value"] = v
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "multiply, balanced 2^24 x 2^24 limbs (sampled at 2^22 x 2^22 on CPU)",
-                       "parallelism": "host threads"},
-            "cpu_baseline": cb,
-            "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    threads = os.cpu_count() or 1
+    dt, sha = run_reference_program(args.digits, threads)
+    v = args.digits / dt
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "digits/s", "n_gpus": args.gpus,
+            "steps": 1, "warmup": 0, "ms_per_step": round(dt * 1e3, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64 limbs (GMP)", "data": "none (pi)",
+            "config": {"workload": f"pi to {args.digits:,} digits (Chudnovsky, binary splitting + mpf finish)",
+                       "parallelism": f"{threads} host threads"},
+            "cpu_baseline": {"value": round(v, 1), "unit": "digits/s", "cores": threads, "kind": "reference",
+                             "sample": f"one full {args.digits:,}-digit run of the reference program "
+                                       f"({dt:.1f} s, sha256 {sha[:16]})"},
+            "e2e": {"value": round(v, 1), "unit": "digits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def product_roofline(pkg, eng, torch, local, logn=24, steps=5) -> dict:
+    """Live roofline of the hot path's unit: balanced 2^logn x 2^logn product, operands in HBM."""
+    lib = eng.lib
+    n = 1 << logn
+    a_h = pkg.random_operand(n, 1234)
+    b_h = pkg.random_operand(n, 5678)
+    a_d = torch.from_numpy(a_h.view(np.int64)).to(f"cuda:{local}")
+    b_d = torch.from_numpy(b_h.view(np.int64)).to(f"cuda:{local}")
+    out_d = torch.empty(2 * n, dtype=torch.int64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(lib.pg_stream(eng.ctx), device=f"cuda:{local}")
+
+    def step():
+        st = lib.pg_mul_device(eng.ctx, a_d.data_ptr(), n, b_d.data_ptr(), n, out_d.data_ptr())
+        if st != 0:
+            raise pkg.PgError(st, eng.last_error())
+
+    step()
+    if lib.pg_sync(eng.ctx) != 0:
+        raise pkg.PgError(-1, eng.last_error())
+    r = out_d.cpu().numpy().view(np.uint64)
+    A, B, R = pkg.limbs_to_int(a_h), pkg.limbs_to_int(b_h), pkg.limbs_to_int(r)
+    for q in (2**61 - 1, 1000000007, 998244353):
+        assert (A % q) * (B % q) % q == R % q, "product check failed"
+    for _ in range(3):
+        step()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    torch.cuda.synchronize()
+    l0 = lib.pg_launch_count(eng.ctx)
+    ev[0].record(stream)
+    for i in range(steps):
+        step()
+        ev[i + 1].record(stream)
+    torch.cuda.synchronize()
+    launches = lib.pg_launch_count(eng.ctx) - l0
+    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]
+    bal = 400 * 2 * n
+    achieved = bal / (statistics.mean(per) / 1e3) / 1e9
+    peaks = measured_peaks()
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get(f"mul_{logn}")
+    return {"bound": "hbm", "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic, "peak_source": peaks["source"],
+            "what": f"one balanced 2^{logn} x 2^{logn}-limb product (all its kernels, {launches // steps} launches) "
+                    f"against B_mul = 400*(na+nb) bytes; {statistics.mean(per):.3f} ms per product",
+            "ms_per_product": round(statistics.mean(per), 4), "launches": int(launches)}
 
 
 def run_b200(args):
@@ -188,37 +228,32 @@ def run_b200(args):
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     torch.cuda.set_device(local)
     pkg = load_pkg()
-    eng = pkg.Engine(local)
-    lib = eng.lib
-
-    n = 1 << args.logn
-    na = nb = n
-    a_h = pkg.random_operand(na, 1234 + rank)
-    b_h = pkg.random_operand(nb, 5678 + rank)
-    a_d = torch.from_numpy(a_h.view(np.int64)).to(f"cuda:{local}")
-    b_d = torch.from_numpy(b_h.view(np.int64)).to(f"cuda:{local}")
-    out_d = torch.empty(na + nb, dtype=torch.int64, device=f"cuda:{local}")
-    stream = torch.cuda.ExternalStream(lib.pg_stream(eng.ctx), device=f"cuda:{local}")
+    lib = ctypes.CDLL(pkg.LIBPIB200)
+    lib.pib_pi.argtypes = [ctypes.c_size_t, ctypes.c_int, ctypes.c_uint, ctypes.c_size_t, ctypes.c_int,
+                           ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_double)]
+    lib.pib_pi.restype = ctypes.c_int
+    lib.pib_last_error.restype = ctypes.c_char_p
+    D = args.digits
+    threads = os.cpu_count() or 1
+    buf = ctypes.create_string_buffer(D + 2)
+    stats = (ctypes.c_double * 8)()
 
     def step():
-        st = lib.pg_mul_device(eng.ctx, a_d.data_ptr(), na, b_d.data_ptr(), nb, out_d.data_ptr())
+        st = lib.pib_pi(D, PIB_MODE_BATCHED, threads, args.threshold, local, buf, D + 2, stats)
         if st != 0:
-            raise pkg.PgError(st, eng.last_error())
+            raise RuntimeError(lib.pib_last_error().decode())
+        return list(stats)
 
-    # correctness gate on this box: residues of the product modulo independent primes
+    # correctness gate: the first computation must equal the reference's digits
     step()
-    if lib.pg_sync(eng.ctx) != 0:
-        raise pkg.PgError(-1, eng.last_error())
-    r = out_d.cpu().numpy().view(np.uint64)
-    A, B, R = pkg.limbs_to_int(a_h), pkg.limbs_to_int(b_h), pkg.limbs_to_int(r)
-    for q in (2**61 - 1, 1000000007, 998244353):
-        assert (A % q) * (B % q) % q == R % q, "product check failed"
-    del A, B, R, r
-
-    for _ in range(args.warmup):
+    want = golden_sha(D)
+    got = hashlib.sha256(buf.raw[: D + 2]).hexdigest()
+    if want is not None and got != want:
+        raise RuntimeError(f"digits differ from the reference run: sha256 {got} != {want}")
+    for _ in range(max(0, args.warmup - 1)):
         step()
     torch.cuda.synchronize()
     if world > 1:
@@ -226,87 +261,77 @@ def run_b200(args):
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    l0 = lib.pg_launch_count(eng.ctx)
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-    ev[0].record(stream)
-    for i in range(args.steps):
-        step()
-        ev[i + 1].record(stream)
-    torch.cuda.synchronize()
-    launches = lib.pg_launch_count(eng.ctx) - l0
-    per = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total_ms = ev[0].elapsed_time(ev[-1])
-    if lib.pg_sync(eng.ctx) != 0:
-        raise pkg.PgError(-1, eng.last_error())
+    per, phases, launches = [], [], 0
+    t_all = time.perf_counter()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        s = step()
+        torch.cuda.synchronize()
+        per.append(time.perf_counter() - t0)
+        phases.append(s[:4])
+        launches += int(s[4])
+    total = time.perf_counter() - t_all
     clk = clocks.stop()
-
-    # end-to-end through the host C ABI (pinned staging, H2D, product, D2H inside the timed region)
-    out_h = np.zeros(na + nb, dtype=np.uint64)
-    for _ in range(max(1, args.warmup // 2)):
-        eng.mul_limbs(a_h, b_h)
-    torch.cuda.synchronize()
-    e2e_steps = max(2, min(args.steps, 5))
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        out_h = eng.mul_limbs(a_h, b_h)
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-
-    t_ms = torch.tensor([total_ms], device=f"cuda:{local}")
+    t = torch.tensor([total], device=f"cuda:{local}", dtype=torch.float64)
     if world > 1:
-        torch.distributed.all_reduce(t_ms, op=torch.distributed.ReduceOp.MAX)
-    total_ms = float(t_ms.item())
-    ms_per_step = total_ms / args.steps
-    bal = b_mul(na, nb)
-    value = bal * args.steps * world / (total_ms / 1e3) / 1e9
-    peaks = measured_peaks()
-    achieved = bal / (statistics.mean(per) / 1e3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get(f"mul_{args.logn}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    total = float(t.item())
+    value = D * args.steps * world / total
+
+    eng = pkg.Engine(local)
+    roof = product_roofline(pkg, eng, torch, local, logn=args.logn)
+    eng.close()
 
     if rank == 0:
+        # end to end through the command-line program, like the reference's pi_compute
+        e2e = None
+        if not args.no_e2e:
+            with tempfile.TemporaryDirectory() as td:
+                out = os.path.join(td, "pi.txt")
+                t0 = time.perf_counter()
+                subprocess.run([pkg.PI_B200_BIN, "--batched", "--digits", str(D), "--threads", str(threads),
+                                "--device", str(local), "--output", out], check=True, stdout=subprocess.DEVNULL)
+                e2e_s = time.perf_counter() - t0
+                sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
+            e2e = {"value": round(D / e2e_s, 1), "unit": "digits/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": D + 2, "seconds": round(e2e_s, 3),
+                   "path": "pi_b200 --batched (process start, CUDA context, output file)",
+                   "sha256_matches_reference": (sha == want) if want else None}
+        ph = np.mean(np.array(phases), axis=0)
         line = {
-            "metric": METRIC, "value": round(value, 2), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod p (NTT), u64 limbs", "data": "synthetic",
-            "config": {"workload": f"multiply, balanced 2^{args.logn} x 2^{args.logn} limbs "
-                                   f"(3-prime NTT, 32-bit coefficients, L = 2^{pkg_logL(na, nb)})",
-                       "na": na, "nb": nb, "parallelism": f"replicas x{world}",
-                       "l2": "inputs larger than L2 (~2.5 GB of HBM traffic per product)"},
-            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                         "frac": round(achieved / peaks["hbm_gbs"], 4), "traffic": traffic,
-                         "peak_source": peaks["source"],
-                         "what": "one whole product (all its kernels) against B_mul = 400*(na+nb) bytes"},
-            "e2e": {"value": round(bal / e2e_s / 1e9, 3), "unit": "GB/s", "h2d_bytes_per_step": 8 * (na + nb),
-                    "d2h_bytes_per_step": 8 * (na + nb), "ms_per_step": round(e2e_s * 1e3, 3),
-                    "path": "pg_mul (host C ABI)"},
-            "gpu_launches": int(launches),
+            "metric": METRIC, "value": round(value, 1), "unit": "digits/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod p (NTT), u64 limbs", "data": "none (pi)",
+            "config": {"workload": f"pi to {D:,} digits: level-batched device binary splitting + Newton finish "
+                                   f"+ D&C decimal conversion on B200 products",
+                       "digits": D, "terms": None, "parallelism": f"replicas x{world}",
+                       "l2": "every product of the top tree levels moves GBs through HBM (far above the 126 MB L2)",
+                       "phases_s": {"binary_splitting": round(ph[0], 3), "final_formula": round(ph[1], 3),
+                                    "decimal_conversion": round(ph[2], 3)},
+                       "digits_sha256": got, "matches_reference": (got == want) if want else None},
+            "roofline": roof,
+            "e2e": e2e,
+            "gpu_launches": launches,
             "clocks": clk,
         }
         if not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_gmp_sample(seconds=args.cpu_seconds)
+            line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
-    eng.close()
     if world > 1:
         torch.distributed.destroy_process_group()
-
-
-def pkg_logL(na, nb):
-    conv = 2 * (na + nb) - 1
-    return max(6, (conv - 1).bit_length())
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="mul", choices=["mul"])
+    ap.add_argument("--digits", type=int, default=100_000_000)
+    ap.add_argument("--threshold", type=int, default=1024)
     ap.add_argument("--logn", type=int, default=24)
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -20,15 +20,20 @@ extern "C" {
 /* Binary-splitting modes. */
 #define PIB_MODE_GMP 0        /* products through GMP's mpz_mul (the reference's GmpMultiplier) */
 #define PIB_MODE_PER_CALL 1   /* products >= threshold limbs through B200Multiplier, one call at a time */
-#define PIB_MODE_BATCHED 2    /* level-batched, device-resident binary splitting */
+#define PIB_MODE_BATCHED 2    /* level-batched, device-resident binary splitting; Newton finish and
+                                divide-and-conquer decimal conversion on B200 products */
+#define PIB_MODE_GMP_NEWTON 3 /* GMP products everywhere, with the Newton finish and conversion
+                                (the same integer algorithms as PIB_MODE_BATCHED, on the CPU) */
 
 /* Compute pi to `digits` decimals; writes "3." + digits (no terminator) into out, which must
- * have room for digits + 2 bytes. threads = host threads issuing per-call products;
- * threshold = min limbs of the smaller operand for the GPU path (PIB_MODE_PER_CALL).
- * times (may be NULL) receives 4 doubles: binary splitting, final formula, conversion, total
- * seconds. Returns 0 on success, non-zero on error (message via pib_last_error). */
+ * have room for digits + 2 bytes. threads = host threads issuing per-call products and
+ * converting digits; threshold = min limbs of the smaller operand for the GPU path.
+ * stats (may be NULL) receives PIB_NSTATS doubles: seconds of binary splitting, final formula,
+ * conversion and total, then the number of GPU kernel launches, GPU product calls and
+ * products routed to GMP. Returns 0 on success, non-zero on error (message via pib_last_error). */
+#define PIB_NSTATS 8
 int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int device, char* out, size_t out_cap,
-           double* times);
+           double* stats);
 
 /* P(a,b), Q(a,b), R(a,b) of the Chudnovsky series as signed little-endian limb arrays.
  * Each output buffer needs `cap` limbs; lengths and signs are written to len[3] and sign[3]. */

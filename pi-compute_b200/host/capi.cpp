@@ -31,7 +31,7 @@ void export_signed(const mpz_t v, uint64_t* out, size_t cap, size_t* len, int* s
 extern "C" {
 
 int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int device, char* out, size_t out_cap,
-           double* times) {
+           double* stats) {
     try {
         if (!out || out_cap < digits + 2) throw std::invalid_argument("output buffer smaller than digits + 2");
         pi::PiConfig cfg;
@@ -39,16 +39,23 @@ int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int devi
         cfg.num_threads = threads ? threads : 1;
         cfg.device = device;
         cfg.mode = (mode == PIB_MODE_BATCHED) ? pi::BSMode::Batched : pi::BSMode::PerCall;
-        std::unique_ptr<pi::Multiplier> m = make_multiplier(mode == PIB_MODE_BATCHED ? PIB_MODE_GMP : mode,
-                                                            threshold, device);
+        cfg.final_mode = (mode == PIB_MODE_BATCHED || mode == PIB_MODE_GMP_NEWTON) ? pi::FinalMode::Newton
+                                                                                   : pi::FinalMode::Mpf;
+        std::unique_ptr<pi::Multiplier> m =
+            make_multiplier((mode == PIB_MODE_BATCHED || mode == PIB_MODE_GMP_NEWTON) ? PIB_MODE_GMP : mode,
+                            threshold, device);
         pi::PiEngine eng(*m);
         pi::PiResult r = eng.compute(cfg);
         std::memcpy(out, r.digits.data(), r.digits.size());
-        if (times) {
-            times[0] = r.t.bs;
-            times[1] = r.t.final;
-            times[2] = r.t.convert;
-            times[3] = r.t.total;
+        if (stats) {
+            stats[0] = r.t.bs;
+            stats[1] = r.t.final;
+            stats[2] = r.t.convert;
+            stats[3] = r.t.total;
+            stats[4] = (double)r.t.gpu_launches;
+            stats[5] = (double)r.t.gpu_calls;
+            stats[6] = (double)r.t.cpu_routed;
+            stats[7] = 0;
         }
         return 0;
     } catch (const std::exception& e) {

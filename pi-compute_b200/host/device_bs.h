@@ -18,6 +18,7 @@ public:
 
     // P may be nullptr when it is not needed (the root of a pi computation).
     void compute(unsigned long a, unsigned long b, mpz_ptr P, mpz_ptr Q, mpz_ptr R);
+    uint64_t launches() const { return pg_launch_count(ctx_); }
 
 private:
     pg_ctx* ctx_ = nullptr;

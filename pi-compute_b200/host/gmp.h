@@ -200,7 +200,8 @@ void __gmp_get_memory_functions(void* (**)(size_t), void* (**)(void*, size_t, si
 #define mpf_get_str __gmpf_get_str
 #define mp_get_memory_functions __gmp_get_memory_functions
 
-/* Documented as a macro in the GMP manual ("mpz_sgn ... is a macro"). */
-#define mpz_sgn(Z) ((Z)->_mp_size < 0 ? -1 : (Z)->_mp_size > 0)
+/* The GMP manual documents mpz_sgn as a macro reading the sign of _mp_size; an inline
+ * function with the same result lets C++ wrappers convert to mpz_srcptr implicitly. */
+static inline int mpz_sgn(mpz_srcptr z) { return z->_mp_size < 0 ? -1 : z->_mp_size > 0; }
 
 #endif /* PI_B200_GMP_DECL_H */

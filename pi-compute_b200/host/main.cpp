@@ -3,7 +3,9 @@
 //
 //   pi_b200 --digits N [--output FILE] [--threads T] [--verbose]
 //           [--gpu | --b200]           products >= --gpu-threshold limbs on the B200, per call
-//           [--batched]                level-batched device-resident binary splitting
+//           [--batched]                level-batched device-resident binary splitting (implies --newton)
+//           [--newton | --mpf]         final formula + radix conversion: Newton iterations and divide-
+//                                      and-conquer conversion on B200 products, or the reference's GMP mpf
 //           [--gpu-threshold N]        (default 10000 like the reference)
 //           [--device D]
 #include <cstdio>
@@ -18,7 +20,7 @@
 static void usage() {
     std::puts(
         "pi_b200 - pi digits with exact big-integer products on one B200\n\n"
-        "USAGE: pi_b200 --digits <N> [--output FILE] [--threads T] [--gpu|--b200] [--batched]\n"
+        "USAGE: pi_b200 --digits <N> [--output FILE] [--threads T] [--gpu|--b200] [--batched] [--newton|--mpf]\n"
         "               [--gpu-threshold N] [--device D] [--verbose]\n");
 }
 
@@ -43,6 +45,11 @@ int main(int argc, char** argv) {
             gpu = true;
         } else if (a == "--batched") {
             cfg.mode = pi::BSMode::Batched;
+            cfg.final_mode = pi::FinalMode::Newton;
+        } else if (a == "--newton") {
+            cfg.final_mode = pi::FinalMode::Newton;
+        } else if (a == "--mpf") {
+            cfg.final_mode = pi::FinalMode::Mpf;
         } else if (a == "--gpu-threshold" && i + 1 < argc) {
             threshold = std::stoul(argv[++i]);
         } else if (a == "--device" && i + 1 < argc) {

@@ -4,10 +4,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <stdexcept>
 
+#include "b200_multiplier.h"
 #include "binary_splitting.h"
 #include "device_bs.h"
+#include "newton.h"
 
 namespace pi {
 
@@ -74,17 +77,44 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
     if (cfg.mode == BSMode::Batched) {
         DeviceBinarySplitting dbs(cfg.device);
         dbs.compute(0, terms, nullptr, Q, R);  // P(0, N) is not needed (pi_engine.cpp:257-258)
+        res.t.gpu_launches += dbs.launches();
     } else {
         BinarySplitting bs(mult_, cfg.num_threads);
         BSResult r = bs.compute(0, terms);
         mpz_swap(Q, r.Q);
         mpz_swap(R, r.R);
+        if (auto* b = dynamic_cast<B200Multiplier*>(&mult_)) {
+            res.t.gpu_launches += pg_launch_count(b->context());
+            res.t.gpu_calls += b->stats().gpu_calls.load();
+            res.t.cpu_routed += b->stats().cpu_routed_calls.load();
+        }
     }
     auto t1 = Clock::now();
-    final_formula_mpf(pi_int, Q, R, cfg.digits);
-    auto t2 = Clock::now();
-    res.digits = format_digits(pi_int, cfg.digits);
-    auto t3 = Clock::now();
+    Clock::time_point t2, t3;
+    if (cfg.final_mode == FinalMode::Newton) {
+        // Products of the finish: the B200 when the splitting ran there, else the engine's multiplier.
+        std::unique_ptr<B200Multiplier> gpu;
+        if (cfg.mode == BSMode::Batched) gpu = std::make_unique<B200Multiplier>(cfg.gpu_threshold, cfg.device);
+        Multiplier& fm = gpu ? static_cast<Multiplier&>(*gpu) : mult_;
+        final_formula_newton(pi_int, Q, R, cfg.digits, fm);
+        t2 = Clock::now();
+        std::string d = to_decimal(pi_int, cfg.digits + 1, fm, cfg.num_threads);
+        if (gpu) {
+            res.t.gpu_launches += pg_launch_count(gpu->context());
+            res.t.gpu_calls += gpu->stats().gpu_calls.load();
+            res.t.cpu_routed += gpu->stats().cpu_routed_calls.load();
+        }
+        res.digits.reserve(cfg.digits + 2);
+        res.digits.push_back(d[0]);
+        res.digits.push_back('.');
+        res.digits.append(d, 1, std::string::npos);
+        t3 = Clock::now();
+    } else {
+        final_formula_mpf(pi_int, Q, R, cfg.digits);
+        t2 = Clock::now();
+        res.digits = format_digits(pi_int, cfg.digits);
+        t3 = Clock::now();
+    }
     res.t.bs = secs(t0, t1);
     res.t.final = secs(t1, t2);
     res.t.convert = secs(t2, t3);

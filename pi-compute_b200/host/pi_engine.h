@@ -9,6 +9,7 @@
 #pragma once
 
 #include <cstddef>
+#include <cstdint>
 #include <string>
 
 #include "multiplier.h"
@@ -17,16 +18,24 @@ namespace pi {
 
 enum class BSMode { PerCall = 0, Batched = 1 };
 
+// Final formula and decimal conversion: the reference's GMP mpf division/square root and
+// mpz_get_str, or integer Newton iterations and divide-and-conquer conversion whose large
+// products run on the B200 (newton.h).
+enum class FinalMode { Mpf = 0, Newton = 1 };
+
 struct PiConfig {
     size_t digits = 1000;
-    unsigned int num_threads = 1;   // host threads issuing per-call products
+    unsigned int num_threads = 1;   // host threads issuing per-call products / converting digits
     BSMode mode = BSMode::PerCall;
-    int device = 0;                 // batched mode
+    FinalMode final_mode = FinalMode::Mpf;
+    int device = 0;                 // batched mode and the Newton finish
+    size_t gpu_threshold = 1024;    // Newton finish: min limbs of the smaller operand for the GPU
     bool verbose = false;
 };
 
 struct PiTimings {
     double bs = 0, final = 0, convert = 0, total = 0;
+    uint64_t gpu_launches = 0, gpu_calls = 0, cpu_routed = 0;
 };
 
 struct PiResult {

@@ -65,7 +65,7 @@ def main() -> None:
     open(os.path.join(HERE, "pi_1000.txt"), "wb").write(pi1000)
 
     pig = {}
-    for d in (1_000_000, 10_000_000):
+    for d in (1_000_000, 10_000_000, 100_000_000):
         s = run_ref(d, os.cpu_count() or 1)
         pig[str(d)] = {"sha256": hashlib.sha256(s).hexdigest(), "bytes": len(s), "head": s[:66].decode(),
                        "tail": s[-64:].decode()}

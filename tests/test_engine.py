@@ -34,7 +34,7 @@ def lib():
 
 def pi_digits(lib, digits, mode, threshold=1024, threads=1):
     buf = ctypes.create_string_buffer(digits + 2)
-    t = (ctypes.c_double * 4)()
+    t = (ctypes.c_double * 8)()
     st = lib.pib_pi(digits, mode, threads, threshold, 0, buf, digits + 2, t)
     assert st == 0, lib.pib_last_error()
     return buf.raw[: digits + 2].decode(), list(t)
@@ -163,4 +163,22 @@ def test_batched_digits_1000_and_1m(lib):
 def test_batched_digits_10m(lib):
     s, t = pi_digits(lib, 10_000_000, BATCHED)
     g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["10000000"]
+    assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
+
+
+# ---------------------------------------------------------------- Newton finish + D&C conversion (CPU)
+GMP_NEWTON = 3
+
+
+@pytest.mark.parametrize("digits", [1, 2, 3, 10, 50, 100, 999, 1000, 4096, 65537])
+def test_newton_finish_matches_reference_digits_cpu(lib, digits):
+    # integer Newton reciprocal / sqrt(10005) and divide-and-conquer decimal conversion (GMP products)
+    s, _ = pi_digits(lib, digits, GMP_NEWTON)
+    ref, _ = pi_digits(lib, digits, GMP)
+    assert s == ref
+
+
+def test_newton_finish_1m_cpu_hash(lib):
+    s, _ = pi_digits(lib, 1_000_000, GMP_NEWTON, threads=8)
+    g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
     assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
