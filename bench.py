@@ -120,6 +120,23 @@ class ClockSampler:
                 "samples_under_load": len(busy)}
 
 
+def dist_max(x: float, device=None) -> float:
+    """Maximum of x over all ranks (identity without an initialised process group)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(units_per_rank: float, steps: int, world: int, max_seconds: float) -> float:
+    """Whole-job throughput of independent replicas: all ranks' units over the slowest rank's time."""
+    return units_per_rank * steps * world / max_seconds
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -272,11 +289,8 @@ def run_b200(args):
         launches += int(s[4])
     total = time.perf_counter() - t_all
     clk = clocks.stop()
-    t = torch.tensor([total], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    total = float(t.item())
-    value = D * args.steps * world / total
+    total = dist_max(total, device=f"cuda:{local}")
+    value = replica_throughput(D, args.steps, world, total)
 
     eng = pkg.Engine(local)
     roof = product_roofline(pkg, eng, torch, local, logn=args.logn)
@@ -321,6 +335,27 @@ def run_b200(args):
         torch.distributed.destroy_process_group()
 
 
+def run_mul(args):
+    """Workload "mul": only the product's live roofline (for profiling the hot path's unit)."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    eng = pkg.Engine(local)
+    roof = product_roofline(pkg, eng, torch, local, logn=args.logn, steps=max(1, args.steps))
+    eng.close()
+    if rank == 0:
+        n = 1 << args.logn
+        ms = roof["ms_per_product"]
+        print(json.dumps({"metric": "mul GB/s vs HBM (B_mul = 400*(na+nb))", "value": roof["achieved"],
+                          "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": 3, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "u32 mod p (NTT), u64 limbs", "data": "synthetic",
+                          "config": {"workload": f"multiply, balanced 2^{args.logn} x 2^{args.logn} limbs", "na": n,
+                                     "nb": n}, "roofline": roof, "gpu_launches": roof["launches"]}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -332,9 +367,12 @@ def main():
     ap.add_argument("--logn", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", default="pi", choices=["pi", "mul"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "mul":
+        run_mul(args)
     else:
         run_b200(args)
 

@@ -18,7 +18,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -288,13 +290,22 @@ __global__ void bs_combine_kernel(uint32_t* base, uint64_t stride, uint64_t L, u
 namespace {
 
 int bitlen128(u128 x) {
-    int n = 0;
-    while (x) {
-        ++n;
-        x >>= 1;
-    }
-    return n;
+    const uint64_t hi = (uint64_t)(x >> 64), lo = (uint64_t)x;
+    if (hi) return 128 - __builtin_clzll(hi);
+    return lo ? 64 - __builtin_clzll(lo) : 0;
 }
+
+}  // namespace
+
+bool trace_on() {
+    static const bool on = [] {
+        const char* e = std::getenv("PI_B200_TRACE");
+        return e && *e && *e != '0';
+    }();
+    return on;
+}
+
+namespace {
 
 // Exact bit lengths of the leaf magnitudes of term k.
 void leaf_bits(uint64_t k, int& bp, int& bq, int& br) {
@@ -336,8 +347,10 @@ struct DeviceBS {
     uint64_t lev_len_cap[2] = {0, 0};
     uint32_t* res = nullptr;
     uint64_t res_cap = 0;
-    uint32_t* sync = nullptr;
+    uint32_t* sync = nullptr;     // look-back tickets and status words (grows)
     uint64_t sync_cap = 0;
+    uint32_t* errw = nullptr;     // device error word, allocated once and never moved
+    uint64_t errw_cap = 0;
 
     ~DeviceBS() { release(); }
     void release() {
@@ -348,6 +361,7 @@ struct DeviceBS {
         }
         if (res) cudaFree(res), res = nullptr, res_cap = 0;
         if (sync) cudaFree(sync), sync = nullptr, sync_cap = 0;
+        if (errw) cudaFree(errw), errw = nullptr, errw_cap = 0;
     }
     static cudaError_t grow(void** p, uint64_t& cap, uint64_t need) {
         if (need <= cap) return cudaSuccess;
@@ -505,17 +519,17 @@ struct DeviceBS {
         uint64_t maxw = 2ull * std::max({out.cap[0], out.cap[1], out.cap[2]});
         const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
         const uint64_t jobs = 3 * M;
-        e = grow((void**)&sync, sync_cap, (1 + jobs + jobs * bpj) * 4);
+        e = grow((void**)&sync, sync_cap, (jobs + jobs * bpj) * 4);
         if (e != cudaSuccess) return e;
-        e = cudaMemsetAsync(sync + 1, 0, (jobs + jobs * bpj) * 4, st);
+        e = cudaMemsetAsync(sync, 0, (jobs + jobs * bpj) * 4, st);
         if (e != cudaSuccess) return e;
         e = cudaMemsetAsync(out.len, 0, 3 * M * 4, st);
         if (e != cudaSuccess) return e;
         CrtParams c{};
         c.L = L;
-        c.error = sync;
-        c.ticket = sync + 1;
-        c.status = sync + 1 + jobs;
+        c.error = errw;
+        c.ticket = sync;
+        c.status = sync + jobs;
         c.blocks_per_job = bpj;
         c.k = make_crt_consts(P.logL);
         c.merge = 1;
@@ -538,11 +552,16 @@ struct DeviceBS {
     // Computes P, Q, R of [a0, b0); results stay in the final level buffers (root = node 0).
     cudaError_t run(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
         int D = 0;
+        const bool tr = trace_on();
+        auto tp0 = std::chrono::steady_clock::now();
         std::vector<DepthPlan> dp = plan(a0, b0, D, err);
+        if (tr)
+            std::fprintf(stderr, "[pg_bs] plan %.3f ms, %d depths\n",
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp0).count(), D);
         if (!err.empty()) return cudaErrorInvalidValue;
-        cudaError_t e = grow((void**)&sync, sync_cap, 4096 * 4);
+        cudaError_t e = grow((void**)&errw, errw_cap, 256);
         if (e != cudaSuccess) return e;
-        e = cudaMemsetAsync(sync, 0, 4, st);
+        e = cudaMemsetAsync(errw, 0, 4, st);
         if (e != cudaSuccess) return e;
         if (D == 0) {
             // single term: the root is a leaf; treat it as a "pair level" of one node of size 1
@@ -590,6 +609,7 @@ struct DeviceBS {
             e = alloc(oslot, P);
             if (e != cudaSuccess) return e;
             LevelView in = view(slot, C), out = view(oslot, P);
+            auto tl0 = std::chrono::steady_clock::now();
             if (P.kind == 1) {
                 bs_warp_merge_kernel<kWarpMaxC><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes, a0,
                                                                                               b0, d);
@@ -599,6 +619,13 @@ struct DeviceBS {
                 e = launch_ntt_level(P, C, in, out, a0, b0, d);
             }
             if (e != cudaSuccess) return e;
+            if (tr) {
+                cudaStreamSynchronize(st);
+                std::fprintf(stderr, "[pg_bs] depth %2d: %8llu merges, caps %u/%u/%u limbs, %s L=2^%d: %.3f ms\n", d,
+                             (unsigned long long)P.nodes, P.cap[0], P.cap[1], P.cap[2],
+                             P.kind == 1 ? "warp" : "ntt ", P.logL,
+                             std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count());
+            }
             slot = oslot;
         }
         root = view(slot, dp[0]);
@@ -618,6 +645,9 @@ std::mutex& ctx_mutex(pg_ctx* c);
 uint64_t* ctx_launches(pg_ctx* c);
 void ctx_set_error(pg_ctx* c, const std::string& msg);
 int ctx_device(pg_ctx* c);
+DeviceBS* ctx_bs(pg_ctx* c);
+DeviceBS* bs_state_new() { return new DeviceBS; }
+void bs_state_delete(DeviceBS* b) { delete b; }
 }  // namespace pg
 
 extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R,
@@ -625,7 +655,7 @@ extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
     if (!ctx || !Q || !R || !len || !sign || b <= a) return PG_ERR_BAD_ARG;
     std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
     cudaSetDevice(pg::ctx_device(ctx));
-    pg::DeviceBS bs;
+    pg::DeviceBS& bs = *pg::ctx_bs(ctx);  // buffers persist in the context across calls
     bs.T = &pg::ctx_tables(ctx);
     bs.st = pg::ctx_stream(ctx);
     bs.launches = pg::ctx_launches(ctx);
@@ -641,10 +671,11 @@ extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
         pg::ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
     }
+    auto tc0 = std::chrono::steady_clock::now();
     uint32_t hl[3] = {0, 0, 0};
     uint32_t herr = 0;
     e = cudaMemcpyAsync(hl, root.len, 12, cudaMemcpyDeviceToHost, bs.st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, bs.sync, 4, cudaMemcpyDeviceToHost, bs.st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, bs.errw, 4, cudaMemcpyDeviceToHost, bs.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(bs.st);
     if (e != cudaSuccess) {
         pg::ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
@@ -665,6 +696,9 @@ extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
     }
     e = cudaStreamSynchronize(bs.st);
     if (e != cudaSuccess) return PG_ERR_DEVICE;
+    if (pg::trace_on())
+        std::fprintf(stderr, "[pg_bs] device sync + copy-out of P/Q/R: %.3f ms\n",
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count());
     // signs over the series: P(a,b) = (-1)^(#k >= 1), Q > 0, R(a,b) has the sign of R(a, a+1)
     const unsigned long neg_terms = (b - a) - (a == 0 ? 1 : 0);
     sign[0] = hl[0] ? ((neg_terms & 1) ? -1 : 1) : 0;

@@ -1,5 +1,6 @@
 // Device engine implementation: twiddle tables, pass dispatch, CRT constants and
 // the per-product launch sequence.
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -80,6 +81,7 @@ static cudaError_t grow(void** ptr, uint64_t bytes) {
 
 cudaError_t Workspace::ensure_res(uint64_t n) {
     if (n <= res_cap) return cudaSuccess;
+    n = std::max(n, res_cap + res_cap / 2);  // geometric growth: products grow level by level
     cudaError_t e = grow((void**)&a_res, n * 4);
     if (e == cudaSuccess) e = grow((void**)&b_res, n * 4);
     res_cap = (e == cudaSuccess) ? n : 0;
@@ -88,7 +90,7 @@ cudaError_t Workspace::ensure_res(uint64_t n) {
 
 cudaError_t Workspace::ensure_limbs(uint64_t n) {
     if (n <= limb_cap) return cudaSuccess;
-    n = n < 1024 ? 1024 : n;
+    n = std::max<uint64_t>({n, 1024, limb_cap + limb_cap / 2});  // pinned allocations are slow: grow geometrically
     cudaError_t e = grow((void**)&in_a, n * 8);
     if (e == cudaSuccess) e = grow((void**)&in_b, n * 8);
     if (e == cudaSuccess) e = grow((void**)&outl, n * 8);
@@ -104,8 +106,12 @@ cudaError_t Workspace::ensure_limbs(uint64_t n) {
 cudaError_t Workspace::ensure_sync(uint64_t nblocks) {
     if (nblocks + 2 <= sync_cap) return cudaSuccess;
     uint64_t n = nblocks + 2 < 4096 ? 4096 : nblocks + 2;
+    // Carry an error recorded by an earlier (asynchronous) product over to the new buffer.
+    uint32_t old_err = 0;
+    if (sync) cudaMemcpy(&old_err, sync, 4, cudaMemcpyDeviceToHost);
     cudaError_t e = grow((void**)&sync, n * 4);
     if (e == cudaSuccess) e = cudaMemset(sync, 0, n * 4);
+    if (e == cudaSuccess && old_err) e = cudaMemcpy(sync, &old_err, 4, cudaMemcpyHostToDevice);
     sync_cap = (e == cudaSuccess) ? n : 0;
     return e;
 }

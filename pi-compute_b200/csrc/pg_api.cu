@@ -1,13 +1,22 @@
 // C ABI of libpigpu.so (declarations and reference citations in include/pi_b200.h).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <new>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/pi_b200.h"
 #include "ntt_engine.cuh"
+
+namespace pg {
+struct DeviceBS;
+DeviceBS* bs_state_new();
+void bs_state_delete(DeviceBS*);
+}  // namespace pg
 
 struct pg_ctx {
     int device = 0;
@@ -17,6 +26,7 @@ struct pg_ctx {
     pg::Workspace ws;
     std::string last_error;
     uint64_t launches = 0;
+    pg::DeviceBS* bs = nullptr;  // binary-splitting buffers, kept for the next pg_bs call
 };
 
 namespace {
@@ -30,6 +40,26 @@ pg_status cuda_fail(pg_ctx* c, cudaError_t e, const char* where) {
     cudaGetLastError();  // clear a sticky launch error so the context stays usable
     if (e == cudaErrorMemoryAllocation) return fail(c, PG_ERR_OOM, std::string(where) + ": out of device memory");
     return fail(c, PG_ERR_DEVICE, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// memcpy split across host threads for large buffers (pinned staging of big operands).
+void copy_parallel(void* dst, const void* src, size_t bytes) {
+    constexpr size_t kChunk = 8u << 20;
+    if (bytes < 2 * kChunk) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    unsigned nt = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    nt = (unsigned)std::min<size_t>(nt, bytes / kChunk);
+    std::vector<std::thread> th;
+    const size_t per = (bytes + nt - 1) / nt;
+    for (unsigned i = 1; i < nt; ++i) {
+        const size_t o = i * per;
+        if (o >= bytes) break;
+        th.emplace_back([=] { std::memcpy((char*)dst + o, (const char*)src + o, std::min(per, bytes - o)); });
+    }
+    std::memcpy(dst, src, std::min(per, bytes));
+    for (auto& t : th) t.join();
 }
 
 size_t trimmed(const uint64_t* x, size_t n) {
@@ -72,10 +102,10 @@ pg_status host_product(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* 
     if (e != cudaSuccess) return cuda_fail(c, e, "workspace");
     // Stage through pinned memory so the copies run at full PCIe/C2C speed and stay async.
     uint64_t* pin = c->ws.pinned;
-    std::memcpy(pin, a, na * 8);
+    copy_parallel(pin, a, na * 8);
     e = cudaMemcpyAsync(c->ws.in_a, pin, na * 8, cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess && !square) {
-        std::memcpy(pin + c->ws.limb_cap, b, nb * 8);
+        copy_parallel(pin + c->ws.limb_cap, b, nb * 8);
         e = cudaMemcpyAsync(c->ws.in_b, pin + c->ws.limb_cap, nb * 8, cudaMemcpyHostToDevice, c->stream);
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "host to device copy");
@@ -87,7 +117,7 @@ pg_status host_product(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* 
     if (e != cudaSuccess) return cuda_fail(c, e, "device to host copy");
     pg_status s = check_device_error(c);
     if (s != PG_OK) return s;
-    std::memcpy(out, pout, (na + nb) * 8);
+    copy_parallel(out, pout, (na + nb) * 8);
     *out_len = trimmed(out, na + nb);
     return PG_OK;
 }
@@ -102,6 +132,10 @@ std::mutex& ctx_mutex(pg_ctx* c) { return c->mu; }
 uint64_t* ctx_launches(pg_ctx* c) { return &c->launches; }
 void ctx_set_error(pg_ctx* c, const std::string& msg) { c->last_error = msg; }
 int ctx_device(pg_ctx* c) { return c->device; }
+DeviceBS* ctx_bs(pg_ctx* c) {
+    if (!c->bs) c->bs = bs_state_new();
+    return c->bs;
+}
 }  // namespace pg
 
 extern "C" {
@@ -138,6 +172,7 @@ void pg_destroy(pg_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->bs) pg::bs_state_delete(c->bs);
     c->ws.release();
     c->tables.release();
     if (c->stream) cudaStreamDestroy(c->stream);

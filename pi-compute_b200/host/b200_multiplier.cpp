@@ -5,6 +5,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
+#include <map>
+#include <mutex>
 #include <stdexcept>
 
 namespace pi {
@@ -14,7 +16,25 @@ B200Multiplier::B200Multiplier(size_t threshold, int device) : threshold_(thresh
     if (s != PG_OK) throw std::runtime_error("B200Multiplier: pg_create failed with status " + std::to_string(s));
 }
 
-B200Multiplier::~B200Multiplier() { pg_destroy(ctx_); }
+B200Multiplier::B200Multiplier(size_t threshold, pg_ctx* shared, int device)
+    : ctx_(shared), owned_(false), threshold_(threshold), device_(device) {}
+
+B200Multiplier::~B200Multiplier() {
+    if (owned_) pg_destroy(ctx_);
+}
+
+pg_ctx* shared_context(int device) {
+    static std::mutex mu;
+    static std::map<int, pg_ctx*> ctxs;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = ctxs.find(device);
+    if (it != ctxs.end()) return it->second;
+    pg_ctx* c = nullptr;
+    pg_status s = pg_create(device, &c);
+    if (s != PG_OK) throw std::runtime_error("pg_create failed with status " + std::to_string(s));
+    ctxs[device] = c;
+    return c;
+}
 
 std::string B200Multiplier::device_name() const {
     cudaDeviceProp prop;

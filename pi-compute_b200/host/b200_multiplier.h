@@ -29,6 +29,8 @@ public:
     // threshold: minimum limb count of the smaller operand for the GPU path (the
     // reference's --gpu-threshold, default 10000, main.cpp:63).
     explicit B200Multiplier(size_t threshold = 10000, int device = 0);
+    // Use an existing context (not destroyed by this multiplier).
+    B200Multiplier(size_t threshold, pg_ctx* shared, int device);
     ~B200Multiplier() override;
     B200Multiplier(const B200Multiplier&) = delete;
     B200Multiplier& operator=(const B200Multiplier&) = delete;
@@ -54,9 +56,14 @@ public:
 private:
     void product(mpz_t result, const mpz_t a, const mpz_t b, bool square);
     pg_ctx* ctx_ = nullptr;
+    bool owned_ = true;
     size_t threshold_;
     int device_;
     mutable Stats stats_;
 };
+
+// One context per device for the whole process (tables, workspace and binary-splitting
+// buffers are built once and reused by every pi computation). Never destroyed.
+pg_ctx* shared_context(int device);
 
 }  // namespace pi

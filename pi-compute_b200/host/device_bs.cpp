@@ -11,7 +11,11 @@ DeviceBinarySplitting::DeviceBinarySplitting(int device) {
     if (s != PG_OK) throw std::runtime_error("DeviceBinarySplitting: pg_create failed with status " + std::to_string(s));
 }
 
-DeviceBinarySplitting::~DeviceBinarySplitting() { pg_destroy(ctx_); }
+DeviceBinarySplitting::DeviceBinarySplitting(pg_ctx* shared) : ctx_(shared), owned_(false) {}
+
+DeviceBinarySplitting::~DeviceBinarySplitting() {
+    if (owned_) pg_destroy(ctx_);
+}
 
 void DeviceBinarySplitting::compute(unsigned long a, unsigned long b, mpz_ptr P, mpz_ptr Q, mpz_ptr R) {
     if (b <= a) throw std::invalid_argument("empty range");

@@ -12,6 +12,8 @@ namespace pi {
 class DeviceBinarySplitting {
 public:
     explicit DeviceBinarySplitting(int device = 0);
+    // Use an existing context (not destroyed here).
+    explicit DeviceBinarySplitting(pg_ctx* shared);
     ~DeviceBinarySplitting();
     DeviceBinarySplitting(const DeviceBinarySplitting&) = delete;
     DeviceBinarySplitting& operator=(const DeviceBinarySplitting&) = delete;
@@ -22,6 +24,7 @@ public:
 
 private:
     pg_ctx* ctx_ = nullptr;
+    bool owned_ = true;
 };
 
 }  // namespace pi

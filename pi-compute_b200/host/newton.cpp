@@ -1,6 +1,9 @@
 #include "newton.h"
 
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <future>
@@ -29,6 +32,25 @@ void pow2(mpz_ptr r, size_t e) {
 }
 
 constexpr size_t kSmallBits = 4096;  // below this, GMP's own division/root on the host
+
+// Phase timer printed to stderr when PI_B200_TRACE is set.
+struct Trace {
+    const char* what;
+    std::chrono::steady_clock::time_point t0;
+    static bool on() {
+        static const bool v = [] {
+            const char* e = std::getenv("PI_B200_TRACE");
+            return e && *e && *e != '0';
+        }();
+        return v;
+    }
+    explicit Trace(const char* w) : what(w), t0(std::chrono::steady_clock::now()) {}
+    ~Trace() {
+        if (on())
+            std::fprintf(stderr, "[newton] %s: %.3f ms\n", what,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    }
+};
 
 }  // namespace
 
@@ -155,9 +177,19 @@ void final_formula_newton(mpz_t pi_int, const mpz_t Q, const mpz_t R, size_t dig
         const long long eR = (long long)bits(R) - (long long)k;
         if (eQ >= 0) mpz_tdiv_q_2exp(Qt, Q, (size_t)eQ); else mpz_mul_2exp(Qt, Q, (size_t)-eQ);
         if (eR >= 0) mpz_tdiv_q_2exp(Rt, R, (size_t)eR); else mpz_mul_2exp(Rt, R, (size_t)-eR);
-        recip_floor(Z, Rt, mul);          // 2^(2k) / Rt
-        sqrt_scaled(S, 10005, k, mul);    // sqrt(10005) 2^k
-        pow5(F, digits, mul);             // 10^digits = 5^digits 2^digits
+        {
+            Trace t("reciprocal of R");
+            recip_floor(Z, Rt, mul);          // 2^(2k) / Rt
+        }
+        {
+            Trace t("sqrt(10005)");
+            sqrt_scaled(S, 10005, k, mul);    // sqrt(10005) 2^k
+        }
+        {
+            Trace t("5^digits");
+            pow5(F, digits, mul);             // 10^digits = 5^digits 2^digits
+        }
+        Trace tprod("three truncated products");
         // pi 10^digits = 426880 Q sqrt(10005) 10^digits / R ~= X 2^e
         mpz_mul_ui(X, Qt, 426880);
         e = eQ - eR - 2 * (long long)k - (long long)k + (long long)digits;
@@ -281,26 +313,32 @@ std::string to_decimal(const mpz_t x, size_t ndigits, Multiplier& mul, unsigned 
     // power tree 10^(2^j) for 2^j < ndigits
     int J = -1;
     while (((size_t)1 << (J + 1)) < ndigits) ++J;
-    for (int j = 0; j <= J; ++j) {
-        Mpz* p = new Mpz;
-        if (j == 0)
-            mpz_set_ui(*p, 10);
-        else
-            mul.square(*p, *c.pw[j - 1]);
-        c.pw.push_back(p);
-        c.K.push_back(bits(*p));
-        // reciprocals for the divisions done above the leaves
-        if (((size_t)1 << j) * 2 > c.leaf && c.K.back() > kSmallBits) {
-            Mpz* z = new Mpz;
-            recip_floor(*z, *p, mul);
-            c.inv.push_back(z);
-        } else {
-            c.inv.push_back(nullptr);
+    {
+        Trace t("power tree and reciprocals");
+        for (int j = 0; j <= J; ++j) {
+            Mpz* p = new Mpz;
+            if (j == 0)
+                mpz_set_ui(*p, 10);
+            else
+                mul.square(*p, *c.pw[j - 1]);
+            c.pw.push_back(p);
+            c.K.push_back(bits(*p));
+            // reciprocals for the divisions done above the leaves
+            if (((size_t)1 << j) * 2 > c.leaf && c.K.back() > kSmallBits) {
+                Mpz* z = new Mpz;
+                recip_floor(*z, *p, mul);
+                c.inv.push_back(z);
+            } else {
+                c.inv.push_back(nullptr);
+            }
         }
     }
-    int depth = 0;
-    for (unsigned t = threads; t > 1; t >>= 1) ++depth;
-    c.rec(x, ndigits, 0, J, depth);
+    {
+        Trace t("divide-and-conquer splits and leaves");
+        int depth = 0;
+        for (unsigned th = threads; th > 1; th >>= 1) ++depth;
+        c.rec(x, ndigits, 0, J, depth);
+    }
     return out;
 }
 

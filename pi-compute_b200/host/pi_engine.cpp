@@ -75,9 +75,11 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
     mpz_init(R);
     mpz_init(pi_int);
     if (cfg.mode == BSMode::Batched) {
-        DeviceBinarySplitting dbs(cfg.device);
+        pg_ctx* ctx = shared_context(cfg.device);
+        const uint64_t l0 = pg_launch_count(ctx);
+        DeviceBinarySplitting dbs(ctx);
         dbs.compute(0, terms, nullptr, Q, R);  // P(0, N) is not needed (pi_engine.cpp:257-258)
-        res.t.gpu_launches += dbs.launches();
+        res.t.gpu_launches += pg_launch_count(ctx) - l0;
     } else {
         BinarySplitting bs(mult_, cfg.num_threads);
         BSResult r = bs.compute(0, terms);
@@ -94,13 +96,18 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
     if (cfg.final_mode == FinalMode::Newton) {
         // Products of the finish: the B200 when the splitting ran there, else the engine's multiplier.
         std::unique_ptr<B200Multiplier> gpu;
-        if (cfg.mode == BSMode::Batched) gpu = std::make_unique<B200Multiplier>(cfg.gpu_threshold, cfg.device);
+        uint64_t l0 = 0;
+        if (cfg.mode == BSMode::Batched) {
+            pg_ctx* ctx = shared_context(cfg.device);
+            l0 = pg_launch_count(ctx);
+            gpu = std::make_unique<B200Multiplier>(cfg.gpu_threshold, ctx, cfg.device);
+        }
         Multiplier& fm = gpu ? static_cast<Multiplier&>(*gpu) : mult_;
         final_formula_newton(pi_int, Q, R, cfg.digits, fm);
         t2 = Clock::now();
         std::string d = to_decimal(pi_int, cfg.digits + 1, fm, cfg.num_threads);
         if (gpu) {
-            res.t.gpu_launches += pg_launch_count(gpu->context());
+            res.t.gpu_launches += pg_launch_count(gpu->context()) - l0;
             res.t.gpu_calls += gpu->stats().gpu_calls.load();
             res.t.cpu_routed += gpu->stats().cpu_routed_calls.load();
         }
@@ -120,7 +127,7 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
     res.t.convert = secs(t2, t3);
     res.t.total = secs(t0, t3);
     res.elapsed_seconds = res.t.total;
-    if (cfg.verbose) {
+    if (cfg.verbose || std::getenv("PI_B200_TRACE")) {
         std::printf("  Terms: %lu\n  Binary splitting: %.3fs\n  Final computation: %.3fs\n"
                     "  String conversion: %.3fs\n  Total: %.3fs\n",
                     terms, res.t.bs, res.t.final, res.t.convert, res.t.total);
