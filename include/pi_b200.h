@@ -110,7 +110,7 @@ pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint
  * framework owns the device allocator, or a plugin callback where allocating (and the device
  * synchronisation an allocation can imply) is not allowed. It needs no pg_ctx: the scratch
  * residues and the twiddle tables live in fixed-size device arrays inside libpigpu.so
- * (about 1.9 MB, held on every GPU that loads the library until the process exits).
+ * (about 2.8 MB, held on every GPU that loads the library until the process exits).
  *
  * Limit: na + nb <= 16384 limbs; larger products return PG_ERR_TOO_LARGE without touching
  * any memory. Pointers are device addresses on the CURRENT device, 16-byte aligned; d_out

@@ -15,6 +15,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -53,13 +54,17 @@ def build_gpu(verbose_ptxas: bool = False) -> str:
                  + glob.glob(os.path.join(INCLUDE, "*.h")))
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for src in cu:
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
         if _newer(obj, [src] + hdr):
             extra = ["-Xptxas", "-v"] if verbose_ptxas else []
-            _run([NVCC, *NVCC_FLAGS, *extra, "-I", INCLUDE, "-c", src, "-o", obj])
+            jobs.append([NVCC, *NVCC_FLAGS, *extra, "-I", INCLUDE, "-c", src, "-o", obj])
+    # translation units compile independently: run them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j) for j in jobs]:
+            f.result()
     if _newer(LIBPIGPU, objs):
         _run([NVCC, *ARCH, "-shared", "-o", LIBPIGPU, *objs, "-lcudart"])
     return LIBPIGPU

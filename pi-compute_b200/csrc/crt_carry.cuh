@@ -87,11 +87,20 @@ struct CrtJob {
 
 __device__ __forceinline__ CrtJob crt_job(const CrtParams& P, uint64_t job) {
     CrtJob J;
-    if (!P.merge) {
-        J.res = P.res;
-        J.out = P.out;
-        J.nwords = P.nwords;
+    if (P.merge == 2) {
+        const DstEntry d = P.dtab[job];
+        J.res = P.res + job * P.res_stride;
+        J.out = d.out;
+        J.nwords = d.nwords;
         J.len = nullptr;
+        J.centred = d.centred != 0;
+        return J;
+    }
+    if (!P.merge) {
+        J.res = P.res + job * P.res_stride;
+        J.out = P.out + job * P.out_stride;
+        J.nwords = P.nwords;
+        J.len = P.dlen ? P.dlen + job : nullptr;
         J.centred = false;
         return J;
     }

@@ -78,6 +78,19 @@ __device__ __forceinline__ uint32_t mul_shoup_lazy(uint32_t x, uint32_t w, uint3
     return x * w - q * p;
 }
 
+// floor((2^64 - 1) / p), used to form Shoup companions on the device without a division.
+__host__ __device__ constexpr uint64_t kRecip64(int j) { return ~0ull / kPrime(j); }
+
+// Shoup companion floor(w * 2^32 / p) of w < p. With R = floor(2^64 / p) = 2^64/p - d
+// (0 <= d < 1), floor(w * R / 2^32) undershoots floor(w * 2^32 / p) by at most one because
+// w * d / 2^32 < 1/2; the remainder w * 2^32 - q * p (in [0, 2p), exact modulo 2^32)
+// says which.
+__device__ __forceinline__ uint32_t shoup_companion_dev(uint32_t w, uint32_t p, uint64_t R) {
+    const uint32_t q = w * (uint32_t)(R >> 32) + __umulhi(w, (uint32_t)R);
+    const uint32_t r = 0u - q * p;
+    return r >= p ? q + 1 : q;
+}
+
 // a * b * 2^-32 mod p for a, b < p; result in [0, p).
 __device__ __forceinline__ uint32_t mul_mont(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
     uint32_t lo = a * b;

@@ -24,14 +24,15 @@ uint32_t inv_mod(uint32_t a, uint32_t p) { return pow_mod(a, p - 2, p); }
 uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
 
 // ---------------------------------------------------------------- tables
-// Layout of the single table allocation, in uint2 entries:
-//   [dir][prime] stage  : 2^13 each, entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
-//   [dir][prime] fs_lo  : 2^13 each
-//   [dir][prime] fs_hi  : 2^13 each
+// Layout of the single table allocation, in uint2 entries, 2^13 per table:
+//   [dir][prime] stage  : entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
+//   [dir][prime] fs_lo  : w_{2^26}^j
+//   [dir][prime] fs_hi  : w_{2^26}^(2^13 j)
+//   [n][dir][prime] row : w_{2^n}^e for four-step blocks of 2^n points, n = 14..26
 cudaError_t DeviceTables::build(int device) {
     (void)device;
     constexpr size_t kEnt = 1u << 13;
-    constexpr size_t kTables = 3 * 2 * kNumPrimes;
+    constexpr size_t kTables = (3 + kRowTables) * 2 * kNumPrimes;
     std::vector<uint2> h(kTables * kEnt);
     for (int dir = 0; dir < 2; ++dir) {
         for (int j = 0; j < kNumPrimes; ++j) {
@@ -52,6 +53,15 @@ cudaError_t DeviceTables::build(int device) {
                 b = b * w26 % p;
                 c = c * w26hi % p;
             }
+            for (int n = kRowLogMin; n <= kMaxLogL; ++n) {
+                const uint64_t wn = pow_mod(w26, 1ull << (kMaxLogL - n), p);  // w_{2^n}
+                uint2* row = h.data() + (((size_t)(3 * 2 + (n - kRowLogMin) * 2 + dir)) * kNumPrimes + j) * kEnt;
+                uint64_t r = 1;
+                for (size_t i = 0; i < kEnt; ++i) {
+                    row[i] = make_uint2((uint32_t)r, shoup_companion((uint32_t)r, p));
+                    r = r * wn % p;
+                }
+            }
         }
     }
     cudaError_t e = cudaMalloc(&base, h.size() * sizeof(uint2));
@@ -64,6 +74,7 @@ cudaError_t DeviceTables::build(int device) {
             tw.fs_lo[dir][j] = base + ((1 * 2 + dir) * kNumPrimes + j) * kEnt;
             tw.fs_hi[dir][j] = base + ((2 * 2 + dir) * kNumPrimes + j) * kEnt;
         }
+    tw.row = base + (size_t)3 * 2 * kNumPrimes * kEnt;
     return cudaSuccess;
 }
 
@@ -132,7 +143,8 @@ template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
 static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cudaStream_t st) {
     constexpr int LOGE = kTileLog;
     auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
-    const size_t smem = (size_t)4 << LOGE;
+    // the tile, plus the four-step row factors of a strided tile
+    const size_t smem = ((size_t)4 << LOGE) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
     uint64_t tiles;
     if constexpr (LAY == Layout::Strided) {
         tiles = (uint64_t)prm.njobs << (prm.logL - LOGE);
@@ -265,6 +277,8 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
         p.data = data;
         p.out = data;
         p.other = nullptr;
+        p.other_stride = 3 * L;
+        p.words_stride = 0;
         p.words = reinterpret_cast<const uint32_t*>(limbs);
         p.ncoef = ncoef;
         p.L = L;

@@ -33,38 +33,34 @@ __device__ __forceinline__ uint32_t bitrev_n(uint32_t x, int logn) {
     return logn == 0 ? 0u : (__brev(x) >> (32 - logn));
 }
 
-// Four-step twiddles for four consecutive columns t..t+3 of one row (output index k):
-// x.x *= w, x.y *= w*s, x.z *= w*s^2, x.w *= w*s^3 with w = w_{N'}^{t k}, s = w_{N'}^k.
-// Only w and s come from the tables (s is the same for a whole row, so its loads broadcast
-// across the warp); the other three twiddles follow by Montgomery products in registers.
-// r32 = 2^32 mod p with Shoup companion r32p (conversion into Montgomery form).
-__device__ __forceinline__ void fourstep_twiddle4(uint4& x, uint64_t t, uint64_t k, int logNp, const uint2* lo,
-                                                  const uint2* hi, uint32_t p, uint32_t pinv, uint32_t r32,
-                                                  uint32_t r32p) {
-    const uint32_t mask26 = (1u << kMaxLogL) - 1, mask13 = (1u << kFsLog) - 1;
-    const uint32_t E0 = (uint32_t)(((t * k) << (kMaxLogL - logNp)) & mask26);
-    const uint32_t Es = (uint32_t)((k << (kMaxLogL - logNp)) & mask26);
-    const uint2 a = __ldg(lo + (E0 & mask13));
-    const uint2 b = __ldg(hi + (E0 >> kFsLog));
-    const uint2 c = __ldg(lo + (Es & mask13));
-    const uint2 d = __ldg(hi + (Es >> kFsLog));
-    const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
-    const uint32_t st = mul_shoup(c.x, d.x, d.y, p);
-    uint32_t wm = mul_shoup(w, r32, r32p, p);   // w * 2^32  (Montgomery form)
-    const uint32_t sm = mul_shoup(st, r32, r32p, p);
-    x.x = mul_mont(x.x, wm, p, pinv);
-    wm = mul_mont(wm, sm, p, pinv);
-    x.y = mul_mont(x.y, wm, p, pinv);
-    wm = mul_mont(wm, sm, p, pinv);
-    x.z = mul_mont(x.z, wm, p, pinv);
-    wm = mul_mont(wm, sm, p, pinv);
-    x.w = mul_mont(x.w, wm, p, pinv);
+// Four-step twiddles of a strided tile. Element (row m, tile column c) of the tile whose
+// first column is t0 is multiplied by w_{N'}^{(t0 + c) k}, k = bitrev(m), written as
+//   A[m] * B[c k],  A[m] = w_{N'}^{t0 k} (per tile, kept in shared memory),
+//                   B[e] = w_{N'}^e, e = c k < C * N = 2^13 (the row power table of N').
+// Each factor is a (w, w') Shoup pair, so an element costs two Shoup products; the first may
+// stay lazy because Shoup accepts any 32-bit input.
+__device__ __forceinline__ void fourstep_twiddle4(uint4& x, uint32_t c, uint32_t k, uint2 A, const uint2* B,
+                                                  uint32_t p) {
+    uint32_t e = c * k;
+    const uint2 b0 = __ldg(B + e);
+    e += k;
+    const uint2 b1 = __ldg(B + e);
+    e += k;
+    const uint2 b2 = __ldg(B + e);
+    e += k;
+    const uint2 b3 = __ldg(B + e);
+    x.x = mul_shoup(mul_shoup_lazy(x.x, b0.x, b0.y, p), A.x, A.y, p);
+    x.y = mul_shoup(mul_shoup_lazy(x.y, b1.x, b1.y, p), A.x, A.y, p);
+    x.z = mul_shoup(mul_shoup_lazy(x.z, b2.x, b2.y, p), A.x, A.y, p);
+    x.w = mul_shoup(mul_shoup_lazy(x.w, b3.x, b3.y, p), A.x, A.y, p);
 }
 
 // One decimation-in-frequency round of radix R = 2^LR on v[0..R), the group's
 // elements sitting at sub-transform positions t' + s*q within a block of R*s.
 // Stage k (half size h = (R/2 >> k) * s) pairs q with q + 2^(LR-1-k) and uses
 // twiddle w_{2h}^(t' + s*(q mod 2^(LR-1-k))).
+// When logs == 0 the group offset t' is 0 and every twiddle exponent is a compile-time
+// constant after unrolling; exponent 0 (twiddle 1) then skips its multiply.
 template <int LR>
 __device__ __forceinline__ void dif_round(uint32_t (&v)[1 << LR], uint32_t tp, int logs, const uint2* stw,
                                           uint32_t p) {
@@ -76,10 +72,14 @@ __device__ __forceinline__ void dif_round(uint32_t (&v)[1 << LR], uint32_t tp, i
         for (int q = 0; q < (1 << LR); ++q) {
             if (q & half) continue;
             uint32_t a = v[q], b = v[q + half];
-            uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
-            uint2 w = __ldg(stw + ((1u << logh) + x));
             v[q] = add_mod(a, b, p);
-            v[q + half] = mul_shoup(a - b + p, w.x, w.y, p);
+            if (logs == 0 && (q & (half - 1)) == 0) {
+                v[q + half] = sub_mod(a, b, p);
+            } else {
+                uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
+                uint2 w = __ldg(stw + ((1u << logh) + x));
+                v[q + half] = mul_shoup(a - b + p, w.x, w.y, p);
+            }
         }
     }
 }
@@ -96,21 +96,29 @@ __device__ __forceinline__ void dit_round(uint32_t (&v)[1 << LR], uint32_t tp, i
 #pragma unroll
         for (int q = 0; q < (1 << LR); ++q) {
             if (q & half) continue;
-            uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
-            uint2 w = __ldg(stw + ((1u << logh) + x));
             uint32_t a = v[q];
-            uint32_t b = mul_shoup(v[q + half], w.x, w.y, p);
+            uint32_t b = v[q + half];
+            if (!(logs == 0 && (q & (half - 1)) == 0)) {
+                uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
+                uint2 w = __ldg(stw + ((1u << logh) + x));
+                b = mul_shoup(b, w.x, w.y, p);
+            }
             v[q] = add_mod(a, b, p);
             v[q + half] = sub_mod(a, b, p);
         }
     }
 }
 
-// Shared-memory address of linear tile index x: 16-byte chunks are permuted inside each
-// 128-byte line by bits of the line index (x >> 5) and (x >> 8), so the strided access
-// patterns of the radix rounds (strides of 16 and 256 words across lanes) and the 16-byte
-// vector accesses of the global<->shared copies all fall on distinct banks.
-__device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ ((((x >> 5) ^ (x >> 8)) & 7u) << 2); }
+// Shared-memory address of linear tile index x: the eight 16-byte chunks of each 128-byte
+// line are permuted by f = ((x >> 5) ^ (x >> 8 << 2)) & 7. The access patterns of a warp:
+//   global<->shared copies, 16-byte vectors of consecutive chunks: one line per 8 lanes;
+//   stride-1 rounds (contiguous tiles), 16-byte vectors at a 64-byte lane stride: lanes
+//     2i and 2i+1 share a line and differ in chunk bit 2, f walks through the lines;
+//   stride-16 rounds, 16 lanes on consecutive words and the other 16 lanes 256 words
+//     further: bit 2 of f flips with bit 8 of x, so the halves take opposite bank halves;
+//   stride >= 256 rounds: 32 consecutive words.
+// Every pattern above touches each bank once per 128 bytes moved.
+__device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ ((((x >> 5) ^ ((x >> 8) << 2)) & 7u) << 2); }
 
 // Shared-memory address of tile element (m, c).
 template <Layout LAY, int LOGN, int LOGE>
@@ -161,14 +169,36 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                 }
                 uint32_t m0 = blk * (R << logs) + tp;
                 uint32_t v[R];
+                // A contiguous tile's stride-1 round reads 16 consecutive words: 4 vectors.
+                const bool vec = (LAY == Layout::Contig) && logs == 0;
+                if (vec) {
+                    const uint32_t x0 = (c << LOGN) + m0;
 #pragma unroll
-                for (int q = 0; q < R; ++q) v[q] = sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)];
+                    for (int q4 = 0; q4 < R / 4; ++q4) {
+                        const uint4 t = *reinterpret_cast<const uint4*>(sm + swz(x0 + 4 * q4));
+                        v[4 * q4] = t.x;
+                        v[4 * q4 + 1] = t.y;
+                        v[4 * q4 + 2] = t.z;
+                        v[4 * q4 + 3] = t.w;
+                    }
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) v[q] = sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)];
+                }
                 if (INV)
                     dit_round<4>(v, tp, logs, stw, p);
                 else
                     dif_round<4>(v, tp, logs, stw, p);
+                if (vec) {
+                    const uint32_t x0 = (c << LOGN) + m0;
 #pragma unroll
-                for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)] = v[q];
+                    for (int q4 = 0; q4 < R / 4; ++q4)
+                        *reinterpret_cast<uint4*>(sm + swz(x0 + 4 * q4)) =
+                            make_uint4(v[4 * q4], v[4 * q4 + 1], v[4 * q4 + 2], v[4 * q4 + 3]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)] = v[q];
+                }
             }
         } else {
             // remainder round: the top LRX stages, stride s = 2^(LOGN - LRX), one block
@@ -227,14 +257,17 @@ __device__ __forceinline__ uint32_t tcol(uint64_t tile, uint32_t c, int logS) {
 // Source limbs of job `job` (first forward pass).
 __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, const uint32_t*& words,
                                            uint64_t& ncoef) {
-    if (P.merge) {
+    if (P.merge == 2) {
+        words = P.src[job].words;
+        ncoef = P.src[job].ncoef;
+    } else if (P.merge == 1) {
         const uint64_t m = job / 6, o = job % 6;
         const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
         const int which = (int)(o % 3);
         words = reinterpret_cast<const uint32_t*>(P.ms.X[which] + child * P.ms.cap[which]);
         ncoef = 2ull * P.ms.len[3 * child + which];
     } else {
-        words = P.words;
+        words = P.words + job * P.words_stride;
         ncoef = P.ncoef;
     }
 }
@@ -251,8 +284,6 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
     const uint32_t p = kPrime(j);
     const int dir = INV ? 1 : 0;
     const uint32_t pinv = inv_mod_2_32(p);
-    const uint32_t r32 = (uint32_t)(0x100000000ull % p);
-    const uint32_t r32p = (uint32_t)(((uint64_t)r32 << 32) / p);
     const uint64_t prime_off = (uint64_t)j * P.L;
 
     // Strided: one job per tile. Contig: row c of the tile is global row R = tile*C + c.
@@ -264,6 +295,27 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
     }
     const uint64_t total_rows = (uint64_t)P.njobs << (P.logL - LOGN);
     const int logRows = P.logL - LOGN;
+
+    // Strided tiles: four-step row factors A[m] = w_{N'}^{t0 bitrev(m)} of this tile's first
+    // column t0, after the tile in shared memory; B is the row power table of N'.
+    uint2* smA = reinterpret_cast<uint2*>(sm + E);
+    const uint2* rowB = nullptr;
+    if constexpr (LAY == Layout::Strided) {
+        rowB = row_table(T, P.logNp, dir, j);
+        const uint32_t t0 = tcol<LAY, LOGN, LOGE>(stile, 0, P.logS);
+        const int sh = kMaxLogL - P.logNp;
+        const uint2* lo = T.fs_lo[dir][j];
+        const uint2* hi = T.fs_hi[dir][j];
+        const uint64_t R = kRecip64(j);
+        for (uint32_t i = threadIdx.x; i < (1u << LOGN); i += NTHREADS) {
+            const uint32_t E0 = (t0 * bitrev_n(i, LOGN)) << sh;  // t0 * k < N', exponent of w_{2^26}
+            const uint2 a = __ldg(lo + (E0 & ((1u << kFsLog) - 1)));
+            const uint2 b = __ldg(hi + (E0 >> kFsLog));
+            const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
+            smA[i] = make_uint2(w, shoup_companion_dev(w, p, R));
+        }
+        if constexpr (INV) __syncthreads();  // used by the load loop below
+    }
 
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
     for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
@@ -306,9 +358,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
         }
         if constexpr (INV && LAY == Layout::Strided) {
             // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m))
-            uint32_t t = tcol<LAY, LOGN, LOGE>(stile, c, P.logS);
-            uint64_t k = bitrev_n(m, LOGN);
-            fourstep_twiddle4(x, t, k, P.logNp, T.fs_lo[1][j], T.fs_hi[1][j], p, pinv, r32, r32p);
+            fourstep_twiddle4(x, c, bitrev_n(m, LOGN), smA[m], rowB, p);
         }
         *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
     }
@@ -327,7 +377,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
             uint4 a = *reinterpret_cast<uint4*>(sm + swz(e4));
             uint4 b;
             if constexpr (FUSE == Fuse::MulInverse) {
-                b = *reinterpret_cast<const uint4*>(P.other + job * P.job_stride + prime_off + g);
+                b = *reinterpret_cast<const uint4*>(P.other + job * P.other_stride + prime_off + g);
             } else {
                 b = a;
             }
@@ -360,9 +410,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
         }
         uint4 x = *reinterpret_cast<uint4*>(sm + swz(e4));
         if constexpr (!INV && LAY == Layout::Strided) {
-            uint32_t t = tcol<LAY, LOGN, LOGE>(stile, c, P.logS);
-            uint64_t k = bitrev_n(m, LOGN);
-            fourstep_twiddle4(x, t, k, P.logNp, T.fs_lo[0][j], T.fs_hi[0][j], p, pinv, r32, r32p);
+            fourstep_twiddle4(x, c, bitrev_n(m, LOGN), smA[m], rowB, p);
         }
         *reinterpret_cast<uint4*>(P.out + job * P.job_stride + prime_off + g) = x;
     }

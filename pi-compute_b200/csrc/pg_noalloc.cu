@@ -8,8 +8,9 @@
 // device arrays of fixed size:
 //   g_noalloc_scratch  residues of both operands for transforms up to 2^15 points plus the
 //                      carry look-back words: 786,688 bytes;
-//   g_noalloc_tables   the twiddle tables (same layout as DeviceTables): 1,179,648 bytes.
-// Every GPU that loads libpigpu.so holds these ~1.9 MB until the process exits.
+//   g_noalloc_tables   the twiddle tables (same layout as DeviceTables, row power tables
+//                      for four-step blocks of 2^14 and 2^15 points only): 1,966,080 bytes.
+// Every GPU that loads libpigpu.so holds these ~2.8 MB until the process exits.
 //
 // Set-up: the first call on a device (with that device current) looks up the arrays'
 // device addresses with cudaGetSymbolAddress and fills the tables with a kernel on the
@@ -35,7 +36,8 @@ constexpr size_t kResWords = (size_t)pg::kNumPrimes << kNoAllocLogL;  // per ope
 constexpr size_t kSyncWords = 64;           // error, ticket, look-back status (<= 8 CRT blocks used)
 constexpr size_t kScratchWords = 2 * kResWords + kSyncWords;
 constexpr size_t kTableEnt = 1u << pg::kFsLog;
-constexpr size_t kTableWords = 3 * 2 * pg::kNumPrimes * kTableEnt;
+constexpr int kRowTypes = kNoAllocLogL - pg::kRowLogMin + 1;  // four-step blocks of 2^14, 2^15 points
+constexpr size_t kTableWords = (3 + kRowTypes) * 2 * pg::kNumPrimes * kTableEnt;
 
 static_assert(kTableEnt == (1u << (pg::kStageLog - 1)), "stage and four-step tables share one length");
 
@@ -68,7 +70,8 @@ __device__ uint32_t dev_pow_mod(uint32_t b, uint64_t e, uint32_t p) {
 }
 
 // Fills the table array in the layout of DeviceTables::build:
-// [type: stage, fs_lo, fs_hi][dir][prime][kTableEnt]; roots[dir][prime] = w_{2^26}^(+-1).
+// [type: stage, fs_lo, fs_hi, row 2^14, row 2^15][dir][prime][kTableEnt];
+// roots[dir][prime] = w_{2^26}^(+-1).
 __global__ void fill_tables_kernel(uint2* t, uint32_t r0f, uint32_t r1f, uint32_t r2f, uint32_t r0i, uint32_t r1i,
                                    uint32_t r2i) {
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -85,8 +88,10 @@ __global__ void fill_tables_kernel(uint2* t, uint32_t r0f, uint32_t r1f, uint32_
         e = (uint64_t)pg::stage_exponent(i) << (pg::kMaxLogL - pg::kStageLog);  // entry h + x = w_{2h}^x
     else if (type == 1)
         e = i;                                                // w_{2^26}^i
-    else
+    else if (type == 2)
         e = (uint64_t)i << pg::kFsLog;                        // w_{2^26}^(2^13 i)
+    else
+        e = (uint64_t)i << (pg::kMaxLogL - (pg::kRowLogMin + type - 3));  // w_{2^n}^i
     const uint32_t w = dev_pow_mod(root, e, p);
     t[idx] = make_uint2(w, (uint32_t)(((uint64_t)w << 32) / p));
 }
@@ -114,6 +119,7 @@ pg_status setup_device(int dev, cudaStream_t st) {
             d.tw.fs_lo[dir][j] = tables + ((1 * 2 + dir) * pg::kNumPrimes + j) * kTableEnt;
             d.tw.fs_hi[dir][j] = tables + ((2 * 2 + dir) * pg::kNumPrimes + j) * kTableEnt;
         }
+    d.tw.row = tables + (size_t)3 * 2 * pg::kNumPrimes * kTableEnt;
     d.scratch = scratch;
     d.ready = true;
     return PG_OK;

@@ -26,16 +26,39 @@ __host__ __device__ inline uint32_t stage_exponent(uint32_t i) {
     return (i - (1u << k)) << (kStageLog - 1 - k);
 }
 
+constexpr int kRowLogMin = 14;  // row power tables exist for four-step blocks of 2^14 .. 2^26 points
+constexpr int kRowTables = kMaxLogL - kRowLogMin + 1;
+
 struct TwiddleTables {
     // (w, w') Shoup pairs, [dir][prime]; dir 0 = forward (w), 1 = inverse (w^-1).
     const uint2* stage[2][kNumPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), 2^13 entries
     const uint2* fs_lo[2][kNumPrimes];  // w_{2^26}^j,           j < 2^13
     const uint2* fs_hi[2][kNumPrimes];  // w_{2^26}^(2^13 * i),  i < 2^13
+    // Row powers of the four-step blocks: for a block of 2^n points (n >= kRowLogMin), table
+    // ((n - kRowLogMin) * 2 + dir) * kNumPrimes + prime holds w_{2^n}^e for e < 2^13.
+    const uint2* row;
 };
+
+__host__ __device__ inline const uint2* row_table(const TwiddleTables& T, int logNp, int dir, int prime) {
+    return T.row + ((size_t)((logNp - kRowLogMin) * 2 + dir) * kNumPrimes + prime) * (1u << kFsLog);
+}
 
 enum class Layout : int { Strided = 0, Contig = 1 };
 enum class Source : int { Residues = 0, Limbs = 1 };
 enum class Fuse : int { None = 0, MulInverse = 1, SqrInverse = 2 };
+
+// Table-driven batch (merge == 2): operand j of a pass launch comes from src[j], CRT job j
+// writes dst[j].
+struct SrcEntry {
+    const uint32_t* words;  // operand as 32-bit words (device)
+    uint64_t ncoef;         // valid words
+};
+struct DstEntry {
+    uint32_t* out;          // output words (device)
+    uint64_t nwords;        // words written
+    uint32_t centred;       // 1: coefficients are signed (lift to (-P/2, P/2])
+    uint32_t pad;
+};
 
 // Child level of a merge batch: node i's P/Q/R limbs at X[k] + i * cap[k] (k = 0, 1, 2),
 // lengths (limbs) at len[3 * i + k].
@@ -48,6 +71,8 @@ struct MergeSrc {
 struct PassParams {
     uint32_t* data;          // residues of job 0: prime i at data + i*L; job j at data + j*job_stride
     const uint32_t* other;   // Fuse::MulInverse: fully transformed other operand (same layout)
+    uint64_t other_stride;   // residue words between jobs' `other` arrays (0: one operand shared by all)
+    uint64_t words_stride;   // Source::Limbs, merge == 0: 32-bit words between jobs' operands
     uint32_t* out;           // where tiles are written (== data for in-place passes)
     const uint32_t* words;   // Source::Limbs, single job: operand as 32-bit words (little-endian)
     uint64_t ncoef;          // Source::Limbs, single job: number of valid 32-bit coefficients
@@ -57,8 +82,10 @@ struct PassParams {
     int logL;
     int logS;                // log2 of the element stride of this pass (0 for Contig)
     int logNp;               // log2 of the block size N' = N * S (four-step twiddle)
-    int merge;               // Source::Limbs resolved per job from `ms` (job = 6*merge + operand)
+    int merge;               // Source::Limbs per job: 0 words + job*words_stride, 1 from `ms`
+                             // (job = 6*merge + operand), 2 from src[job]
     MergeSrc ms;
+    const SrcEntry* src;
 };
 
 struct CrtConsts {
@@ -85,6 +112,9 @@ struct CrtParams {
     uint32_t* error;         // set non-zero on a look-back timeout or a final carry
     uint64_t blocks_per_job; // grid = jobs * blocks_per_job
     CrtConsts k;
+    // plain batch (merge == 0): job i's residues at res + i * res_stride, its words at
+    // out + i * out_stride, its length (if dlen) at dlen[i]; every job has `nwords` words.
+    uint64_t out_stride;
     // merge batch: job = 3 * merge + {P, Q, R}; residues of merge m, output k (0..2) at
     // res + (6m + 3 + k) * res_stride; the words go to dst[k] + m * dcap[k] (limbs), the
     // length to dlen[3m + k]; node ranges of the level come from [a0, b0) and depth.
@@ -95,6 +125,8 @@ struct CrtParams {
     uint32_t* dlen;
     uint64_t a0, b0;
     int depth;
+    // table batch (merge == 2): job i's residues at res + i * res_stride, output per dtab[i]
+    const DstEntry* dtab;
 };
 
 constexpr int kCrtThreads = 256;
