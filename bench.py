@@ -356,6 +356,90 @@ def run_mul(args):
                                      "nb": n}, "roofline": roof, "gpu_launches": roof["launches"]}), flush=True)
 
 
+def run_batch_workload(args):
+    """Workload "batch": a synthetic batch of products with sizes drawn log-uniform in
+    [2^6, 2^18] limbs from one seed, run as one pg_mul_batch call and, for comparison, as the
+    same products issued one pg_mul_device call at a time (the per-call drop-in's pattern).
+    Metric: sum of B_mul = 400*(na+nb) bytes over the batch / batch time."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    eng = pkg.Engine(local)
+    lib = eng.lib
+    dev = f"cuda:{local}"
+    rng = np.random.default_rng(3)
+    nj = args.batch_jobs
+    na = np.maximum(1, (2.0 ** rng.uniform(6, 18, nj)).astype(np.int64))
+    nb = np.maximum(1, (2.0 ** rng.uniform(6, 18, nj)).astype(np.int64))
+    pad = lambda x: (x + 1) // 2 * 2  # keep every operand 16-byte aligned
+    oa = np.concatenate([[0], np.cumsum(pad(na))])
+    ob = np.concatenate([[0], np.cumsum(pad(nb))])
+    oo = np.concatenate([[0], np.cumsum(pad(na + nb))])
+    g = torch.Generator(device=dev).manual_seed(5)
+    A = torch.randint(-2**63, 2**63 - 1, (int(oa[-1]),), dtype=torch.int64, device=dev, generator=g)
+    B = torch.randint(-2**63, 2**63 - 1, (int(ob[-1]),), dtype=torch.int64, device=dev, generator=g)
+    O1 = torch.zeros(int(oo[-1]), dtype=torch.int64, device=dev)
+    O2 = torch.zeros_like(O1)
+    a0, b0, o1, o2 = A.data_ptr(), B.data_ptr(), O1.data_ptr(), O2.data_ptr()
+    jobs = (pkg.PgJob * nj)()
+    for i in range(nj):
+        jobs[i] = pkg.PgJob(a0 + 8 * int(oa[i]), int(na[i]), b0 + 8 * int(ob[i]), int(nb[i]), None, 0, None, 0, 0,
+                            o1 + 8 * int(oo[i]), int(na[i] + nb[i]))
+    stream = torch.cuda.ExternalStream(lib.pg_stream(eng.ctx), device=dev)
+
+    def batch():
+        st = lib.pg_mul_batch(eng.ctx, jobs, nj)
+        if st != 0:
+            raise pkg.PgError(st, eng.last_error())
+
+    def per_call():
+        for i in range(nj):
+            st = lib.pg_mul_device(eng.ctx, a0 + 8 * int(oa[i]), int(na[i]), b0 + 8 * int(ob[i]), int(nb[i]),
+                                   o2 + 8 * int(oo[i]))
+            if st != 0:
+                raise pkg.PgError(st, eng.last_error())
+        if lib.pg_sync(eng.ctx) != 0:
+            raise pkg.PgError(-1, eng.last_error())
+
+    def timed(fn, steps):
+        for _ in range(max(3, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        l0 = lib.pg_launch_count(eng.ctx)
+        ev[0].record(stream)
+        for i in range(steps):
+            fn()
+            ev[i + 1].record(stream)
+        torch.cuda.synchronize()
+        return statistics.median([ev[i].elapsed_time(ev[i + 1]) for i in range(steps)]), \
+            (lib.pg_launch_count(eng.ctx) - l0) // steps
+
+    ms_b, launches_b = timed(batch, args.steps)
+    ms_p, launches_p = timed(per_call, args.steps)
+    same = bool(torch.equal(O1, O2))
+    eng.close()
+    bytes_alg = 400.0 * float(np.sum(na + nb))
+    gbs = bytes_alg / (ms_b / 1e3) / 1e9
+    peaks = measured_peaks()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "batched products: sum B_mul / batch time", "value": round(gbs, 2), "unit": "GB/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(ms_b, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod p (NTT), u64 limbs",
+            "data": "synthetic",
+            "config": {"workload": f"{nj} products, na and nb log-uniform in [2^6, 2^18] limbs (seed 3)",
+                       "sum_limbs": int(np.sum(na + nb))},
+            "per_call": {"ms": round(ms_p, 4), "launches": int(launches_p),
+                         "value": round(bytes_alg / (ms_p / 1e3) / 1e9, 2)},
+            "speedup_vs_per_call": round(ms_p / ms_b, 3), "results_identical": same,
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 2), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                         "frac": round(gbs / peaks["hbm_gbs"], 4), "traffic": None, "peak_source": peaks["source"]},
+            "gpu_launches": int(launches_b)}), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -367,12 +451,15 @@ def main():
     ap.add_argument("--logn", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="pi", choices=["pi", "mul"])
+    ap.add_argument("--workload", default="pi", choices=["pi", "mul", "batch"])
+    ap.add_argument("--batch-jobs", type=int, default=4096)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "mul":
         run_mul(args)
+    elif args.workload == "batch":
+        run_batch_workload(args)
     else:
         run_b200(args)
 

@@ -103,6 +103,62 @@ uint64_t pg_launch_count(const pg_ctx* ctx);
 pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R, size_t cap,
                 size_t* len, int* sign);
 
+/* ---- Library-owned device buffers (device-resident operands between calls). A buffer holds
+ * `cap` limbs on the context's device and a length; upload sets the length and zero-fills
+ * the rest, download copies `len` limbs and reports the length without leading zeros.
+ * The reference keeps every operand in host mpz_t and copies it per call
+ * (gpu_ntt_multiplier.cpp:74-142, int_ntt.cu:322-340); these handles let callers keep
+ * operands in HBM across products instead. */
+typedef struct pg_buf pg_buf;
+pg_status pg_buf_alloc(pg_ctx* ctx, size_t cap, pg_buf** out);
+void pg_buf_free(pg_ctx* ctx, pg_buf* buf);
+pg_status pg_buf_upload(pg_ctx* ctx, pg_buf* buf, const uint64_t* src, size_t n);
+pg_status pg_buf_download(pg_ctx* ctx, const pg_buf* buf, uint64_t* dst, size_t dst_cap, size_t* len);
+uint64_t* pg_buf_device(pg_buf* buf);       /* device address (16-byte aligned) */
+size_t pg_buf_len(const pg_buf* buf);
+size_t pg_buf_capacity(const pg_buf* buf);
+pg_status pg_buf_set_len(pg_buf* buf, size_t n);
+
+/* ---- Batched products. Job i computes, on device-resident magnitudes (16-byte aligned),
+ *     acc == 0:  out = a * b                     (b == NULL: a * a)
+ *     acc == +1: out = a * b + c * d             (d == NULL: c * c)
+ *     acc == -1: out = a * b - c * d             (the result must not be negative)
+ * and writes exactly max(na + nb, nc + nd) (+1 when acc == +1) limbs to out (out_cap at
+ * least that). The accumulating forms combine the two products in the transform domain, as
+ * the binary-splitting merge R = Qr*Rl + Pl*Rr needs (binary_splitting.cpp:184-200, where the
+ * reference issues two Multiplier calls and an mpz_add); their exactness bound asks
+ * min(na, nb) + min(nc, nd) <= 2^24 (PG_ERR_TOO_LARGE otherwise).
+ * Jobs are grouped by transform length and every group runs as one launch per pass over all of
+ * its jobs. Outputs must not overlap each other or any operand. The call returns when every job
+ * is complete; a negative acc == -1 result returns PG_ERR_BAD_ARG. Replaces the per-call
+ * Multiplier::multiply sequence of a tree level (binary_splitting.cpp:183-238). */
+typedef struct pg_job {
+    const uint64_t* a;
+    size_t na;
+    const uint64_t* b;
+    size_t nb;
+    const uint64_t* c;
+    size_t nc;
+    const uint64_t* d;
+    size_t nd;
+    int acc;
+    uint64_t* out;
+    size_t out_cap;
+} pg_job;
+pg_status pg_mul_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs);
+
+/* ---- Autotuner of the transform's pass split. pg_tune times, for every transform length 2^l
+ * with lo <= l <= hi (6 <= lo <= hi <= 26), each valid split into one to three passes on a
+ * balanced product of that length, checks that it reproduces the built-in split's product
+ * word for word, and makes the fastest the context's choice; best_us (if not NULL, hi-lo+1
+ * entries) receives the winning times in microseconds. pg_tune_save writes the context's
+ * choices as text ("logL npass logN0 logN1 logN2" per line), pg_tune_load reads such a file
+ * (every split is validated). No counterpart in the reference, whose engines use one fixed
+ * schedule per length (int_ntt.cu:57-104, ntt_engine.cu:76-107). */
+pg_status pg_tune(pg_ctx* ctx, int lo, int hi, double* best_us);
+pg_status pg_tune_save(pg_ctx* ctx, const char* path);
+pg_status pg_tune_load(pg_ctx* ctx, const char* path);
+
 /* d_out = d_a * d_b without allocating any device memory. This entry point has no
  * counterpart in the reference.
  *

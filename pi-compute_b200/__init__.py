@@ -44,6 +44,13 @@ class PgError(RuntimeError):
 _lib: Optional[ctypes.CDLL] = None
 
 
+class PgJob(ctypes.Structure):
+    """struct pg_job of include/pi_b200.h (device addresses and limb counts)."""
+    _fields_ = [("a", ctypes.c_void_p), ("na", ctypes.c_size_t), ("b", ctypes.c_void_p), ("nb", ctypes.c_size_t),
+                ("c", ctypes.c_void_p), ("nc", ctypes.c_size_t), ("d", ctypes.c_void_p), ("nd", ctypes.c_size_t),
+                ("acc", ctypes.c_int), ("out", ctypes.c_void_p), ("out_cap", ctypes.c_size_t)]
+
+
 def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     """Load libpigpu.so and declare the C ABI signatures. Raises if the library is missing."""
     global _lib
@@ -76,6 +83,31 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     lib.pg_stream.restype = ctypes.c_void_p
     lib.pg_launch_count.argtypes = [ctypes.c_void_p]
     lib.pg_launch_count.restype = ctypes.c_uint64
+    vp, sz = ctypes.c_void_p, ctypes.c_size_t
+    lib.pg_buf_alloc.argtypes = [vp, sz, ctypes.POINTER(vp)]
+    lib.pg_buf_alloc.restype = ctypes.c_int
+    lib.pg_buf_free.argtypes = [vp, vp]
+    lib.pg_buf_free.restype = None
+    lib.pg_buf_upload.argtypes = [vp, vp, _u64p, sz]
+    lib.pg_buf_upload.restype = ctypes.c_int
+    lib.pg_buf_download.argtypes = [vp, vp, _u64p, sz, _sizep]
+    lib.pg_buf_download.restype = ctypes.c_int
+    lib.pg_buf_device.argtypes = [vp]
+    lib.pg_buf_device.restype = vp
+    lib.pg_buf_len.argtypes = [vp]
+    lib.pg_buf_len.restype = sz
+    lib.pg_buf_capacity.argtypes = [vp]
+    lib.pg_buf_capacity.restype = sz
+    lib.pg_buf_set_len.argtypes = [vp, sz]
+    lib.pg_buf_set_len.restype = ctypes.c_int
+    lib.pg_mul_batch.argtypes = [vp, ctypes.POINTER(PgJob), sz]
+    lib.pg_mul_batch.restype = ctypes.c_int
+    lib.pg_tune.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    lib.pg_tune.restype = ctypes.c_int
+    lib.pg_tune_save.argtypes = [vp, ctypes.c_char_p]
+    lib.pg_tune_save.restype = ctypes.c_int
+    lib.pg_tune_load.argtypes = [vp, ctypes.c_char_p]
+    lib.pg_tune_load.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -188,3 +220,91 @@ class Engine:
 
     def sqr(self, a: int) -> int:
         return limbs_to_int(self.sqr_limbs(int_to_limbs(a)))
+
+    # -------------------------------------------------- autotuner
+    def tune(self, lo: int, hi: int) -> list:
+        """Run pg_tune over transform lengths 2^lo .. 2^hi; returns the winning times (us)."""
+        out = (ctypes.c_double * (hi - lo + 1))()
+        self._check(self.lib.pg_tune(self.ctx, lo, hi, out))
+        return list(out)
+
+    def tune_save(self, path: str) -> None:
+        self._check(self.lib.pg_tune_save(self.ctx, path.encode()))
+
+    def tune_load(self, path: str) -> None:
+        self._check(self.lib.pg_tune_load(self.ctx, path.encode()))
+
+    # -------------------------------------------------- device buffers and batches
+    def buffer(self, limbs) -> "DeviceBuffer":
+        """A pg_buf holding `limbs` (numpy uint64 array or int), capacity at least 1 limb."""
+        a = limbs if isinstance(limbs, np.ndarray) else int_to_limbs(limbs)
+        a = np.ascontiguousarray(a, dtype=np.uint64)
+        return DeviceBuffer(self, max(len(a), 1), a)
+
+    def mul_batch(self, jobs: list) -> list:
+        """Products of a list of jobs through pg_mul_batch. Each job is (a, b) for a*b, (a, None)
+        for a*a, or (a, b, c, d, acc) for a*b + acc*c*d (d may be None for c*c); operands are ints
+        (magnitudes) or limb arrays. Returns the results as Python ints."""
+        keep, cj, outs = [], [], []
+        for j in jobs:
+            a, b = j[0], j[1]
+            c, d, acc = (j[2], j[3], j[4]) if len(j) > 2 else (None, None, 0)
+            ba = self.buffer(a)
+            bb = self.buffer(b) if b is not None else None
+            bc = self.buffer(c) if acc else None
+            bd = self.buffer(d) if acc and d is not None else None
+            na, nb = ba.len, (bb.len if bb else ba.len)
+            nc = bc.len if bc else 0
+            nd = (bd.len if bd else nc) if acc else 0
+            top = max(na + nb, nc + nd) + (1 if acc > 0 else 0)
+            bo = DeviceBuffer(self, max(top, 1), None)
+            keep += [x for x in (ba, bb, bc, bd, bo) if x is not None]
+            pj = PgJob(ba.ptr, na, bb.ptr if bb else None, nb, bc.ptr if bc else None, nc,
+                       bd.ptr if bd else None, nd if bd else 0, acc, bo.ptr, bo.cap)
+            if acc and bd is None:
+                pj.nd = 0
+            cj.append(pj)
+            outs.append((bo, top))
+        arr = (PgJob * len(cj))(*cj)
+        self._check(self.lib.pg_mul_batch(self.ctx, arr, len(cj)))
+        res = []
+        for bo, top in outs:
+            bo.set_len(top)
+            res.append(limbs_to_int(bo.download()))
+        for x in keep:
+            x.free()
+        return res
+
+
+class DeviceBuffer:
+    """A pg_buf: `cap` limbs of device memory owned by the library, with a length."""
+
+    def __init__(self, eng: Engine, cap: int, data: Optional[np.ndarray]):
+        self.eng, self.cap = eng, cap
+        h = ctypes.c_void_p()
+        eng._check(eng.lib.pg_buf_alloc(eng.ctx, cap, ctypes.byref(h)))
+        self.h = h
+        if data is not None and len(data):
+            eng._check(eng.lib.pg_buf_upload(eng.ctx, h, _ptr(data), len(data)))
+
+    @property
+    def ptr(self) -> int:
+        return self.eng.lib.pg_buf_device(self.h)
+
+    @property
+    def len(self) -> int:
+        return self.eng.lib.pg_buf_len(self.h)
+
+    def set_len(self, n: int) -> None:
+        self.eng._check(self.eng.lib.pg_buf_set_len(self.h, n))
+
+    def download(self) -> np.ndarray:
+        out = np.zeros(max(self.len, 1), dtype=np.uint64)
+        n = ctypes.c_size_t(0)
+        self.eng._check(self.eng.lib.pg_buf_download(self.eng.ctx, self.h, _ptr(out), len(out), ctypes.byref(n)))
+        return out[: n.value]
+
+    def free(self) -> None:
+        if self.h:
+            self.eng.lib.pg_buf_free(self.eng.ctx, self.h)
+            self.h = None

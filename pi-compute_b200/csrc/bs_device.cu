@@ -460,7 +460,7 @@ struct DeviceBS {
 
     cudaError_t launch_ntt_level(const DepthPlan& P, const DepthPlan& C, const LevelView& in, const LevelView& out,
                                  uint64_t a0, uint64_t b0, int depth) {
-        const Plan plan = make_plan(P.logL);
+        const Plan plan = T->plan(P.logL);
         const uint64_t L = 1ull << P.logL;
         const uint64_t M = P.nodes;
         const uint64_t stride = 3 * L;

@@ -28,6 +28,16 @@ void set_pass(PassParams& p, const Plan& plan, int i);
 struct DeviceTables {
     uint2* base = nullptr;  // one allocation holding every table
     TwiddleTables tw{};
+    // Pass splits chosen by the autotuner (pg_tune / pg_tune_load): tuned[logL] = {npass,
+    // logN[0..2]}, npass == 0 meaning the built-in make_plan split.
+    int8_t tuned[kMaxLogL + 1][4] = {};
+    Plan plan(int logL) const {
+        if (logL >= 0 && logL <= kMaxLogL && tuned[logL][0] > 0) {
+            const int n[3] = {tuned[logL][1], tuned[logL][2], tuned[logL][3]};
+            return plan_from(logL, tuned[logL][0], n);
+        }
+        return make_plan(logL);
+    }
     cudaError_t build(int device);
     void release();
 };

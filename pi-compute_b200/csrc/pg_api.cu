@@ -16,6 +16,9 @@ namespace pg {
 struct DeviceBS;
 DeviceBS* bs_state_new();
 void bs_state_delete(DeviceBS*);
+struct BatchWork;
+BatchWork* batch_state_new();
+void batch_state_delete(BatchWork*);
 }  // namespace pg
 
 struct pg_ctx {
@@ -27,6 +30,7 @@ struct pg_ctx {
     std::string last_error;
     uint64_t launches = 0;
     pg::DeviceBS* bs = nullptr;  // binary-splitting buffers, kept for the next pg_bs call
+    pg::BatchWork* batch = nullptr;  // pg_mul_batch buffers, kept for the next batch
 };
 
 namespace {
@@ -127,6 +131,8 @@ pg_status host_product(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* 
 // Accessors used by the binary-splitting module (bs_device.cu).
 namespace pg {
 const DeviceTables& ctx_tables(pg_ctx* c) { return c->tables; }
+DeviceTables& ctx_tables_mut(pg_ctx* c) { return c->tables; }
+Workspace& ctx_workspace(pg_ctx* c) { return c->ws; }
 cudaStream_t ctx_stream(pg_ctx* c) { return c->stream; }
 std::mutex& ctx_mutex(pg_ctx* c) { return c->mu; }
 uint64_t* ctx_launches(pg_ctx* c) { return &c->launches; }
@@ -135,6 +141,10 @@ int ctx_device(pg_ctx* c) { return c->device; }
 DeviceBS* ctx_bs(pg_ctx* c) {
     if (!c->bs) c->bs = bs_state_new();
     return c->bs;
+}
+BatchWork* ctx_batch(pg_ctx* c) {
+    if (!c->batch) c->batch = batch_state_new();
+    return c->batch;
 }
 }  // namespace pg
 
@@ -173,6 +183,7 @@ void pg_destroy(pg_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->bs) pg::bs_state_delete(c->bs);
+    if (c->batch) pg::batch_state_delete(c->batch);
     c->ws.release();
     c->tables.release();
     if (c->stream) cudaStreamDestroy(c->stream);

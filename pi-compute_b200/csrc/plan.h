@@ -46,6 +46,40 @@ inline Plan make_plan(int logL) {
     return p;
 }
 
+// Whether a pass split can run: one contiguous last pass of 2^6..2^13 points, strided passes of
+// 2^5..2^10 points whose tiles (2^(13 - N) columns) fit in their stride, every strided pass's
+// four-step block at least 2^14 points (the row power tables' range), lengths summing to logL.
+inline bool plan_valid(const Plan& p) {
+    if (p.npass < 1 || p.npass > 3) return false;
+    int sum = 0;
+    for (int i = 0; i < p.npass; ++i) sum += p.logN[i];
+    if (sum != p.logL) return false;
+    const int last = p.npass - 1;
+    if (p.logN[last] < kMinLogL || p.logN[last] > kTileLog) return false;
+    int s = p.logL;
+    for (int i = 0; i < last; ++i) {
+        s -= p.logN[i];  // stride of pass i
+        if (p.logN[i] < 5 || p.logN[i] > kMaxStridedLog) return false;
+        if (s < kTileLog - p.logN[i]) return false;     // C = 2^(13 - N) columns <= S
+        if (p.logN[i] + s < 14) return false;           // four-step block >= 2^14
+    }
+    return true;
+}
+
+// Plan with the given pass lengths (strides filled in).
+inline Plan plan_from(int logL, int npass, const int* n) {
+    Plan p;
+    p.logL = logL;
+    p.npass = npass;
+    int s = logL;
+    for (int i = 0; i < npass; ++i) {
+        p.logN[i] = n[i];
+        s -= n[i];
+        p.logS[i] = s;
+    }
+    return p;
+}
+
 inline int ceil_log2(uint64_t x) {
     int l = 0;
     while ((1ull << l) < x) ++l;

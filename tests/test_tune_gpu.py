@@ -1,0 +1,45 @@
+"""GPU tests of the pass-split autotuner (pg_tune, pg_tune_save, pg_tune_load).
+
+A tuned context must produce products identical to the oracle (libgmp's mpz_mul) at every
+transform length it tuned; files with invalid splits are rejected.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from helpers import oracle, pkg
+
+pytestmark = pytest.mark.gpu
+
+
+def test_tune_save_load_and_products(tmp_path):
+    path = str(tmp_path / "splits.txt")
+    with pkg.Engine(0) as eng:
+        times = eng.tune(10, 21)
+        assert len(times) == 12 and all(t > 0 for t in times)
+        eng.tune_save(path)
+    lines = [l.split() for l in open(path) if not l.startswith("#")]
+    assert [int(l[0]) for l in lines] == list(range(10, 22))
+    for l in lines:
+        logl, npass, *n = map(int, l)
+        assert sum(n[:npass]) == logl
+    with pkg.Engine(0) as eng:
+        eng.tune_load(path)
+        for logl in range(10, 22):
+            n = 1 << (logl - 2)
+            for na, nb in ((n, n), (n + n // 2 - 3, n // 2 + 1)):
+                a, b = pkg.random_operand(na, 7 * logl), pkg.random_operand(nb, 11 * logl)
+                assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b)), (logl, na, nb)
+
+
+@pytest.mark.parametrize("text", ["14 2 7 8 0\n", "20 2 4 16 0\n", "26 1 26 0 0\n", "x\n", "14 4 5 5 4\n"])
+def test_tune_load_rejects_invalid(tmp_path, text):
+    path = str(tmp_path / "bad.txt")
+    open(path, "w").write(text)
+    with pkg.Engine(0) as eng:
+        with pytest.raises(pkg.PgError) as ei:
+            eng.tune_load(path)
+        assert ei.value.status == pkg.PG_ERR_BAD_ARG
+        a, b = pkg.random_operand(5000, 1), pkg.random_operand(4000, 2)
+        assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b))
