@@ -147,6 +147,32 @@ typedef struct pg_job {
 } pg_job;
 pg_status pg_mul_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs);
 
+/* ---- Device-resident finish of a pi computation. Every operand stays in HBM; products run
+ * on the transform above, additions, shifts and comparisons on carry-chain kernels.
+ *
+ * pg_recip_floor: z = floor(2^(2k) / r), k = bit length of r > 0 (Newton iteration at doubling
+ *   precision with an exact final correction). The reference divides with mpf_div
+ *   (src/arithmetic/newton_divider.cpp:13-25); this is its quotient core, exact to the last
+ *   unit. z needs k/64 + 2 limbs.
+ * pg_sqrt_scaled: out = floor(sqrt(a) * 2^s) for a >= 1 (Newton on the inverse
+ *   square root, exact correction). Replaces mpf_sqrt (newton_divider.cpp:27-74).
+ * pg_to_decimal: the ndigits decimal digits of x (x < 10^ndigits, leading zeros written) into
+ *   out[0 .. ndigits), no terminator. Divide-and-conquer by 10^(2^j) batched per level on the
+ *   device. Replaces BaseConverter / mpz_get_str (src/io/base_converter.cpp:48-147, 201-246).
+ * pg_pi_finish: "3." followed by `digits` digits of pi (digits + 2 characters, no terminator)
+ *   from the series root Q, R = Q(0, N), R(0, N) (host magnitudes, both positive).
+ *   Replaces PiEngine::compute's final section (src/engine/pi_engine.cpp:432-491).
+ * pg_pi: the whole computation on one device: level-batched binary splitting over the
+ *   reference's term count, then pg_pi_finish's steps, all in HBM. out receives digits + 2
+ *   characters; seconds (if not NULL, 4 entries) receives splitting, final formula,
+ *   conversion and total wall time. */
+pg_status pg_recip_floor(pg_ctx* ctx, const uint64_t* r, size_t nr, uint64_t* z, size_t zcap, size_t* zlen);
+pg_status pg_sqrt_scaled(pg_ctx* ctx, uint64_t a, size_t s, uint64_t* out, size_t cap, size_t* len);
+pg_status pg_to_decimal(pg_ctx* ctx, const uint64_t* x, size_t nx, size_t ndigits, char* out);
+pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t* r, size_t nr, size_t digits,
+                       char* out);
+pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds);
+
 /* ---- Autotuner of the transform's pass split. pg_tune times, for every transform length 2^l
  * with lo <= l <= hi (6 <= lo <= hi <= 26), each valid split into one to three passes on a
  * balanced product of that length, checks that it reproduces the built-in split's product

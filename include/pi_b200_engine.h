@@ -20,10 +20,12 @@ extern "C" {
 /* Binary-splitting modes. */
 #define PIB_MODE_GMP 0        /* products through GMP's mpz_mul (the reference's GmpMultiplier) */
 #define PIB_MODE_PER_CALL 1   /* products >= threshold limbs through B200Multiplier, one call at a time */
-#define PIB_MODE_BATCHED 2    /* level-batched, device-resident binary splitting; Newton finish and
-                                divide-and-conquer decimal conversion on B200 products */
+#define PIB_MODE_BATCHED 2    /* the whole computation on the device (pg_pi): level-batched binary
+                                splitting, Newton finish and batched decimal conversion in HBM */
 #define PIB_MODE_GMP_NEWTON 3 /* GMP products everywhere, with the Newton finish and conversion
                                 (the same integer algorithms as PIB_MODE_BATCHED, on the CPU) */
+#define PIB_MODE_BATCHED_HOST_FINISH 4 /* level-batched splitting on the device, Newton finish and
+                                conversion on the host with B200 products */
 
 /* Compute pi to `digits` decimals; writes "3." + digits (no terminator) into out, which must
  * have room for digits + 2 bytes. threads = host threads issuing per-call products and

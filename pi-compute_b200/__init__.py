@@ -102,6 +102,16 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     lib.pg_buf_set_len.restype = ctypes.c_int
     lib.pg_mul_batch.argtypes = [vp, ctypes.POINTER(PgJob), sz]
     lib.pg_mul_batch.restype = ctypes.c_int
+    lib.pg_recip_floor.argtypes = [vp, _u64p, sz, _u64p, sz, _sizep]
+    lib.pg_recip_floor.restype = ctypes.c_int
+    lib.pg_sqrt_scaled.argtypes = [vp, ctypes.c_uint64, sz, _u64p, sz, _sizep]
+    lib.pg_sqrt_scaled.restype = ctypes.c_int
+    lib.pg_to_decimal.argtypes = [vp, _u64p, sz, sz, ctypes.c_char_p]
+    lib.pg_to_decimal.restype = ctypes.c_int
+    lib.pg_pi_finish.argtypes = [vp, _u64p, sz, _u64p, sz, sz, ctypes.c_char_p]
+    lib.pg_pi_finish.restype = ctypes.c_int
+    lib.pg_pi.argtypes = [vp, sz, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+    lib.pg_pi.restype = ctypes.c_int
     lib.pg_tune.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
     lib.pg_tune.restype = ctypes.c_int
     lib.pg_tune_save.argtypes = [vp, ctypes.c_char_p]
@@ -220,6 +230,45 @@ class Engine:
 
     def sqr(self, a: int) -> int:
         return limbs_to_int(self.sqr_limbs(int_to_limbs(a)))
+
+    # -------------------------------------------------- device-resident finish
+    def recip_floor(self, r: int) -> int:
+        """floor(2^(2k) / r), k = r.bit_length() (pg_recip_floor)."""
+        a = int_to_limbs(r)
+        out = np.zeros(len(a) + 2, dtype=np.uint64)
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.pg_recip_floor(self.ctx, _ptr(a), len(a), _ptr(out), len(out), ctypes.byref(n)))
+        return limbs_to_int(out[: n.value])
+
+    def sqrt_scaled(self, a: int, s: int) -> int:
+        """floor(sqrt(a) * 2^s) (pg_sqrt_scaled)."""
+        out = np.zeros(s // 64 + 4, dtype=np.uint64)
+        n = ctypes.c_size_t(0)
+        self._check(self.lib.pg_sqrt_scaled(self.ctx, a, s, _ptr(out), len(out), ctypes.byref(n)))
+        return limbs_to_int(out[: n.value])
+
+    def to_decimal(self, x: int, ndigits: int) -> str:
+        """The ndigits decimal digits of x (leading zeros kept) (pg_to_decimal)."""
+        a = int_to_limbs(x)
+        buf = ctypes.create_string_buffer(max(ndigits, 1))
+        self._check(self.lib.pg_to_decimal(self.ctx, _ptr(a), len(a), ndigits, buf))
+        return buf.raw[:ndigits].decode()
+
+    def pi_finish(self, q: int, r: int, digits: int) -> str:
+        """"3." + digits of pi from the series root Q, R (pg_pi_finish)."""
+        qa, ra = int_to_limbs(q), int_to_limbs(r)
+        buf = ctypes.create_string_buffer(digits + 2)
+        self._check(self.lib.pg_pi_finish(self.ctx, _ptr(qa), len(qa), _ptr(ra), len(ra), digits, buf))
+        return buf.raw[: digits + 2].decode()
+
+    def pi(self, digits: int, seconds: Optional[list] = None) -> bytes:
+        """"3." + digits of pi computed entirely on the device (pg_pi)."""
+        buf = ctypes.create_string_buffer(digits + 2)
+        t = (ctypes.c_double * 4)()
+        self._check(self.lib.pg_pi(self.ctx, digits, buf, t))
+        if seconds is not None:
+            seconds[:] = list(t)
+        return buf.raw[: digits + 2]
 
     # -------------------------------------------------- autotuner
     def tune(self, lo: int, hi: int) -> list:

@@ -1,0 +1,778 @@
+// Device big-integer kernels (bigint.cuh) and the DevArith host wrapper (devnum.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+
+#include "bigint.cuh"
+#include "devnum.h"
+
+namespace pg {
+namespace {
+
+// ------------------------------------------------------------------ carry-chain sums
+template <AddForm F>
+__device__ __forceinline__ void add_fetch(const AddArgs& A, uint64_t job, uint64_t i, uint64_t& u, uint64_t& v) {
+    const uint64_t* x = A.x + job * A.sx;
+    if constexpr (F == AddForm::Plain) {
+        const uint64_t xi = i < A.nx ? x[i] : 0;
+        const uint64_t yi = (A.y && i < A.ny) ? A.y[job * A.sy + i] : 0;
+        u = xi ^ A.mx;
+        v = yi ^ A.my;
+    } else {
+        const uint64_t xi = i < A.nx ? x[i] : 0;
+        const uint64_t xp = (i >= 1 && i - 1 < A.nx) ? x[i - 1] : 0;
+        u = xi * A.c;
+        v = __umul64hi(xp, A.c);
+    }
+}
+
+// (g, p) of a range: bit 0 = carry out with carry-in 0, bit 1 = a carry-in passes through.
+__device__ __forceinline__ uint32_t gp_compose(uint32_t hi, uint32_t lo) {
+    const uint32_t g = (hi & 1u) | ((hi >> 1) & lo & 1u);
+    const uint32_t p = (hi >> 1) & (lo >> 1) & 1u;
+    return g | (p << 1);
+}
+__device__ __forceinline__ uint32_t gp_apply(uint32_t gp, uint32_t cin) { return (gp & 1u) | ((gp >> 1) & cin); }
+
+// Inclusive warp scan of (g, p) pairs, lane order = limb order.
+__device__ __forceinline__ uint32_t gp_warp_scan(uint32_t gp, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t lo = __shfl_up_sync(0xffffffffu, gp, off);
+        if (lane >= off) gp = gp_compose(gp, lo);
+    }
+    return gp;
+}
+
+// Short numbers: one warp per job, K = ceil(n / 32) <= 8 limbs per lane.
+template <AddForm F>
+__global__ void add_warp_kernel(AddArgs A) {
+    const uint64_t job = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (job >= A.njobs) return;
+    if (A.enable && !A.enable[job]) return;
+    const uint32_t K = (uint32_t)((A.n + 31) / 32);
+    const uint64_t base = (uint64_t)lane * K;
+    uint64_t s[kBigLimbs];
+    uint32_t gen = 0, gp = 2;  // empty range: passes carries
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        s[k] = 0;
+        if ((uint32_t)k < K && base + k < A.n) {
+            uint64_t u, v;
+            add_fetch<F>(A, job, base + k, u, v);
+            s[k] = u + v;
+            const uint32_t gk = s[k] < u ? 1u : 0u;
+            gen |= gk << k;
+            gp = gp_compose(gk | ((s[k] == ~0ull ? 1u : 0u) << 1), gp);
+        }
+    }
+    const uint32_t incl = gp_warp_scan(gp, lane);
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, incl, 1);
+    uint32_t carry = lane == 0 ? A.cin : gp_apply(prev, A.cin);
+    uint64_t* z = A.z + job * A.sz;
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        if ((uint32_t)k < K && base + k < A.n) {
+            const uint64_t r = s[k] + carry;
+            carry = ((gen >> k) & 1u) | (r < s[k] ? 1u : 0u);
+            z[base + k] = r;
+        }
+    }
+    if (lane == 31 && A.carry_out) A.carry_out[job] = carry;
+}
+
+// Long numbers, phase 1: (g, p) of each 2048-limb segment.
+template <AddForm F>
+__global__ void __launch_bounds__(kBigThreads) add_seg_kernel(AddArgs A, uint64_t nseg) {
+    __shared__ uint32_t s_w[kBigThreads / 32];
+    const uint64_t job = blockIdx.x / nseg, seg = blockIdx.x % nseg;
+    if (A.enable && !A.enable[job]) return;
+    const uint64_t base = seg * kBigSeg + (uint64_t)threadIdx.x * kBigLimbs;
+    uint32_t gp = 2;
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        if (base + k < A.n) {
+            uint64_t u, v;
+            add_fetch<F>(A, job, base + k, u, v);
+            const uint64_t s = u + v;
+            gp = gp_compose((s < u ? 1u : 0u) | ((s == ~0ull ? 1u : 0u) << 1), gp);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t incl = gp_warp_scan(gp, lane);
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 2;
+        for (int w = 0; w < kBigThreads / 32; ++w) t = gp_compose(s_w[w], t);
+        A.seg[blockIdx.x] = t;
+    }
+}
+
+// Phase 2: carry into every segment of a job (bit 2 of its word) and the job's carry out.
+__global__ void add_scan_kernel(AddArgs A, uint64_t nseg) {
+    const uint64_t job = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (job >= A.njobs) return;
+    if (A.enable && !A.enable[job]) return;
+    uint32_t carry = A.cin;
+    uint32_t* w = A.seg + job * nseg;
+    for (uint64_t s = 0; s < nseg; ++s) {
+        const uint32_t gp = w[s];
+        w[s] = gp | (carry << 2);
+        carry = gp_apply(gp, carry);
+    }
+    if (A.carry_out) A.carry_out[job] = carry;
+}
+
+// Phase 3: the sums with each segment's carry in.
+template <AddForm F>
+__global__ void __launch_bounds__(kBigThreads) add_final_kernel(AddArgs A, uint64_t nseg) {
+    __shared__ uint32_t s_w[kBigThreads / 32];
+    const uint64_t job = blockIdx.x / nseg, seg = blockIdx.x % nseg;
+    if (A.enable && !A.enable[job]) return;
+    const uint64_t base = seg * kBigSeg + (uint64_t)threadIdx.x * kBigLimbs;
+    uint64_t s[kBigLimbs];
+    uint32_t gen = 0, gp = 2;
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        s[k] = 0;
+        if (base + k < A.n) {
+            uint64_t u, v;
+            add_fetch<F>(A, job, base + k, u, v);
+            s[k] = u + v;
+            const uint32_t gk = s[k] < u ? 1u : 0u;
+            gen |= gk << k;
+            gp = gp_compose(gk | ((s[k] == ~0ull ? 1u : 0u) << 1), gp);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t incl = gp_warp_scan(gp, lane);
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    const uint32_t segcin = (A.seg[blockIdx.x] >> 2) & 1u;
+    // carry into this warp: segment carry-in through the earlier warps
+    uint32_t cw = segcin;
+    for (int w = 0; w < warp; ++w) cw = gp_apply(s_w[w], cw);
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, incl, 1);
+    uint32_t carry = lane == 0 ? cw : gp_apply(prev, cw);
+    uint64_t* z = A.z + job * A.sz;
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        if (base + k < A.n) {
+            const uint64_t r = s[k] + carry;
+            carry = ((gen >> k) & 1u) | (r < s[k] ? 1u : 0u);
+            z[base + k] = r;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ shifts, compares, lengths
+// z_j[0..n) = floor(x_j / 2^s) (x_j has nx limbs, z != x).
+__global__ void shr_kernel(const uint64_t* x, uint64_t sx, uint64_t nx, uint64_t* z, uint64_t sz, uint64_t n,
+                           uint64_t s, uint64_t njobs) {
+    const uint64_t w = s >> 6;
+    const uint32_t b = (uint32_t)(s & 63);
+    const uint64_t total = n * njobs;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t job = t / n, i = t - job * n;
+        const uint64_t* xj = x + job * sx;
+        const uint64_t lo = (i + w < nx) ? xj[i + w] : 0;
+        const uint64_t hi = (i + w + 1 < nx) ? xj[i + w + 1] : 0;
+        z[job * sz + i] = b ? ((lo >> b) | (hi << (64 - b))) : lo;
+    }
+}
+
+// z[0..n) = x * 2^s (single job, z != x).
+__global__ void shl_kernel(const uint64_t* x, uint64_t nx, uint64_t* z, uint64_t n, uint64_t s) {
+    const uint64_t w = s >> 6;
+    const uint32_t b = (uint32_t)(s & 63);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t lo = (i >= w + 1 && i - w - 1 < nx) ? x[i - w - 1] : 0;
+        const uint64_t hi = (i >= w && i - w < nx) ? x[i - w] : 0;
+        z[i] = b ? ((hi << b) | (lo >> (64 - b))) : hi;
+    }
+}
+
+// z[0..n) = x[0..n) masked to its low s bits (s <= 64 n).
+__global__ void lowbits_kernel(const uint64_t* x, uint64_t nx, uint64_t* z, uint64_t n, uint64_t s) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t v = i < nx ? x[i] : 0;
+        if (64 * (i + 1) > s) v = (64 * i >= s) ? 0 : (v & ((1ull << (s - 64 * i)) - 1));
+        z[i] = v;
+    }
+}
+
+// flag |= 1 if any of the low s bits of x is set.
+__global__ void sticky_kernel(const uint64_t* x, uint64_t nx, uint64_t s, uint32_t* flag) {
+    const uint64_t w = s >> 6;
+    const uint32_t b = (uint32_t)(s & 63);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= w && i < nx;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = x[i];
+        const bool hit = (i < w) ? (v != 0) : (b && (v & ((1ull << b) - 1)) != 0);
+        if (hit) atomicOr(flag, 1u);
+    }
+}
+
+// top[j] = 1 + index of the highest non-zero limb of x_j (0 if x_j == 0); top zeroed before.
+__global__ void top_kernel(const uint64_t* x, uint64_t sx, uint64_t n, uint64_t njobs, unsigned long long* top) {
+    const uint64_t total = n * njobs;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t job = t / n, i = t - job * n;
+        if (x[job * sx + i] != 0) atomicMax(top + job, (unsigned long long)(i + 1));
+    }
+}
+
+// diff[j] = 1 + highest index where x_j and y_j differ (0: equal); diff zeroed before.
+__global__ void diff_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n, uint64_t njobs,
+                            unsigned long long* diff) {
+    const uint64_t total = n * njobs;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t job = t / n, i = t - job * n;
+        if (x[job * sx + i] != y[job * sy + i]) atomicMax(diff + job, (unsigned long long)(i + 1));
+    }
+}
+
+// ge[j] = x_j >= y_j, from diff[j].
+__global__ void ge_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t njobs,
+                          const unsigned long long* diff, uint32_t* ge) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = diff[j];
+        ge[j] = (k == 0) ? 1u : (x[j * sx + k - 1] > y[j * sy + k - 1] ? 1u : 0u);
+    }
+}
+
+// Decimal digits of job j (< 10^digits) written most significant first to out[j * digits ...];
+// only characters at global positions [skip, total) are stored, shifted down by skip. *bad is
+// set when a job does not fit its digits or a digit below `skip` is not zero.
+__global__ void leaves_kernel(const uint64_t* x, uint64_t sx, uint64_t nl, uint64_t njobs, uint64_t digits, char* out,
+                              uint64_t skip, uint64_t total, uint32_t* bad) {
+    constexpr uint64_t kTen19 = 10000000000000000000ull;
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t v[16];
+        const uint64_t* xj = x + j * sx;
+        for (uint64_t i = 0; i < 16; ++i) v[i] = i < nl ? xj[i] : 0;
+        uint64_t top = nl;
+        int64_t pos = (int64_t)(j * digits + digits);  // one past the last digit of this job
+        uint64_t left = digits;
+        while (left > 0) {
+            // remainder of v / 10^19, v <- quotient
+            unsigned __int128 r = 0;
+            for (int64_t i = (int64_t)top - 1; i >= 0; --i) {
+                const unsigned __int128 cur = (r << 64) | v[i];
+                v[i] = (uint64_t)(cur / kTen19);
+                r = cur % kTen19;
+            }
+            while (top > 0 && v[top - 1] == 0) --top;
+            uint64_t g = (uint64_t)r;
+            const uint64_t nd = left < 19 ? left : 19;
+            for (uint64_t d = 0; d < nd; ++d) {
+                --pos;
+                const char ch = (char)('0' + (g % 10));
+                g /= 10;
+                if ((uint64_t)pos >= skip && (uint64_t)pos < total)
+                    out[pos - skip] = ch;
+                else if (ch != '0')
+                    atomicOr(bad, 1u);
+            }
+            left -= nd;
+        }
+        if (top != 0) atomicOr(bad, 1u);
+    }
+}
+
+unsigned grid_for(uint64_t work, unsigned per = 256) {
+    const uint64_t b = (work + per - 1) / per;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 32));
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ DevArith
+void DevPool::trim() {
+    for (auto& p : all_) cudaFree(p.first);
+    all_.clear();
+    free_.clear();
+    if (scratch_) cudaFree(scratch_);
+    if (flags_) cudaFree(flags_);
+    if (seg_) cudaFree(seg_);
+    if (host_word_) cudaFreeHost(host_word_);
+    scratch_ = nullptr;
+    flags_ = nullptr;
+    seg_ = nullptr;
+    host_word_ = nullptr;
+    scratch_cap_ = flags_cap_ = seg_cap_ = 0;
+}
+
+DevArith::DevArith(const DeviceTables& T, Workspace& W, cudaStream_t st, uint64_t* launches, DevPool& pool)
+    : T_(T), W_(W), st_(st), launches_(launches), P_(pool), pool_(pool.free_), all_(pool.all_),
+      scratch_(pool.scratch_), scratch_cap_(pool.scratch_cap_), flags_(pool.flags_), flags_cap_(pool.flags_cap_),
+      seg_(pool.seg_), seg_cap_(pool.seg_cap_), host_word_(pool.host_word_) {
+    if (!host_word_ && cudaMallocHost((void**)&host_word_, 64) != cudaSuccess) throw DevError(4, "pinned word");
+}
+
+DevArith::~DevArith() { cudaStreamSynchronize(st_); }
+
+static void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw DevError(e == cudaErrorMemoryAllocation ? 1 : 4, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+void DevArith::reserve(DevNum& x, size_t limbs) {
+    limbs = std::max<size_t>(limbs, 2);
+    if (x.d && x.cap >= limbs) return;
+    release(x);
+    size_t cap = 2;
+    while (cap < limbs) cap <<= 1;  // size classes: powers of two
+    auto it = pool_.find(cap);
+    if (it != pool_.end()) {
+        x.d = it->second;
+        pool_.erase(it);
+    } else {
+        check(cudaMalloc((void**)&x.d, cap * 8), "DevArith allocation");
+        all_.push_back({x.d, cap});
+    }
+    x.cap = cap;
+}
+
+void DevArith::release(DevNum& x) {
+    if (x.d) pool_.insert({x.cap, x.d});
+    x.d = nullptr;
+    x.cap = x.n = 0;
+    x.sign = 0;
+}
+
+uint64_t* DevArith::scratch(size_t limbs) {
+    if (limbs > scratch_cap_) {
+        if (scratch_) {
+            cudaStreamSynchronize(st_);
+            cudaFree(scratch_);
+        }
+        scratch_ = nullptr;
+        scratch_cap_ = 0;
+        const size_t cap = std::max(limbs, scratch_cap_ * 3 / 2);
+        check(cudaMalloc((void**)&scratch_, cap * 8), "DevArith scratch");
+        scratch_cap_ = cap;
+    }
+    return scratch_;
+}
+
+uint32_t* DevArith::flags(size_t n) {
+    if (n > flags_cap_) {
+        if (flags_) {
+            cudaStreamSynchronize(st_);
+            cudaFree(flags_);
+        }
+        flags_ = nullptr;
+        const size_t cap = std::max<size_t>(n, 1024);
+        check(cudaMalloc((void**)&flags_, cap * 8), "DevArith flags");
+        flags_cap_ = cap;
+    }
+    return flags_;
+}
+
+void DevArith::sync() {
+    check(cudaStreamSynchronize(st_), "DevArith");
+}
+
+void DevArith::run_add(const AddArgs& a0, int form) {
+    AddArgs a = a0;
+    if (a.n == 0) return;
+    if (a.n <= kBigWarpMax) {
+        const uint64_t threads = a.njobs * 32;
+        const unsigned blocks = (unsigned)((threads + 255) / 256);
+        if (form == 0)
+            add_warp_kernel<AddForm::Plain><<<blocks, 256, 0, st_>>>(a);
+        else
+            add_warp_kernel<AddForm::MulSmall><<<blocks, 256, 0, st_>>>(a);
+        check(cudaGetLastError(), "add");
+        ++*launches_;
+        return;
+    }
+    const uint64_t nseg = (a.n + kBigSeg - 1) / kBigSeg;
+    if (a.njobs * nseg > seg_cap_) {
+        if (seg_) {
+            cudaStreamSynchronize(st_);
+            cudaFree(seg_);
+        }
+        seg_ = nullptr;
+        const size_t cap = std::max<size_t>(a.njobs * nseg, 4096);
+        check(cudaMalloc((void**)&seg_, cap * 4), "DevArith segments");
+        seg_cap_ = cap;
+    }
+    a.seg = seg_;
+    const unsigned blocks = (unsigned)(a.njobs * nseg);
+    if (form == 0)
+        add_seg_kernel<AddForm::Plain><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
+    else
+        add_seg_kernel<AddForm::MulSmall><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
+    add_scan_kernel<<<(unsigned)((a.njobs + 127) / 128), 128, 0, st_>>>(a, nseg);
+    if (form == 0)
+        add_final_kernel<AddForm::Plain><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
+    else
+        add_final_kernel<AddForm::MulSmall><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
+    check(cudaGetLastError(), "add");
+    *launches_ += 3;
+}
+
+void DevArith::normalize(DevNum& x) {
+    if (x.n == 0) {
+        x.sign = 0;
+        return;
+    }
+    unsigned long long* top = reinterpret_cast<unsigned long long*>(flags(2));
+    check(cudaMemsetAsync(top, 0, 8, st_), "normalize");
+    top_kernel<<<grid_for(x.n), 256, 0, st_>>>(x.d, 0, x.n, 1, top);
+    ++*launches_;
+    check(cudaMemcpyAsync(host_word_, top, 8, cudaMemcpyDeviceToHost, st_), "normalize");
+    sync();
+    x.n = (size_t)host_word_[0];
+    if (x.n == 0) x.sign = 0;
+}
+
+void DevArith::set_ui(DevNum& x, uint64_t v) {
+    reserve(x, 2);
+    host_word_[1] = v;
+    check(cudaMemcpyAsync(x.d, host_word_ + 1, 8, cudaMemcpyHostToDevice, st_), "set_ui");
+    sync();  // the pinned word is reused
+    x.n = v ? 1 : 0;
+    x.sign = v ? 1 : 0;
+}
+
+void DevArith::set_pow2(DevNum& x, size_t e) {
+    const size_t n = e / 64 + 1;
+    reserve(x, n);
+    check(cudaMemsetAsync(x.d, 0, n * 8, st_), "set_pow2");
+    host_word_[1] = 1ull << (e % 64);
+    check(cudaMemcpyAsync(x.d + n - 1, host_word_ + 1, 8, cudaMemcpyHostToDevice, st_), "set_pow2");
+    sync();
+    x.n = n;
+    x.sign = 1;
+}
+
+void DevArith::copy(DevNum& z, const DevNum& x) {
+    if (&z == &x) return;
+    reserve(z, x.n);
+    if (x.n) check(cudaMemcpyAsync(z.d, x.d, x.n * 8, cudaMemcpyDeviceToDevice, st_), "copy");
+    z.n = x.n;
+    z.sign = x.sign;
+}
+
+void DevArith::upload(DevNum& x, const uint64_t* host, size_t n, int sign) {
+    while (n && host[n - 1] == 0) --n;
+    reserve(x, n);
+    if (n) check(cudaMemcpyAsync(x.d, host, n * 8, cudaMemcpyHostToDevice, st_), "upload");
+    sync();
+    x.n = n;
+    x.sign = n ? (sign < 0 ? -1 : 1) : 0;
+}
+
+void DevArith::download(const DevNum& x, uint64_t* host) {
+    if (x.n) check(cudaMemcpyAsync(host, x.d, x.n * 8, cudaMemcpyDeviceToHost, st_), "download");
+    sync();
+}
+
+size_t DevArith::bits(const DevNum& x) {
+    if (x.n == 0) return 0;
+    check(cudaMemcpyAsync(host_word_, x.d + x.n - 1, 8, cudaMemcpyDeviceToHost, st_), "bits");
+    sync();
+    const uint64_t top = host_word_[0];
+    return 64 * (x.n - 1) + (64 - (size_t)__builtin_clzll(top));
+}
+
+int DevArith::cmp_abs(const DevNum& x, const DevNum& y) {
+    if (x.n != y.n) return x.n < y.n ? -1 : 1;
+    if (x.n == 0) return 0;
+    unsigned long long* diff = reinterpret_cast<unsigned long long*>(flags(2));
+    check(cudaMemsetAsync(diff, 0, 8, st_), "cmp");
+    diff_kernel<<<grid_for(x.n), 256, 0, st_>>>(x.d, 0, y.d, 0, x.n, 1, diff);
+    ++*launches_;
+    check(cudaMemcpyAsync(host_word_, diff, 8, cudaMemcpyDeviceToHost, st_), "cmp");
+    sync();
+    const uint64_t k = host_word_[0];
+    if (k == 0) return 0;
+    check(cudaMemcpyAsync(host_word_ + 1, x.d + k - 1, 8, cudaMemcpyDeviceToHost, st_), "cmp");
+    check(cudaMemcpyAsync(host_word_ + 2, y.d + k - 1, 8, cudaMemcpyDeviceToHost, st_), "cmp");
+    sync();
+    return host_word_[1] > host_word_[2] ? 1 : -1;
+}
+
+int DevArith::cmp(const DevNum& x, const DevNum& y) {
+    if (x.sign != y.sign) return x.sign < y.sign ? -1 : 1;
+    const int c = cmp_abs(x, y);
+    return x.sign >= 0 ? c : -c;
+}
+
+// |z| = |x| + |y| with sign `sign`.
+void DevArith::add_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign) {
+    const size_t n = std::max(x.n, y.n) + 1;
+    DevNum t;
+    const bool alias = (&z == &x) || (&z == &y);
+    DevNum& out = alias ? t : z;
+    reserve(out, n);
+    AddArgs a{};
+    a.x = x.d;
+    a.nx = x.n;
+    a.y = y.d;
+    a.ny = y.n;
+    a.z = out.d;
+    a.n = n;
+    a.njobs = 1;
+    run_add(a, 0);
+    out.n = n;
+    out.sign = sign;
+    normalize(out);
+    if (alias) {
+        std::swap(z, t);
+        release(t);
+    }
+}
+
+// z = |x| - |y|, signed: sign_if_pos when |x| >= |y|, else -sign_if_pos.
+void DevArith::sub_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign_if_pos) {
+    const size_t n = std::max(x.n, y.n);
+    DevNum t;
+    const bool alias = (&z == &x) || (&z == &y);
+    DevNum& out = alias ? t : z;
+    reserve(out, n);
+    uint32_t* co = flags(1);
+    AddArgs a{};
+    a.x = x.d;
+    a.nx = x.n;
+    a.y = y.d;
+    a.ny = y.n;
+    a.my = ~0ull;
+    a.cin = 1;
+    a.z = out.d;
+    a.n = n;
+    a.njobs = 1;
+    a.carry_out = co;
+    run_add(a, 0);
+    check(cudaMemcpyAsync(host_word_, co, 4, cudaMemcpyDeviceToHost, st_), "sub");
+    sync();
+    const bool borrow = (host_word_[0] & 1u) == 0;  // carry out 0 <=> |x| < |y|
+    out.n = n;
+    out.sign = sign_if_pos;
+    if (borrow) {  // two's complement: magnitude = ~out + 1
+        AddArgs b{};
+        b.x = out.d;
+        b.nx = n;
+        b.mx = ~0ull;
+        b.cin = 1;
+        b.z = out.d;
+        b.n = n;
+        b.njobs = 1;
+        run_add(b, 0);
+        out.sign = -sign_if_pos;
+    }
+    normalize(out);
+    if (alias) {
+        std::swap(z, t);
+        release(t);
+    }
+}
+
+void DevArith::add(DevNum& z, const DevNum& x, const DevNum& y) {
+    if (y.sign == 0) return copy(z, x);
+    if (x.sign == 0) return copy(z, y);
+    if (x.sign == y.sign) return add_mag(z, x, y, x.sign);
+    sub_mag(z, x, y, x.sign);
+}
+
+void DevArith::sub(DevNum& z, const DevNum& x, const DevNum& y) {
+    if (y.sign == 0) return copy(z, x);
+    if (x.sign == 0) {
+        copy(z, y);
+        z.sign = -z.sign;
+        return;
+    }
+    if (x.sign != y.sign) return add_mag(z, x, y, x.sign);
+    sub_mag(z, x, y, x.sign);
+}
+
+void DevArith::add_si(DevNum& z, const DevNum& x, int64_t v) {
+    DevNum c;
+    set_ui(c, (uint64_t)(v < 0 ? -v : v));
+    c.sign = v < 0 ? -1 : (v > 0 ? 1 : 0);
+    add(z, x, c);
+    release(c);
+}
+
+void DevArith::mul_raw(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out) {
+    check(enqueue_product(T_, W_, a, na, b, nb, out, st_, launches_), "product");
+}
+
+void DevArith::mul(DevNum& z, const DevNum& x, const DevNum& y) {
+    if (x.sign == 0 || y.sign == 0) {
+        reserve(z, 1);
+        z.n = 0;
+        z.sign = 0;
+        return;
+    }
+    DevNum t;
+    reserve(t, x.n + y.n);
+    if (&x == &y || x.d == y.d)
+        check(enqueue_product(T_, W_, x.d, x.n, nullptr, x.n, t.d, st_, launches_), "square");
+    else
+        check(enqueue_product(T_, W_, x.d, x.n, y.d, y.n, t.d, st_, launches_), "product");
+    t.n = x.n + y.n;
+    t.sign = x.sign * y.sign;
+    normalize(t);
+    std::swap(z, t);
+    release(t);
+}
+
+void DevArith::sqr(DevNum& z, const DevNum& x) { mul(z, x, x); }
+
+void DevArith::mul_ui(DevNum& z, const DevNum& x, uint64_t c) {
+    if (x.sign == 0 || c == 0) {
+        reserve(z, 1);
+        z.n = 0;
+        z.sign = 0;
+        return;
+    }
+    DevNum t;
+    reserve(t, x.n + 1);
+    AddArgs a{};
+    a.x = x.d;
+    a.nx = x.n;
+    a.c = c;
+    a.z = t.d;
+    a.n = x.n + 1;
+    a.njobs = 1;
+    run_add(a, 1);
+    t.n = x.n + 1;
+    t.sign = x.sign;
+    normalize(t);
+    std::swap(z, t);
+    release(t);
+}
+
+void DevArith::shl(DevNum& z, const DevNum& x, size_t s) {
+    if (x.sign == 0) return copy(z, x);
+    DevNum t;
+    const size_t n = x.n + s / 64 + 1;
+    reserve(t, n);
+    shl_kernel<<<grid_for(n), 256, 0, st_>>>(x.d, x.n, t.d, n, s);
+    check(cudaGetLastError(), "shl");
+    ++*launches_;
+    t.n = n;
+    t.sign = x.sign;
+    normalize(t);
+    std::swap(z, t);
+    release(t);
+}
+
+void DevArith::tdiv_q_2exp(DevNum& z, const DevNum& x, size_t s) {
+    if (x.sign == 0 || s >= 64 * x.n) {
+        reserve(z, 1);
+        z.n = 0;
+        z.sign = 0;
+        return;
+    }
+    DevNum t;
+    const size_t n = x.n - s / 64;
+    reserve(t, n);
+    shr_kernel<<<grid_for(n), 256, 0, st_>>>(x.d, 0, x.n, t.d, 0, n, s, 1);
+    check(cudaGetLastError(), "shr");
+    ++*launches_;
+    t.n = n;
+    t.sign = x.sign;
+    normalize(t);
+    std::swap(z, t);
+    release(t);
+}
+
+void DevArith::fdiv_q_2exp(DevNum& z, const DevNum& x, size_t s) {
+    if (x.sign >= 0) return tdiv_q_2exp(z, x, s);
+    // floor of a negative quotient: -(ceil(|x| / 2^s)) = -(trunc + (any low bit set))
+    uint32_t* f = flags(1);
+    check(cudaMemsetAsync(f, 0, 4, st_), "fdiv");
+    sticky_kernel<<<grid_for(std::min<uint64_t>(x.n, s / 64 + 1)), 256, 0, st_>>>(x.d, x.n, s, f);
+    ++*launches_;
+    check(cudaMemcpyAsync(host_word_, f, 4, cudaMemcpyDeviceToHost, st_), "fdiv");
+    sync();
+    const bool sticky = (host_word_[0] & 1u) != 0;
+    tdiv_q_2exp(z, x, s);
+    if (sticky) {
+        if (z.sign == 0) {
+            set_ui(z, 1);
+            z.sign = -1;
+        } else {
+            add_si(z, z, -1);  // z is negative: -1 grows its magnitude
+        }
+    }
+}
+
+void DevArith::tdiv_r_2exp(DevNum& z, const DevNum& x, size_t s) {
+    DevNum t;
+    const size_t n = std::min<size_t>(x.n, (s + 63) / 64);
+    reserve(t, std::max<size_t>(n, 1));
+    if (n) {
+        lowbits_kernel<<<grid_for(n), 256, 0, st_>>>(x.d, x.n, t.d, n, s);
+        check(cudaGetLastError(), "lowbits");
+        ++*launches_;
+    }
+    t.n = n;
+    t.sign = x.sign;
+    normalize(t);
+    std::swap(z, t);
+    release(t);
+}
+
+// ------------------------------------------------------------------ batched forms
+void DevArith::batch_add(const uint64_t* x, uint64_t sx, uint64_t nx, const uint64_t* y, uint64_t sy, uint64_t ny,
+                         uint64_t* z, uint64_t sz, uint64_t n, bool subtract, uint32_t cin, const uint32_t* enable,
+                         uint64_t njobs) {
+    AddArgs a{};
+    a.x = x;
+    a.sx = sx;
+    a.nx = nx;
+    a.y = y;
+    a.sy = sy;
+    a.ny = ny;
+    a.z = z;
+    a.sz = sz;
+    a.n = n;
+    a.my = subtract ? ~0ull : 0;
+    a.cin = subtract ? 1u : cin;
+    a.enable = enable;
+    a.njobs = njobs;
+    run_add(a, 0);
+}
+
+void DevArith::batch_shr(const uint64_t* x, uint64_t sx, uint64_t nx, uint64_t* z, uint64_t sz, uint64_t n, uint64_t s,
+                         uint64_t njobs) {
+    shr_kernel<<<grid_for(n * njobs), 256, 0, st_>>>(x, sx, nx, z, sz, n, s, njobs);
+    check(cudaGetLastError(), "batch shr");
+    ++*launches_;
+}
+
+void DevArith::batch_ge(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n, uint32_t* ge,
+                        uint64_t njobs) {
+    unsigned long long* diff = reinterpret_cast<unsigned long long*>(scratch(njobs));
+    check(cudaMemsetAsync(diff, 0, njobs * 8, st_), "batch ge");
+    diff_kernel<<<grid_for(n * njobs), 256, 0, st_>>>(x, sx, y, sy, n, njobs, diff);
+    ge_kernel<<<grid_for(njobs), 256, 0, st_>>>(x, sx, y, sy, njobs, diff, ge);
+    check(cudaGetLastError(), "batch ge");
+    *launches_ += 2;
+}
+
+bool DevArith::leaves(const uint64_t* x, uint64_t sx, uint64_t nlimbs, uint64_t njobs, uint64_t digits, char* out,
+                      uint64_t skip, uint64_t total) {
+    if (nlimbs > 16) throw DevError(3, "leaves: chunk longer than 16 limbs");
+    uint32_t* bad = flags(1);
+    check(cudaMemsetAsync(bad, 0, 4, st_), "leaves");
+    leaves_kernel<<<grid_for(njobs, 128), 128, 0, st_>>>(x, sx, nlimbs, njobs, digits, out, skip, total, bad);
+    check(cudaGetLastError(), "leaves");
+    ++*launches_;
+    check(cudaMemcpyAsync(host_word_, bad, 4, cudaMemcpyDeviceToHost, st_), "leaves");
+    sync();
+    return (host_word_[0] & 1u) == 0;
+}
+
+}  // namespace pg

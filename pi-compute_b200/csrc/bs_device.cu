@@ -99,11 +99,6 @@ __device__ void leaf_values(uint64_t k, uint64_t P[2], int& nP, uint64_t Q[3], i
     nR = sb_len(R, 3);
 }
 
-struct LevelView {
-    uint64_t* X[3];    // P, Q, R slot arrays
-    uint32_t cap[3];   // limbs per slot
-    uint32_t* len;     // len[3 i + k]
-};
 
 // Depth D-1: node i covers 1 or 2 terms. Caps: P 4, Q 6, R 8 limbs (7 needed, kept even).
 __global__ void bs_pair_kernel(LevelView out, uint64_t nodes, uint64_t a0, uint64_t b0, int depth) {
@@ -650,41 +645,54 @@ DeviceBS* bs_state_new() { return new DeviceBS; }
 void bs_state_delete(DeviceBS* b) { delete b; }
 }  // namespace pg
 
-extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R,
-                           size_t cap, size_t* len, int* sign) {
-    if (!ctx || !Q || !R || !len || !sign || b <= a) return PG_ERR_BAD_ARG;
-    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
-    cudaSetDevice(pg::ctx_device(ctx));
-    pg::DeviceBS& bs = *pg::ctx_bs(ctx);  // buffers persist in the context across calls
-    bs.T = &pg::ctx_tables(ctx);
-    bs.st = pg::ctx_stream(ctx);
-    bs.launches = pg::ctx_launches(ctx);
-    pg::LevelView root;
+namespace pg {
+// Runs the level-batched splitting of [a, b) with the context lock held by the caller. On
+// PG_OK the root's P, Q, R stay in the context's level buffers (root.X[k], hl[k] limbs) until
+// the next splitting on this context.
+pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3]) {
+    cudaSetDevice(ctx_device(ctx));
+    DeviceBS& bs = *ctx_bs(ctx);  // buffers persist in the context across calls
+    bs.T = &ctx_tables(ctx);
+    bs.st = ctx_stream(ctx);
+    bs.launches = ctx_launches(ctx);
     std::string err;
     cudaError_t e = bs.run(a, b, root, err);
     if (!err.empty()) {
-        pg::ctx_set_error(ctx, err);
+        ctx_set_error(ctx, err);
         return PG_ERR_TOO_LARGE;
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
-        pg::ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
+        ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
     }
-    auto tc0 = std::chrono::steady_clock::now();
-    uint32_t hl[3] = {0, 0, 0};
     uint32_t herr = 0;
+    hl[0] = hl[1] = hl[2] = 0;
     e = cudaMemcpyAsync(hl, root.len, 12, cudaMemcpyDeviceToHost, bs.st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, bs.errw, 4, cudaMemcpyDeviceToHost, bs.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(bs.st);
     if (e != cudaSuccess) {
-        pg::ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
+        ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
         return PG_ERR_DEVICE;
     }
     if (herr) {
-        pg::ctx_set_error(ctx, herr == 1 ? "carry look-back wait ran out of iterations" : "carry out of the top word");
+        ctx_set_error(ctx, herr == 1 ? "carry look-back wait ran out of iterations" : "carry out of the top word");
         return herr == 1 ? PG_ERR_TIMEOUT : PG_ERR_INTERNAL;
     }
+    return PG_OK;
+}
+}  // namespace pg
+
+extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R,
+                           size_t cap, size_t* len, int* sign) {
+    if (!ctx || !Q || !R || !len || !sign || b <= a) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    pg::LevelView root;
+    uint32_t hl[3];
+    pg_status s = pg::bs_run_locked(ctx, a, b, root, hl);
+    if (s != PG_OK) return s;
+    cudaStream_t st = pg::ctx_stream(ctx);
+    auto tc0 = std::chrono::steady_clock::now();
     if (hl[1] > cap || hl[2] > cap || (P && hl[0] > cap)) {
         pg::ctx_set_error(ctx, "output buffers smaller than the result");
         return PG_ERR_BAD_ARG;
@@ -692,12 +700,12 @@ extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
     uint64_t* dsts[3] = {P, Q, R};
     for (int k = 0; k < 3; ++k) {
         len[k] = hl[k];
-        if (dsts[k] && hl[k]) cudaMemcpyAsync(dsts[k], root.X[k], hl[k] * 8, cudaMemcpyDeviceToHost, bs.st);
+        if (dsts[k] && hl[k]) cudaMemcpyAsync(dsts[k], root.X[k], hl[k] * 8, cudaMemcpyDeviceToHost, st);
     }
-    e = cudaStreamSynchronize(bs.st);
+    cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return PG_ERR_DEVICE;
     if (pg::trace_on())
-        std::fprintf(stderr, "[pg_bs] device sync + copy-out of P/Q/R: %.3f ms\n",
+        std::fprintf(stderr, "[pg_bs] copy-out of P/Q/R: %.3f ms\n",
                      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count());
     // signs over the series: P(a,b) = (-1)^(#k >= 1), Q > 0, R(a,b) has the sign of R(a, a+1)
     const unsigned long neg_terms = (b - a) - (a == 0 ? 1 : 0);

@@ -1,0 +1,130 @@
+// DevArith: signed multi-limb integers in device memory with mpz-like operations, for the
+// pieces of the pi pipeline that follow binary splitting (Newton reciprocal, square root,
+// final products, radix conversion). Magnitudes are little-endian 64-bit limb arrays in HBM;
+// the sign and the exact limb count are kept on the host (operations whose result length or
+// sign depends on the data read one small word back, which waits for the stream).
+//
+// Products go through the NTT engine (enqueue_product); additions, shifts, comparisons and
+// small multiples through the carry-chain kernels of bigint.cuh.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "ntt_engine.cuh"
+
+namespace pg {
+
+struct DevNum {
+    uint64_t* d = nullptr;
+    size_t cap = 0;   // limbs allocated
+    size_t n = 0;     // limbs in use (top limb non-zero when n > 0)
+    int sign = 0;     // -1, 0, +1
+};
+
+class DevError : public std::runtime_error {
+public:
+    DevError(int status, const std::string& m) : std::runtime_error(m), status(status) {}
+    int status;
+};
+
+// Device memory behind DevArith: limb buffers cached by power-of-two size class, scratch and
+// flag words, and a pinned word for small reads. Kept by the context across calls, released
+// with it (or by trim()).
+struct DevPool {
+    std::multimap<size_t, uint64_t*> free_;   // free buffers by capacity (limbs)
+    std::vector<std::pair<uint64_t*, size_t>> all_;
+    uint64_t* scratch_ = nullptr;
+    size_t scratch_cap_ = 0;
+    uint32_t* flags_ = nullptr;
+    size_t flags_cap_ = 0;
+    uint32_t* seg_ = nullptr;
+    size_t seg_cap_ = 0;
+    uint64_t* host_word_ = nullptr;           // pinned, 8 words
+    ~DevPool() { trim(); }
+    void trim();                              // frees everything (no DevNum may be live)
+};
+
+class DevArith {
+public:
+    DevArith(const DeviceTables& T, Workspace& W, cudaStream_t st, uint64_t* launches, DevPool& pool);
+    ~DevArith();
+    DevArith(const DevArith&) = delete;
+    DevArith& operator=(const DevArith&) = delete;
+
+    // memory (cached by size class; released with the DevArith)
+    void reserve(DevNum& x, size_t limbs);   // capacity >= limbs (contents undefined)
+    void release(DevNum& x);
+    uint64_t* scratch(size_t limbs);          // temporary, valid until the next scratch call
+    cudaStream_t stream() const { return st_; }
+
+    void set_ui(DevNum& x, uint64_t v);
+    void set_pow2(DevNum& x, size_t e);
+    void copy(DevNum& z, const DevNum& x);
+    void upload(DevNum& x, const uint64_t* host, size_t n, int sign);
+    void download(const DevNum& x, uint64_t* host);  // x.n limbs
+
+    size_t bits(const DevNum& x);             // bit length of |x|
+    int cmp_abs(const DevNum& x, const DevNum& y);
+    int cmp(const DevNum& x, const DevNum& y);
+
+    void add(DevNum& z, const DevNum& x, const DevNum& y);
+    void sub(DevNum& z, const DevNum& x, const DevNum& y);
+    void add_si(DevNum& z, const DevNum& x, int64_t v);
+    void mul(DevNum& z, const DevNum& x, const DevNum& y);
+    void sqr(DevNum& z, const DevNum& x);
+    void mul_ui(DevNum& z, const DevNum& x, uint64_t c);
+    void shl(DevNum& z, const DevNum& x, size_t s);
+    void tdiv_q_2exp(DevNum& z, const DevNum& x, size_t s);   // truncate toward zero
+    void fdiv_q_2exp(DevNum& z, const DevNum& x, size_t s);   // floor
+    void tdiv_r_2exp(DevNum& z, const DevNum& x, size_t s);   // |x| mod 2^s with x's sign
+
+    // Batched kernels for the radix conversion (jobs at base + j * stride, see bigint.cuh).
+    void batch_add(const uint64_t* x, uint64_t sx, uint64_t nx, const uint64_t* y, uint64_t sy, uint64_t ny,
+                   uint64_t* z, uint64_t sz, uint64_t n, bool subtract, uint32_t cin, const uint32_t* enable,
+                   uint64_t njobs);
+    void batch_shr(const uint64_t* x, uint64_t sx, uint64_t nx, uint64_t* z, uint64_t sz, uint64_t n, uint64_t s,
+                   uint64_t njobs);
+    void batch_ge(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n, uint32_t* ge,
+                  uint64_t njobs);  // ge[j] = (x_j >= y_j), y shared when sy == 0
+    // decimal digits of each job into out (device); false when a job has more digits than its
+    // slot or the digits below `skip` are not all zero
+    bool leaves(const uint64_t* x, uint64_t sx, uint64_t nlimbs, uint64_t njobs, uint64_t digits, char* out,
+                uint64_t skip, uint64_t total);
+
+    // Product of device magnitudes, exactly na + nb limbs at out (no normalisation).
+    void mul_raw(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out);
+
+    const DeviceTables& tables() const { return T_; }
+    Workspace& workspace() { return W_; }
+    void sync();                              // wait and check the product error word
+    uint64_t* launches() { return launches_; }
+
+private:
+    void normalize(DevNum& x);                // exact length (waits)
+    void add_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign);          // |z| = |x| + |y|
+    void sub_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign_if_pos);   // z = |x| - |y| signed
+    void run_add(const struct AddArgs& a, int form);
+    uint32_t* flags(size_t n);
+
+    const DeviceTables& T_;
+    Workspace& W_;
+    cudaStream_t st_;
+    uint64_t* launches_;
+    DevPool& P_;
+    std::multimap<size_t, uint64_t*>& pool_;
+    std::vector<std::pair<uint64_t*, size_t>>& all_;
+    uint64_t*& scratch_;
+    size_t& scratch_cap_;
+    uint32_t*& flags_;
+    size_t& flags_cap_;
+    uint32_t*& seg_;
+    size_t& seg_cap_;
+    uint64_t*& host_word_;
+};
+
+}  // namespace pg

@@ -19,6 +19,9 @@ void bs_state_delete(DeviceBS*);
 struct BatchWork;
 BatchWork* batch_state_new();
 void batch_state_delete(BatchWork*);
+struct FinishState;
+FinishState* finish_state_new();
+void finish_state_delete(FinishState*);
 }  // namespace pg
 
 struct pg_ctx {
@@ -31,6 +34,7 @@ struct pg_ctx {
     uint64_t launches = 0;
     pg::DeviceBS* bs = nullptr;  // binary-splitting buffers, kept for the next pg_bs call
     pg::BatchWork* batch = nullptr;  // pg_mul_batch buffers, kept for the next batch
+    pg::FinishState* finish = nullptr;  // device finish pool, kept for the next pi computation
 };
 
 namespace {
@@ -146,6 +150,10 @@ BatchWork* ctx_batch(pg_ctx* c) {
     if (!c->batch) c->batch = batch_state_new();
     return c->batch;
 }
+FinishState* ctx_finish(pg_ctx* c) {
+    if (!c->finish) c->finish = finish_state_new();
+    return c->finish;
+}
 }  // namespace pg
 
 extern "C" {
@@ -184,6 +192,7 @@ void pg_destroy(pg_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->bs) pg::bs_state_delete(c->bs);
     if (c->batch) pg::batch_state_delete(c->batch);
+    if (c->finish) pg::finish_state_delete(c->finish);
     c->ws.release();
     c->tables.release();
     if (c->stream) cudaStreamDestroy(c->stream);

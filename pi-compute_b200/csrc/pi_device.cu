@@ -1,0 +1,717 @@
+// Device-resident finish of the pi computation: the final formula and the decimal
+// conversion with every operand in HBM (DevArith, devnum.h), products on the NTT engine.
+//
+//   final formula   pi 10^d = floor(426880 Q sqrt(10005) 10^d / R)  (reference:
+//                   src/engine/pi_engine.cpp:437-491, mpf_sqrt / mpf_div / mpf_mul at
+//                   d * log2(10) + 64 bits). Here: Newton reciprocal of R and Newton inverse
+//                   square root of 10005 at doubling precision, each finished by an exact
+//                   integer correction, 5^d by squaring, three truncated products, and a floor
+//                   that is accepted only when the rigorous error bound keeps it away from an
+//                   integer (otherwise the guard grows and the formula reruns).
+//   conversion      the decimal digits of an integer < 10^n (reference: src/io/base_converter.cpp
+//                   PowerTree::build + parallel_convert, :48-147): the number is split in
+//                   halves of 2^j digits by q = floor(c * inv / 2^(2K)) with inv = floor(2^(2K)
+//                   / 10^(2^j)), r = c - q 10^(2^j) and at most two corrections; every level
+//                   of the split runs batched over all chunks of that level (two shared-operand
+//                   batched products, a shift, a subtraction, the corrections), down to
+//                   128-digit chunks written as ASCII by one thread each.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/pi_b200.h"
+#include "devnum.h"
+
+namespace pg {
+
+const DeviceTables& ctx_tables(pg_ctx* c);
+Workspace& ctx_workspace(pg_ctx* c);
+cudaStream_t ctx_stream(pg_ctx* c);
+std::mutex& ctx_mutex(pg_ctx* c);
+uint64_t* ctx_launches(pg_ctx* c);
+void ctx_set_error(pg_ctx* c, const std::string& msg);
+int ctx_device(pg_ctx* c);
+pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3]);
+bool trace_on();
+
+// ------------------------------------------------------------------ batched shared-operand product
+// out_j[0 .. na + nb) = a_j * b for j < njobs; a_j at a + j * sa (na limbs), out_j at
+// out + j * so. The shared operand is transformed once; the batch's last forward pass fuses the
+// pointwise product with it (other_stride 0) and the CRT writes every job's words.
+struct SharedProduct {
+    uint32_t* res = nullptr;
+    uint64_t res_cap = 0;
+    uint32_t* bres = nullptr;
+    uint64_t bres_cap = 0;
+    uint32_t* sync = nullptr;
+    uint64_t sync_cap = 0;
+    uint32_t* errw = nullptr;
+
+    ~SharedProduct() {
+        if (res) cudaFree(res);
+        if (bres) cudaFree(bres);
+        if (sync) cudaFree(sync);
+        if (errw) cudaFree(errw);
+    }
+
+    static void grow(uint32_t** p, uint64_t& cap, uint64_t words, cudaStream_t st) {
+        if (words <= cap) return;
+        cudaStreamSynchronize(st);
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        cap = 0;
+        const uint64_t want = std::max(words, cap + cap / 2);
+        cudaError_t e = cudaMalloc((void**)p, want * 4);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw DevError(e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE, "batched product buffers");
+        }
+        cap = want;
+    }
+
+    void run(const DeviceTables& T, cudaStream_t st, uint64_t* launches, const uint64_t* a, uint64_t sa, uint64_t na,
+             uint64_t njobs, const uint64_t* b, uint64_t nb, uint64_t* out, uint64_t so) {
+        if (!njobs) return;
+        if (na + nb > ((uint64_t)1 << (kMaxLogL - 1))) throw DevError(PG_ERR_TOO_LARGE, "batched product too long");
+        if ((sa | so) & 1) throw DevError(PG_ERR_INTERNAL, "batched product strides must be even");
+        if (!errw) {
+            if (cudaMalloc((void**)&errw, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "error word");
+            cudaMemsetAsync(errw, 0, 4, st);
+        }
+        const int logL = product_logL(na, nb);
+        const Plan plan = T.plan(logL);
+        const int last = plan.npass - 1;
+        const uint64_t L = 1ull << logL, per = 3 * L;
+        auto check = [](cudaError_t e) {
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                throw DevError(PG_ERR_DEVICE, std::string("batched product: ") + cudaGetErrorString(e));
+            }
+        };
+        // shared operand: full forward transform
+        grow(&bres, bres_cap, per, st);
+        {
+            PassParams p{};
+            p.data = bres;
+            p.out = bres;
+            p.words = reinterpret_cast<const uint32_t*>(b);
+            p.ncoef = 2 * nb;
+            p.L = L;
+            p.logL = logL;
+            p.job_stride = per;
+            p.other_stride = per;
+            p.njobs = 1;
+            for (int i = 0; i < plan.npass; ++i) {
+                set_pass(p, plan, i);
+                check(launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, Fuse::None, p, T.tw, st));
+                ++*launches;
+            }
+        }
+        const uint64_t budget = 256ull << 20;  // residue words per chunk of jobs
+        const uint64_t m_max = std::max<uint64_t>(1, budget / per);
+        const uint64_t nwords = 2 * (na + nb);
+        const uint64_t bpj = (nwords + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+        for (uint64_t j0 = 0; j0 < njobs; j0 += m_max) {
+            const uint64_t m = std::min(m_max, njobs - j0);
+            grow(&res, res_cap, m * per, st);
+            PassParams p{};
+            p.data = res;
+            p.out = res;
+            p.words = reinterpret_cast<const uint32_t*>(a + j0 * sa);
+            p.words_stride = 2 * sa;
+            p.ncoef = 2 * na;
+            p.L = L;
+            p.logL = logL;
+            p.job_stride = per;
+            p.other = bres;
+            p.other_stride = 0;
+            p.njobs = (uint32_t)m;
+            for (int i = 0; i < plan.npass; ++i) {
+                set_pass(p, plan, i);
+                check(launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues,
+                                  i == last ? Fuse::MulInverse : Fuse::None, p, T.tw, st));
+                ++*launches;
+            }
+            for (int i = last - 1; i >= 0; --i) {
+                set_pass(p, plan, i);
+                check(launch_pass(plan, i, true, Source::Residues, Fuse::None, p, T.tw, st));
+                ++*launches;
+            }
+            grow(&sync, sync_cap, m + m * bpj, st);
+            check(cudaMemsetAsync(sync, 0, (m + m * bpj) * 4, st));
+            CrtParams c{};
+            c.res = res;
+            c.res_stride = per;
+            c.L = L;
+            c.nwords = nwords;
+            c.out = reinterpret_cast<uint32_t*>(out + j0 * so);
+            c.out_stride = 2 * so;
+            c.ticket = sync;
+            c.status = sync + m;
+            c.error = errw;
+            c.blocks_per_job = bpj;
+            c.k = make_crt_consts(logL);
+            c.merge = 0;
+            check(launch_crt(c, m * bpj, st));
+            ++*launches;
+        }
+    }
+
+    uint32_t error(cudaStream_t st) {
+        uint32_t h = 0;
+        if (!errw) return 0;
+        cudaMemcpyAsync(&h, errw, 4, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+        return h;
+    }
+};
+
+// Per-context state of the device finish, kept across calls: the arithmetic pool and the
+// batched-product buffers.
+struct FinishState {
+    DevPool pool;
+    SharedProduct sp;
+};
+FinishState* finish_state_new() { return new FinishState; }
+void finish_state_delete(FinishState* f) { delete f; }
+FinishState* ctx_finish(pg_ctx* c);
+
+namespace {
+
+typedef unsigned __int128 u128;
+
+// A DevNum released when it goes out of scope.
+struct Num {
+    DevArith& A;
+    DevNum v;
+    explicit Num(DevArith& a) : A(a) {}
+    ~Num() { A.release(v); }
+    Num(const Num&) = delete;
+    Num& operator=(const Num&) = delete;
+    operator DevNum&() { return v; }
+};
+
+struct Timer {
+    const char* what;
+    std::chrono::steady_clock::time_point t0;
+    explicit Timer(const char* w) : what(w), t0(std::chrono::steady_clock::now()) {}
+    double ms() const { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
+    ~Timer() {
+        if (trace_on()) std::fprintf(stderr, "[pi_device] %s: %.3f ms\n", what, ms());
+    }
+};
+
+void upload_u128(DevArith& A, DevNum& x, u128 v) {
+    uint64_t w[2] = {(uint64_t)v, (uint64_t)(v >> 64)};
+    A.upload(x, w, 2, 1);
+}
+
+u128 download_u128(DevArith& A, const DevNum& x) {
+    if (x.n > 2) throw DevError(PG_ERR_INTERNAL, "download_u128: value too long");
+    uint64_t w[2] = {0, 0};
+    if (x.n) A.download(x, w);
+    return ((u128)w[1] << 64) | w[0];
+}
+
+u128 isqrt128(u128 v) {
+    if (v == 0) return 0;
+    const int bl = (v >> 64) ? 128 - __builtin_clzll((uint64_t)(v >> 64)) : 64 - __builtin_clzll((uint64_t)v);
+    u128 x = (u128)1 << ((bl + 1) / 2);  // > sqrt(v): v < 2^bl
+    for (;;) {                           // Newton from above decreases to floor(sqrt(v))
+        const u128 y = (x + v / x) / 2;
+        if (y >= x) break;
+        x = y;
+    }
+    while (x > v / x) --x;                // x^2 > v, without overflow
+    while (x + 1 <= v / (x + 1)) ++x;     // (x+1)^2 <= v
+    return x;
+}
+
+// Z = floor(2^(2k) / R), k = bits(R) (R > 0). Newton doubling: Zh = floor(2^(2h) / Rh) for the
+// top h = k/2 + 32 bits of R, Z0 = Zh 2^(k-h), one Newton step, then the exact correction
+// 0 <= 2^(2k) - R Z < R.
+void recip_floor(DevArith& A, DevNum& Z, const DevNum& R) {
+    const size_t k = A.bits(R);
+    if (k == 0 || R.sign < 0) throw DevError(PG_ERR_BAD_ARG, "recip_floor: R must be positive");
+    if (k <= 64) {
+        const uint64_t r = (uint64_t)download_u128(A, R);
+        u128 z;
+        if ((r & (r - 1)) == 0)
+            z = (u128)1 << (k + 1);  // r = 2^(k-1)
+        else
+            z = (k == 64 ? ~(u128)0 : ((u128)1 << (2 * k))) / r;  // r odd part > 1: 2^128 / r = (2^128 - 1) / r
+        upload_u128(A, Z, z);
+        return;
+    }
+    const size_t h = k / 2 + 32;
+    Num Rh(A), Zh(A), Z0(A), T(A), E(A), D(A);
+    A.tdiv_q_2exp(Rh, R, k - h);
+    recip_floor(A, Zh, Rh);
+    A.shl(Z0, Zh, k - h);
+    A.mul(T, R, Z0);
+    A.set_pow2(E, 2 * k);
+    A.sub(E, E, T);                 // E = 2^(2k) - R Z0
+    A.mul(D, Zh, E);                // Z0 E / 2^(2k) = Zh E / 2^(k+h)
+    A.fdiv_q_2exp(D, D, k + h);
+    A.add(Z, Z0, D);
+    A.mul(T, R, D);
+    A.sub(E, E, T);                 // E = 2^(2k) - R Z
+    int steps = 0;
+    while (E.v.sign < 0) {
+        A.add_si(Z, Z, -1);
+        A.add(E, E, R);
+        if (++steps > 64) throw DevError(PG_ERR_INTERNAL, "recip_floor: correction did not converge");
+    }
+    while (A.cmp(E, R) >= 0) {
+        A.add_si(Z, Z, 1);
+        A.sub(E, E, R);
+        if (++steps > 64) throw DevError(PG_ERR_INTERNAL, "recip_floor: correction did not converge");
+    }
+}
+
+// u ~= 2^q / sqrt(a) within a few units (Newton on the inverse square root).
+void rsqrt_approx(DevArith& A, DevNum& u, uint64_t a, size_t q) {
+    if (q <= 64) {
+        // 2^128 - 1 stands in for 2^128 at q = 64: the estimate may be one unit low
+        const u128 t = (q == 64 ? ~(u128)0 : ((u128)1 << (2 * q))) / a;
+        upload_u128(A, u, isqrt128(t));
+        return;
+    }
+    const size_t qh = q / 2 + 32;
+    Num uh(A), u0(A), T(A), e(A), D(A);
+    rsqrt_approx(A, uh, a, qh);
+    A.shl(u0, uh, q - qh);
+    A.sqr(T, u0);
+    A.mul_ui(T, T, a);
+    A.set_pow2(e, 2 * q);
+    A.sub(e, e, T);                 // 2^(2q) - a u0^2
+    A.mul(D, uh, e);                // u0 e / 2^(2q+1) = uh e / 2^(q + qh + 1)
+    A.fdiv_q_2exp(D, D, q + qh + 1);
+    A.add(u, u0, D);
+}
+
+// S = floor(sqrt(a) 2^s), exactly.
+void sqrt_scaled(DevArith& A, DevNum& S, uint64_t a, size_t s) {
+    const size_t q = s + 64;
+    Num u(A), N(A), V(A), t(A);
+    rsqrt_approx(A, u, a, q);
+    A.mul_ui(S, u, a);              // a 2^q / sqrt(a)
+    A.tdiv_q_2exp(S, S, q - s);
+    A.set_pow2(N, 2 * s);
+    A.mul_ui(N, N, a);
+    A.sqr(t, S);
+    A.sub(V, N, t);                 // V = N - S^2
+    int steps = 0;
+    while (V.v.sign < 0) {          // (S-1)^2 = S^2 - 2S + 1
+        A.add(V, V, S);
+        A.add(V, V, S);
+        A.add_si(V, V, -1);
+        A.add_si(S, S, -1);
+        if (++steps > 64) throw DevError(PG_ERR_INTERNAL, "sqrt_scaled: correction did not converge");
+    }
+    for (;;) {                      // (S+1)^2 = S^2 + 2S + 1 <= N ?
+        A.shl(t, S, 1);
+        A.add_si(t, t, 1);
+        if (A.cmp(V, t) < 0) break;
+        A.sub(V, V, t);
+        A.add_si(S, S, 1);
+        if (++steps > 64) throw DevError(PG_ERR_INTERNAL, "sqrt_scaled: correction did not converge");
+    }
+}
+
+void pow5(DevArith& A, DevNum& F, size_t n) {
+    A.set_ui(F, 1);
+    if (n == 0) return;
+    int top = 63;
+    while (!((n >> top) & 1)) --top;
+    for (int b = top; b >= 0; --b) {
+        A.sqr(F, F);
+        if ((n >> b) & 1) A.mul_ui(F, F, 5);
+    }
+}
+
+// pi_int = floor(pi 10^digits) from the series root Q, R (both > 0).
+void final_formula(DevArith& A, DevNum& pi_int, const DevNum& Q, const DevNum& R, size_t digits) {
+    if (Q.sign <= 0 || R.sign <= 0) throw DevError(PG_ERR_BAD_ARG, "final formula needs Q, R > 0");
+    const size_t bQ = A.bits(Q), bR = A.bits(R);
+    for (size_t guard = 128; guard <= 128 + 4 * 256; guard += 256) {
+        const size_t P = (size_t)std::ceil((double)digits * 3.3219280948873623) + 2 + guard;
+        const size_t k = P + 64;
+        Num Qt(A), Rt(A), Z(A), S(A), F(A), X(A), t(A);
+        const long long eQ = (long long)bQ - (long long)k;
+        const long long eR = (long long)bR - (long long)k;
+        if (eQ >= 0) A.tdiv_q_2exp(Qt, Q, (size_t)eQ); else A.shl(Qt, Q, (size_t)-eQ);
+        if (eR >= 0) A.tdiv_q_2exp(Rt, R, (size_t)eR); else A.shl(Rt, R, (size_t)-eR);
+        {
+            Timer tm("reciprocal of R");
+            recip_floor(A, Z, Rt);      // 2^(2k) / Rt
+        }
+        {
+            Timer tm("sqrt(10005)");
+            sqrt_scaled(A, S, 10005, k);
+        }
+        {
+            Timer tm("5^digits");
+            pow5(A, F, digits);
+        }
+        Timer tm("three truncated products and the floor");
+        A.mul_ui(X, Qt, 426880);
+        long long e = eQ - eR - 3 * (long long)k + (long long)digits;
+        auto mul_trunc = [&](const DevNum& y) {
+            A.mul(t, X, y);
+            const long long over = (long long)A.bits(t) - (long long)k;
+            if (over > 0) {
+                A.tdiv_q_2exp(X, t, (size_t)over);
+                e += over;
+            } else {
+                A.copy(X, t);
+            }
+        };
+        mul_trunc(S);
+        mul_trunc(Z);
+        mul_trunc(F);
+        if (e >= -160) throw DevError(PG_ERR_INTERNAL, "final formula: not enough fraction bits");
+        const size_t fb = (size_t)(-e);
+        // Relative error < 8 * 2^-(k-1) and pi 10^d < 2^(P - guard): absolute error below
+        // 2^-(guard + 60); the floor is certain unless the fraction is within 2^-100 of an
+        // integer. fr = X mod 2^fb; top = fr >> (fb - 100) (100 bits), low = fr mod 2^(fb-100).
+        Num fr(A), top(A), low(A);
+        A.tdiv_r_2exp(fr, X, fb);
+        A.tdiv_q_2exp(top, fr, fb - 100);
+        A.tdiv_r_2exp(low, fr, fb - 100);
+        const u128 tv = download_u128(A, top);
+        const u128 all_ones = ((u128)1 << 100) - 1;
+        const bool below = tv == 0;                          // fr < 2^(fb-100)
+        const bool above = tv == all_ones && low.v.sign != 0;  // fr > 2^fb - 2^(fb-100)
+        if (!below && !above) {
+            A.tdiv_q_2exp(pi_int, X, fb);
+            return;
+        }
+    }
+    throw DevError(PG_ERR_INTERNAL, "final formula: the result stayed within the error bound of an integer");
+}
+
+// ------------------------------------------------------------------ decimal conversion
+constexpr int kLeafLog = 7;  // 128-digit leaves
+
+// Decimal digits of x (0 <= x < 10^nd) into host out[0 .. nd).
+void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char* out) {
+    cudaStream_t st = A.stream();
+    if (nd == 0) return;
+    if (x.n == 0) {
+        std::memset(out, '0', nd);
+        return;
+    }
+    int J = kLeafLog;
+    while (((size_t)1 << J) < nd) ++J;
+    const size_t total = (size_t)1 << J, skip = total - nd;
+    char* d_out = nullptr;
+    if (cudaMalloc((void**)&d_out, nd) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
+    struct Free {
+        char* p;
+        ~Free() { cudaFree(p); }
+    } free_out{d_out};
+    cudaMemsetAsync(d_out, '0', nd, st);
+    // powers P[j] = 10^(2^j) and reciprocals for j = kLeafLog .. J-1
+    std::vector<Num*> P, inv;
+    std::vector<size_t> K;
+    struct Owner {
+        std::vector<Num*>& a;
+        std::vector<Num*>& b;
+        ~Owner() {
+            for (auto* p : a) delete p;
+            for (auto* p : b) delete p;
+        }
+    } own{P, inv};
+    {
+        Timer tm("power tree and reciprocals");
+        Num p(A);
+        A.set_ui(p, 10);
+        for (int j = 0; j < J; ++j) {
+            if (j >= kLeafLog) {
+                P.push_back(new Num(A));
+                A.copy(*P.back(), p);
+                K.push_back(A.bits(p));
+                inv.push_back(new Num(A));
+            }
+            if (j + 1 < J) A.sqr(p, p);
+        }
+        // The top reciprocal by Newton; every lower one from the one above it:
+        // with Y = floor(2^(2K') / P^2) (K' = bits(P^2)), floor(P Y / 2^(2K' - 2K)) undershoots
+        // floor(2^(2K) / P) by at most one (the error P 2^(2K - 2K') is below 2^(2 - K)), so one
+        // exact check 0 <= 2^(2K) - P Z < P finishes it.
+        const int top = J - 1;
+        if (top >= kLeafLog) recip_floor(A, inv[top - kLeafLog]->v, P[top - kLeafLog]->v);
+        Num T(A), E(A);
+        for (int j = top - 1; j >= kLeafLog; --j) {
+            DevNum& Pj = P[j - kLeafLog]->v;
+            DevNum& Z = inv[j - kLeafLog]->v;
+            const size_t k = K[j - kLeafLog], k2 = K[j + 1 - kLeafLog];
+            A.mul(T, Pj, inv[j + 1 - kLeafLog]->v);
+            A.tdiv_q_2exp(Z, T, 2 * k2 - 2 * k);
+            A.mul(T, Pj, Z);
+            A.set_pow2(E, 2 * k);
+            A.sub(E, E, T);
+            int steps = 0;
+            while (E.v.sign < 0) {
+                A.add_si(Z, Z, -1);
+                A.add(E, E, Pj);
+                if (++steps > 4) throw DevError(PG_ERR_INTERNAL, "to_decimal: reciprocal step did not converge");
+            }
+            while (A.cmp(E, Pj) >= 0) {
+                A.add_si(Z, Z, 1);
+                A.sub(E, E, Pj);
+                if (++steps > 4) throw DevError(PG_ERR_INTERNAL, "to_decimal: reciprocal step did not converge");
+            }
+        }
+    }
+    auto pw = [&](int j) -> DevNum& { return P[j - kLeafLog]->v; };
+    auto iv = [&](int j) -> DevNum& { return inv[j - kLeafLog]->v; };
+    auto kb = [&](int j) { return K[j - kLeafLog]; };
+    auto even = [](size_t n) { return (n + 1) & ~(size_t)1; };
+    // capacity (limbs, even) of a chunk < 10^(2^j): bits(10^(2^j)) / 64 + 1
+    auto cap_of = [&](int j) { return even(kb(j) / 64 + 2); };
+
+    Timer tm("divide-and-conquer levels and leaves");
+    const uint64_t* cur = x.d;
+    size_t cur_s = even(std::max<size_t>(x.n, 1)), cur_n = x.n;
+    // the top chunk needs an even stride: copy when x.n is odd (only the layout matters)
+    Num xcopy(A), lvl_a(A), lvl_b(A), Tbuf(A), Ubuf(A), Rbuf(A), Ppad(A);
+    if (x.n & 1) {
+        A.reserve(xcopy, cur_s);
+        cudaMemsetAsync(xcopy.v.d, 0, cur_s * 8, st);
+        cudaMemcpyAsync(xcopy.v.d, x.d, x.n * 8, cudaMemcpyDeviceToDevice, st);
+        cur = xcopy.v.d;
+    }
+    DevNum* next = &lvl_a.v;
+    DevNum* spare = &lvl_b.v;
+    uint32_t* ge = nullptr;
+    struct FreeGe {
+        uint32_t*& p;
+        ~FreeGe() {
+            if (p) cudaFree(p);
+        }
+    } free_ge{ge};
+    uint64_t ge_cap = 0;
+    for (int t = 0; J - t > kLeafLog; ++t) {
+        const int j = J - t - 1;  // split power 10^(2^j)
+        const uint64_t njobs = 1ull << t;
+        const size_t cap = cap_of(j);             // next level's chunk capacity
+        const DevNum& Pj = pw(j);
+        const DevNum& Ij = iv(j);
+        const size_t ni = Ij.n, np = Pj.n;
+        if (cur_n == 0) cur_n = 1;
+        // T = c * inv, q = T >> 2K into the even slots of the next level
+        const size_t sT = even(cur_n + ni);
+        A.reserve(Tbuf, sT * njobs);
+        sp.run(A.tables(), st, A.launches(), cur, cur_s, cur_n, njobs, Ij.d, ni, Tbuf.v.d, sT);
+        A.reserve(*next, 2 * cap * njobs);
+        A.batch_shr(Tbuf.v.d, sT, cur_n + ni, next->d, 2 * cap, cap, 2 * kb(j), njobs);
+        // U = q * P, r = c - U (< 3 P) into the odd slots
+        const size_t sU = even(cap + np);
+        A.reserve(Ubuf, sU * njobs);
+        sp.run(A.tables(), st, A.launches(), next->d, 2 * cap, cap, njobs, Pj.d, np, Ubuf.v.d, sU);
+        A.reserve(Rbuf, cur_s * njobs);
+        A.batch_add(cur, cur_s, cur_n, Ubuf.v.d, sU, std::min(cap + np, cur_n), Rbuf.v.d, cur_s, cur_n, true, 0,
+                    nullptr, njobs);
+        A.batch_shr(Rbuf.v.d, cur_s, cur_n, next->d + cap, 2 * cap, cap, 0, njobs);
+        // corrections: while r >= P: r -= P, q += 1 (at most twice)
+        A.reserve(Ppad, cap);
+        cudaMemsetAsync(Ppad.v.d, 0, cap * 8, st);
+        cudaMemcpyAsync(Ppad.v.d, Pj.d, np * 8, cudaMemcpyDeviceToDevice, st);
+        if (njobs > ge_cap) {
+            A.sync();
+            if (ge) cudaFree(ge);
+            ge = nullptr;
+            if (cudaMalloc((void**)&ge, njobs * 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
+            ge_cap = njobs;
+        }
+        for (int round = 0; round < 2; ++round) {
+            A.batch_ge(next->d + cap, 2 * cap, Ppad.v.d, 0, cap, ge, njobs);
+            A.batch_add(next->d + cap, 2 * cap, cap, Ppad.v.d, 0, np, next->d + cap, 2 * cap, cap, true, 0, ge, njobs);
+            A.batch_add(next->d, 2 * cap, cap, nullptr, 0, 0, next->d, 2 * cap, cap, false, 1, ge, njobs);
+        }
+        // a third check must find every remainder below P
+        A.batch_ge(next->d + cap, 2 * cap, Ppad.v.d, 0, cap, ge, njobs);
+        {
+            std::vector<uint32_t> h(njobs);
+            cudaMemcpyAsync(h.data(), ge, njobs * 4, cudaMemcpyDeviceToHost, st);
+            A.sync();
+            for (uint32_t v : h)
+                if (v) throw DevError(PG_ERR_INTERNAL, "to_decimal: remainder above the split power");
+        }
+        cur = next->d;
+        cur_s = cap;
+        cur_n = cap;
+        std::swap(next, spare);
+    }
+    if (sp.error(st)) throw DevError(PG_ERR_INTERNAL, "to_decimal: product check failed");
+    if (!A.leaves(cur, cur_s, std::min<size_t>(cur_n, 16), (uint64_t)1 << (J - kLeafLog), (uint64_t)1 << kLeafLog,
+                  d_out, skip, total))
+        throw DevError(PG_ERR_BAD_ARG, "to_decimal: the number has more digits than requested");
+    if (cudaMemcpyAsync(out, d_out, nd, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        throw DevError(PG_ERR_DEVICE, "digit copy");
+    A.sync();
+}
+
+pg_status fail(pg_ctx* c, pg_status s, const std::string& m) {
+    ctx_set_error(c, m);
+    return s;
+}
+
+// Reads and clears the product engine's error word.
+pg_status product_errors(pg_ctx* ctx) {
+    Workspace& W = ctx_workspace(ctx);
+    cudaStream_t st = ctx_stream(ctx);
+    uint32_t err = 0;
+    cudaMemcpyAsync(&err, W.sync, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(ctx, PG_ERR_DEVICE, "device error");
+    if (err) {
+        cudaMemsetAsync(W.sync, 0, 4, st);
+        cudaStreamSynchronize(st);
+        return fail(ctx, err == 1 ? PG_ERR_TIMEOUT : PG_ERR_INTERNAL,
+                    err == 1 ? "carry look-back wait ran out of iterations" : "carry out of the top word");
+    }
+    return PG_OK;
+}
+
+template <class F>
+pg_status guarded(pg_ctx* ctx, F&& f) {
+    try {
+        f();
+    } catch (const DevError& e) {
+        return fail(ctx, e.status, e.what());
+    } catch (const std::exception& e) {
+        return fail(ctx, PG_ERR_INTERNAL, e.what());
+    }
+    return product_errors(ctx);
+}
+
+}  // namespace
+}  // namespace pg
+
+extern "C" {
+
+pg_status pg_recip_floor(pg_ctx* ctx, const uint64_t* r, size_t nr, uint64_t* z, size_t zcap, size_t* zlen) {
+    if (!ctx || !r || !z || !zlen || nr == 0) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    return pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Num R(A), Z(A);
+        A.upload(R, r, nr, 1);
+        if (R.v.sign == 0) throw pg::DevError(PG_ERR_BAD_ARG, "pg_recip_floor: R is zero");
+        pg::recip_floor(A, Z, R);
+        if (Z.v.n > zcap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_recip_floor: output buffer too small");
+        A.download(Z, z);
+        *zlen = Z.v.n;
+    });
+}
+
+pg_status pg_sqrt_scaled(pg_ctx* ctx, uint64_t a, size_t s, uint64_t* out, size_t cap, size_t* len) {
+    if (!ctx || !out || !len || a < 1) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    return pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Num S(A);
+        pg::sqrt_scaled(A, S, a, s);
+        if (S.v.n > cap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_sqrt_scaled: output buffer too small");
+        A.download(S, out);
+        *len = S.v.n;
+    });
+}
+
+pg_status pg_to_decimal(pg_ctx* ctx, const uint64_t* x, size_t nx, size_t ndigits, char* out) {
+    if (!ctx || (nx && !x) || (ndigits && !out)) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    return pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Num X(A);
+        A.upload(X, x, nx, 1);
+        // x < 10^ndigits is required: check by bit length against 10^ndigits's (upper bound)
+        if ((double)A.bits(X) > (double)ndigits * 3.3219280948873623 + 1)
+            throw pg::DevError(PG_ERR_BAD_ARG, "pg_to_decimal: x has more than ndigits digits");
+        pg::to_decimal(A, fs.sp, X, ndigits, out);
+    });
+}
+
+pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t* r, size_t nr, size_t digits,
+                       char* out) {
+    if (!ctx || !q || !r || !out || nq == 0 || nr == 0) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    return pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Num Q(A), R(A), X(A);
+        A.upload(Q, q, nq, 1);
+        A.upload(R, r, nr, 1);
+        pg::final_formula(A, X, Q, R, digits);
+        // floor(pi 10^digits) has digits + 1 decimal digits: "3" then the fraction
+        pg::to_decimal(A, fs.sp, X, digits + 1, out + 1);
+        out[0] = out[1];
+        out[1] = '.';
+    });
+}
+
+pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
+    if (!ctx || !out || digits == 0) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    const auto t0 = std::chrono::steady_clock::now();
+    auto secs = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count();
+    };
+    // terms as the reference's PiEngine: terms_needed(digits + 100) (pi_engine.cpp:214-220,
+    // binary_splitting.cpp terms_needed); each term adds log10(151931373056000) ~= 14.18 digits
+    const unsigned long terms = (unsigned long)std::ceil((double)(digits + 100) / 14.1816474627) + 1;
+    pg::LevelView root;
+    uint32_t hl[3];
+    pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl);
+    if (s != PG_OK) return s;
+    const double t_bs = secs(t0);
+    const auto t1 = std::chrono::steady_clock::now();
+    double t_final = 0;
+    s = pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        // Q, R of the root (both positive for a = 0), copied out of the splitting buffers
+        pg::Num Q(A), R(A), X(A);
+        A.reserve(Q, hl[1]);
+        A.reserve(R, hl[2]);
+        cudaMemcpyAsync(Q.v.d, root.X[1], (size_t)hl[1] * 8, cudaMemcpyDeviceToDevice, A.stream());
+        cudaMemcpyAsync(R.v.d, root.X[2], (size_t)hl[2] * 8, cudaMemcpyDeviceToDevice, A.stream());
+        Q.v.n = hl[1];
+        Q.v.sign = hl[1] ? 1 : 0;
+        R.v.n = hl[2];
+        R.v.sign = hl[2] ? 1 : 0;
+        pg::final_formula(A, X, Q, R, digits);
+        t_final = secs(t1);
+        char* body = out + 1;  // the integer's digits: "3" then the fraction digits
+        pg::to_decimal(A, fs.sp, X, digits + 1, body);
+        out[0] = body[0];
+        out[1] = '.';
+    });
+    if (seconds) {
+        seconds[0] = t_bs;
+        seconds[1] = t_final;
+        seconds[2] = secs(t1) - t_final;
+        seconds[3] = secs(t0);
+    }
+    return s;
+}
+
+}  // extern "C"

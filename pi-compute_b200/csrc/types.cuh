@@ -60,6 +60,14 @@ struct DstEntry {
     uint32_t pad;
 };
 
+// One depth of the binary-splitting tree in device memory: node i's P, Q, R magnitudes at
+// X[k] + i * cap[k] (k = 0, 1, 2), lengths in limbs at len[3 i + k].
+struct LevelView {
+    uint64_t* X[3];    // P, Q, R slot arrays
+    uint32_t cap[3];   // limbs per slot
+    uint32_t* len;     // len[3 i + k]
+};
+
 // Child level of a merge batch: node i's P/Q/R limbs at X[k] + i * cap[k] (k = 0, 1, 2),
 // lengths (limbs) at len[3 * i + k].
 struct MergeSrc {

@@ -38,12 +38,13 @@ int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int devi
         cfg.digits = digits;
         cfg.num_threads = threads ? threads : 1;
         cfg.device = device;
-        cfg.mode = (mode == PIB_MODE_BATCHED) ? pi::BSMode::Batched : pi::BSMode::PerCall;
-        cfg.final_mode = (mode == PIB_MODE_BATCHED || mode == PIB_MODE_GMP_NEWTON) ? pi::FinalMode::Newton
-                                                                                   : pi::FinalMode::Mpf;
+        const bool batched = mode == PIB_MODE_BATCHED || mode == PIB_MODE_BATCHED_HOST_FINISH;
+        cfg.mode = batched ? pi::BSMode::Batched : pi::BSMode::PerCall;
+        cfg.final_mode = mode == PIB_MODE_BATCHED ? pi::FinalMode::Device
+                         : (batched || mode == PIB_MODE_GMP_NEWTON) ? pi::FinalMode::Newton
+                                                                    : pi::FinalMode::Mpf;
         std::unique_ptr<pi::Multiplier> m =
-            make_multiplier((mode == PIB_MODE_BATCHED || mode == PIB_MODE_GMP_NEWTON) ? PIB_MODE_GMP : mode,
-                            threshold, device);
+            make_multiplier((batched || mode == PIB_MODE_GMP_NEWTON) ? PIB_MODE_GMP : mode, threshold, device);
         pi::PiEngine eng(*m);
         pi::PiResult r = eng.compute(cfg);
         std::memcpy(out, r.digits.data(), r.digits.size());

@@ -3,7 +3,10 @@
 //
 //   pi_b200 --digits N [--output FILE] [--threads T] [--verbose]
 //           [--gpu | --b200]           products >= --gpu-threshold limbs on the B200, per call
-//           [--batched]                level-batched device-resident binary splitting (implies --newton)
+//           [--batched]                the whole computation in HBM: level-batched binary splitting,
+//                                      Newton finish and batched decimal conversion on the device
+//           [--host-finish]            batched splitting on the device, Newton finish and conversion on
+//                                      the host with B200 products
 //           [--newton | --mpf]         final formula + radix conversion: Newton iterations and divide-
 //                                      and-conquer conversion on B200 products, or the reference's GMP mpf
 //           [--gpu-threshold N]        (default 10000 like the reference)
@@ -20,7 +23,8 @@
 static void usage() {
     std::puts(
         "pi_b200 - pi digits with exact big-integer products on one B200\n\n"
-        "USAGE: pi_b200 --digits <N> [--output FILE] [--threads T] [--gpu|--b200] [--batched] [--newton|--mpf]\n"
+        "USAGE: pi_b200 --digits <N> [--output FILE] [--threads T] [--gpu|--b200] [--batched|--host-finish]\n"
+        "               [--newton|--mpf]\n"
         "               [--gpu-threshold N] [--device D] [--verbose]\n");
 }
 
@@ -44,6 +48,9 @@ int main(int argc, char** argv) {
         } else if (a == "--gpu" || a == "--b200" || a == "--ntt") {
             gpu = true;
         } else if (a == "--batched") {
+            cfg.mode = pi::BSMode::Batched;
+            cfg.final_mode = pi::FinalMode::Device;
+        } else if (a == "--host-finish") {
             cfg.mode = pi::BSMode::Batched;
             cfg.final_mode = pi::FinalMode::Newton;
         } else if (a == "--newton") {

@@ -74,6 +74,31 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
     mpz_init(Q);
     mpz_init(R);
     mpz_init(pi_int);
+    if (cfg.mode == BSMode::Batched && cfg.final_mode == FinalMode::Device) {
+        // The whole computation on the device (pg_pi): splitting, final formula, conversion.
+        pg_ctx* ctx = shared_context(cfg.device);
+        const uint64_t l0 = pg_launch_count(ctx);
+        std::string s(cfg.digits + 2, '0');
+        double sec[4] = {0, 0, 0, 0};
+        const pg_status st = pg_pi(ctx, cfg.digits, &s[0], sec);
+        if (st != PG_OK)
+            throw std::runtime_error(std::string("pg_pi: ") + pg_last_error(ctx) + " (status " + std::to_string(st) + ")");
+        res.digits.swap(s);
+        res.t.gpu_launches += pg_launch_count(ctx) - l0;
+        res.t.bs = sec[0];
+        res.t.final = sec[1];
+        res.t.convert = sec[2];
+        res.t.total = secs(t0, Clock::now());
+        res.elapsed_seconds = res.t.total;
+        if (cfg.verbose || std::getenv("PI_B200_TRACE"))
+            std::printf("  Terms: %lu\n  Binary splitting: %.3fs\n  Final computation: %.3fs\n"
+                        "  String conversion: %.3fs\n  Total: %.3fs\n",
+                        terms, res.t.bs, res.t.final, res.t.convert, res.t.total);
+        mpz_clear(Q);
+        mpz_clear(R);
+        mpz_clear(pi_int);
+        return res;
+    }
     if (cfg.mode == BSMode::Batched) {
         pg_ctx* ctx = shared_context(cfg.device);
         const uint64_t l0 = pg_launch_count(ctx);

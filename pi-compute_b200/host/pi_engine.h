@@ -21,7 +21,7 @@ enum class BSMode { PerCall = 0, Batched = 1 };
 // Final formula and decimal conversion: the reference's GMP mpf division/square root and
 // mpz_get_str, or integer Newton iterations and divide-and-conquer conversion whose large
 // products run on the B200 (newton.h).
-enum class FinalMode { Mpf = 0, Newton = 1 };
+enum class FinalMode { Mpf = 0, Newton = 1, Device = 2 };  // Device: pg_pi, every step in HBM
 
 struct PiConfig {
     size_t digits = 1000;

@@ -166,6 +166,19 @@ def test_batched_digits_10m(lib):
     assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
 
 
+BATCHED_HOST_FINISH = 4
+
+
+@pytest.mark.gpu
+def test_batched_host_finish_digits_1m(lib):
+    """Batched splitting with the Newton finish on the host (B200 products) gives the same bytes."""
+    s, _ = pi_digits(lib, 1000, BATCHED_HOST_FINISH)
+    assert s == open(os.path.join(GOLDEN, "pi_1000.txt")).read()
+    s, _ = pi_digits(lib, 1_000_000, BATCHED_HOST_FINISH)
+    g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
+    assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
+
+
 # ---------------------------------------------------------------- Newton finish + D&C conversion (CPU)
 GMP_NEWTON = 3
 
