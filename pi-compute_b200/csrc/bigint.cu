@@ -112,18 +112,31 @@ __global__ void __launch_bounds__(kBigThreads) add_seg_kernel(AddArgs A, uint64_
 }
 
 // Phase 2: carry into every segment of a job (bit 2 of its word) and the job's carry out.
-__global__ void add_scan_kernel(AddArgs A, uint64_t nseg) {
-    const uint64_t job = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (job >= A.njobs) return;
+// One block per job scans the job's segment words 256 at a time.
+__global__ void __launch_bounds__(kBigThreads) add_scan_kernel(AddArgs A, uint64_t nseg) {
+    __shared__ uint32_t s_w[kBigThreads / 32];
+    const uint64_t job = blockIdx.x;
     if (A.enable && !A.enable[job]) return;
-    uint32_t carry = A.cin;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t carry = A.cin;  // carry into the current chunk of segments
     uint32_t* w = A.seg + job * nseg;
-    for (uint64_t s = 0; s < nseg; ++s) {
-        const uint32_t gp = w[s];
-        w[s] = gp | (carry << 2);
-        carry = gp_apply(gp, carry);
+    for (uint64_t base = 0; base < nseg; base += kBigThreads) {
+        const uint64_t s = base + threadIdx.x;
+        const uint32_t gp = s < nseg ? w[s] : 2u;
+        const uint32_t incl = gp_warp_scan(gp, lane);
+        if (lane == 31) s_w[warp] = incl;
+        __syncthreads();
+        uint32_t cw = carry;
+        for (int k = 0; k < warp; ++k) cw = gp_apply(s_w[k], cw);
+        const uint32_t prev = __shfl_up_sync(0xffffffffu, incl, 1);
+        const uint32_t cin = lane == 0 ? cw : gp_apply(prev, cw);
+        if (s < nseg) w[s] = gp | (cin << 2);
+        uint32_t tot = carry;
+        for (int k = 0; k < kBigThreads / 32; ++k) tot = gp_apply(s_w[k], tot);
+        __syncthreads();  // s_w is rewritten by the next chunk
+        carry = tot;
     }
-    if (A.carry_out) A.carry_out[job] = carry;
+    if (threadIdx.x == 0 && A.carry_out) A.carry_out[job] = carry;
 }
 
 // Phase 3: the sums with each segment's carry in.
@@ -204,44 +217,78 @@ __global__ void lowbits_kernel(const uint64_t* x, uint64_t nx, uint64_t* z, uint
     }
 }
 
-// flag |= 1 if any of the low s bits of x is set.
+// Block-wide maximum (unsigned), result valid in thread 0.
+__device__ __forceinline__ unsigned long long block_max(unsigned long long v) {
+    __shared__ unsigned long long s_m[32];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, off));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) s_m[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) v = max(v, s_m[w]);
+    return v;
+}
+
+// flag |= 1 if any of the low s bits of x is set (one atomic per block).
 __global__ void sticky_kernel(const uint64_t* x, uint64_t nx, uint64_t s, uint32_t* flag) {
     const uint64_t w = s >> 6;
     const uint32_t b = (uint32_t)(s & 63);
+    unsigned long long hit = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= w && i < nx;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t v = x[i];
-        const bool hit = (i < w) ? (v != 0) : (b && (v & ((1ull << b) - 1)) != 0);
-        if (hit) atomicOr(flag, 1u);
+        if ((i < w) ? (v != 0) : (b && (v & ((1ull << b) - 1)) != 0)) hit = 1;
     }
+    hit = block_max(hit);
+    if (threadIdx.x == 0 && hit) atomicOr(flag, 1u);
 }
 
-// top[j] = 1 + index of the highest non-zero limb of x_j (0 if x_j == 0); top zeroed before.
-__global__ void top_kernel(const uint64_t* x, uint64_t sx, uint64_t n, uint64_t njobs, unsigned long long* top) {
-    const uint64_t total = n * njobs;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t job = t / n, i = t - job * n;
-        if (x[job * sx + i] != 0) atomicMax(top + job, (unsigned long long)(i + 1));
-    }
+// *top = 1 + index of the highest non-zero limb of x (0 if x == 0); *top zeroed before.
+__global__ void top_kernel(const uint64_t* x, uint64_t n, unsigned long long* top) {
+    unsigned long long m = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (x[i] != 0) m = i + 1;
+    m = block_max(m);
+    if (threadIdx.x == 0 && m) atomicMax(top, m);
 }
 
-// diff[j] = 1 + highest index where x_j and y_j differ (0: equal); diff zeroed before.
-__global__ void diff_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n, uint64_t njobs,
-                            unsigned long long* diff) {
-    const uint64_t total = n * njobs;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t job = t / n, i = t - job * n;
-        if (x[job * sx + i] != y[job * sy + i]) atomicMax(diff + job, (unsigned long long)(i + 1));
-    }
+// *diff = 1 + highest index where x and y differ (0: equal); *diff zeroed before.
+__global__ void diff_kernel(const uint64_t* x, const uint64_t* y, uint64_t n, unsigned long long* diff) {
+    unsigned long long m = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (x[i] != y[i]) m = i + 1;
+    m = block_max(m);
+    if (threadIdx.x == 0 && m) atomicMax(diff, m);
 }
 
-// ge[j] = x_j >= y_j, from diff[j].
-__global__ void ge_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t njobs,
-                          const unsigned long long* diff, uint32_t* ge) {
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += (uint64_t)gridDim.x * blockDim.x) {
-        const unsigned long long k = diff[j];
-        ge[j] = (k == 0) ? 1u : (x[j * sx + k - 1] > y[j * sy + k - 1] ? 1u : 0u);
-    }
+// ge[j] = x_j >= y_j over n limbs, one warp per job (no atomics).
+__global__ void ge_warp_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n,
+                               uint64_t njobs, uint32_t* ge) {
+    const uint64_t job = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (job >= njobs) return;
+    const uint64_t* xj = x + job * sx;
+    const uint64_t* yj = y + job * sy;
+    unsigned long long m = 0;
+    for (uint64_t i = lane; i < n; i += 32)
+        if (xj[i] != yj[i]) m = i + 1;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, off));
+    if (lane == 0) ge[job] = (m == 0) ? 1u : (xj[m - 1] > yj[m - 1] ? 1u : 0u);
+}
+
+// The same with one block per job (long numbers).
+__global__ void __launch_bounds__(256) ge_block_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy,
+                                                       uint64_t n, uint32_t* ge) {
+    const uint64_t job = blockIdx.x;
+    const uint64_t* xj = x + job * sx;
+    const uint64_t* yj = y + job * sy;
+    unsigned long long m = 0;
+    for (uint64_t i = threadIdx.x; i < n; i += blockDim.x)
+        if (xj[i] != yj[i]) m = i + 1;
+    m = block_max(m);
+    if (threadIdx.x == 0) ge[job] = (m == 0) ? 1u : (xj[m - 1] > yj[m - 1] ? 1u : 0u);
 }
 
 // Decimal digits of job j (< 10^digits) written most significant first to out[j * digits ...];
@@ -410,7 +457,7 @@ void DevArith::run_add(const AddArgs& a0, int form) {
         add_seg_kernel<AddForm::Plain><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
     else
         add_seg_kernel<AddForm::MulSmall><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
-    add_scan_kernel<<<(unsigned)((a.njobs + 127) / 128), 128, 0, st_>>>(a, nseg);
+    add_scan_kernel<<<(unsigned)a.njobs, kBigThreads, 0, st_>>>(a, nseg);
     if (form == 0)
         add_final_kernel<AddForm::Plain><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
     else
@@ -426,7 +473,7 @@ void DevArith::normalize(DevNum& x) {
     }
     unsigned long long* top = reinterpret_cast<unsigned long long*>(flags(2));
     check(cudaMemsetAsync(top, 0, 8, st_), "normalize");
-    top_kernel<<<grid_for(x.n), 256, 0, st_>>>(x.d, 0, x.n, 1, top);
+    top_kernel<<<grid_for(x.n), 256, 0, st_>>>(x.d, x.n, top);
     ++*launches_;
     check(cudaMemcpyAsync(host_word_, top, 8, cudaMemcpyDeviceToHost, st_), "normalize");
     sync();
@@ -489,7 +536,7 @@ int DevArith::cmp_abs(const DevNum& x, const DevNum& y) {
     if (x.n == 0) return 0;
     unsigned long long* diff = reinterpret_cast<unsigned long long*>(flags(2));
     check(cudaMemsetAsync(diff, 0, 8, st_), "cmp");
-    diff_kernel<<<grid_for(x.n), 256, 0, st_>>>(x.d, 0, y.d, 0, x.n, 1, diff);
+    diff_kernel<<<grid_for(x.n), 256, 0, st_>>>(x.d, y.d, x.n, diff);
     ++*launches_;
     check(cudaMemcpyAsync(host_word_, diff, 8, cudaMemcpyDeviceToHost, st_), "cmp");
     sync();
@@ -754,12 +801,12 @@ void DevArith::batch_shr(const uint64_t* x, uint64_t sx, uint64_t nx, uint64_t* 
 
 void DevArith::batch_ge(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n, uint32_t* ge,
                         uint64_t njobs) {
-    unsigned long long* diff = reinterpret_cast<unsigned long long*>(scratch(njobs));
-    check(cudaMemsetAsync(diff, 0, njobs * 8, st_), "batch ge");
-    diff_kernel<<<grid_for(n * njobs), 256, 0, st_>>>(x, sx, y, sy, n, njobs, diff);
-    ge_kernel<<<grid_for(njobs), 256, 0, st_>>>(x, sx, y, sy, njobs, diff, ge);
+    if (n <= 1024)
+        ge_warp_kernel<<<(unsigned)((njobs * 32 + 255) / 256), 256, 0, st_>>>(x, sx, y, sy, n, njobs, ge);
+    else
+        ge_block_kernel<<<(unsigned)njobs, 256, 0, st_>>>(x, sx, y, sy, n, ge);
     check(cudaGetLastError(), "batch ge");
-    *launches_ += 2;
+    ++*launches_;
 }
 
 bool DevArith::leaves(const uint64_t* x, uint64_t sx, uint64_t nlimbs, uint64_t njobs, uint64_t digits, char* out,
