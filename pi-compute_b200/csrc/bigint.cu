@@ -278,6 +278,28 @@ __global__ void ge_warp_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y
     if (lane == 0) ge[job] = (m == 0) ? 1u : (xj[m - 1] > yj[m - 1] ? 1u : 0u);
 }
 
+// Long numbers, many blocks per job: diff[j] = 1 + highest differing index (grid (blocks, jobs),
+// one atomic per block), then ge_from_diff_kernel decides.
+__global__ void diff_jobs_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n,
+                                 unsigned long long* diff) {
+    const uint64_t job = blockIdx.y;
+    const uint64_t* xj = x + job * sx;
+    const uint64_t* yj = y + job * sy;
+    unsigned long long m = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (xj[i] != yj[i]) m = i + 1;
+    m = block_max(m);
+    if (threadIdx.x == 0 && m) atomicMax(diff + job, m);
+}
+
+__global__ void ge_from_diff_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t njobs,
+                                    const unsigned long long* diff, uint32_t* ge) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = diff[j];
+        ge[j] = (k == 0) ? 1u : (x[j * sx + k - 1] > y[j * sy + k - 1] ? 1u : 0u);
+    }
+}
+
 // The same with one block per job (long numbers).
 __global__ void __launch_bounds__(256) ge_block_kernel(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy,
                                                        uint64_t n, uint32_t* ge) {
@@ -801,12 +823,23 @@ void DevArith::batch_shr(const uint64_t* x, uint64_t sx, uint64_t nx, uint64_t* 
 
 void DevArith::batch_ge(const uint64_t* x, uint64_t sx, const uint64_t* y, uint64_t sy, uint64_t n, uint32_t* ge,
                         uint64_t njobs) {
-    if (n <= 1024)
+    if (n <= 1024) {
         ge_warp_kernel<<<(unsigned)((njobs * 32 + 255) / 256), 256, 0, st_>>>(x, sx, y, sy, n, njobs, ge);
-    else
+        ++*launches_;
+    } else if (n <= 16384 || njobs >= 1024) {
         ge_block_kernel<<<(unsigned)njobs, 256, 0, st_>>>(x, sx, y, sy, n, ge);
+        ++*launches_;
+    } else {
+        // few long jobs: spread each over many blocks
+        unsigned long long* diff = reinterpret_cast<unsigned long long*>(scratch(njobs));
+        check(cudaMemsetAsync(diff, 0, njobs * 8, st_), "batch ge");
+        const unsigned per = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(n / 8192, 148ull * 8 / njobs + 1));
+        dim3 grid(per, (unsigned)njobs);
+        diff_jobs_kernel<<<grid, 256, 0, st_>>>(x, sx, y, sy, n, diff);
+        ge_from_diff_kernel<<<grid_for(njobs), 256, 0, st_>>>(x, sx, y, sy, njobs, diff, ge);
+        *launches_ += 2;
+    }
     check(cudaGetLastError(), "batch ge");
-    ++*launches_;
 }
 
 bool DevArith::leaves(const uint64_t* x, uint64_t sx, uint64_t nlimbs, uint64_t njobs, uint64_t digits, char* out,

@@ -24,6 +24,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pi_b200.h"
@@ -382,18 +383,45 @@ struct DeviceBS {
                 if (hi - lo > 1) lo = lo + (hi - lo) / 2;
             }
         }
-        // bit sums over the rightmost node of each depth
+        // Bit sums over the rightmost node of each depth. The nodes are nested, so the terms
+        // [b0 - s[0], b0) split into disjoint segments [b0 - s[d], b0 - s[d+1]) (d < D) and
+        // [b0 - s[D], b0); one pass over the terms (spread over host threads) sums each segment,
+        // and depth d's sum is the suffix sum of segments d..D.
         std::vector<uint64_t> sp(D + 1), sq(D + 1);
-        for (int d = 0; d <= D; ++d) {
-            uint64_t bp = 0, bq = 0;
-            for (uint64_t k = b0 - s[d]; k < b0; ++k) {
-                int p, q, r;
-                leaf_bits(k, p, q, r);
-                bp += p;
-                bq += q;
+        {
+            std::vector<uint64_t> lo(D + 1);
+            for (int d = 0; d <= D; ++d) lo[d] = b0 - s[d];  // non-decreasing in d
+            const uint64_t first = lo[0];
+            const uint64_t nterms = b0 - first;
+            const unsigned nt = (unsigned)std::max<uint64_t>(
+                1, std::min<uint64_t>(std::max(1u, std::thread::hardware_concurrency()), nterms / 65536 + 1));
+            std::vector<std::vector<uint64_t>> segp(nt, std::vector<uint64_t>(D + 1, 0)),
+                segq(nt, std::vector<uint64_t>(D + 1, 0));
+            auto work = [&](unsigned t) {
+                const uint64_t k0 = first + nterms * t / nt, k1 = first + nterms * (t + 1) / nt;
+                int seg = 0;
+                while (seg < D && lo[seg + 1] <= k0) ++seg;
+                for (uint64_t k = k0; k < k1; ++k) {
+                    while (seg < D && lo[seg + 1] <= k) ++seg;
+                    int bp, bq, br;
+                    leaf_bits(k, bp, bq, br);
+                    segp[t][seg] += (uint64_t)bp;
+                    segq[t][seg] += (uint64_t)bq;
+                }
+            };
+            std::vector<std::thread> th;
+            for (unsigned t = 1; t < nt; ++t) th.emplace_back(work, t);
+            work(0);
+            for (auto& x : th) x.join();
+            uint64_t accp = 0, accq = 0;
+            for (int d = D; d >= 0; --d) {
+                for (unsigned t = 0; t < nt; ++t) {
+                    accp += segp[t][d];
+                    accq += segq[t][d];
+                }
+                sp[d] = accp;
+                sq[d] = accq;
             }
-            sp[d] = bp;
-            sq[d] = bq;
         }
         dp.resize(D);
         // depth D-1: pair nodes

@@ -187,6 +187,17 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cuda
     auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
     // the tile, plus the four-step row factors of a strided tile
     const size_t smem = ((size_t)4 << LOGE) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
+#ifdef PG_PASS_CARVEOUT
+    {
+        // shared-memory share of the unified L1 (percent): the rest caches the twiddle tables
+        static std::atomic<int> set[64];
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !set[dev].load()) {
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, PG_PASS_CARVEOUT);
+            set[dev].store(1);
+        }
+    }
+#endif
     dim3 grid((unsigned)tiles, kNumPrimes);
     kern<<<grid, kPassThreads, smem, st>>>(prm, tw);
 #endif
