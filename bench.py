@@ -322,6 +322,8 @@ def run_b200(args):
                        "l2": "every product of the top tree levels moves GBs through HBM (far above the 126 MB L2)",
                        "phases_s": {"binary_splitting": round(ph[0], 3), "final_formula": round(ph[1], 3),
                                     "decimal_conversion": round(ph[2], 3)},
+                       "step_s": [round(x, 4) for x in per],
+                       "step_phases_s": [[round(v, 4) for v in s3[:3]] for s3 in phases],
                        "digits_sha256": got, "matches_reference": (got == want) if want else None},
             "roofline": roof,
             "e2e": e2e,

@@ -347,8 +347,19 @@ struct DeviceBS {
     uint64_t sync_cap = 0;
     uint32_t* errw = nullptr;     // device error word, allocated once and never moved
     uint64_t errw_cap = 0;
+    // CUDA graph of the last range's launch sequence (replayed when the same range comes back
+    // and no buffer moved since it was captured)
+    uint64_t moves = 0;           // buffer reallocations so far
+    uint64_t seen_a0 = ~0ull, seen_b0 = 0, seen_moves = ~0ull;  // last range run directly
+    cudaGraphExec_t gexec = nullptr;  // captured for [g_a0, g_b0); destroyed when a buffer moves
+    uint64_t g_a0 = ~0ull, g_b0 = 0;
+    LevelView groot{};
+    uint64_t glaunches = 0;
 
-    ~DeviceBS() { release(); }
+    ~DeviceBS() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        release();
+    }
     void release() {
         for (int s = 0; s < 2; ++s) {
             for (int k = 0; k < 3; ++k)
@@ -359,13 +370,91 @@ struct DeviceBS {
         if (sync) cudaFree(sync), sync = nullptr, sync_cap = 0;
         if (errw) cudaFree(errw), errw = nullptr, errw_cap = 0;
     }
-    static cudaError_t grow(void** p, uint64_t& cap, uint64_t need) {
+    cudaError_t grow(void** p, uint64_t& cap, uint64_t need) {
         if (need <= cap) return cudaSuccess;
+        ++moves;
+        if (gexec) {  // the graph refers to the buffer about to be freed
+            cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+        }
         if (*p) cudaFree(*p);
         *p = nullptr;
         cap = 0;
         cudaError_t e = cudaMalloc(p, need);
         if (e == cudaSuccess) cap = need;
+        return e;
+    }
+
+    // run() through a CUDA graph: the first call on a range runs directly (and sizes the buffers);
+    // a second call on the same range with no buffer moved since captures the launch sequence
+    // (it has no host waits and, the buffers being sized, no allocation); later calls replay it.
+    cudaError_t run_graph(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
+        if (trace_on()) return run(a0, b0, root, err);  // tracing waits between depths
+        if (gexec && g_a0 == a0 && g_b0 == b0) {  // no buffer moved since the capture
+            root = groot;
+            if (launches) *launches += glaunches;
+            return cudaGraphLaunch(gexec, st);
+        }
+        const bool same = seen_a0 == a0 && seen_b0 == b0 && seen_moves == moves;
+        if (!same) {
+            cudaError_t e = run(a0, b0, root, err);
+            seen_a0 = a0;
+            seen_b0 = b0;
+            seen_moves = (e == cudaSuccess && err.empty()) ? moves : ~0ull;
+            return e;
+        }
+        // capture
+        if (gexec) {
+            cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+        }
+        uint64_t* saved = launches;
+        uint64_t counted = 0;
+        launches = &counted;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+#ifdef PG_GRAPH_DEBUG
+        std::fprintf(stderr, "[graph] begin capture: %s\n", cudaGetErrorString(e));
+#endif
+        if (e != cudaSuccess) {
+            launches = saved;
+            cudaGetLastError();
+            return run(a0, b0, root, err);
+        }
+        const uint64_t m0 = moves;
+        cudaError_t er = run(a0, b0, root, err);
+        e = cudaStreamEndCapture(st, &g);
+        launches = saved;
+#ifdef PG_GRAPH_DEBUG
+        std::fprintf(stderr, "[graph] run in capture: %s, end capture: %s, moves %llu -> %llu\n",
+                     cudaGetErrorString(er), cudaGetErrorString(e), (unsigned long long)m0, (unsigned long long)moves);
+#endif
+        if (er != cudaSuccess || e != cudaSuccess || !err.empty() || moves != m0) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            seen_moves = ~0ull;
+            if (!err.empty()) return cudaErrorInvalidValue;
+            return run(a0, b0, root, err);  // run directly instead
+        }
+        e = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+#ifdef PG_GRAPH_DEBUG
+        std::fprintf(stderr, "[graph] instantiate: %s\n", cudaGetErrorString(e));
+#endif
+        if (e != cudaSuccess) {
+            gexec = nullptr;
+            cudaGetLastError();
+            return run(a0, b0, root, err);
+        }
+        groot = root;
+        g_a0 = a0;
+        g_b0 = b0;
+        glaunches = counted;
+        if (launches) *launches += counted;
+        e = cudaGraphLaunch(gexec, st);
+#ifdef PG_GRAPH_DEBUG
+        std::fprintf(stderr, "[graph] first launch: %s\n", cudaGetErrorString(e));
+#endif
         return e;
     }
 
@@ -566,7 +655,7 @@ struct DeviceBS {
         c.a0 = a0;
         c.b0 = b0;
         c.depth = depth;
-        e = launch_crt(c, jobs * bpj, st);
+        e = launch_crt(c, jobs * bpj, st, maxw);
         if (launches) ++*launches;
         (void)C;
         return e;
@@ -684,7 +773,7 @@ pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView
     bs.st = ctx_stream(ctx);
     bs.launches = ctx_launches(ctx);
     std::string err;
-    cudaError_t e = bs.run(a, b, root, err);
+    cudaError_t e = bs.run_graph(a, b, root, err);
     if (!err.empty()) {
         ctx_set_error(ctx, err);
         return PG_ERR_TOO_LARGE;

@@ -346,4 +346,114 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
     }
 }
 
+// Short jobs (at most 32 * kCrtWords output words): one warp per job, no look-back. The same
+// arithmetic as crt_carry_kernel: Garner lift, word sums, per-lane carry transfer functions, a
+// warp scan; the job's final carry must be zero.
+constexpr uint64_t kCrtWarpWords = 32 * kCrtWords;
+
+__global__ void __launch_bounds__(256) crt_warp_kernel(CrtParams P, uint64_t njobs) {
+    const uint64_t job = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (job >= njobs) return;
+    const CrtJob J = crt_job(P, job);
+    const uint64_t j0 = (uint64_t)lane * kCrtWords;
+    const uint32_t* r0 = J.res;
+    const uint32_t* r1 = J.res + P.L;
+    const uint32_t* r2 = J.res + 2 * P.L;
+    const bool cen = J.centred;
+    uint32_t a0[kCrtWords], a1[kCrtWords], a2[kCrtWords];
+#pragma unroll
+    for (int u = 0; u < kCrtWords; ++u) {
+        const uint64_t i = j0 + u;
+        if (i < P.L) {
+            const X3 x = crt3(r0[i], r1[i], r2[i], P.k, cen);
+            a0[u] = x.w0;
+            a1[u] = x.w1;
+            a2[u] = x.w2;
+        } else {
+            a0[u] = a1[u] = a2[u] = 0;
+        }
+    }
+    uint32_t pw1 = __shfl_up_sync(0xffffffffu, a1[kCrtWords - 1], 1);
+    uint32_t pw2a = __shfl_up_sync(0xffffffffu, a2[kCrtWords - 1], 1);
+    uint32_t pw2b = __shfl_up_sync(0xffffffffu, a2[kCrtWords - 2], 1);
+    if (lane == 0) pw1 = pw2a = pw2b = 0;
+    int64_t W[kCrtWords];
+#pragma unroll
+    for (int u = 0; u < kCrtWords; ++u) {
+        int64_t w = (int64_t)a0[u];
+        w += (int64_t)((u >= 1) ? a1[u - 1] : pw1);
+        w += (int64_t)(int32_t)((u >= 2) ? a2[u - 2] : (u == 1 ? pw2a : pw2b));
+        W[u] = w;
+    }
+    uint32_t f;
+    {
+        int64_t acc = 0;
+        bool ones_hi = true, zero_hi = true;
+        uint32_t low0 = 0;
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u) {
+            acc += W[u];
+            const uint32_t o = (uint32_t)acc;
+            if (u == 0) {
+                low0 = o;
+            } else {
+                ones_hi &= (o == 0xffffffffu);
+                zero_hi &= (o == 0u);
+            }
+            acc >>= 32;
+        }
+        const int c0 = (int)acc;
+        const int fm1 = c0 - ((zero_hi && low0 == 0u) ? 1 : 0);
+        const int f1 = c0 + ((ones_hi && low0 == 0xffffffffu) ? 1 : 0);
+        const int f2 = c0 + ((ones_hi && low0 >= 0xfffffffeu) ? 1 : 0);
+        f = (uint32_t)(fm1 + 1) | ((uint32_t)(c0 + 1) << 2) | ((uint32_t)(f1 + 1) << 4) | ((uint32_t)(f2 + 1) << 6);
+    }
+    uint32_t incl = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = fcompose(incl, o);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = kFIdentity;
+    const int c = (int)fapply(excl, 1u) - 1;  // carry into this lane's words (job carry-in 0)
+    uint32_t o[kCrtWords];
+    int top = -1;
+    bool spill = false;  // a non-zero word past the job's end
+    {
+        int64_t acc = c;
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u) {
+            acc += W[u];
+            o[u] = (uint32_t)acc;
+            if (o[u] != 0) {
+                if (j0 + u < J.nwords)
+                    top = u;
+                else
+                    spill = true;
+            }
+            acc >>= 32;
+        }
+    }
+    if (j0 + kCrtWords <= J.nwords) {
+#pragma unroll
+        for (int u = 0; u < kCrtWords; u += 4)
+            *reinterpret_cast<uint4*>(J.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < kCrtWords; ++u)
+            if (j0 + u < J.nwords) J.out[j0 + u] = o[u];
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const bool bad = __any_sync(0xffffffffu, spill) || fapply(total, 1u) != 1u;
+    if (lane == 0 && bad) atomicExch(P.error, 2u);  // the result does not fit its words
+    if (J.len) {
+        uint32_t lim = top >= 0 ? (uint32_t)((j0 + top) / 2 + 1) : 0u;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) lim = max(lim, __shfl_xor_sync(0xffffffffu, lim, off));
+        if (lane == 0 && lim) atomicMax(J.len, lim);
+    }
+}
+
 }  // namespace pg

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "crt_carry.cuh"
@@ -29,14 +30,16 @@ uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)
 //   [dir][prime] stage  : entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
 //   [dir][prime] fs_lo  : w_{2^26}^j
 //   [dir][prime] fs_hi  : w_{2^26}^(2^13 j)
-//   [n][dir][prime] row : w_{2^n}^e for four-step blocks of 2^n points, n = 14..26
+//   [n][l][dir][prime] row : w_{2^n}^(c bitrev_l(m)) at m * 2^(13-l) + c, for four-step blocks of
+//                            2^n points (n = 14..26) and strided sub-transforms of 2^l points (l = 5..10)
 cudaError_t DeviceTables::build(int device) {
     (void)device;
     constexpr size_t kEnt = 1u << 13;
     constexpr size_t kTables = (3 + kRowTables) * 2 * kNumPrimes;
     std::vector<uint2> h(kTables * kEnt);
-    for (int dir = 0; dir < 2; ++dir) {
-        for (int j = 0; j < kNumPrimes; ++j) {
+    // one host thread per (direction, prime): the tables of each pair are independent
+    auto fill = [&](int dir, int j) {
+        {
             const uint32_t p = kPrime(j);
             uint32_t w26 = pow_mod(kGenerator(j), (uint64_t)(p - 1) >> kMaxLogL, p);  // primitive 2^26-th root
             if (dir == 1) w26 = inv_mod(w26, p);
@@ -56,14 +59,29 @@ cudaError_t DeviceTables::build(int device) {
             }
             for (int n = kRowLogMin; n <= kMaxLogL; ++n) {
                 const uint64_t wn = pow_mod(w26, 1ull << (kMaxLogL - n), p);  // w_{2^n}
-                uint2* row = h.data() + (((size_t)(3 * 2 + (n - kRowLogMin) * 2 + dir)) * kNumPrimes + j) * kEnt;
-                uint64_t r = 1;
-                for (size_t i = 0; i < kEnt; ++i) {
-                    row[i] = make_uint2((uint32_t)r, shoup_companion((uint32_t)r, p));
-                    r = r * wn % p;
+                for (int l = kRowNMin; l <= kRowNMax; ++l) {
+                    const int t = ((n - kRowLogMin) * (kRowNMax - kRowNMin + 1) + (l - kRowNMin)) * 2 + dir;
+                    uint2* row = h.data() + ((size_t)(3 * 2 * kNumPrimes) + (size_t)t * kNumPrimes + j) * kEnt;
+                    const uint32_t C = 1u << (kTileLog - l);
+                    for (uint32_t m = 0; m < (1u << l); ++m) {
+                        uint32_t k = 0;  // bitrev_l(m)
+                        for (int b = 0; b < l; ++b) k |= ((m >> b) & 1u) << (l - 1 - b);
+                        const uint64_t step = pow_mod((uint32_t)wn, k, p);
+                        uint64_t r = 1;
+                        for (uint32_t c = 0; c < C; ++c) {
+                            row[m * C + c] = make_uint2((uint32_t)r, shoup_companion((uint32_t)r, p));
+                            r = r * step % p;
+                        }
+                    }
                 }
             }
         }
+    };
+    {
+        std::vector<std::thread> th;
+        for (int dir = 0; dir < 2; ++dir)
+            for (int j = 0; j < kNumPrimes; ++j) th.emplace_back(fill, dir, j);
+        for (auto& t : th) t.join();
     }
     cudaError_t e = cudaMalloc(&base, h.size() * sizeof(uint2));
     if (e != cudaSuccess) return e;
@@ -223,10 +241,15 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cuda
         if (src == Source::Limbs) return run_pass<Layout::Strided, N, false, Source::Limbs, Fuse::None>(prm, tw, st); \
         return run_pass<Layout::Strided, N, false, Source::Residues, Fuse::None>(prm, tw, st);
 
-cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm,
+cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm0,
                         const TwiddleTables& tw, cudaStream_t st) {
     const int logN = plan.logN[pass];
     const bool contig = (pass == plan.npass - 1);
+    PassParams prm = prm0;
+    if (!contig) {
+        prm.rowB = row_table(tw, plan.logN[pass] + plan.logS[pass], logN, inverse ? 1 : 0);
+        if (!prm.rowB) return cudaErrorInvalidValue;  // no four-step table for this split
+    }
     if (contig) {
         if (inverse && (src != Source::Residues || fuse != Fuse::None)) return cudaErrorInvalidValue;
         switch (logN) {
@@ -255,7 +278,12 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
     }
 }
 
-cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st) {
+cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st, uint64_t max_words) {
+    if (max_words && max_words <= kCrtWarpWords && c.blocks_per_job == 1) {
+        // blocks == jobs here: one warp per job
+        crt_warp_kernel<<<(unsigned)((blocks * 32 + 255) / 256), 256, 0, st>>>(c, blocks);
+        return cudaGetLastError();
+    }
     crt_carry_kernel<<<(unsigned)blocks, kCrtThreads, 0, st>>>(c);
     return cudaGetLastError();
 }
@@ -392,7 +420,8 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
     c.blocks_per_job = crt_blocks;
     c.merge = 0;
     c.k = make_crt_consts(logL);
-    crt_carry_kernel<<<(unsigned)crt_blocks, kCrtThreads, 0, st>>>(c);
+    e = launch_crt(c, crt_blocks, st, nwords);
+    if (e != cudaSuccess) return e;
     if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + 1;
     return cudaGetLastError();
 }

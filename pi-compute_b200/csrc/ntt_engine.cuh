@@ -19,8 +19,9 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
 
 CrtConsts make_crt_consts(int logL);
 
-// Launch the CRT + carry kernel over `blocks` blocks.
-cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st);
+// Launch the CRT + carry over `blocks` blocks (jobs * blocks_per_job). max_words, when given, is
+// the longest job's word count: jobs of at most 32 * 16 words run one warp each.
+cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st, uint64_t max_words = 0);
 
 // Stride and four-step block size of pass i.
 void set_pass(PassParams& p, const Plan& plan, int i);

@@ -29,30 +29,32 @@
 
 namespace pg {
 
+// CTAs per SM each pass layout's register budget is sized for: strided tiles 3 (<= 80 registers;
+// fewer registers spill the four-step factors), contiguous tiles 4 (<= 64 registers).
+template <Layout LAY>
+constexpr int pass_min_blocks() {
+    return LAY == Layout::Strided ? 3 : 4;
+}
+
 __device__ __forceinline__ uint32_t bitrev_n(uint32_t x, int logn) {
     return logn == 0 ? 0u : (__brev(x) >> (32 - logn));
 }
 
 // Four-step twiddles of a strided tile. Element (row m, tile column c) of the tile whose
 // first column is t0 is multiplied by w_{N'}^{(t0 + c) k}, k = bitrev(m), written as
-//   A[m] * B[c k],  A[m] = w_{N'}^{t0 k} (per tile, kept in shared memory),
-//                   B[e] = w_{N'}^e, e = c k < C * N = 2^13 (the row power table of N').
-// Each factor is a (w, w') Shoup pair, so an element costs two Shoup products; the first may
-// stay lazy because Shoup accepts any 32-bit input.
-__device__ __forceinline__ void fourstep_twiddle4(uint4& x, uint32_t c, uint32_t k, uint2 A, const uint2* B,
-                                                  uint32_t p) {
-    uint32_t e = c * k;
-    const uint2 b0 = __ldg(B + e);
-    e += k;
-    const uint2 b1 = __ldg(B + e);
-    e += k;
-    const uint2 b2 = __ldg(B + e);
-    e += k;
-    const uint2 b3 = __ldg(B + e);
-    x.x = mul_shoup(mul_shoup_lazy(x.x, b0.x, b0.y, p), A.x, A.y, p);
-    x.y = mul_shoup(mul_shoup_lazy(x.y, b1.x, b1.y, p), A.x, A.y, p);
-    x.z = mul_shoup(mul_shoup_lazy(x.z, b2.x, b2.y, p), A.x, A.y, p);
-    x.w = mul_shoup(mul_shoup_lazy(x.w, b3.x, b3.y, p), A.x, A.y, p);
+//   A[m] * B[m][c],  A[m] = w_{N'}^{t0 k} (per tile, kept in shared memory),
+//                    B[m][c] = w_{N'}^{c k} (the tile-shape table of (N', N), row-major).
+// The four consecutive columns c..c+3 of one row are two 16-byte loads, consecutive across the
+// lanes of a warp. Each factor is a (w, w') Shoup pair, so an element costs two Shoup products;
+// the first may stay lazy because Shoup accepts any 32-bit input.
+__device__ __forceinline__ void fourstep_twiddle4(uint4& x, uint32_t c, uint32_t m, int logc, uint2 A,
+                                                  const uint2* B, uint32_t p) {
+    const uint4* b = reinterpret_cast<const uint4*>(B + ((size_t)m << logc) + c);
+    const uint4 b01 = __ldg(b), b23 = __ldg(b + 1);
+    x.x = mul_shoup(mul_shoup_lazy(x.x, b01.x, b01.y, p), A.x, A.y, p);
+    x.y = mul_shoup(mul_shoup_lazy(x.y, b01.z, b01.w, p), A.x, A.y, p);
+    x.z = mul_shoup(mul_shoup_lazy(x.z, b23.x, b23.y, p), A.x, A.y, p);
+    x.w = mul_shoup(mul_shoup_lazy(x.w, b23.z, b23.w, p), A.x, A.y, p);
 }
 
 // One decimation-in-frequency round of radix R = 2^LR on v[0..R), the group's
@@ -276,7 +278,7 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
 template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE>
-__global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, TwiddleTables T) {
+__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
     extern __shared__ uint32_t sm[];
     constexpr int LOGC = LOGE - LOGN;
     constexpr uint32_t E = 1u << LOGE;
@@ -301,7 +303,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
     uint2* smA = reinterpret_cast<uint2*>(sm + E);
     const uint2* rowB = nullptr;
     if constexpr (LAY == Layout::Strided) {
-        rowB = row_table(T, P.logNp, dir, j);
+        rowB = P.rowB + (size_t)j * (1u << kFsLog);
         const uint32_t t0 = tcol<LAY, LOGN, LOGE>(stile, 0, P.logS);
         const int sh = kMaxLogL - P.logNp;
         const uint2* lo = T.fs_lo[dir][j];
@@ -358,7 +360,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
         }
         if constexpr (INV && LAY == Layout::Strided) {
             // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m))
-            fourstep_twiddle4(x, c, bitrev_n(m, LOGN), smA[m], rowB, p);
+            fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
         }
         *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
     }
@@ -410,7 +412,7 @@ __global__ void __launch_bounds__(NTHREADS) ntt_pass_kernel(PassParams P, Twiddl
         }
         uint4 x = *reinterpret_cast<uint4*>(sm + swz(e4));
         if constexpr (!INV && LAY == Layout::Strided) {
-            fourstep_twiddle4(x, c, bitrev_n(m, LOGN), smA[m], rowB, p);
+            fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
         }
         *reinterpret_cast<uint4*>(P.out + job * P.job_stride + prime_off + g) = x;
     }
@@ -557,7 +559,7 @@ __global__ void __launch_bounds__(NTHREADS, pipe_min_blocks<FUSE>())
         const uint2* rowB = nullptr;
         if constexpr (LAY == Layout::Strided) {
             // four-step row factors of this tile (no dependence on its data: overlaps the copies)
-            rowB = row_table(T, P.logNp, dir, j);
+            rowB = P.rowB + (size_t)j * (1u << kFsLog);
             const uint32_t t0 = tcol<LAY, LOGN, LOGE>(t & ((1ull << logTpj) - 1), 0, P.logS);
             const int sh = kMaxLogL - P.logNp;
             const uint2* lo = pick3(T.fs_lo[dir], j);
@@ -586,7 +588,7 @@ __global__ void __launch_bounds__(NTHREADS, pipe_min_blocks<FUSE>())
                                    reduce_u32(x.w, p, one_p));
                 } else {
                     const uint32_t m = e4 >> LOGC, c = e4 & ((1u << LOGC) - 1);
-                    fourstep_twiddle4(x, c, bitrev_n(m, LOGN), smA[m], rowB, p);
+                    fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
                 }
                 *reinterpret_cast<uint4*>(cur + swz(e4)) = x;
             }
@@ -621,7 +623,7 @@ __global__ void __launch_bounds__(NTHREADS, pipe_min_blocks<FUSE>())
             uint64_t job, g;
             if (!locate(t, e4, m, c, job, g)) continue;
             uint4 x = *reinterpret_cast<uint4*>(cur + swz(e4));
-            if constexpr (!INV && LAY == Layout::Strided) fourstep_twiddle4(x, c, bitrev_n(m, LOGN), smA[m], rowB, p);
+            if constexpr (!INV && LAY == Layout::Strided) fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
             *reinterpret_cast<uint4*>(P.out + job * P.job_stride + prime_off + g) = x;
         }
         __syncthreads();  // cur, oth and smA are reused by the next iteration

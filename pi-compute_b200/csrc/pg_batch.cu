@@ -349,7 +349,7 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
         c.k = make_crt_consts(logL);
         c.merge = 2;
         c.dtab = W->d_dst + k0;
-        e = launch_crt(c, m * bpj, st);
+        e = launch_crt(c, m * bpj, st, maxw);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "batch CRT");
         ++*launches;
         k0 = k1;

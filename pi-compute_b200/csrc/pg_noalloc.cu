@@ -8,8 +8,9 @@
 // device arrays of fixed size:
 //   g_noalloc_scratch  residues of both operands for transforms up to 2^15 points plus the
 //                      carry look-back words: 786,688 bytes;
-//   g_noalloc_tables   the twiddle tables (same layout as DeviceTables, row power tables
-//                      for four-step blocks of 2^14 and 2^15 points only): 1,966,080 bytes.
+//   g_noalloc_tables   the twiddle tables (DeviceTables' layout, four-step factor tables only
+//                      for the strided passes these sizes use: blocks of 2^14 and 2^15 points
+//                      split into sub-transforms of 2^7): 1,966,080 bytes.
 // Every GPU that loads libpigpu.so holds these ~2.8 MB until the process exits.
 //
 // Set-up: the first call on a device (with that device current) looks up the arrays'
@@ -36,7 +37,10 @@ constexpr size_t kResWords = (size_t)pg::kNumPrimes << kNoAllocLogL;  // per ope
 constexpr size_t kSyncWords = 64;           // error, ticket, look-back status (<= 8 CRT blocks used)
 constexpr size_t kScratchWords = 2 * kResWords + kSyncWords;
 constexpr size_t kTableEnt = 1u << pg::kFsLog;
-constexpr int kRowTypes = kNoAllocLogL - pg::kRowLogMin + 1;  // four-step blocks of 2^14, 2^15 points
+// Four-step factor tables of the strided passes of these sizes (make_plan: L = 2^14 -> 2^7 x 2^7,
+// L = 2^15 -> 2^7 x 2^8): block 2^14 or 2^15, sub-transform 2^7.
+constexpr int kRowTypes = 2;
+constexpr int kRowLogN = 7;
 constexpr size_t kTableWords = (3 + kRowTypes) * 2 * pg::kNumPrimes * kTableEnt;
 
 static_assert(kTableEnt == (1u << (pg::kStageLog - 1)), "stage and four-step tables share one length");
@@ -69,9 +73,8 @@ __device__ uint32_t dev_pow_mod(uint32_t b, uint64_t e, uint32_t p) {
     return (uint32_t)r;
 }
 
-// Fills the table array in the layout of DeviceTables::build:
-// [type: stage, fs_lo, fs_hi, row 2^14, row 2^15][dir][prime][kTableEnt];
-// roots[dir][prime] = w_{2^26}^(+-1).
+// Fills the table array: [type: stage, fs_lo, fs_hi, four-step (2^14, 2^7), four-step (2^15, 2^7)]
+// [dir][prime][kTableEnt]; roots[dir][prime] = w_{2^26}^(+-1).
 __global__ void fill_tables_kernel(uint2* t, uint32_t r0f, uint32_t r1f, uint32_t r2f, uint32_t r0i, uint32_t r1i,
                                    uint32_t r2i) {
     const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -90,8 +93,12 @@ __global__ void fill_tables_kernel(uint2* t, uint32_t r0f, uint32_t r1f, uint32_
         e = i;                                                // w_{2^26}^i
     else if (type == 2)
         e = (uint64_t)i << pg::kFsLog;                        // w_{2^26}^(2^13 i)
-    else
-        e = (uint64_t)i << (pg::kMaxLogL - (pg::kRowLogMin + type - 3));  // w_{2^n}^i
+    else {
+        // w_{2^n}^(c bitrev_7(m)) at m * 2^6 + c, n = 14 + (type - 3)
+        const uint32_t m = i >> (pg::kTileLog - kRowLogN), c = i & ((1u << (pg::kTileLog - kRowLogN)) - 1);
+        const uint32_t k = __brev(m) >> (32 - kRowLogN);
+        e = (uint64_t)(c * k) << (pg::kMaxLogL - (pg::kRowLogMin + type - 3));
+    }
     const uint32_t w = dev_pow_mod(root, e, p);
     t[idx] = make_uint2(w, (uint32_t)(((uint64_t)w << 32) / p));
 }
@@ -120,6 +127,7 @@ pg_status setup_device(int dev, cudaStream_t st) {
             d.tw.fs_hi[dir][j] = tables + ((2 * 2 + dir) * pg::kNumPrimes + j) * kTableEnt;
         }
     d.tw.row = tables + (size_t)3 * 2 * pg::kNumPrimes * kTableEnt;
+    d.tw.row_layout = 1;
     d.scratch = scratch;
     d.ready = true;
     return PG_OK;

@@ -160,7 +160,7 @@ struct SharedProduct {
             c.blocks_per_job = bpj;
             c.k = make_crt_consts(logL);
             c.merge = 0;
-            check(launch_crt(c, m * bpj, st));
+            check(launch_crt(c, m * bpj, st, nwords));
             ++*launches;
         }
     }

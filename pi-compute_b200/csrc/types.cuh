@@ -26,21 +26,34 @@ __host__ __device__ inline uint32_t stage_exponent(uint32_t i) {
     return (i - (1u << k)) << (kStageLog - 1 - k);
 }
 
-constexpr int kRowLogMin = 14;  // row power tables exist for four-step blocks of 2^14 .. 2^26 points
-constexpr int kRowTables = kMaxLogL - kRowLogMin + 1;
+constexpr int kRowLogMin = 14;  // row tables exist for four-step blocks of 2^14 .. 2^26 points
+constexpr int kRowNMin = 5, kRowNMax = 10;  // and strided sub-transforms of 2^5 .. 2^10 points
+constexpr int kRowTables = (kMaxLogL - kRowLogMin + 1) * (kRowNMax - kRowNMin + 1);  // per (dir, prime)
 
 struct TwiddleTables {
     // (w, w') Shoup pairs, [dir][prime]; dir 0 = forward (w), 1 = inverse (w^-1).
     const uint2* stage[2][kNumPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), 2^13 entries
     const uint2* fs_lo[2][kNumPrimes];  // w_{2^26}^j,           j < 2^13
     const uint2* fs_hi[2][kNumPrimes];  // w_{2^26}^(2^13 * i),  i < 2^13
-    // Row powers of the four-step blocks: for a block of 2^n points (n >= kRowLogMin), table
-    // ((n - kRowLogMin) * 2 + dir) * kNumPrimes + prime holds w_{2^n}^e for e < 2^13.
+    // Four-step factors of strided tiles: for a block of N' = 2^n points split into sub-transforms
+    // of N = 2^l points (tile of C = 2^(13 - l) columns), table
+    // (((n - kRowLogMin) * 6 + l - kRowNMin) * 2 + dir) * kNumPrimes + prime holds
+    // w_{N'}^(c * bitrev_l(m)) at entry m * C + c (row-major, so a tile row reads consecutively).
     const uint2* row;
+    // 0: the layout above for every (n, l); 1: only (14, 7) then (15, 7) (the fixed-size tables
+    // of pg_mul_noalloc), [n][dir][prime].
+    int row_layout;
 };
 
-__host__ __device__ inline const uint2* row_table(const TwiddleTables& T, int logNp, int dir, int prime) {
-    return T.row + ((size_t)((logNp - kRowLogMin) * 2 + dir) * kNumPrimes + prime) * (1u << kFsLog);
+// Prime-0 four-step factor table of a strided pass (prime j at + j * 2^13), or null.
+inline const uint2* row_table(const TwiddleTables& T, int logNp, int logN, int dir) {
+    if (T.row_layout == 1) {
+        if (logN != 7 || logNp < 14 || logNp > 15) return nullptr;
+        return T.row + ((size_t)((logNp - 14) * 2 + dir) * kNumPrimes) * (1u << kFsLog);
+    }
+    if (logNp < kRowLogMin || logNp > kMaxLogL || logN < kRowNMin || logN > kRowNMax) return nullptr;
+    const int t = ((logNp - kRowLogMin) * (kRowNMax - kRowNMin + 1) + (logN - kRowNMin)) * 2 + dir;
+    return T.row + ((size_t)t * kNumPrimes) * (1u << kFsLog);
 }
 
 enum class Layout : int { Strided = 0, Contig = 1 };
@@ -94,6 +107,7 @@ struct PassParams {
                              // (job = 6*merge + operand), 2 from src[job]
     MergeSrc ms;
     const SrcEntry* src;
+    const uint2* rowB;       // strided passes: four-step factor table of prime 0 (set by launch_pass)
 };
 
 struct CrtConsts {

@@ -151,6 +151,18 @@ def test_batched_bs_golden_hash_1m_terms(lib):
 
 
 @pytest.mark.gpu
+def test_batched_bs_repeated_range_replays_graph(lib):
+    """The same range split three times: run directly, then captured into a CUDA graph, then
+    replayed; every result equals the oracle's."""
+    want = oracle.bs(0, 5000)
+    for _ in range(3):
+        assert bs(lib, 0, 5000, BATCHED) == want
+    # a different range in between invalidates nothing it should not
+    assert bs(lib, 100, 357, BATCHED) == oracle.bs(100, 357)
+    assert bs(lib, 0, 5000, BATCHED) == want
+
+
+@pytest.mark.gpu
 def test_batched_digits_1000_and_1m(lib):
     s, _ = pi_digits(lib, 1000, BATCHED)
     assert s == open(os.path.join(GOLDEN, "pi_1000.txt")).read()

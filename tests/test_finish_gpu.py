@@ -90,6 +90,20 @@ def test_pg_pi_prefixes(eng, digits):
         assert got[:1002] == ref
 
 
+def test_pg_pi_repeated_and_interleaved_runs(eng):
+    """Runs that repeat a digit count replay the splitting's captured CUDA graph; interleaving
+    other counts (which reallocate its buffers) must never replay a stale graph."""
+    ref = open(os.path.join(GOLDEN, "pi_1000.txt")).read().strip()
+    first = eng.pi(30_000)
+    assert first.decode()[:1002] == ref
+    for d in (30_000, 30_000, 200, 30_000, 200_000, 30_000, 30_000):
+        got = eng.pi(d)
+        if d == 30_000:
+            assert got == first
+        else:
+            assert got.decode()[:202] == ref[:202]
+
+
 @pytest.mark.parametrize("digits", [1_000_000, 10_000_000, 100_000_000])
 def test_pg_pi_matches_reference_hash(eng, digits):
     golden = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))[str(digits)]
