@@ -29,11 +29,14 @@
 
 namespace pg {
 
+#ifndef PG_STRIDED_MINB
+#define PG_STRIDED_MINB 3
+#endif
 // CTAs per SM each pass layout's register budget is sized for: strided tiles 3 (<= 80 registers;
 // fewer registers spill the four-step factors), contiguous tiles 4 (<= 64 registers).
 template <Layout LAY>
 constexpr int pass_min_blocks() {
-    return LAY == Layout::Strided ? 3 : 4;
+    return LAY == Layout::Strided ? PG_STRIDED_MINB : 4;
 }
 
 __device__ __forceinline__ uint32_t bitrev_n(uint32_t x, int logn) {

@@ -1,5 +1,9 @@
 // C ABI of libpigpu.so (declarations and reference citations in include/pi_b200.h).
 #include <cuda_runtime.h>
+#include <dlfcn.h>
+
+#include <cstdio>
+#include <cstdlib>
 
 #include <algorithm>
 #include <cstring>
@@ -181,6 +185,28 @@ pg_status pg_create(int device, pg_ctx** out) {
         cudaGetLastError();
         pg_destroy(c);
         return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
+    }
+    // Pass splits measured by pg_tune on this GPU model: PG_TUNE_FILE, else tune_b200.txt beside
+    // the library (an empty PG_TUNE_FILE keeps the built-in splits). A missing file changes
+    // nothing; an invalid one is reported in pg_last_error and ignored.
+    {
+        std::string path;
+        if (const char* env = std::getenv("PG_TUNE_FILE")) {
+            path = env;
+        } else {
+            Dl_info info;
+            if (dladdr(reinterpret_cast<void*>(&pg_version), &info) && info.dli_fname) {
+                std::string lib = info.dli_fname;
+                const size_t slash = lib.rfind('/');
+                path = (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/tune_b200.txt";
+            }
+        }
+        if (!path.empty()) {
+            if (FILE* f = std::fopen(path.c_str(), "r")) {
+                std::fclose(f);
+                if (pg_tune_load(c, path.c_str()) != PG_OK) c->last_error = "ignored " + path + ": " + c->last_error;
+            }
+        }
     }
     *out = c;
     return PG_OK;
