@@ -30,13 +30,17 @@
 namespace pg {
 
 #ifndef PG_STRIDED_MINB
-#define PG_STRIDED_MINB 3
+#define PG_STRIDED_MINB 4
 #endif
-// CTAs per SM each pass layout's register budget is sized for: strided tiles 3 (<= 80 registers;
-// fewer registers spill the four-step factors), contiguous tiles 4 (<= 64 registers).
-template <Layout LAY>
+// CTAs per SM each pass kernel's register budget is sized for (4: <= 64 registers). At 4 the
+// strided passes spill a few words to L1 and still run faster than at 3 (80 registers): more
+// warps hide the global-load latency they are bound by.
+#ifndef PG_FUSED_MINB
+#define PG_FUSED_MINB 4
+#endif
+template <Layout LAY, Fuse FUSE>
 constexpr int pass_min_blocks() {
-    return LAY == Layout::Strided ? PG_STRIDED_MINB : 4;
+    return LAY == Layout::Strided ? PG_STRIDED_MINB : (FUSE == Fuse::None ? 4 : PG_FUSED_MINB);
 }
 
 __device__ __forceinline__ uint32_t bitrev_n(uint32_t x, int logn) {
@@ -82,7 +86,10 @@ __device__ __forceinline__ void dif_round(uint32_t (&v)[1 << LR], uint32_t tp, i
                 v[q + half] = sub_mod(a, b, p);
             } else {
                 uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
-                uint2 w = __ldg(stw + ((1u << logh) + x));
+                // stride 1: w_{2h}^x = w_{2^LR}^(x 2^k), all from the round's top entries, so equal
+                // twiddles of different stages share one load
+                const uint32_t idx = logs == 0 ? (1u << (LR - 1)) + (x << k) : (1u << logh) + x;
+                uint2 w = __ldg(stw + idx);
                 v[q + half] = mul_shoup(a - b + p, w.x, w.y, p);
             }
         }
@@ -105,7 +112,9 @@ __device__ __forceinline__ void dit_round(uint32_t (&v)[1 << LR], uint32_t tp, i
             uint32_t b = v[q + half];
             if (!(logs == 0 && (q & (half - 1)) == 0)) {
                 uint32_t x = tp + ((uint32_t)(q & (half - 1)) << logs);
-                uint2 w = __ldg(stw + ((1u << logh) + x));
+                // stride 1: stage k's w_{2^(k+1)}^x = w_{2^LR}^(x 2^(LR-1-k)) from the top entries
+                const uint32_t idx = logs == 0 ? (1u << (LR - 1)) + (x << (LR - 1 - k)) : (1u << logh) + x;
+                uint2 w = __ldg(stw + idx);
                 b = mul_shoup(b, w.x, w.y, p);
             }
             v[q] = add_mod(a, b, p);
@@ -137,7 +146,8 @@ __device__ __forceinline__ uint32_t sidx(uint32_t m, uint32_t c) {
 
 // Run the radix rounds of one sub-transform direction over the whole tile.
 // Stages are processed from half size N/2 down to 1 (DIF) or 1 up to N/2 (DIT).
-template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV>
+// Rounds [RR0, RR1) of the schedule run (in the direction's order); the default is all of them.
+template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, int RR0 = 0, int RR1 = 64>
 __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, uint32_t p) {
     constexpr int LOGC = LOGE - LOGN;
     // Radix schedule: the remainder (LOGN % 4 stages) is the top round (largest stride), then
@@ -148,6 +158,7 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
     constexpr int NROUND = NFULL + (REM ? 1 : 0);
 #pragma unroll
     for (int rr = 0; rr < NROUND; ++rr) {
+        if (rr < RR0 || rr >= RR1) continue;
         // DIF: the first rounds take the highest stages. DIT: reversed order.
         const int r = INV ? (NROUND - 1 - rr) : rr;
         const bool is_rem = (REM != 0) && (r == 0);
@@ -281,7 +292,7 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
 template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE>
-__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
+__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
     extern __shared__ uint32_t sm[];
     constexpr int LOGC = LOGE - LOGN;
     constexpr uint32_t E = 1u << LOGE;
@@ -369,31 +380,67 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY>()) ntt_pass_ker
     }
     __syncthreads();
 
-    tile_transform<LAY, LOGN, LOGE, NTHREADS, INV>(sm, T.stage[dir][j], p);
-
-    if constexpr (FUSE != Fuse::None) {
+    if constexpr (FUSE == Fuse::None) {
+        tile_transform<LAY, LOGN, LOGE, NTHREADS, INV>(sm, T.stage[dir][j], p);
+    } else {
+        // Forward rounds but the last; then, per 16-word group, the last forward round (stride 1),
+        // the pointwise product and the first inverse round (stride 1, the same 16 words) in
+        // registers; then the remaining inverse rounds.
         static_assert(LAY == Layout::Contig && !INV, "pointwise fusion happens in the last forward pass");
-        for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
-            uint32_t c = e4 >> LOGN, m = e4 & ((1u << LOGN) - 1);
+        constexpr int NROUND = LOGN / 4 + ((LOGN % 4) ? 1 : 0);
+        const uint2* stw_f = T.stage[0][j];
+        const uint2* stw_i = T.stage[1][j];
+        tile_transform<LAY, LOGN, LOGE, NTHREADS, false, 0, NROUND - 1>(sm, stw_f, p);
+        constexpr int NG = (1 << LOGE) / 16;
+#pragma unroll 1
+        for (uint32_t g = threadIdx.x; g < NG; g += NTHREADS) {
+            const uint32_t blk = g & ((1u << (LOGN - 4)) - 1);
+            const uint32_t c = g >> (LOGN - 4);
+            const uint32_t m0 = blk * 16;
+            const uint32_t x0 = (c << LOGN) + m0;
             const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
-            if (R >= total_rows) continue;
-            const uint64_t job = R >> logRows;
-            uint64_t g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);
-            uint4 a = *reinterpret_cast<uint4*>(sm + swz(e4));
-            uint4 b;
+            const bool live = R < total_rows;
+            uint4 o[4];
             if constexpr (FUSE == Fuse::MulInverse) {
-                b = *reinterpret_cast<const uint4*>(P.other + job * P.other_stride + prime_off + g);
-            } else {
-                b = a;
+                // the other operand's 16 words, issued before the butterflies so the load overlaps
+                // them (rows past the end hold zeros: skip them)
+                const uint64_t job = R >> logRows;
+                const uint4* src = reinterpret_cast<const uint4*>(
+                    P.other + job * P.other_stride + prime_off + ((R & ((1ull << logRows) - 1)) << LOGN) + m0);
+#pragma unroll
+                for (int q4 = 0; q4 < 4; ++q4) o[q4] = live ? __ldg(src + q4) : make_uint4(0, 0, 0, 0);
             }
-            a.x = mul_mont(a.x, b.x, p, pinv);
-            a.y = mul_mont(a.y, b.y, p, pinv);
-            a.z = mul_mont(a.z, b.z, p, pinv);
-            a.w = mul_mont(a.w, b.w, p, pinv);
-            *reinterpret_cast<uint4*>(sm + swz(e4)) = a;
+            uint32_t v[16];
+#pragma unroll
+            for (int q4 = 0; q4 < 4; ++q4) {
+                const uint4 t = *reinterpret_cast<const uint4*>(sm + swz(x0 + 4 * q4));
+                v[4 * q4] = t.x;
+                v[4 * q4 + 1] = t.y;
+                v[4 * q4 + 2] = t.z;
+                v[4 * q4 + 3] = t.w;
+            }
+            dif_round<4>(v, 0, 0, stw_f, p);
+            if constexpr (FUSE == Fuse::MulInverse) {
+#pragma unroll
+                for (int q4 = 0; q4 < 4; ++q4) {
+                    const uint4 b = o[q4];
+                    v[4 * q4] = mul_mont(v[4 * q4], b.x, p, pinv);
+                    v[4 * q4 + 1] = mul_mont(v[4 * q4 + 1], b.y, p, pinv);
+                    v[4 * q4 + 2] = mul_mont(v[4 * q4 + 2], b.z, p, pinv);
+                    v[4 * q4 + 3] = mul_mont(v[4 * q4 + 3], b.w, p, pinv);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; ++q) v[q] = mul_mont(v[q], v[q], p, pinv);
+            }
+            dit_round<4>(v, 0, 0, stw_i, p);
+#pragma unroll
+            for (int q4 = 0; q4 < 4; ++q4)
+                *reinterpret_cast<uint4*>(sm + swz(x0 + 4 * q4)) =
+                    make_uint4(v[4 * q4], v[4 * q4 + 1], v[4 * q4 + 2], v[4 * q4 + 3]);
         }
         __syncthreads();
-        tile_transform<LAY, LOGN, LOGE, NTHREADS, true>(sm, T.stage[1][j], p);
+        tile_transform<LAY, LOGN, LOGE, NTHREADS, true, 1, 64>(sm, stw_i, p);
     }
 
     // ---- store

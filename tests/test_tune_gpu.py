@@ -13,7 +13,8 @@ from helpers import oracle, pkg
 pytestmark = pytest.mark.gpu
 
 
-def test_tune_save_load_and_products(tmp_path):
+def test_tune_save_load_and_products(tmp_path, monkeypatch):
+    monkeypatch.setenv("PG_TUNE_FILE", "")  # a context with the built-in splits only
     path = str(tmp_path / "splits.txt")
     with pkg.Engine(0) as eng:
         times = eng.tune(10, 21)
@@ -33,8 +34,23 @@ def test_tune_save_load_and_products(tmp_path):
                 assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b)), (logl, na, nb)
 
 
+def test_tuned_table_loaded_at_context_creation(tmp_path, monkeypatch):
+    """PG_TUNE_FILE (or tune_b200.txt beside the library) is applied when the context is made."""
+    src = str(tmp_path / "mine.txt")
+    open(src, "w").write("# test\n14 2 7 7 0\n20 2 10 10 0\n24 3 5 6 13\n")
+    monkeypatch.setenv("PG_TUNE_FILE", src)
+    out = str(tmp_path / "saved.txt")
+    with pkg.Engine(0) as eng:
+        eng.tune_save(out)
+        for n in (1 << 12, 1 << 18, 1 << 22):
+            a, b = pkg.random_operand(n, 5), pkg.random_operand(n - 7, 6)
+            assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b))
+    saved = [l.split() for l in open(out) if not l.startswith("#")]
+    assert saved == [["14", "2", "7", "7", "0"], ["20", "2", "10", "10", "0"], ["24", "3", "5", "6", "13"]]
+
+
 @pytest.mark.parametrize("text", ["14 2 7 8 0\n", "20 2 4 16 0\n", "26 1 26 0 0\n", "x\n", "14 4 5 5 4\n"])
-def test_tune_load_rejects_invalid(tmp_path, text):
+def test_tune_load_rejects_invalid(tmp_path, text, monkeypatch):
     path = str(tmp_path / "bad.txt")
     open(path, "w").write(text)
     with pkg.Engine(0) as eng:
