@@ -270,14 +270,16 @@ def run_b200(args):
     got = hashlib.sha256(buf.raw[: D + 2]).hexdigest()
     if want is not None and got != want:
         raise RuntimeError(f"digits differ from the reference run: sha256 {got} != {want}")
+    # the clock sampler (an nvidia-smi process) starts during the warm-up, so that its start-up
+    # does not compete with the timed steps' host work; it keeps sampling through the timed region
+    clocks = ClockSampler(local)
+    clocks.start()
     for _ in range(max(0, args.warmup - 1)):
         step()
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
-    clocks.start()
     per, phases, launches = [], [], 0
     t_all = time.perf_counter()
     for _ in range(args.steps):

@@ -141,6 +141,55 @@ __global__ void bs_pair_kernel(LevelView out, uint64_t nodes, uint64_t a0, uint6
     out.len[3 * i + 2] = nR;
 }
 
+// One thread per merge for children of at most MAXC limbs (schoolbook in thread-local arrays):
+// the bottom depths have millions of merges of a few limbs each.
+template <int MAXC>
+__global__ void __launch_bounds__(128) bs_thread_merge_kernel(LevelView in, LevelView out, uint64_t merges,
+                                                              uint64_t a0, uint64_t b0, int depth) {
+    const uint64_t m = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= merges) return;
+    uint64_t op[6][MAXC];
+    int n[6];
+#pragma unroll
+    for (int o = 0; o < 6; ++o) {
+        const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
+        const int k = o % 3;
+        n[o] = (int)in.len[3 * child + k];
+        const uint64_t* src = in.X[k] + child * in.cap[k];
+        for (int t = 0; t < n[o]; ++t) op[o][t] = src[t];
+    }
+    uint64_t a, b;
+    node_range(a0, b0, depth, m, a, b);
+    const int sgn = merge_r_sign(a, b);
+    uint64_t r0[2 * MAXC + 1], r1[2 * MAXC];
+    auto emit = [&](int k, const uint64_t* v, int nv) {
+        uint64_t* dst = out.X[k] + m * out.cap[k];
+        const int l = sb_len(v, nv < (int)out.cap[k] ? nv : (int)out.cap[k]);
+        for (int t = 0; t < (int)out.cap[k]; ++t) dst[t] = t < l ? v[t] : 0;
+        out.len[3 * m + k] = l;
+    };
+    // P = Pl * Pr
+    if (n[0] && n[3]) {
+        sb_mul(op[0], n[0], op[3], n[3], r0);
+        emit(0, r0, n[0] + n[3]);
+    } else {
+        emit(0, r0, 0);
+    }
+    // Q = Ql * Qr
+    sb_mul(op[1], n[1], op[4], n[4], r0);
+    emit(1, r0, n[1] + n[4]);
+    // R = Qr * Rl + s * Pl * Rr
+    const int lx = n[4] + n[2], ly = n[0] + n[5];
+    sb_mul(op[4], n[4], op[2], n[2], r0);
+    if (n[0] && n[5]) {
+        sb_mul(op[0], n[0], op[5], n[5], r1);
+    }
+    const int nr = (lx > ly ? lx : ly) + 1;
+    for (int t = lx; t < nr; ++t) r0[t] = 0;
+    if (n[0] && n[5]) sb_addsub(r0, nr, r1, ly, sgn);
+    emit(2, r0, nr);
+}
+
 // One warp per merge with operands of at most MAXC limbs (shared memory schoolbook).
 // Column sums are computed in parallel by the lanes; lane 0 propagates carries.
 template <int MAXC>
@@ -231,16 +280,17 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
     {
         const int lx = product(4, 2, s_res[warp][0]);
         const int ly = product(0, 5, s_res[warp][1]);
-        const int nmax = 2 * MAXC + 1;
+        // |R| < 2 max(|Qr Rl|, |Pl Rr|): max(lx, ly) + 1 limbs
+        const int nr = (lx > ly ? lx : ly) + 1;
         if (lane == 0) {
             uint64_t* x = s_res[warp][0];
-            for (int t = lx; t < nmax; ++t) x[t] = 0;
-            sb_addsub(x, nmax, s_res[warp][1], ly, sgn);
+            for (int t = lx; t < nr; ++t) x[t] = 0;
+            sb_addsub(x, nr, s_res[warp][1], ly, sgn);
         }
         __syncwarp();
         uint64_t* dst = out.X[2] + m * out.cap[2];
-        for (int t = lane; t < (int)out.cap[2]; t += 32) dst[t] = t < nmax ? s_res[warp][0][t] : 0;
-        if (lane == 0) out.len[3 * m + 2] = sb_len(s_res[warp][0], nmax < (int)out.cap[2] ? nmax : out.cap[2]);
+        for (int t = lane; t < (int)out.cap[2]; t += 32) dst[t] = t < nr ? s_res[warp][0][t] : 0;
+        if (lane == 0) out.len[3 * m + 2] = sb_len(s_res[warp][0], nr < (int)out.cap[2] ? nr : out.cap[2]);
         __syncwarp();
     }
 }
@@ -723,8 +773,21 @@ struct DeviceBS {
             LevelView in = view(slot, C), out = view(oslot, P);
             auto tl0 = std::chrono::steady_clock::now();
             if (P.kind == 1) {
-                bs_warp_merge_kernel<kWarpMaxC><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes, a0,
-                                                                                              b0, d);
+                // children's largest slot decides the kernel: a thread per merge up to 16 limbs,
+                // a warp per merge (shared-memory schoolbook sized to the children) above
+                const uint32_t cmax = std::max({C.cap[0], C.cap[1], C.cap[2]});
+                if (cmax <= 8)
+                    bs_thread_merge_kernel<8><<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(in, out, P.nodes, a0,
+                                                                                                 b0, d);
+                else if (cmax <= 16)
+                    bs_thread_merge_kernel<16><<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(in, out, P.nodes,
+                                                                                                  a0, b0, d);
+                else if (cmax <= 32)
+                    bs_warp_merge_kernel<32><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes, a0, b0,
+                                                                                            d);
+                else
+                    bs_warp_merge_kernel<kWarpMaxC><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes,
+                                                                                                  a0, b0, d);
                 e = cudaGetLastError();
                 if (launches) ++*launches;
             } else {

@@ -158,27 +158,6 @@ void Workspace::release() {
 }
 
 // ---------------------------------------------------------------- pass dispatch
-#ifndef PG_PASS_PIPE
-#define PG_PASS_PIPE 0
-#endif
-
-// Resident CTAs of one pipelined pass kernel on a device: sets the kernel's dynamic shared
-// memory limit there on first use. `resident` is the cache of that one kernel (every kernel
-// has the same function type, so the cache cannot be keyed by type).
-template <class K>
-static int pipe_resident(K kern, size_t smem, int dev, std::atomic<int>* resident) {
-    if (dev < 0 || dev >= 64) return 0;
-    int r = resident[dev].load(std::memory_order_relaxed);
-    if (r > 0) return r;
-    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-    int nb = 0, sms = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kPassThreads, smem) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    r = std::max(1, nb) * sms;
-    resident[dev].store(r, std::memory_order_relaxed);
-    return r;
-}
-
 template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
 static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cudaStream_t st) {
     constexpr int LOGE = kTileLog;
@@ -190,35 +169,11 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cuda
         const uint64_t per = 1ull << (LOGE - LOGN);
         tiles = (rows + per - 1) / per;
     }
-#if PG_PASS_PIPE
-    auto kern = ntt_pipe_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
-    constexpr size_t smem = pipe_smem_bytes<LAY, LOGN, LOGE, FUSE>();
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    static std::atomic<int> cache[64];  // per instantiation of run_pass, i.e. per kernel
-    const int resident = pipe_resident(kern, smem, dev, cache);
-    if (resident <= 0) return cudaErrorInvalidConfiguration;
-    const uint64_t grid = std::min<uint64_t>(kNumPrimes * tiles, (uint64_t)resident);
-    kern<<<(unsigned)grid, kPassThreads, smem, st>>>(prm, tw);
-#else
     auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
     // the tile, plus the four-step row factors of a strided tile
     const size_t smem = ((size_t)4 << LOGE) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
-#ifdef PG_PASS_CARVEOUT
-    {
-        // shared-memory share of the unified L1 (percent): the rest caches the twiddle tables
-        static std::atomic<int> set[64];
-        int dev = 0;
-        if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64 && !set[dev].load()) {
-            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, PG_PASS_CARVEOUT);
-            set[dev].store(1);
-        }
-    }
-#endif
     dim3 grid((unsigned)tiles, kNumPrimes);
     kern<<<grid, kPassThreads, smem, st>>>(prm, tw);
-#endif
     return cudaGetLastError();
 }
 

@@ -469,216 +469,4 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
 }
 
 
-// ---------------------------------------------------------------- pipelined pass
-// 16-byte asynchronous global -> shared copies (sm_80+ cp.async). src_bytes < 16 zero-fills
-// the rest of the 16 bytes; src_bytes == 0 reads nothing (the address is still a valid one).
-__device__ __forceinline__ void cp_async16(uint32_t* smem, const void* gmem, uint32_t src_bytes) {
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// Table pointers of prime j without indexing the parameter arrays by a runtime value.
-__device__ __forceinline__ const uint2* pick3(const uint2* const (&t)[kNumPrimes], int j) {
-    return j == 0 ? t[0] : (j == 1 ? t[1] : t[2]);
-}
-
-// Shared memory of the pipelined pass: two tile buffers, then the strided tile's row factors
-// (N uint2), then (Fuse::MulInverse) the other operand's tile.
-template <Layout LAY, int LOGN, int LOGE, Fuse FUSE>
-__host__ __device__ constexpr size_t pipe_smem_bytes() {
-    return ((size_t)8 << LOGE) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0) +
-           (FUSE == Fuse::MulInverse ? ((size_t)4 << LOGE) : 0);
-}
-template <Fuse FUSE>
-constexpr int pipe_min_blocks() {
-    return FUSE == Fuse::MulInverse ? 2 : 3;
-}
-
-// Persistent pass kernel. grid.x CTAs walk the tiles id = blockIdx.x, blockIdx.x + gridDim.x,
-// ... of all primes (prime-major: id = prime * tiles_per_prime + tile). Each CTA keeps two tile
-// buffers: while it transforms tile i, the copies of tile i + 1 are in flight (cp.async), so
-// HBM latency overlaps the butterflies. Per tile:
-//   wait for its copies -> (limb reduction or inverse four-step twiddle in place) -> radix
-//   rounds -> (fused pointwise product and inverse rounds) -> store with the forward
-//   four-step twiddle.
-template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE>
-__global__ void __launch_bounds__(NTHREADS, pipe_min_blocks<FUSE>())
-    ntt_pipe_kernel(PassParams P, TwiddleTables T) {
-    extern __shared__ uint4 smem_raw[];
-    constexpr int LOGC = LOGE - LOGN;
-    constexpr uint32_t E = 1u << LOGE;
-    constexpr int dir = INV ? 1 : 0;
-    uint32_t* const buf0 = reinterpret_cast<uint32_t*>(smem_raw);
-    uint32_t* const buf1 = buf0 + E;
-    uint2* const smA = reinterpret_cast<uint2*>(buf0 + 2 * E);
-    uint32_t* const oth = reinterpret_cast<uint32_t*>(smA + (LAY == Layout::Strided ? (1u << LOGN) : 0));
-
-    const int logRows = P.logL - LOGN;
-    const uint64_t total_rows = (uint64_t)P.njobs << logRows;
-    const int logTpj = P.logL - LOGE;  // strided: tiles per job (log)
-    const uint64_t tpp = (LAY == Layout::Strided) ? ((uint64_t)P.njobs << logTpj)
-                                                  : ((total_rows + (1u << LOGC) - 1) >> LOGC);
-    const uint64_t total = 3 * tpp;
-
-    // Global position of the 4 consecutive elements at tile index e4 of tile `t` (within its
-    // prime); returns false for rows past the end (contiguous tiles only).
-    auto locate = [&](uint64_t t, uint32_t e4, uint32_t& m, uint32_t& c, uint64_t& job, uint64_t& g) -> bool {
-        if constexpr (LAY == Layout::Strided) {
-            m = e4 >> LOGC;
-            c = e4 & ((1u << LOGC) - 1);
-            job = t >> logTpj;
-            g = gidx<LAY, LOGN, LOGE>(t & ((1ull << logTpj) - 1), m, c, P.logS);
-            return true;
-        } else {
-            c = e4 >> LOGN;
-            m = e4 & ((1u << LOGN) - 1);
-            const uint64_t R = (t << LOGC) + c;
-            if (R >= total_rows) return false;
-            job = R >> logRows;
-            g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);
-            return true;
-        }
-    };
-    auto issue = [&](uint64_t id, uint32_t* dst) {
-        const int j = (int)(id / tpp);
-        const uint64_t t = id - (uint64_t)j * tpp;
-        const uint64_t prime_off = (uint64_t)j * P.L;
-        for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
-            uint32_t m, c;
-            uint64_t job, g;
-            const void* src = P.data;
-            uint32_t bytes = 0;
-            if (locate(t, e4, m, c, job, g)) {
-                if constexpr (SRC == Source::Limbs) {
-                    const uint32_t* words;
-                    uint64_t ncoef;
-                    job_source(P, job, words, ncoef);
-                    src = words;
-                    if (g < ncoef) {
-                        src = words + g;
-                        bytes = (uint32_t)(ncoef - g >= 4 ? 16 : (ncoef - g) * 4);
-                    }
-                } else {
-                    src = P.data + job * P.job_stride + prime_off + g;
-                    bytes = 16;
-                }
-            }
-            cp_async16(dst + swz(e4), src, bytes);
-        }
-    };
-    auto issue_other = [&](uint64_t id) {
-        const int j = (int)(id / tpp);
-        const uint64_t t = id - (uint64_t)j * tpp;
-        const uint64_t prime_off = (uint64_t)j * P.L;
-        for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
-            uint32_t m, c;
-            uint64_t job, g;
-            const void* src = P.other;
-            uint32_t bytes = 0;
-            if (locate(t, e4, m, c, job, g)) {
-                src = P.other + job * P.other_stride + prime_off + g;
-                bytes = 16;
-            }
-            cp_async16(oth + swz(e4), src, bytes);
-        }
-    };
-
-    uint64_t id = blockIdx.x;
-    if (id < total) issue(id, buf0);
-    cp_async_commit();
-    for (int it = 0; id < total; ++it, id += gridDim.x) {
-        uint32_t* const cur = (it & 1) ? buf1 : buf0;
-        uint32_t* const nxt = (it & 1) ? buf0 : buf1;
-        const int j = (int)(id / tpp);
-        const uint64_t t = id - (uint64_t)j * tpp;
-        const uint32_t p = kPrime(j);
-        const uint32_t pinv = inv_mod_2_32(p);
-        const uint64_t prime_off = (uint64_t)j * P.L;
-        if constexpr (FUSE == Fuse::MulInverse) {
-            issue_other(id);
-            cp_async_commit();
-        }
-        if (id + gridDim.x < total) issue(id + gridDim.x, nxt);
-        cp_async_commit();
-
-        const uint2* rowB = nullptr;
-        if constexpr (LAY == Layout::Strided) {
-            // four-step row factors of this tile (no dependence on its data: overlaps the copies)
-            rowB = P.rowB + (size_t)j * (1u << kFsLog);
-            const uint32_t t0 = tcol<LAY, LOGN, LOGE>(t & ((1ull << logTpj) - 1), 0, P.logS);
-            const int sh = kMaxLogL - P.logNp;
-            const uint2* lo = pick3(T.fs_lo[dir], j);
-            const uint2* hi = pick3(T.fs_hi[dir], j);
-            const uint64_t R = kRecip64(j);
-            for (uint32_t i = threadIdx.x; i < (1u << LOGN); i += NTHREADS) {
-                const uint32_t E0 = (t0 * bitrev_n(i, LOGN)) << sh;  // t0 * k < N'
-                const uint2 a = __ldg(lo + (E0 & ((1u << kFsLog) - 1)));
-                const uint2 b = __ldg(hi + (E0 >> kFsLog));
-                const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
-                smA[i] = make_uint2(w, shoup_companion_dev(w, p, R));
-            }
-        }
-        if constexpr (FUSE == Fuse::MulInverse)
-            cp_async_wait<2>();
-        else
-            cp_async_wait<1>();
-        __syncthreads();
-
-        if constexpr (SRC == Source::Limbs || (INV && LAY == Layout::Strided)) {
-            const uint32_t one_p = (uint32_t)(0x100000000ull / p);
-            for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
-                uint4 x = *reinterpret_cast<uint4*>(cur + swz(e4));
-                if constexpr (SRC == Source::Limbs) {
-                    x = make_uint4(reduce_u32(x.x, p, one_p), reduce_u32(x.y, p, one_p), reduce_u32(x.z, p, one_p),
-                                   reduce_u32(x.w, p, one_p));
-                } else {
-                    const uint32_t m = e4 >> LOGC, c = e4 & ((1u << LOGC) - 1);
-                    fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
-                }
-                *reinterpret_cast<uint4*>(cur + swz(e4)) = x;
-            }
-            __syncthreads();
-        }
-
-        tile_transform<LAY, LOGN, LOGE, NTHREADS, INV>(cur, pick3(T.stage[dir], j), p);
-
-        if constexpr (FUSE != Fuse::None) {
-            static_assert(LAY == Layout::Contig && !INV, "pointwise fusion happens in the last forward pass");
-            if constexpr (FUSE == Fuse::MulInverse) {
-                cp_async_wait<1>();
-                __syncthreads();
-            }
-            // both tiles use the same swizzled layout: the product is elementwise on storage
-            for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
-                uint4 a = *reinterpret_cast<uint4*>(cur + e4);
-                uint4 b = a;
-                if constexpr (FUSE == Fuse::MulInverse) b = *reinterpret_cast<const uint4*>(oth + e4);
-                a.x = mul_mont(a.x, b.x, p, pinv);
-                a.y = mul_mont(a.y, b.y, p, pinv);
-                a.z = mul_mont(a.z, b.z, p, pinv);
-                a.w = mul_mont(a.w, b.w, p, pinv);
-                *reinterpret_cast<uint4*>(cur + e4) = a;
-            }
-            __syncthreads();
-            tile_transform<LAY, LOGN, LOGE, NTHREADS, true>(cur, pick3(T.stage[1], j), p);
-        }
-
-        for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
-            uint32_t m, c;
-            uint64_t job, g;
-            if (!locate(t, e4, m, c, job, g)) continue;
-            uint4 x = *reinterpret_cast<uint4*>(cur + swz(e4));
-            if constexpr (!INV && LAY == Layout::Strided) fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
-            *reinterpret_cast<uint4*>(P.out + job * P.job_stride + prime_off + g) = x;
-        }
-        __syncthreads();  // cur, oth and smA are reused by the next iteration
-    }
-    cp_async_wait<0>();
-}
-
 }  // namespace pg

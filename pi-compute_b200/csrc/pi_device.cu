@@ -502,6 +502,7 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
     } free_ge{ge};
     uint64_t ge_cap = 0;
     for (int t = 0; J - t > kLeafLog; ++t) {
+        const auto tl0 = std::chrono::steady_clock::now();
         const int j = J - t - 1;  // split power 10^(2^j)
         const uint64_t njobs = 1ull << t;
         const size_t cap = cap_of(j);             // next level's chunk capacity
@@ -552,6 +553,10 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         cur_s = cap;
         cur_n = cap;
         std::swap(next, spare);
+        if (trace_on())
+            std::fprintf(stderr, "[pi_device] conversion level %2d: %8llu chunks of %zu limbs: %.3f ms\n", t,
+                         (unsigned long long)njobs, cur_s,
+                         std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count());
     }
     if (sp.error(st)) throw DevError(PG_ERR_INTERNAL, "to_decimal: product check failed");
     if (!A.leaves(cur, cur_s, std::min<size_t>(cur_n, 16), (uint64_t)1 << (J - kLeafLog), (uint64_t)1 << kLeafLog,
