@@ -121,6 +121,8 @@ def ref() -> ctypes.CDLL:
         r.ref_bs.argtypes = [ctypes.c_ulong, ctypes.c_ulong, ctypes.c_uint, ctypes.c_void_p, ctypes.c_void_p,
                              ctypes.c_void_p]
         r.ref_bs.restype = ctypes.c_int
+        r.ref_bs_checkpoint.argtypes = [ctypes.c_ulong, ctypes.c_ulong, ctypes.c_uint, ctypes.c_char_p]
+        r.ref_bs_checkpoint.restype = ctypes.c_int
         r.ref_pi.argtypes = [ctypes.c_ulong, ctypes.c_uint]
         r.ref_pi.restype = ctypes.c_void_p
         r.ref_terms_needed.argtypes = [ctypes.c_ulong]
@@ -145,6 +147,13 @@ def ref_bs(a: int, b: int, threads: int = 1) -> tuple[int, int, int]:
         r.ref_free(p)
         out.append(int(s, 16))
     return tuple(out)
+
+
+def ref_bs_checkpoint(a: int, b: int, directory: str, threads: int = 1) -> str:
+    """Path of bs_<a>_<b>.ckpt as the reference's own BinarySplitting writes it into `directory`."""
+    if ref().ref_bs_checkpoint(a, b, threads, directory.encode()) != 0:
+        raise RuntimeError("ref_bs_checkpoint failed")
+    return os.path.join(directory, f"bs_{a}_{b}.ckpt")
 
 
 def ref_pi(digits: int, threads: int = 1) -> str:

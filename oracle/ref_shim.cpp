@@ -6,6 +6,9 @@
 //   ref_bs        pi::BinarySplitting::compute(a, b) with pi::GmpMultiplier
 //                 (src/engine/binary_splitting.cpp:605-644), P/Q/R as hex strings
 //   ref_pi        pi::PiEngine::compute(config).digits (src/engine/pi_engine.cpp:207-603)
+//   ref_bs_checkpoint  pi::BinarySplitting::compute(a, b) with checkpointing enabled, so the
+//                 reference's own save_bs_result writes <dir>/bs_<a>_<b>.ckpt
+//                 (src/engine/binary_splitting.cpp:48-71, 104-109, 605-644)
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -40,6 +43,19 @@ int ref_bs(unsigned long a, unsigned long b, unsigned int threads, char** P, cha
         *P = mpz_hex(r.P);
         *Q = mpz_hex(r.Q);
         *R = mpz_hex(r.R);
+        return 0;
+    } catch (...) {
+        return 1;
+    }
+}
+
+int ref_bs_checkpoint(unsigned long a, unsigned long b, unsigned int threads, const char* dir) {
+    try {
+        pi::GmpMultiplier mult;
+        pi::BinarySplitting bs(mult, threads);
+        bs.enable_checkpointing(dir);
+        pi::BSResult r = bs.compute(a, b);
+        (void)r;
         return 0;
     } catch (...) {
         return 1;

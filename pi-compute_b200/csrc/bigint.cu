@@ -316,26 +316,49 @@ __global__ void __launch_bounds__(256) ge_block_kernel(const uint64_t* x, uint64
 // Decimal digits of job j (< 10^digits) written most significant first to out[j * digits ...];
 // only characters at global positions [skip, total) are stored, shifted down by skip. *bad is
 // set when a job does not fit its digits or a digit below `skip` is not zero.
+// (u1 2^64 + u0) / d for the normalised divisor d = 10^19 (d >= 2^63) and u1 < d, with the
+// precomputed v = floor((2^128 - 1) / d) - 2^64: the division by an invariant integer of Moller and
+// Granlund ("Improved division by invariant integers", IEEE Trans. Computers 60(2), 2011, Alg. 4):
+// one 64x64 -> 128 product and at most two corrections instead of a 128-bit division.
+__device__ __forceinline__ uint64_t div_ten19(uint64_t u1, uint64_t u0, uint64_t& rem) {
+    constexpr uint64_t d = 10000000000000000000ull;
+    constexpr uint64_t v = 0xd83c94fb6d2ac34aull;
+    uint64_t q0 = v * u1;
+    uint64_t q1 = __umul64hi(v, u1);
+    const uint64_t s = q0 + u0;
+    q1 += u1 + 1 + (s < q0 ? 1 : 0);
+    q0 = s;
+    uint64_t r = u0 - q1 * d;
+    if (r > q0) {
+        --q1;
+        r += d;
+    }
+    if (r >= d) {
+        ++q1;
+        r -= d;
+    }
+    rem = r;
+    return q1;
+}
+
+constexpr int kLeafMaxLimbs = 64;
+
 __global__ void leaves_kernel(const uint64_t* x, uint64_t sx, uint64_t nl, uint64_t njobs, uint64_t digits, char* out,
                               uint64_t skip, uint64_t total, uint32_t* bad) {
-    constexpr uint64_t kTen19 = 10000000000000000000ull;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t v[16];
+        uint64_t v[kLeafMaxLimbs];
         const uint64_t* xj = x + j * sx;
-        for (uint64_t i = 0; i < 16; ++i) v[i] = i < nl ? xj[i] : 0;
+        for (uint64_t i = 0; i < nl; ++i) v[i] = xj[i];
         uint64_t top = nl;
+        while (top > 0 && v[top - 1] == 0) --top;
         int64_t pos = (int64_t)(j * digits + digits);  // one past the last digit of this job
         uint64_t left = digits;
         while (left > 0) {
             // remainder of v / 10^19, v <- quotient
-            unsigned __int128 r = 0;
-            for (int64_t i = (int64_t)top - 1; i >= 0; --i) {
-                const unsigned __int128 cur = (r << 64) | v[i];
-                v[i] = (uint64_t)(cur / kTen19);
-                r = cur % kTen19;
-            }
+            uint64_t r = 0;
+            for (int64_t i = (int64_t)top - 1; i >= 0; --i) v[i] = div_ten19(r, v[i], r);
             while (top > 0 && v[top - 1] == 0) --top;
-            uint64_t g = (uint64_t)r;
+            uint64_t g = r;
             const uint64_t nd = left < 19 ? left : 19;
             for (uint64_t d = 0; d < nd; ++d) {
                 --pos;
@@ -844,7 +867,7 @@ void DevArith::batch_ge(const uint64_t* x, uint64_t sx, const uint64_t* y, uint6
 
 bool DevArith::leaves(const uint64_t* x, uint64_t sx, uint64_t nlimbs, uint64_t njobs, uint64_t digits, char* out,
                       uint64_t skip, uint64_t total) {
-    if (nlimbs > 16) throw DevError(3, "leaves: chunk longer than 16 limbs");
+    if (nlimbs > (uint64_t)kLeafMaxLimbs) throw DevError(3, "leaves: chunk longer than 64 limbs");
     uint32_t* bad = flags(1);
     check(cudaMemsetAsync(bad, 0, 4, st_), "leaves");
     leaves_kernel<<<grid_for(njobs, 128), 128, 0, st_>>>(x, sx, nlimbs, njobs, digits, out, skip, total, bad);

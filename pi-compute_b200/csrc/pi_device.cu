@@ -14,7 +14,7 @@
 //                   / 10^(2^j)), r = c - q 10^(2^j) and at most two corrections; every level
 //                   of the split runs batched over all chunks of that level (two shared-operand
 //                   batched products, a shift, a subtraction, the corrections), down to
-//                   128-digit chunks written as ASCII by one thread each.
+//                   1024-digit chunks written as ASCII by one thread each.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -54,12 +54,18 @@ struct SharedProduct {
     uint32_t* sync = nullptr;
     uint64_t sync_cap = 0;
     uint32_t* errw = nullptr;
+    uint32_t* flags = nullptr;  // per-chunk flags of the conversion, kept across calls
+    uint64_t flags_cap = 0;
+    char* digits = nullptr;     // the conversion's ASCII output, kept across calls
+    uint64_t digits_cap = 0;
 
     ~SharedProduct() {
         if (res) cudaFree(res);
         if (bres) cudaFree(bres);
         if (sync) cudaFree(sync);
         if (errw) cudaFree(errw);
+        if (flags) cudaFree(flags);
+        if (digits) cudaFree(digits);
     }
 
     static void grow(uint32_t** p, uint64_t& cap, uint64_t words, cudaStream_t st) {
@@ -400,7 +406,15 @@ void final_formula(DevArith& A, DevNum& pi_int, const DevNum& Q, const DevNum& R
 }
 
 // ------------------------------------------------------------------ decimal conversion
-constexpr int kLeafLog = 7;  // 128-digit leaves
+constexpr int kLeafLog = 10;  // 1024-digit leaves (56-limb chunks, one thread each)
+
+// *out |= 1 if any flag is set (the conversion's remainders must all be below the split power).
+__global__ void flag_any_kernel(const uint32_t* f, uint64_t n, uint32_t* out) {
+    bool any = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        any |= f[i] != 0;
+    if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(out, 1u);
+}
 
 // Decimal digits of x (0 <= x < 10^nd) into host out[0 .. nd).
 void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char* out) {
@@ -413,12 +427,17 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
     int J = kLeafLog;
     while (((size_t)1 << J) < nd) ++J;
     const size_t total = (size_t)1 << J, skip = total - nd;
-    char* d_out = nullptr;
-    if (cudaMalloc((void**)&d_out, nd) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
-    struct Free {
-        char* p;
-        ~Free() { cudaFree(p); }
-    } free_out{d_out};
+    // the digit buffer stays with the context: a 100 MB cudaMalloc / cudaFree per call costs a
+    // device synchronisation each and, now and then, tens of milliseconds
+    if (nd > sp.digits_cap) {
+        A.sync();
+        if (sp.digits) cudaFree(sp.digits);
+        sp.digits = nullptr;
+        sp.digits_cap = 0;
+        if (cudaMalloc((void**)&sp.digits, nd) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
+        sp.digits_cap = nd;
+    }
+    char* d_out = sp.digits;
     cudaMemsetAsync(d_out, '0', nd, st);
     // powers P[j] = 10^(2^j) and reciprocals for j = kLeafLog .. J-1
     std::vector<Num*> P, inv;
@@ -493,14 +512,22 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
     }
     DevNum* next = &lvl_a.v;
     DevNum* spare = &lvl_b.v;
-    uint32_t* ge = nullptr;
-    struct FreeGe {
-        uint32_t*& p;
-        ~FreeGe() {
-            if (p) cudaFree(p);
+    // chunk flags (grown in the context's state) and one word for "a remainder stayed >= P"
+    uint32_t* bad = nullptr;
+    {
+        const uint64_t most = (uint64_t)1 << (J - kLeafLog);
+        if (most + 1 > sp.flags_cap) {
+            A.sync();
+            if (sp.flags) cudaFree(sp.flags);
+            sp.flags = nullptr;
+            sp.flags_cap = 0;
+            if (cudaMalloc((void**)&sp.flags, (most + 1) * 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
+            sp.flags_cap = most + 1;
         }
-    } free_ge{ge};
-    uint64_t ge_cap = 0;
+        bad = sp.flags + most;
+        cudaMemsetAsync(bad, 0, 4, st);
+    }
+    uint32_t* ge = sp.flags;
     for (int t = 0; J - t > kLeafLog; ++t) {
         const auto tl0 = std::chrono::steady_clock::now();
         const int j = J - t - 1;  // split power 10^(2^j)
@@ -528,27 +555,14 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         A.reserve(Ppad, cap);
         cudaMemsetAsync(Ppad.v.d, 0, cap * 8, st);
         cudaMemcpyAsync(Ppad.v.d, Pj.d, np * 8, cudaMemcpyDeviceToDevice, st);
-        if (njobs > ge_cap) {
-            A.sync();
-            if (ge) cudaFree(ge);
-            ge = nullptr;
-            if (cudaMalloc((void**)&ge, njobs * 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
-            ge_cap = njobs;
-        }
         for (int round = 0; round < 2; ++round) {
             A.batch_ge(next->d + cap, 2 * cap, Ppad.v.d, 0, cap, ge, njobs);
             A.batch_add(next->d + cap, 2 * cap, cap, Ppad.v.d, 0, np, next->d + cap, 2 * cap, cap, true, 0, ge, njobs);
             A.batch_add(next->d, 2 * cap, cap, nullptr, 0, 0, next->d, 2 * cap, cap, false, 1, ge, njobs);
         }
-        // a third check must find every remainder below P
+        // a third check must find every remainder below P (read once, after the last level)
         A.batch_ge(next->d + cap, 2 * cap, Ppad.v.d, 0, cap, ge, njobs);
-        {
-            std::vector<uint32_t> h(njobs);
-            cudaMemcpyAsync(h.data(), ge, njobs * 4, cudaMemcpyDeviceToHost, st);
-            A.sync();
-            for (uint32_t v : h)
-                if (v) throw DevError(PG_ERR_INTERNAL, "to_decimal: remainder above the split power");
-        }
+        flag_any_kernel<<<(unsigned)std::min<uint64_t>((njobs + 255) / 256, 148 * 8), 256, 0, st>>>(ge, njobs, bad);
         cur = next->d;
         cur_s = cap;
         cur_n = cap;
@@ -558,13 +572,22 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
                          (unsigned long long)njobs, cur_s,
                          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count());
     }
+    const auto tw0 = std::chrono::steady_clock::now();
     if (sp.error(st)) throw DevError(PG_ERR_INTERNAL, "to_decimal: product check failed");
-    if (!A.leaves(cur, cur_s, std::min<size_t>(cur_n, 16), (uint64_t)1 << (J - kLeafLog), (uint64_t)1 << kLeafLog,
-                  d_out, skip, total))
+    {
+        uint32_t hb = 0;
+        cudaMemcpyAsync(&hb, bad, 4, cudaMemcpyDeviceToHost, st);
+        A.sync();
+        if (hb) throw DevError(PG_ERR_INTERNAL, "to_decimal: remainder above the split power");
+    }
+    if (!A.leaves(cur, cur_s, cur_n, (uint64_t)1 << (J - kLeafLog), (uint64_t)1 << kLeafLog, d_out, skip, total))
         throw DevError(PG_ERR_BAD_ARG, "to_decimal: the number has more digits than requested");
     if (cudaMemcpyAsync(out, d_out, nd, cudaMemcpyDeviceToHost, st) != cudaSuccess)
         throw DevError(PG_ERR_DEVICE, "digit copy");
     A.sync();
+    if (trace_on())
+        std::fprintf(stderr, "[pi_device] conversion levels drained, leaves, digit copy: %.3f ms\n",
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count());
 }
 
 pg_status fail(pg_ctx* c, pg_status s, const std::string& m) {

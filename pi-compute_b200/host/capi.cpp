@@ -34,6 +34,22 @@ int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int devi
            double* stats) {
     try {
         if (!out || out_cap < digits + 2) throw std::invalid_argument("output buffer smaller than digits + 2");
+        if (mode == PIB_MODE_BATCHED) {
+            // the whole computation on the device, digits written straight into the caller's buffer
+            pg_ctx* ctx = pi::shared_context(device);
+            const uint64_t l0 = pg_launch_count(ctx);
+            double sec[4] = {0, 0, 0, 0};
+            const pg_status st = pg_pi(ctx, digits, out, sec);
+            if (st != PG_OK)
+                throw std::runtime_error(std::string("pg_pi: ") + pg_last_error(ctx) + " (status " +
+                                         std::to_string(st) + ")");
+            if (stats) {
+                for (int i = 0; i < 4; ++i) stats[i] = sec[i];
+                stats[4] = (double)(pg_launch_count(ctx) - l0);
+                stats[5] = stats[6] = stats[7] = 0;
+            }
+            return 0;
+        }
         pi::PiConfig cfg;
         cfg.digits = digits;
         cfg.num_threads = threads ? threads : 1;
