@@ -42,6 +42,7 @@ typedef int pg_status;
 #define PG_ERR_DEVICE 4       /* CUDA runtime error (message in pg_last_error) */
 #define PG_ERR_TIMEOUT 5      /* a bounded device-side wait ran out (carry look-back) */
 #define PG_ERR_INTERNAL 6     /* device consistency check failed (carry out of the top word) */
+#define PG_ERR_IO 7           /* checkpoint file missing, unreadable, short, or not writable */
 
 typedef struct pg_ctx pg_ctx;
 
@@ -172,6 +173,50 @@ pg_status pg_to_decimal(pg_ctx* ctx, const uint64_t* x, size_t nx, size_t ndigit
 pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t* r, size_t nr, size_t digits,
                        char* out);
 pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds);
+
+/* ---- Checkpoints, in the reference's file formats, so that files move between the two
+ * programs in both directions:
+ *   <dir>/bs_<a>_<b>.ckpt    P, Q, R of the splitting node [a, b): for each, int sign (-1, 0, 1),
+ *                            size_t byte count, the bytes of |x| least significant first
+ *                            (src/engine/binary_splitting.cpp:44-90: mpz_export order -1, size 1)
+ *   <dir>/pi_int_<D>.ckpt    floor(pi 10^D): size_t byte count, then the bytes
+ *                            (src/engine/pi_engine.cpp:263-284, 417-430)
+ * int and size_t in the machine's own 4- and 8-byte little-endian form, as the reference writes.
+ *
+ * pg_ckpt_write_bs / pg_ckpt_read_bs, pg_ckpt_write_pi_int / pg_ckpt_read_pi_int: the formats on
+ *   host limb arrays (no context, no device work). Reading with x == NULL (read_bs: all three
+ *   NULL) only reports the capacities in limbs that the values need (and the signs); otherwise
+ *   every non-NULL x[k] must hold `cap` limbs and receives the value, n[k] its length without
+ *   leading zeros. PG_ERR_IO for a missing, short or unwritable file, PG_ERR_BAD_ARG for a
+ *   capacity that is too small (n[k] then holds the capacity needed).
+ * pg_bs_checkpointed: pg_bs resumed from and saved to `dir` like the reference's
+ *   BinarySplitting::compute(a, b) with checkpointing on (binary_splitting.cpp:104-135, 295-302,
+ *   350-360, 605-644): a node of the splitting tree whose file loads is taken from it; halves
+ *   holding files below them are merged on the device; every other subtree is one level-batched
+ *   device splitting; at the end bs_<a>_<b>.ckpt is written (unless it was loaded) and the
+ *   files of its two children removed. P may be NULL. Results as pg_bs.
+ * pg_pi_checkpointed: pg_pi with the reference's --checkpoint DIR behaviour: the root splitting
+ *   as above, then pi_int_<digits>.ckpt loaded when present (no final formula) or written after
+ *   the final formula, then the conversion. The directory is created when missing; files that
+ *   cannot be written are skipped (the report says which were saved). */
+typedef struct pg_ckpt_report {
+    int root_loaded;           /* bs_0_<N>.ckpt (bs_<a>_<b>.ckpt) was read */
+    int root_saved;            /* ... was written */
+    int pi_int_loaded;         /* pi_int_<digits>.ckpt was read: no final formula */
+    int pi_int_saved;          /* ... was written */
+    size_t nodes_loaded;       /* splitting nodes read from files, the root included */
+    size_t subtrees_computed;  /* level-batched device splittings of ranges with no file below */
+    size_t merges;             /* device merges above loaded or computed nodes */
+} pg_ckpt_report;
+
+pg_status pg_ckpt_write_bs(const char* path, const uint64_t* const x[3], const size_t n[3], const int sign[3]);
+pg_status pg_ckpt_read_bs(const char* path, uint64_t* const x[3], size_t cap, size_t n[3], int sign[3]);
+pg_status pg_ckpt_write_pi_int(const char* path, const uint64_t* x, size_t n);
+pg_status pg_ckpt_read_pi_int(const char* path, uint64_t* x, size_t cap, size_t* n);
+pg_status pg_bs_checkpointed(pg_ctx* ctx, unsigned long a, unsigned long b, const char* dir, uint64_t* P, uint64_t* Q,
+                             uint64_t* R, size_t cap, size_t* len, int* sign, pg_ckpt_report* report);
+pg_status pg_pi_checkpointed(pg_ctx* ctx, size_t digits, const char* dir, char* out, double* seconds,
+                             pg_ckpt_report* report);
 
 /* ---- Autotuner of the transform's pass split. pg_tune times, for every transform length 2^l
  * with lo <= l <= hi (6 <= lo <= hi <= 26), each valid split into one to three passes on a

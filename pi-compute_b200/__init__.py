@@ -30,6 +30,7 @@ PG_ERR_BAD_ARG = 3
 PG_ERR_DEVICE = 4
 PG_ERR_TIMEOUT = 5
 PG_ERR_INTERNAL = 6
+PG_ERR_IO = 7
 
 _u64p = ctypes.POINTER(ctypes.c_uint64)
 _sizep = ctypes.POINTER(ctypes.c_size_t)
@@ -49,6 +50,16 @@ class PgJob(ctypes.Structure):
     _fields_ = [("a", ctypes.c_void_p), ("na", ctypes.c_size_t), ("b", ctypes.c_void_p), ("nb", ctypes.c_size_t),
                 ("c", ctypes.c_void_p), ("nc", ctypes.c_size_t), ("d", ctypes.c_void_p), ("nd", ctypes.c_size_t),
                 ("acc", ctypes.c_int), ("out", ctypes.c_void_p), ("out_cap", ctypes.c_size_t)]
+
+
+class PgCkptReport(ctypes.Structure):
+    """struct pg_ckpt_report of include/pi_b200.h."""
+    _fields_ = [("root_loaded", ctypes.c_int), ("root_saved", ctypes.c_int), ("pi_int_loaded", ctypes.c_int),
+                ("pi_int_saved", ctypes.c_int), ("nodes_loaded", ctypes.c_size_t),
+                ("subtrees_computed", ctypes.c_size_t), ("merges", ctypes.c_size_t)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
@@ -118,6 +129,21 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     lib.pg_tune_save.restype = ctypes.c_int
     lib.pg_tune_load.argtypes = [vp, ctypes.c_char_p]
     lib.pg_tune_load.restype = ctypes.c_int
+    p3 = ctypes.c_void_p * 3
+    lib.pg_ckpt_write_bs.argtypes = [ctypes.c_char_p, p3, ctypes.c_size_t * 3, ctypes.c_int * 3]
+    lib.pg_ckpt_write_bs.restype = ctypes.c_int
+    lib.pg_ckpt_read_bs.argtypes = [ctypes.c_char_p, ctypes.c_void_p, sz, ctypes.c_size_t * 3, ctypes.c_int * 3]
+    lib.pg_ckpt_read_bs.restype = ctypes.c_int
+    lib.pg_ckpt_write_pi_int.argtypes = [ctypes.c_char_p, _u64p, sz]
+    lib.pg_ckpt_write_pi_int.restype = ctypes.c_int
+    lib.pg_ckpt_read_pi_int.argtypes = [ctypes.c_char_p, ctypes.c_void_p, sz, _sizep]
+    lib.pg_ckpt_read_pi_int.restype = ctypes.c_int
+    lib.pg_bs_checkpointed.argtypes = [vp, ctypes.c_ulong, ctypes.c_ulong, ctypes.c_char_p, ctypes.c_void_p, _u64p, _u64p,
+                                       sz, ctypes.c_size_t * 3, ctypes.c_int * 3, ctypes.POINTER(PgCkptReport)]
+    lib.pg_bs_checkpointed.restype = ctypes.c_int
+    lib.pg_pi_checkpointed.argtypes = [vp, sz, ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_double),
+                                       ctypes.POINTER(PgCkptReport)]
+    lib.pg_pi_checkpointed.restype = ctypes.c_int
     _lib = lib
     return lib
 
@@ -270,6 +296,31 @@ class Engine:
             seconds[:] = list(t)
         return buf.raw[: digits + 2]
 
+    # -------------------------------------------------- checkpoints
+    def bs_checkpointed(self, a: int, b: int, directory: str) -> tuple:
+        """((P, Q, R), report) for the term range [a, b) resumed from and saved to `directory`
+        (pg_bs_checkpointed), the values as signed ints."""
+        cap = 64 + 8 * (b - a)
+        bufs = [np.zeros(cap, dtype=np.uint64) for _ in range(3)]
+        n = (ctypes.c_size_t * 3)()
+        sg = (ctypes.c_int * 3)()
+        rep = PgCkptReport()
+        self._check(self.lib.pg_bs_checkpointed(self.ctx, a, b, directory.encode(), bufs[0].ctypes.data,
+                                                _ptr(bufs[1]), _ptr(bufs[2]), cap, n, sg, ctypes.byref(rep)))
+        vals = tuple(sg[k] * limbs_to_int(bufs[k][: n[k]]) for k in range(3))
+        return vals, rep.as_dict()
+
+    def pi_checkpointed(self, digits: int, directory: str, seconds: Optional[list] = None) -> tuple:
+        """("3." + digits of pi, report) with the reference's --checkpoint behaviour
+        (pg_pi_checkpointed)."""
+        buf = ctypes.create_string_buffer(digits + 2)
+        t = (ctypes.c_double * 4)()
+        rep = PgCkptReport()
+        self._check(self.lib.pg_pi_checkpointed(self.ctx, digits, directory.encode(), buf, t, ctypes.byref(rep)))
+        if seconds is not None:
+            seconds[:] = list(t)
+        return buf.raw[: digits + 2], rep.as_dict()
+
     # -------------------------------------------------- autotuner
     def tune(self, lo: int, hi: int) -> list:
         """Run pg_tune over transform lengths 2^lo .. 2^hi; returns the winning times (us)."""
@@ -323,6 +374,53 @@ class Engine:
         for x in keep:
             x.free()
         return res
+
+
+# ------------------------------------------------------------------ checkpoint files (no device)
+def _ckpt_check(st: int, what: str) -> None:
+    if st != PG_OK:
+        raise PgError(st, what)
+
+
+def ckpt_write_bs(path: str, P: int, Q: int, R: int) -> None:
+    """Write bs_<a>_<b>.ckpt content for signed P, Q, R (pg_ckpt_write_bs)."""
+    lib = load_library()
+    arrs = [int_to_limbs(abs(v)) for v in (P, Q, R)]
+    ptrs = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in arrs])
+    n = (ctypes.c_size_t * 3)(*[len(a) if v else 0 for a, v in zip(arrs, (P, Q, R))])
+    sg = (ctypes.c_int * 3)(*[(v > 0) - (v < 0) for v in (P, Q, R)])
+    _ckpt_check(lib.pg_ckpt_write_bs(path.encode(), ptrs, n, sg), f"pg_ckpt_write_bs {path}")
+
+
+def ckpt_read_bs(path: str) -> tuple:
+    """Signed (P, Q, R) from a splitting checkpoint file (pg_ckpt_read_bs)."""
+    lib = load_library()
+    n = (ctypes.c_size_t * 3)()
+    sg = (ctypes.c_int * 3)()
+    _ckpt_check(lib.pg_ckpt_read_bs(path.encode(), None, 0, n, sg), f"pg_ckpt_read_bs {path}")
+    cap = max(1, max(n))
+    arrs = [np.zeros(cap, dtype=np.uint64) for _ in range(3)]
+    ptrs = (ctypes.c_void_p * 3)(*[a.ctypes.data for a in arrs])
+    _ckpt_check(lib.pg_ckpt_read_bs(path.encode(), ptrs, cap, n, sg), f"pg_ckpt_read_bs {path}")
+    return tuple(sg[k] * limbs_to_int(arrs[k][: n[k]]) for k in range(3))
+
+
+def ckpt_write_pi_int(path: str, x: int) -> None:
+    """Write a pi_int_<digits>.ckpt file for x >= 0 (pg_ckpt_write_pi_int)."""
+    a = int_to_limbs(x)
+    _ckpt_check(load_library().pg_ckpt_write_pi_int(path.encode(), _ptr(a), len(a) if x else 0),
+                f"pg_ckpt_write_pi_int {path}")
+
+
+def ckpt_read_pi_int(path: str) -> int:
+    """The integer of a pi_int checkpoint file (pg_ckpt_read_pi_int)."""
+    lib = load_library()
+    n = ctypes.c_size_t()
+    _ckpt_check(lib.pg_ckpt_read_pi_int(path.encode(), None, 0, ctypes.byref(n)), f"pg_ckpt_read_pi_int {path}")
+    a = np.zeros(max(1, n.value), dtype=np.uint64)
+    _ckpt_check(lib.pg_ckpt_read_pi_int(path.encode(), a.ctypes.data, len(a), ctypes.byref(n)),
+                f"pg_ckpt_read_pi_int {path}")
+    return limbs_to_int(a[: n.value])
 
 
 class DeviceBuffer:

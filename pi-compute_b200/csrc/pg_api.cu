@@ -6,6 +6,7 @@
 #include <cstdlib>
 
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -17,6 +18,7 @@
 #include "ntt_engine.cuh"
 
 namespace pg {
+bool trace_on();
 struct DeviceBS;
 DeviceBS* bs_state_new();
 void bs_state_delete(DeviceBS*);
@@ -177,10 +179,18 @@ pg_status pg_create(int device, pg_ctx** out) {
     pg_ctx* c = new (std::nothrow) pg_ctx;
     if (!c) return PG_ERR_OOM;
     c->device = device;
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    };
     cudaError_t e = cudaSetDevice(device);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    const double t_ctx = ms(t0);
     if (e == cudaSuccess) e = c->tables.build(device);
     if (e == cudaSuccess) e = c->ws.ensure_sync(1);
+    if (pg::trace_on())
+        std::fprintf(stderr, "[pg_create] device %d: context and stream %.3f ms, twiddle tables %.3f ms\n", device, t_ctx,
+                     ms(t0) - t_ctx);
     if (e != cudaSuccess) {
         cudaGetLastError();
         pg_destroy(c);

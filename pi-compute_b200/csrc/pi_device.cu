@@ -27,7 +27,14 @@
 #include <string>
 #include <vector>
 
+#include <dirent.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <set>
+
 #include "../../include/pi_b200.h"
+#include "ckpt_io.h"
 #include "devnum.h"
 
 namespace pg {
@@ -180,11 +187,34 @@ struct SharedProduct {
     }
 };
 
-// Per-context state of the device finish, kept across calls: the arithmetic pool and the
-// batched-product buffers.
+// Pinned host staging for checkpoint files: two buffers, so that the copy of one chunk runs
+// while the other is read from or written to the file.
+struct CkptStaging {
+    static constexpr size_t kChunk = (size_t)32 << 20;  // bytes per buffer
+    char* buf[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    ~CkptStaging() {
+        for (int i = 0; i < 2; ++i) {
+            if (buf[i]) cudaFreeHost(buf[i]);
+            if (ev[i]) cudaEventDestroy(ev[i]);
+        }
+    }
+    void ensure() {
+        for (int i = 0; i < 2; ++i) {
+            if (!buf[i] && cudaMallocHost((void**)&buf[i], kChunk) != cudaSuccess)
+                throw DevError(PG_ERR_OOM, "checkpoint staging buffer");
+            if (!ev[i] && cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess)
+                throw DevError(PG_ERR_DEVICE, "checkpoint staging event");
+        }
+    }
+};
+
+// Per-context state of the device finish, kept across calls: the arithmetic pool, the
+// batched-product buffers and the checkpoint staging.
 struct FinishState {
     DevPool pool;
     SharedProduct sp;
+    CkptStaging stage;
 };
 FinishState* finish_state_new() { return new FinishState; }
 void finish_state_delete(FinishState* f) { delete f; }
@@ -590,6 +620,216 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
                      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count());
 }
 
+// ------------------------------------------------------------------ checkpoints
+// Writes one integer held in HBM in the checkpoint format (ckpt_io.h): the header, then its
+// bytes streamed through the pinned staging buffers.
+bool write_dev(ckpt::File& f, DevArith& A, CkptStaging& S, const DevNum& x, bool with_sign) {
+    cudaStream_t st = A.stream();
+    S.ensure();
+    size_t n = x.n;
+    uint64_t top = 0;
+    while (n) {  // the top limb (lengths are normalised; a zero top limb is only skipped)
+        cudaMemcpyAsync(S.buf[0], x.d + n - 1, 8, cudaMemcpyDeviceToHost, st);
+        A.sync();
+        std::memcpy(&top, S.buf[0], 8);
+        if (top) break;
+        --n;
+    }
+    const size_t count = ckpt::byte_count(n, top);
+    if (!ckpt::put_header(f, with_sign, n ? (x.sign < 0 ? -1 : 1) : 0, count)) return false;
+    const char* src = reinterpret_cast<const char*>(x.d);
+    auto issue = [&](size_t o, int b) {
+        cudaMemcpyAsync(S.buf[b], src + o, std::min(CkptStaging::kChunk, count - o), cudaMemcpyDeviceToHost, st);
+        cudaEventRecord(S.ev[b], st);
+    };
+    if (count) issue(0, 0);
+    int b = 0;
+    for (size_t o = 0; o < count; o += CkptStaging::kChunk, b ^= 1) {
+        if (o + CkptStaging::kChunk < count) issue(o + CkptStaging::kChunk, b ^ 1);
+        if (cudaEventSynchronize(S.ev[b]) != cudaSuccess) throw DevError(PG_ERR_DEVICE, "checkpoint copy");
+        if (!f.put(S.buf[b], std::min(CkptStaging::kChunk, count - o))) {
+            A.sync();
+            return false;
+        }
+    }
+    return true;
+}
+
+// Reads one integer of the checkpoint format into x (HBM); false when the file is short.
+bool read_dev(ckpt::File& f, DevArith& A, CkptStaging& S, DevNum& x, bool with_sign) {
+    cudaStream_t st = A.stream();
+    S.ensure();
+    int sign = 1;
+    size_t count = 0;
+    if (!ckpt::get_header(f, with_sign, sign, count)) return false;
+    const size_t nl = (count + 7) / 8;
+    A.reserve(x, std::max<size_t>(nl, 1));
+    if (nl) cudaMemsetAsync(x.d + nl - 1, 0, 8, st);  // the partial top limb
+    char* dst = reinterpret_cast<char*>(x.d);
+    size_t used = 0;  // bytes up to the last nonzero byte
+    bool ok = true;
+    int b = 0;
+    for (size_t o = 0; o < count; o += CkptStaging::kChunk, b ^= 1) {
+        const size_t len = std::min(CkptStaging::kChunk, count - o);
+        if (cudaEventSynchronize(S.ev[b]) != cudaSuccess) throw DevError(PG_ERR_DEVICE, "checkpoint copy");
+        if (!f.get(S.buf[b], len)) {
+            ok = false;
+            break;
+        }
+        for (size_t k = len; k > 0; --k)
+            if (S.buf[b][k - 1]) {
+                used = o + k;
+                break;
+            }
+        cudaMemcpyAsync(dst + o, S.buf[b], len, cudaMemcpyHostToDevice, st);
+        cudaEventRecord(S.ev[b], st);
+    }
+    A.sync();
+    if (!ok) return false;
+    x.n = (used + 7) / 8;
+    x.sign = x.n ? (sign < 0 ? -1 : 1) : 0;
+    return true;
+}
+
+// P, Q, R of one splitting node in HBM.
+struct Node {
+    Num P, Q, R;
+    explicit Node(DevArith& A) : P(A), Q(A), R(A) {}
+    DevNum& at(int k) { return k == 0 ? P.v : (k == 1 ? Q.v : R.v); }
+};
+
+bool save_node(const std::string& path, DevArith& A, CkptStaging& S, Node& x) {
+    ckpt::File f(path, "wb");
+    if (!f) return false;
+    for (int k = 0; k < 3; ++k)
+        if (!write_dev(f, A, S, x.at(k), true)) return false;
+    return f.close();
+}
+
+bool load_node(const std::string& path, DevArith& A, CkptStaging& S, Node& x) {
+    ckpt::File f(path, "rb");
+    if (!f) return false;
+    for (int k = 0; k < 3; ++k)
+        if (!read_dev(f, A, S, x.at(k), true)) return false;
+    return true;
+}
+
+// The splitting of [a, b) resumed from the checkpoint files of a directory, as the reference's
+// BinarySplitting::compute / compute_parallel / compute_sequential do with checkpointing on
+// (src/engine/binary_splitting.cpp:295-302, 350-360, 605-644): a node of the tree (split point
+// m = a + (b - a) / 2) whose bs_<a>_<b>.ckpt loads is taken from the file. Otherwise, when a
+// file lies on a node below it, its halves are resolved and merged on the device
+// (P = Pl Pr, Q = Ql Qr, R = Qr Rl + Pl Rr, binary_splitting.cpp:161-293); otherwise the whole
+// range is one level-batched device splitting. A file that does not load (short or unreadable)
+// counts as absent, as in the reference's load_bs_result.
+class CkptSplit {
+public:
+    CkptSplit(pg_ctx* ctx, DevArith& A, CkptStaging& S, const std::string& dir, pg_ckpt_report& rep)
+        : ctx_(ctx), A_(A), S_(S), dir_(dir), rep_(rep) {
+        if (DIR* d = opendir(dir.c_str())) {
+            while (dirent* e = readdir(d)) {
+                unsigned long fa = 0, fb = 0;
+                int used = 0;
+                if (std::sscanf(e->d_name, "bs_%lu_%lu.ckpt%n", &fa, &fb, &used) == 2 &&
+                    e->d_name[used] == '\0' && fb > fa &&
+                    std::string(e->d_name) == ckpt::bs_path("", fa, fb).substr(1))
+                    files_.insert({fa, fb});
+            }
+            closedir(d);
+        }
+    }
+
+    // Resolves [a, b) into x; true when x came from the file bs_<a>_<b>.ckpt itself.
+    bool resolve(unsigned long a, unsigned long b, Node& x) {
+        if (files_.count({a, b}) && load_node(ckpt::bs_path(dir_, a, b), A_, S_, x)) {
+            ++rep_.nodes_loaded;
+            return true;
+        }
+        const unsigned long m = a + (b - a) / 2;
+        if (b - a > 1 && has_inner(a, b)) {
+            Node L(A_), Rn(A_);
+            resolve(a, m, L);
+            resolve(m, b, Rn);
+            A_.mul(x.P, L.P, Rn.P);
+            A_.mul(x.Q, L.Q, Rn.Q);
+            Num t(A_), u(A_);
+            A_.mul(t, Rn.Q, L.R);
+            A_.mul(u, L.P, Rn.R);
+            A_.add(x.R, t, u);
+            ++rep_.merges;
+            return false;
+        }
+        LevelView root;
+        uint32_t hl[3];
+        const pg_status s = bs_run_locked(ctx_, a, b, root, hl);
+        if (s != PG_OK) throw DevError(s, pg_last_error(ctx_));
+        // signs over the series: P(a,b) = (-1)^(#k >= 1), Q > 0, R(a,b) has the sign of R(a, a+1)
+        const unsigned long neg_terms = (b - a) - (a == 0 ? 1 : 0);
+        const int sg[3] = {(neg_terms & 1) ? -1 : 1, 1, a == 0 ? 1 : -1};
+        for (int k = 0; k < 3; ++k) {
+            DevNum& v = x.at(k);
+            A_.reserve(v, std::max<uint32_t>(hl[k], 1));
+            if (hl[k]) cudaMemcpyAsync(v.d, root.X[k], (size_t)hl[k] * 8, cudaMemcpyDeviceToDevice, A_.stream());
+            v.n = hl[k];
+            v.sign = hl[k] ? sg[k] : 0;
+        }
+        ++rep_.subtrees_computed;
+        return false;
+    }
+
+private:
+    // Is [fa, fb) a node of the tree rooted at [a, b)?
+    static bool is_node(unsigned long a, unsigned long b, unsigned long fa, unsigned long fb) {
+        while (true) {
+            if (a == fa && b == fb) return true;
+            if (b - a < 2) return false;
+            const unsigned long m = a + (b - a) / 2;
+            if (fb <= m)
+                b = m;
+            else if (fa >= m)
+                a = m;
+            else
+                return false;
+        }
+    }
+    // A file on a node strictly below [a, b)?
+    bool has_inner(unsigned long a, unsigned long b) const {
+        for (auto it = files_.lower_bound({a, 0}); it != files_.end() && it->first < b; ++it)
+            if (it->second <= b && !(it->first == a && it->second == b) && is_node(a, b, it->first, it->second))
+                return true;
+        return false;
+    }
+
+    pg_ctx* ctx_;
+    DevArith& A_;
+    CkptStaging& S_;
+    std::string dir_;
+    pg_ckpt_report& rep_;
+    std::set<std::pair<unsigned long, unsigned long>> files_;
+};
+
+// The reference's BinarySplitting::compute(a, b) with checkpointing on: resume from the
+// directory, and save bs_<a>_<b>.ckpt at the end unless it was loaded, removing the two
+// children's files (save_checkpoint, binary_splitting.cpp:121-135; compute always saves its
+// final result, :639-641).
+void split_checkpointed(pg_ctx* ctx, DevArith& A, CkptStaging& S, const std::string& dir, unsigned long a,
+                        unsigned long b, Node& x, pg_ckpt_report& rep) {
+    mkdir(dir.c_str(), 0755);  // enable_checkpointing (binary_splitting.cpp:104-109)
+    CkptSplit split(ctx, A, S, dir, rep);
+    if (split.resolve(a, b, x)) {
+        rep.root_loaded = 1;
+        return;
+    }
+    if (save_node(ckpt::bs_path(dir, a, b), A, S, x)) {
+        rep.root_saved = 1;
+        if (b - a > 1) {
+            const unsigned long m = a + (b - a) / 2;
+            std::remove(ckpt::bs_path(dir, a, m).c_str());
+            std::remove(ckpt::bs_path(dir, m, b).c_str());
+        }
+    }
+}
+
 pg_status fail(pg_ctx* c, pg_status s, const std::string& m) {
     ctx_set_error(c, m);
     return s;
@@ -737,6 +977,85 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
         seconds[0] = t_bs;
         seconds[1] = t_final;
         seconds[2] = secs(t1) - t_final;
+        seconds[3] = secs(t0);
+    }
+    return s;
+}
+
+pg_status pg_bs_checkpointed(pg_ctx* ctx, unsigned long a, unsigned long b, const char* dir, uint64_t* P, uint64_t* Q,
+                             uint64_t* R, size_t cap, size_t* len, int* sign, pg_ckpt_report* report) {
+    if (!ctx || !dir || !*dir || !Q || !R || !len || !sign || b <= a) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    pg_ckpt_report rep{};
+    const pg_status s = pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Node x(A);
+        pg::split_checkpointed(ctx, A, fs.stage, dir, a, b, x, rep);
+        uint64_t* dst[3] = {P, Q, R};
+        for (int k = 0; k < 3; ++k)
+            if (dst[k] && x.at(k).n > cap) throw pg::DevError(PG_ERR_BAD_ARG, "output buffers smaller than the result");
+        for (int k = 0; k < 3; ++k) {
+            len[k] = x.at(k).n;
+            sign[k] = x.at(k).sign;
+            if (dst[k]) A.download(x.at(k), dst[k]);
+        }
+    });
+    if (report) *report = rep;
+    return s;
+}
+
+pg_status pg_pi_checkpointed(pg_ctx* ctx, size_t digits, const char* dir, char* out, double* seconds,
+                             pg_ckpt_report* report) {
+    if (!ctx || !out || !dir || !*dir || digits == 0) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    const auto t0 = std::chrono::steady_clock::now();
+    auto secs = [](std::chrono::steady_clock::time_point t) {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t).count();
+    };
+    const unsigned long terms = (unsigned long)std::ceil((double)(digits + 100) / 14.1816474627) + 1;
+    pg_ckpt_report rep{};
+    double t_bs = 0, t_final = 0, t_conv = 0;
+    const pg_status s = pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Num X(A);
+        {
+            // the splitting first, resumed or not, then the pi_int file: the reference's order
+            // (pi_engine.cpp:245, then 263-284)
+            pg::Node root(A);
+            pg::split_checkpointed(ctx, A, fs.stage, dir, 0, terms, root, rep);
+            t_bs = secs(t0);
+            const auto t1 = std::chrono::steady_clock::now();
+            const std::string path = pg::ckpt::pi_int_path(dir, digits);
+            bool loaded = false;
+            {
+                pg::ckpt::File f(path, "rb");
+                loaded = f && pg::read_dev(f, A, fs.stage, X.v, false) && X.v.n > 0;
+            }
+            if (loaded) {
+                rep.pi_int_loaded = 1;
+            } else {
+                pg::final_formula(A, X, root.Q, root.R, digits);
+                pg::ckpt::File f(path, "wb");
+                if (f && pg::write_dev(f, A, fs.stage, X.v, false) && f.close()) rep.pi_int_saved = 1;
+            }
+            t_final = secs(t1);
+        }
+        const auto t2 = std::chrono::steady_clock::now();
+        char* body = out + 1;
+        pg::to_decimal(A, fs.sp, X, digits + 1, body);
+        out[0] = body[0];
+        out[1] = '.';
+        t_conv = secs(t2);
+    });
+    if (report) *report = rep;
+    if (seconds) {
+        seconds[0] = t_bs;
+        seconds[1] = t_final;
+        seconds[2] = t_conv;
         seconds[3] = secs(t0);
     }
     return s;

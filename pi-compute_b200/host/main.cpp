@@ -11,7 +11,13 @@
 //                                      and-conquer conversion on B200 products, or the reference's GMP mpf
 //           [--gpu-threshold N]        (default 10000 like the reference)
 //           [--device D]
+//           [--checkpoint DIR]         with --batched: resume from and save the reference's checkpoint
+//                                      files (bs_<a>_<b>.ckpt, pi_int_<N>.ckpt) in DIR
+//           [--resume]                 accepted like the reference's flag; checkpoints found in DIR are
+//                                      always used, as in the reference (src/main.cpp:94-97)
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -25,12 +31,13 @@ static void usage() {
         "pi_b200 - pi digits with exact big-integer products on one B200\n\n"
         "USAGE: pi_b200 --digits <N> [--output FILE] [--threads T] [--gpu|--b200] [--batched|--host-finish]\n"
         "               [--newton|--mpf]\n"
-        "               [--gpu-threshold N] [--device D] [--verbose]\n");
+        "               [--gpu-threshold N] [--device D] [--checkpoint DIR [--resume]] [--verbose]\n");
 }
 
 int main(int argc, char** argv) {
+    const auto t_main = std::chrono::steady_clock::now();
     pi::PiConfig cfg;
-    bool has_digits = false, gpu = false;
+    bool has_digits = false, gpu = false, resume = false;
     size_t threshold = 10000;
     std::string output = "pi_digits.txt";
     for (int i = 1; i < argc; ++i) {
@@ -61,6 +68,10 @@ int main(int argc, char** argv) {
             threshold = std::stoul(argv[++i]);
         } else if (a == "--device" && i + 1 < argc) {
             cfg.device = std::stoi(argv[++i]);
+        } else if (a == "--checkpoint" && i + 1 < argc) {
+            cfg.checkpoint_dir = argv[++i];
+        } else if (a == "--resume") {
+            resume = true;
         } else if (a == "--verbose" || a == "-v") {
             cfg.verbose = true;
         } else {
@@ -71,6 +82,15 @@ int main(int argc, char** argv) {
     }
     if (!has_digits || cfg.digits == 0) {
         std::fprintf(stderr, "Error: --digits <N> (N > 0) is required\n");
+        return 1;
+    }
+    if (resume && cfg.checkpoint_dir.empty()) {
+        std::fprintf(stderr, "Error: --resume requires --checkpoint <DIR>\n");
+        return 1;
+    }
+    if (!cfg.checkpoint_dir.empty() &&
+        !(cfg.mode == pi::BSMode::Batched && cfg.final_mode == pi::FinalMode::Device)) {
+        std::fprintf(stderr, "Error: --checkpoint needs --batched (the device-resident pipeline)\n");
         return 1;
     }
     try {
@@ -84,11 +104,21 @@ int main(int argc, char** argv) {
             if (cfg.mode == pi::BSMode::Batched) mode = "B200 batched";
         }
         pi::PiEngine eng(*mult);
+        const auto t_compute = std::chrono::steady_clock::now();
         pi::PiResult r = eng.compute(cfg);
+        const auto t_write = std::chrono::steady_clock::now();
         FILE* f = std::fopen(output.c_str(), "wb");
         if (!f) throw std::runtime_error("cannot open " + output);
-        std::fwrite(r.digits.data(), 1, r.digits.size(), f);
-        std::fclose(f);
+        const bool written = std::fwrite(r.digits.data(), 1, r.digits.size(), f) == r.digits.size();
+        if (std::fclose(f) != 0 || !written) throw std::runtime_error("cannot write " + output);
+        if (cfg.verbose || std::getenv("PI_B200_TRACE")) {
+            auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+                return std::chrono::duration<double, std::milli>(b - a).count();
+            };
+            const auto t_end = std::chrono::steady_clock::now();
+            std::printf("  Process: start to compute %.1f ms, compute (context included) %.1f ms, file %.1f ms\n",
+                        ms(t_main, t_compute), ms(t_compute, t_write), ms(t_write, t_end));
+        }
         std::printf("Computed %zu digits of pi in %g seconds (%lu terms, %s).\nOutput written to: %s\n", cfg.digits,
                     r.elapsed_seconds, r.terms_used, mode, output.c_str());
         if (auto* b = dynamic_cast<pi::B200Multiplier*>(mult.get())) {

@@ -80,9 +80,19 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
         const uint64_t l0 = pg_launch_count(ctx);
         std::string s(cfg.digits + 2, '0');
         double sec[4] = {0, 0, 0, 0};
-        const pg_status st = pg_pi(ctx, cfg.digits, &s[0], sec);
+        pg_ckpt_report rep{};
+        const bool ckpt = !cfg.checkpoint_dir.empty();
+        const pg_status st = ckpt ? pg_pi_checkpointed(ctx, cfg.digits, cfg.checkpoint_dir.c_str(), &s[0], sec, &rep)
+                                  : pg_pi(ctx, cfg.digits, &s[0], sec);
         if (st != PG_OK)
-            throw std::runtime_error(std::string("pg_pi: ") + pg_last_error(ctx) + " (status " + std::to_string(st) + ")");
+            throw std::runtime_error(std::string(ckpt ? "pg_pi_checkpointed: " : "pg_pi: ") + pg_last_error(ctx) +
+                                     " (status " + std::to_string(st) + ")");
+        if (ckpt && cfg.verbose)
+            std::printf("  Checkpoints in %s: splitting %s, %zu node(s) loaded, %zu subtree(s) computed, %zu merge(s);"
+                        " pi_int %s\n",
+                        cfg.checkpoint_dir.c_str(), rep.root_loaded ? "resumed" : (rep.root_saved ? "saved" : "not saved"),
+                        rep.nodes_loaded, rep.subtrees_computed, rep.merges,
+                        rep.pi_int_loaded ? "resumed" : (rep.pi_int_saved ? "saved" : "not saved"));
         res.digits.swap(s);
         res.t.gpu_launches += pg_launch_count(ctx) - l0;
         res.t.bs = sec[0];

@@ -31,6 +31,7 @@ struct PiConfig {
     int device = 0;                 // batched mode and the Newton finish
     size_t gpu_threshold = 1024;    // Newton finish: min limbs of the smaller operand for the GPU
     bool verbose = false;
+    std::string checkpoint_dir;     // batched device mode: resume from / save checkpoint files here
 };
 
 struct PiTimings {
