@@ -55,6 +55,17 @@ def load_pkg():
     return mod
 
 
+def load_oracle():
+    """oracle/oracle.py (the cpu_baseline leg times the reference's own GmpMultiplier through it)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("pi_oracle", os.path.join(ROOT, "oracle", "oracle.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["pi_oracle"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def measured_peaks() -> dict:
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -302,15 +313,21 @@ def run_b200(args):
         # end to end through the command-line program, like the reference's pi_compute
         e2e = None
         if not args.no_e2e:
+            # three fresh processes (CUDA start-up dominates and varies from run to run): the median
+            runs, sha = [], None
             with tempfile.TemporaryDirectory() as td:
                 out = os.path.join(td, "pi.txt")
-                t0 = time.perf_counter()
-                subprocess.run([pkg.PI_B200_BIN, "--batched", "--digits", str(D), "--threads", str(threads),
-                                "--device", str(local), "--output", out], check=True, stdout=subprocess.DEVNULL)
-                e2e_s = time.perf_counter() - t0
-                sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    subprocess.run([pkg.PI_B200_BIN, "--batched", "--digits", str(D), "--threads", str(threads),
+                                    "--device", str(local), "--output", out], check=True, stdout=subprocess.DEVNULL)
+                    runs.append(time.perf_counter() - t0)
+                    got_sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
+                    sha = got_sha if sha in (None, got_sha) else "differs between runs"
+            e2e_s = float(np.median(runs))
             e2e = {"value": round(D / e2e_s, 1), "unit": "digits/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": D + 2, "seconds": round(e2e_s, 3),
+                   "runs_s": [round(x, 3) for x in runs],
                    "path": "pi_b200 --batched (process start, CUDA context, output file)",
                    "sha256_matches_reference": (sha == want) if want else None}
         ph = np.mean(np.array(phases), axis=0)
@@ -358,6 +375,102 @@ def run_mul(args):
                           "dtype": "u32 mod p (NTT), u64 limbs", "data": "synthetic",
                           "config": {"workload": f"multiply, balanced 2^{args.logn} x 2^{args.logn} limbs", "na": n,
                                      "nb": n}, "roofline": roof, "gpu_launches": roof["launches"]}), flush=True)
+
+
+def run_sweep(args):
+    """Workload "sweep": the standalone multiply sweep. Seeded operands (splitmix64, a seed per size,
+    shape and trial) of n = 2^j and 3*2^(j-1) limbs, j = 10..24; balanced a*b, 1:4, 1:16 and
+    squares; every product's first run checked modulo three primes, then `--trials` timed runs
+    (CUDA events on the context's stream, operands in HBM). Reports median ms, GB/s of
+    B_mul = 400 (na + nb) / B_sqr = 536 n and the fraction of measured HBM bandwidth; GMP's mpz_mul
+    (the reference's GmpMultiplier, one core) beside it up to 2^20 limbs."""
+    import torch
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    pkg = load_pkg()
+    eng = pkg.Engine(local)
+    lib = eng.lib
+    dev = f"cuda:{local}"
+    stream = torch.cuda.ExternalStream(lib.pg_stream(eng.ctx), device=dev)
+    peaks = measured_peaks()
+    sizes = []
+    for j in range(10, 25):
+        sizes.append(1 << j)
+        if j < 24:
+            sizes.append(3 << (j - 1))
+    rows = []
+    launches0 = lib.pg_launch_count(eng.ctx)
+    for n in sizes:
+        for shape, nb in (("balanced", n), ("1:4", n // 4), ("1:16", n // 16), ("square", 0)):
+            seed = n * 8 + len(rows) % 4
+            a_h = pkg.random_operand(n, seed)
+            b_h = pkg.random_operand(nb, seed + 1) if nb else a_h
+            a_d = torch.from_numpy(a_h.view(np.int64)).to(dev)
+            b_d = torch.from_numpy(b_h.view(np.int64)).to(dev) if nb else a_d
+            m = n + (nb if nb else n)
+            out_d = torch.empty(m, dtype=torch.int64, device=dev)
+
+            def step():
+                if nb:
+                    st = lib.pg_mul_device(eng.ctx, a_d.data_ptr(), n, b_d.data_ptr(), nb, out_d.data_ptr())
+                else:
+                    st = lib.pg_sqr_device(eng.ctx, a_d.data_ptr(), n, out_d.data_ptr())
+                if st != 0:
+                    raise pkg.PgError(st, eng.last_error())
+
+            step()
+            if lib.pg_sync(eng.ctx) != 0:
+                raise pkg.PgError(-1, eng.last_error())
+            A, B = pkg.limbs_to_int(a_h), pkg.limbs_to_int(b_h)
+            R = pkg.limbs_to_int(out_d.cpu().numpy().view(np.uint64))
+            ok = all((A % q) * (B % q) % q == R % q for q in (2**61 - 1, 1000000007, 998244353))
+            if not ok:
+                raise RuntimeError(f"product check failed at n={n} shape={shape}")
+            step()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.trials + 1)]
+            torch.cuda.synchronize()
+            ev[0].record(stream)
+            for i in range(args.trials):
+                step()
+                ev[i + 1].record(stream)
+            torch.cuda.synchronize()
+            ms = statistics.median(ev[i].elapsed_time(ev[i + 1]) for i in range(args.trials))
+            balg = 400 * (n + nb) if nb else 536 * n
+            gbs = balg / (ms / 1e3) / 1e9
+            rows.append({"na": n, "nb": nb if nb else n, "shape": shape, "ms": round(ms, 4), "gbs": round(gbs, 1),
+                         "frac": round(gbs / peaks["hbm_gbs"], 4), "checked": "mod 2^61-1, 1e9+7, 998244353"})
+            del a_d, b_d, out_d
+    launches = lib.pg_launch_count(eng.ctx) - launches0
+    eng.close()
+    # GMP mpz_mul on one host core, the reference's GmpMultiplier::multiply (oracle/_ref)
+    cpu = []
+    oracle = None
+    try:
+        oracle = load_oracle()
+    except Exception:
+        pass
+    if oracle is not None and oracle.ref_available():
+        for n in (1 << 10, 1 << 14, 1 << 18, 1 << 20):
+            a_h, b_h = pkg.random_operand(n, 7), pkg.random_operand(n, 8)
+            reps = max(1, (1 << 20) // n)
+            t0 = time.perf_counter()
+            for _ in range(reps):
+                oracle.ref_mul(a_h, b_h)
+            cpu.append({"na": n, "nb": n, "ms": round((time.perf_counter() - t0) * 1e3 / reps, 3)})
+    if rank == 0:
+        head = next(r for r in rows if r["na"] == 1 << 24 and r["shape"] == "balanced")
+        print(json.dumps({"metric": "mul GB/s vs HBM (B_mul = 400*(na+nb))", "value": head["gbs"], "unit": "GB/s",
+                          "n_gpus": 1, "steps": args.trials, "warmup": 1, "ms_per_step": head["ms"],
+                          "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "u32 mod p (NTT), u64 limbs", "data": "synthetic (splitmix64)",
+                          "config": {"workload": "multiply sweep: 2^10..2^24 limbs and 3*2^(j-1), balanced, 1:4, "
+                                                 "1:16, square", "trials": args.trials,
+                                     "l2": "timed back to back; operands above 2^21 limbs exceed the 126 MB L2"},
+                          "sweep": rows, "gpu_launches": int(launches),
+                          "cpu_baseline": {"kind": "reference", "cores": 1,
+                                           "sample": "GmpMultiplier::multiply (mpz_mul) on balanced operands",
+                                           "rows": cpu}}), flush=True)
 
 
 def run_batch_workload(args):
@@ -455,7 +568,8 @@ def main():
     ap.add_argument("--logn", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="pi", choices=["pi", "mul", "batch"])
+    ap.add_argument("--workload", default="pi", choices=["pi", "mul", "batch", "sweep"])
+    ap.add_argument("--trials", type=int, default=5, help="timed runs per size and shape (sweep)")
     ap.add_argument("--batch-jobs", type=int, default=4096)
     args = ap.parse_args()
     if args.impl == "reference":
@@ -464,6 +578,8 @@ def main():
         run_mul(args)
     elif args.workload == "batch":
         run_batch_workload(args)
+    elif args.workload == "sweep":
+        run_sweep(args)
     else:
         run_b200(args)
 

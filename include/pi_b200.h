@@ -168,6 +168,12 @@ pg_status pg_mul_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs);
  *   characters; seconds (if not NULL, 4 entries) receives splitting, final formula,
  *   conversion and total wall time. */
 pg_status pg_recip_floor(pg_ctx* ctx, const uint64_t* r, size_t nr, uint64_t* z, size_t zcap, size_t* zlen);
+/* out = a * b mod (2^(32 L) - 1), L = 2^logL (6 <= logL <= 26), for na, nb <= L/2 limbs: one
+ * L-point transform product (the product wraps around) and a fold of its top words. The result
+ * lies in [0, 2^(32 L) - 1]; the modulus itself may stand for 0. The Newton steps of
+ * pg_recip_floor / pg_sqrt_scaled take their residues this way when that halves the transform. */
+pg_status pg_mul_wrap(pg_ctx* ctx, const uint64_t* a, size_t na, const uint64_t* b, size_t nb, int logL, uint64_t* out,
+                      size_t cap, size_t* len);
 pg_status pg_sqrt_scaled(pg_ctx* ctx, uint64_t a, size_t s, uint64_t* out, size_t cap, size_t* len);
 pg_status pg_to_decimal(pg_ctx* ctx, const uint64_t* x, size_t nx, size_t ndigits, char* out);
 pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t* r, size_t nr, size_t digits,

@@ -115,6 +115,8 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     lib.pg_mul_batch.restype = ctypes.c_int
     lib.pg_recip_floor.argtypes = [vp, _u64p, sz, _u64p, sz, _sizep]
     lib.pg_recip_floor.restype = ctypes.c_int
+    lib.pg_mul_wrap.argtypes = [vp, _u64p, sz, _u64p, sz, ctypes.c_int, _u64p, sz, _sizep]
+    lib.pg_mul_wrap.restype = ctypes.c_int
     lib.pg_sqrt_scaled.argtypes = [vp, ctypes.c_uint64, sz, _u64p, sz, _sizep]
     lib.pg_sqrt_scaled.restype = ctypes.c_int
     lib.pg_to_decimal.argtypes = [vp, _u64p, sz, sz, ctypes.c_char_p]
@@ -129,6 +131,9 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     lib.pg_tune_save.restype = ctypes.c_int
     lib.pg_tune_load.argtypes = [vp, ctypes.c_char_p]
     lib.pg_tune_load.restype = ctypes.c_int
+    lib.pg_bs.argtypes = [vp, ctypes.c_ulong, ctypes.c_ulong, ctypes.c_void_p, _u64p, _u64p, sz, _sizep,
+                          ctypes.POINTER(ctypes.c_int)]
+    lib.pg_bs.restype = ctypes.c_int
     p3 = ctypes.c_void_p * 3
     lib.pg_ckpt_write_bs.argtypes = [ctypes.c_char_p, p3, ctypes.c_size_t * 3, ctypes.c_int * 3]
     lib.pg_ckpt_write_bs.restype = ctypes.c_int
@@ -266,6 +271,16 @@ class Engine:
         self._check(self.lib.pg_recip_floor(self.ctx, _ptr(a), len(a), _ptr(out), len(out), ctypes.byref(n)))
         return limbs_to_int(out[: n.value])
 
+    def mul_wrap(self, a: int, b: int, logl: int) -> int:
+        """a * b mod (2^(32 * 2^logl) - 1) for a, b >= 0 of at most 2^(logl - 1) limbs (pg_mul_wrap)."""
+        aa, bb = int_to_limbs(a), int_to_limbs(b)
+        cap = (1 << (logl - 1)) + 2
+        out = np.zeros(cap, dtype=np.uint64)
+        n = ctypes.c_size_t()
+        self._check(self.lib.pg_mul_wrap(self.ctx, _ptr(aa), len(aa), _ptr(bb), len(bb), logl, _ptr(out), cap,
+                                         ctypes.byref(n)))
+        return limbs_to_int(out[: n.value])
+
     def sqrt_scaled(self, a: int, s: int) -> int:
         """floor(sqrt(a) * 2^s) (pg_sqrt_scaled)."""
         out = np.zeros(s // 64 + 4, dtype=np.uint64)
@@ -295,6 +310,15 @@ class Engine:
         if seconds is not None:
             seconds[:] = list(t)
         return buf.raw[: digits + 2]
+
+    def bs(self, a: int, b: int) -> tuple:
+        """(P, Q, R) of the term range [a, b) by the device splitting (pg_bs), as signed ints."""
+        cap = 64 + 8 * (b - a)
+        bufs = [np.zeros(cap, dtype=np.uint64) for _ in range(3)]
+        n = (ctypes.c_size_t * 3)()
+        sg = (ctypes.c_int * 3)()
+        self._check(self.lib.pg_bs(self.ctx, a, b, bufs[0].ctypes.data, _ptr(bufs[1]), _ptr(bufs[2]), cap, n, sg))
+        return tuple(sg[k] * limbs_to_int(bufs[k][: n[k]]) for k in range(3))
 
     # -------------------------------------------------- checkpoints
     def bs_checkpointed(self, a: int, b: int, directory: str) -> tuple:

@@ -694,10 +694,6 @@ void DevArith::add_si(DevNum& z, const DevNum& x, int64_t v) {
     release(c);
 }
 
-void DevArith::mul_raw(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out) {
-    check(enqueue_product(T_, W_, a, na, b, nb, out, st_, launches_), "product");
-}
-
 void DevArith::mul(DevNum& z, const DevNum& x, const DevNum& y) {
     if (x.sign == 0 || y.sign == 0) {
         reserve(z, 1);
@@ -707,10 +703,7 @@ void DevArith::mul(DevNum& z, const DevNum& x, const DevNum& y) {
     }
     DevNum t;
     reserve(t, x.n + y.n);
-    if (&x == &y || x.d == y.d)
-        check(enqueue_product(T_, W_, x.d, x.n, nullptr, x.n, t.d, st_, launches_), "square");
-    else
-        check(enqueue_product(T_, W_, x.d, x.n, y.d, y.n, t.d, st_, launches_), "product");
+    mul_limbs(x.d, x.n, y.d, y.n, t.d);
     t.n = x.n + y.n;
     t.sign = x.sign * y.sign;
     normalize(t);
@@ -719,6 +712,95 @@ void DevArith::mul(DevNum& z, const DevNum& x, const DevNum& y) {
 }
 
 void DevArith::sqr(DevNum& z, const DevNum& x) { mul(z, x, x); }
+
+void DevArith::mul_limbs(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out) {
+    const bool square = (a == b && na == nb);
+    // the transform's first pass reads operand limbs with 16-byte vector loads
+    if ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b) | reinterpret_cast<uintptr_t>(out)) & 15)
+        throw DevError(3, "product: operands must be 16-byte aligned");
+    if (product_logL(na, nb) <= split_logL()) {
+        check(enqueue_product(T_, W_, a, na, square ? nullptr : b, nb, out, st_, launches_), square ? "square" : "product");
+        return;
+    }
+    // Blocks of at most 2^(l-2) limbs, so that a block product (< 2^(l-1) limbs) fits one
+    // transform of 2^l points; k_a x k_b block products, each added into out at its offset.
+    // Block sizes are even: every block (and every offset in out) starts on a 16-byte boundary,
+    // which the transform's vector loads of the operand limbs need.
+    const size_t cap = (size_t)1 << (split_logL() - 2);
+    const size_t ka = (na + cap - 1) / cap, kb = (nb + cap - 1) / cap;
+    const size_t Ba = ((na + ka - 1) / ka + 1) & ~(size_t)1, Bb = ((nb + kb - 1) / kb + 1) & ~(size_t)1;
+    const size_t total = na + nb;
+    check(cudaMemsetAsync(out, 0, total * 8, st_), "block product");
+    DevNum t;
+    reserve(t, Ba + Bb);
+    for (size_t i = 0; i < ka && i * Ba < na; ++i) {
+        const size_t la = std::min(Ba, na - i * Ba);
+        for (size_t j = (square ? i : 0); j < kb && j * Bb < nb; ++j) {
+            const size_t lb = std::min(Bb, nb - j * Bb);
+            const uint64_t* bj = (square && i == j) ? nullptr : b + j * Bb;
+            check(enqueue_product(T_, W_, a + i * Ba, la, bj, lb, t.d, st_, launches_), "block product");
+            // out[off ..) += t (twice for an off-diagonal block of a square)
+            const size_t off = i * Ba + j * Bb;
+            for (int rep = 0; rep < ((square && i != j) ? 2 : 1); ++rep) {
+                AddArgs g{};
+                g.x = out + off;
+                g.nx = total - off;
+                g.y = t.d;
+                g.ny = la + lb;
+                g.z = out + off;
+                g.n = total - off;
+                g.njobs = 1;
+                run_add(g, 0);
+            }
+        }
+    }
+    release(t);
+}
+
+void DevArith::fold(DevNum& z, const DevNum& x, int logL) {
+    const size_t half = (size_t)1 << (logL - 1);  // limbs of 2^(32 L)
+    if (x.n <= half) return copy(z, x);
+    if (x.n > half + 2) throw DevError(3, "fold: value too long");
+    const int sign = x.sign;
+    DevNum lo, hi;  // views of x (never released)
+    lo.d = x.d;
+    lo.n = half;
+    lo.sign = 1;
+    normalize(lo);
+    hi.d = x.d + half;
+    hi.n = x.n - half;
+    hi.sign = 1;
+    DevNum t;
+    add(t, lo, hi);  // < 2^(32 L) + 2^128
+    if (t.n > half) {  // 2^(32 L) = M + 1: drop it and add one
+        tdiv_r_2exp(t, t, 64 * half);
+        add_si(t, t, 1);
+    }
+    if (t.n) t.sign = sign;
+    std::swap(z, t);
+    release(t);
+}
+
+void DevArith::mul_wrap(DevNum& z, const DevNum& x, const DevNum& y, int logL) {
+    const size_t half = (size_t)1 << (logL - 1);
+    if (x.sign == 0 || y.sign == 0) {
+        reserve(z, 1);
+        z.n = 0;
+        z.sign = 0;
+        return;
+    }
+    if (2 * x.n > 2 * half || 2 * y.n > 2 * half) throw DevError(3, "mul_wrap: operand longer than the transform");
+    DevNum t;
+    reserve(t, half + 1);
+    const bool sq = (&x == &y || x.d == y.d);
+    check(enqueue_product_wrap(T_, W_, x.d, x.n, sq ? nullptr : y.d, y.n, logL, t.d, st_, launches_), "wrapped product");
+    t.n = half + 1;
+    t.sign = 1;
+    normalize(t);
+    fold(z, t, logL);
+    release(t);
+    if (z.n) z.sign = x.sign * y.sign;
+}
 
 void DevArith::mul_ui(DevNum& z, const DevNum& x, uint64_t c) {
     if (x.sign == 0 || c == 0) {

@@ -513,6 +513,20 @@ struct DeviceBS {
         const uint64_t n = b0 - a0;
         D = 0;
         while ((1ull << D) < n) ++D;
+        // Quick rejection before the pass over all terms: q(k) = 10939058860032000 k^3 > 2^53 k^3,
+        // so Q(a0, b0) has more than 53 (b0 - lo) + 3 (b0 - mid) floor(log2 mid) bits (lo =
+        // max(a0, 1), mid = the middle of [lo, b0)), and the root merge's Q product needs a
+        // transform of at least that many bits / 32 points.
+        if (n >= 2) {
+            const uint64_t lo = std::max<uint64_t>(a0, 1), mid = lo + (b0 - lo) / 2;
+            int lg = 0;
+            while ((2ull << lg) <= mid) ++lg;
+            const uint64_t qmin = 53 * (b0 - lo) + 3 * (b0 - mid) * (uint64_t)lg;
+            if (qmin / 32 > (1ull << split_logL())) {
+                err = "binary-splitting product exceeds the transform range";
+                return {};
+            }
+        }
         // rightmost node at each depth: [b0 - s_d, b0)
         std::vector<uint64_t> s(D + 1);
         {
@@ -602,7 +616,7 @@ struct DeviceBS {
                 int l = 0;
                 while ((1ull << l) < conv) ++l;
                 P.logL = std::max(l, kMinLogL);
-                if (P.logL > kMaxLogL) {
+                if (P.logL > split_logL()) {
                     err = "binary-splitting product exceeds the transform range";
                     return {};
                 }
@@ -821,6 +835,9 @@ uint64_t* ctx_launches(pg_ctx* c);
 void ctx_set_error(pg_ctx* c, const std::string& msg);
 int ctx_device(pg_ctx* c);
 DeviceBS* ctx_bs(pg_ctx* c);
+// defined in pi_device.cu: [a, b) as subtrees merged on the device, into host buffers like pg_bs
+pg_status bs_split_to_host(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R,
+                           size_t cap, size_t* len, int* sign);
 DeviceBS* bs_state_new() { return new DeviceBS; }
 void bs_state_delete(DeviceBS* b) { delete b; }
 }  // namespace pg
@@ -870,6 +887,10 @@ extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
     pg::LevelView root;
     uint32_t hl[3];
     pg_status s = pg::bs_run_locked(ctx, a, b, root, hl);
+    if (s == PG_ERR_TOO_LARGE && b - a > 1) {  // subtrees merged with block products
+        pg::ctx_set_error(ctx, "");
+        return pg::bs_split_to_host(ctx, a, b, P, Q, R, cap, len, sign);
+    }
     if (s != PG_OK) return s;
     cudaStream_t st = pg::ctx_stream(ctx);
     auto tc0 = std::chrono::steady_clock::now();

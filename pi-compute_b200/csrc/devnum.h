@@ -75,7 +75,13 @@ public:
     void add(DevNum& z, const DevNum& x, const DevNum& y);
     void sub(DevNum& z, const DevNum& x, const DevNum& y);
     void add_si(DevNum& z, const DevNum& x, int64_t v);
-    void mul(DevNum& z, const DevNum& x, const DevNum& y);
+    void mul(DevNum& z, const DevNum& x, const DevNum& y);   // any length (block products beyond one transform)
+    // z = x * y reduced modulo M = 2^(32 L) - 1, L = 2^logL words: |z| in [0, M] with the
+    // product's sign (M itself stands for 0). 2 |x|.n <= L and 2 |y|.n <= L. One L-point
+    // transform product instead of the 2 (x.n + y.n)-word one.
+    void mul_wrap(DevNum& z, const DevNum& x, const DevNum& y, int logL);
+    // z = |x| mod M (M = 2^(32 L) - 1) with x's sign, for |x| < 2^(32 L + 128); M stays M.
+    void fold(DevNum& z, const DevNum& x, int logL);
     void sqr(DevNum& z, const DevNum& x);
     void mul_ui(DevNum& z, const DevNum& x, uint64_t c);
     void shl(DevNum& z, const DevNum& x, size_t s);
@@ -96,13 +102,16 @@ public:
     bool leaves(const uint64_t* x, uint64_t sx, uint64_t nlimbs, uint64_t njobs, uint64_t digits, char* out,
                 uint64_t skip, uint64_t total);
 
-    // Product of device magnitudes, exactly na + nb limbs at out (no normalisation).
-    void mul_raw(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out);
 
     const DeviceTables& tables() const { return T_; }
     Workspace& workspace() { return W_; }
     void sync();                              // wait and check the product error word
     uint64_t* launches() { return launches_; }
+
+    // out[0 .. na + nb) = a * b for any lengths (b == a allowed): one transform product when it
+    // fits split_logL(), otherwise products of blocks of at most half that length each, added
+    // into out at their offsets with exact carries.
+    void mul_limbs(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, uint64_t* out);
 
 private:
     void normalize(DevNum& x);                // exact length (waits)

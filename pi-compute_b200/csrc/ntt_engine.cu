@@ -286,17 +286,15 @@ CrtConsts make_crt_consts(int logL) {
 }
 
 // ---------------------------------------------------------------- one product
-cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
-                            const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
-                            uint64_t* launches) {
+static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                                const uint64_t* d_b, size_t nb, int logL, uint64_t nwords, uint64_t* d_out,
+                                cudaStream_t st, uint64_t* launches) {
     const bool square = (d_b == nullptr);
     if (square) nb = na;
-    const int logL = product_logL(na, nb);
     const Plan plan = T.plan(logL);
     const uint64_t L = 1ull << logL;
     cudaError_t e = W.ensure_res(3 * L);
     if (e != cudaSuccess) return e;
-    const uint64_t nwords = 2ull * (na + nb);
     const uint64_t crt_blocks = (nwords + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
     e = W.ensure_sync(crt_blocks);
     if (e != cudaSuccess) return e;
@@ -379,6 +377,25 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
     if (e != cudaSuccess) return e;
     if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + 1;
     return cudaGetLastError();
+}
+
+cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                            const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
+                            uint64_t* launches) {
+    const size_t mb = d_b ? nb : na;
+    return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL(na, mb), 2ull * (na + mb), d_out, st, launches);
+}
+
+cudaError_t enqueue_product_wrap(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                                 const uint64_t* d_b, size_t nb, int logL, uint64_t* d_out, cudaStream_t st,
+                                 uint64_t* launches) {
+    if (logL < kMinLogL || logL > kMaxLogL) return cudaErrorInvalidValue;
+    const uint64_t L = 1ull << logL;
+    if (2ull * na > L || (d_b && 2ull * nb > L)) return cudaErrorInvalidValue;
+    // the L-point transform wraps the product: coefficient i sums a_j b_k over j + k = i mod L,
+    // at most L terms of < 2^64 (< 2^90 <= the CRT range for L <= 2^26); their weighted sum
+    // over i < L is below 2^(32 (L - 1) + 91), i.e. it fits in L + 2 words
+    return enqueue_impl(T, W, d_a, na, d_b, nb, logL, L + 2, d_out, st, launches);
 }
 
 }  // namespace pg

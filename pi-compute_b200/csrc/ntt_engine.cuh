@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 
@@ -10,6 +11,23 @@
 #include "types.cuh"
 
 namespace pg {
+
+// Longest transform (log2 of its length) that one product of the splitting, the device
+// arithmetic and the conversion may use: kMaxLogL (26), or less when the environment variable
+// PG_MAX_LOGL asks for it (read once; tests lower it to drive the block-product and split-tree
+// paths at small sizes). Products beyond it are computed as blocks, and splitting ranges whose
+// top merges exceed it are split into subtrees merged with the device arithmetic.
+inline int split_logL() {
+    static const int v = [] {
+        int l = kMaxLogL;
+        if (const char* e = std::getenv("PG_MAX_LOGL")) {
+            const int x = std::atoi(e);
+            if (x >= 10 && x < kMaxLogL) l = x;
+        }
+        return l;
+    }();
+    return v;
+}
 
 constexpr int kPassThreads = 256;
 
@@ -66,5 +84,15 @@ struct Workspace {
 cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
                             const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
                             uint64_t* launches = nullptr);
+
+// Enqueue the wrapped product for a caller-chosen transform length L = 2^logL (2 na <= L and
+// 2 nb <= L words; b == nullptr means square): out[0 .. L/2 + 1) receives sum_{i<L} c_i 2^(32 i)
+// for the L-point cyclic convolution c of the operands' 32-bit words, a number congruent to
+// a * b modulo 2^(32 L) - 1 (fold its words above L to reduce it). Half the transform length
+// of the full product when only the product's residue is needed (Newton corrections, division
+// remainders).
+cudaError_t enqueue_product_wrap(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                                 const uint64_t* d_b, size_t nb, int logL, uint64_t* d_out, cudaStream_t st,
+                                 uint64_t* launches = nullptr);
 
 }  // namespace pg

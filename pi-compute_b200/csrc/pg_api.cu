@@ -172,6 +172,7 @@ pg_status pg_create(int device, pg_ctx** out) {
     if (!out) return PG_ERR_BAD_ARG;
     *out = nullptr;
     int n = 0;
+    const auto t_init = std::chrono::steady_clock::now();
     if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
         cudaGetLastError();
         return PG_ERR_BAD_ARG;
@@ -180,6 +181,7 @@ pg_status pg_create(int device, pg_ctx** out) {
     if (!c) return PG_ERR_OOM;
     c->device = device;
     const auto t0 = std::chrono::steady_clock::now();
+    const double t_driver = std::chrono::duration<double, std::milli>(t0 - t_init).count();
     auto ms = [](std::chrono::steady_clock::time_point a) {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
     };
@@ -189,8 +191,10 @@ pg_status pg_create(int device, pg_ctx** out) {
     if (e == cudaSuccess) e = c->tables.build(device);
     if (e == cudaSuccess) e = c->ws.ensure_sync(1);
     if (pg::trace_on())
-        std::fprintf(stderr, "[pg_create] device %d: context and stream %.3f ms, twiddle tables %.3f ms\n", device, t_ctx,
-                     ms(t0) - t_ctx);
+        std::fprintf(stderr,
+                     "[pg_create] device %d: driver and device count %.3f ms, context and stream %.3f ms, twiddle "
+                     "tables %.3f ms\n",
+                     device, t_driver, t_ctx, ms(t0) - t_ctx);
     if (e != cudaSuccess) {
         cudaGetLastError();
         pg_destroy(c);

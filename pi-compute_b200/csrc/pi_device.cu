@@ -93,7 +93,7 @@ struct SharedProduct {
     void run(const DeviceTables& T, cudaStream_t st, uint64_t* launches, const uint64_t* a, uint64_t sa, uint64_t na,
              uint64_t njobs, const uint64_t* b, uint64_t nb, uint64_t* out, uint64_t so) {
         if (!njobs) return;
-        if (na + nb > ((uint64_t)1 << (kMaxLogL - 1))) throw DevError(PG_ERR_TOO_LARGE, "batched product too long");
+        if (product_logL(na, nb) > split_logL()) throw DevError(PG_ERR_TOO_LARGE, "batched product too long");
         if ((sa | so) & 1) throw DevError(PG_ERR_INTERNAL, "batched product strides must be even");
         if (!errw) {
             if (cudaMalloc((void**)&errw, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "error word");
@@ -274,6 +274,37 @@ u128 isqrt128(u128 v) {
 // Z = floor(2^(2k) / R), k = bits(R) (R > 0). Newton doubling: Zh = floor(2^(2h) / Rh) for the
 // top h = k/2 + 32 bits of R, Z0 = Zh 2^(k-h), one Newton step, then the exact correction
 // 0 <= 2^(2k) - R Z < R.
+// Transform length (log2 of L words) of a wrapped product whose modulus M = 2^(32 L) - 1
+// leaves room for a value of `bits` bits and a sign (32 L >= bits + 2), with operands of na, nb
+// limbs fitting the transform; 0 when that is not shorter than the full product's transform.
+int wrap_logL(size_t bits, size_t na, size_t nb) {
+    int l = kMinLogL;
+    while (((uint64_t)32 << l) < (uint64_t)bits + 2 || ((uint64_t)1 << l) < 2 * (uint64_t)std::max(na, nb)) ++l;
+    if (l > split_logL() || l >= product_logL(na, nb)) return 0;
+    return l;
+}
+
+// e from its representative in (-M, M), M = 2^(32 L) - 1, when the value itself has
+// |e| < 2^(32 L - 2): a representative with 32 L - 1 or more bits is off by M.
+void centre(DevArith& A, DevNum& e, int logL) {
+    const size_t lbits = (size_t)32 << logL;
+    if (A.bits(e) + 1 < lbits) return;
+    Num M(A);
+    A.set_pow2(M, lbits);
+    A.add_si(M, M, -1);
+    if (e.sign > 0)
+        A.sub(e, e, M);
+    else
+        A.add(e, e, M);
+}
+
+// e = 2^p - x (|e| < 2^(bits)) with x a product known modulo M = 2^(32 L) - 1 (xm in [0, M]).
+void residue_diff(DevArith& A, DevNum& e, size_t p, const DevNum& xm, int logL) {
+    A.set_pow2(e, p % ((size_t)32 << logL));  // 2^(32 L) = 1 mod M
+    A.sub(e, e, xm);
+    centre(A, e, logL);
+}
+
 void recip_floor(DevArith& A, DevNum& Z, const DevNum& R) {
     const size_t k = A.bits(R);
     if (k == 0 || R.sign < 0) throw DevError(PG_ERR_BAD_ARG, "recip_floor: R must be positive");
@@ -292,11 +323,25 @@ void recip_floor(DevArith& A, DevNum& Z, const DevNum& R) {
     A.tdiv_q_2exp(Rh, R, k - h);
     recip_floor(A, Zh, Rh);
     A.shl(Z0, Zh, k - h);
-    A.mul(T, R, Z0);
-    A.set_pow2(E, 2 * k);
-    A.sub(E, E, T);                 // E = 2^(2k) - R Z0
-    A.mul(D, Zh, E);                // Z0 E / 2^(2k) = Zh E / 2^(k+h)
-    A.fdiv_q_2exp(D, D, k + h);
+    // E = 2^(2k) - R Z0. With R = 2^(k-h) (Rh + f), 0 <= f < 1, and Rh >= 2^(h-1):
+    // |2^(2k)/R - Z0| <= 2^(k-h+2), so |E| < 2^(2k-h+2): E follows from R Z0 modulo
+    // 2^(32 L) - 1 for a transform about 3/4 the length of the full product's.
+    const int lw = wrap_logL(2 * k - h + 3, R.n, Z0.v.n);
+    if (lw) {
+        A.mul_wrap(T, R, Z0, lw);
+        residue_diff(A, E, 2 * k, T, lw);
+    } else {
+        A.mul(T, R, Z0);
+        A.set_pow2(E, 2 * k);
+        A.sub(E, E, T);
+    }
+    // D = floor(Z0 E / 2^(2k)) = floor(Zh E / 2^(k+h)) from E's top bits: dropping the low
+    // s = k - 2 bits of E lowers Zh E / 2^(k+h) by less than Zh 2^s / 2^(k+h) <= 1/2
+    // (Zh <= 2^(h+1)), so D is exact or one low; the final correction absorbs that.
+    const size_t s = k - 2;
+    A.fdiv_q_2exp(T, E, s);
+    A.mul(D, Zh, T);
+    A.fdiv_q_2exp(D, D, k + h - s);
     A.add(Z, Z0, D);
     A.mul(T, R, D);
     A.sub(E, E, T);                 // E = 2^(2k) - R Z
@@ -325,12 +370,27 @@ void rsqrt_approx(DevArith& A, DevNum& u, uint64_t a, size_t q) {
     Num uh(A), u0(A), T(A), e(A), D(A);
     rsqrt_approx(A, uh, a, qh);
     A.shl(u0, uh, q - qh);
-    A.sqr(T, u0);
-    A.mul_ui(T, T, a);
-    A.set_pow2(e, 2 * q);
-    A.sub(e, e, T);                 // 2^(2q) - a u0^2
-    A.mul(D, uh, e);                // u0 e / 2^(2q+1) = uh e / 2^(q + qh + 1)
-    A.fdiv_q_2exp(D, D, q + qh + 1);
+    // e = 2^(2q) - a u0^2 = a (v + u0)(v - u0), v = 2^q / sqrt(a): with uh within c units of
+    // 2^qh / sqrt(a), |e| <= 2 c sqrt(a) 2^(2q - qh) (plus a far smaller square term); c <= 2^4
+    // and a < 2^64 give |e| < 2^(2q - qh + 38)
+    const int lw = wrap_logL(2 * q - qh + 38, u0.v.n, u0.v.n);
+    if (lw) {
+        A.mul_wrap(T, u0, u0, lw);
+        A.mul_ui(T, T, a);
+        A.fold(T, T, lw);
+        residue_diff(A, e, 2 * q, T, lw);
+    } else {
+        A.sqr(T, u0);
+        A.mul_ui(T, T, a);
+        A.set_pow2(e, 2 * q);
+        A.sub(e, e, T);
+    }
+    // D = floor(u0 e / 2^(2q+1)) = floor(uh e / 2^(q + qh + 1)) from e's top bits: dropping
+    // s = q - 1 low bits lowers it by less than uh 2^s / 2^(q + qh + 1) < 1/4 (uh < 2^qh)
+    const size_t s = q - 1;
+    A.fdiv_q_2exp(T, e, s);
+    A.mul(D, uh, T);
+    A.fdiv_q_2exp(D, D, q + qh + 1 - s);
     A.add(u, u0, D);
 }
 
@@ -341,10 +401,22 @@ void sqrt_scaled(DevArith& A, DevNum& S, uint64_t a, size_t s) {
     rsqrt_approx(A, u, a, q);
     A.mul_ui(S, u, a);              // a 2^q / sqrt(a)
     A.tdiv_q_2exp(S, S, q - s);
-    A.set_pow2(N, 2 * s);
-    A.mul_ui(N, N, a);
-    A.sqr(t, S);
-    A.sub(V, N, t);                 // V = N - S^2
+    // V = N - S^2 with N = a 2^(2s); S is within a few units of sqrt(N), so |V| is about
+    // 2 S c < 2^(s + 40) for a < 2^64: S^2 modulo 2^(32 L) - 1 is enough
+    const int lw = wrap_logL(s + 40, S.n, S.n);
+    if (lw) {
+        A.mul_wrap(t, S, S, lw);
+        A.set_pow2(N, (2 * s) % ((size_t)32 << lw));
+        A.mul_ui(N, N, a);
+        A.fold(N, N, lw);
+        A.sub(V, N, t);
+        centre(A, V, lw);
+    } else {
+        A.set_pow2(N, 2 * s);
+        A.mul_ui(N, N, a);
+        A.sqr(t, S);
+        A.sub(V, N, t);             // V = N - S^2
+    }
     int steps = 0;
     while (V.v.sign < 0) {          // (S-1)^2 = S^2 - 2S + 1
         A.add(V, V, S);
@@ -496,7 +568,7 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         // The top reciprocal by Newton; every lower one from the one above it:
         // with Y = floor(2^(2K') / P^2) (K' = bits(P^2)), floor(P Y / 2^(2K' - 2K)) undershoots
         // floor(2^(2K) / P) by at most one (the error P 2^(2K - 2K') is below 2^(2 - K)), so one
-        // exact check 0 <= 2^(2K) - P Z < P finishes it.
+        // exact check 0 <= 2^(2K) - P Z < P finishes it (two with Y's low bits dropped, below).
         const int top = J - 1;
         if (top >= kLeafLog) recip_floor(A, inv[top - kLeafLog]->v, P[top - kLeafLog]->v);
         Num T(A), E(A);
@@ -504,11 +576,23 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
             DevNum& Pj = P[j - kLeafLog]->v;
             DevNum& Z = inv[j - kLeafLog]->v;
             const size_t k = K[j - kLeafLog], k2 = K[j + 1 - kLeafLog];
-            A.mul(T, Pj, inv[j + 1 - kLeafLog]->v);
-            A.tdiv_q_2exp(Z, T, 2 * k2 - 2 * k);
-            A.mul(T, Pj, Z);
-            A.set_pow2(E, 2 * k);
-            A.sub(E, E, T);
+            // Z from the top bits of the reciprocal above: dropping its low s = sh - k - 1 bits
+            // lowers P Y / 2^sh by less than P 2^s / 2^sh < 1/2, so Z undershoots by at most 2
+            const size_t sh = 2 * k2 - 2 * k;
+            const size_t s = sh > k + 1 ? sh - k - 1 : 0;
+            A.tdiv_q_2exp(E, inv[j + 1 - kLeafLog]->v, s);
+            A.mul(T, Pj, E);
+            A.tdiv_q_2exp(Z, T, sh - s);
+            // E = 2^(2K) - P Z lies in [0, 3P): P Z modulo 2^(32 L) - 1 suffices
+            const int lw = wrap_logL(k + 3, Pj.n, Z.n);
+            if (lw) {
+                A.mul_wrap(T, Pj, Z, lw);
+                residue_diff(A, E, 2 * k, T, lw);
+            } else {
+                A.mul(T, Pj, Z);
+                A.set_pow2(E, 2 * k);
+                A.sub(E, E, T);
+            }
             int steps = 0;
             while (E.v.sign < 0) {
                 A.add_si(Z, Z, -1);
@@ -528,6 +612,17 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
     auto even = [](size_t n) { return (n + 1) & ~(size_t)1; };
     // capacity (limbs, even) of a chunk < 10^(2^j): bits(10^(2^j)) / 64 + 1
     auto cap_of = [&](int j) { return even(kb(j) / 64 + 2); };
+
+    // the level's products with one shared operand: one batch, or (chunks too long for one
+    // transform, the top levels beyond ~300M digits) a block product per chunk
+    auto shared_mul = [&](const uint64_t* a, uint64_t sa, uint64_t na, uint64_t njobs, const uint64_t* b, uint64_t nb,
+                          uint64_t* out, uint64_t so) {
+        if (product_logL(na, nb) <= split_logL()) {
+            sp.run(A.tables(), st, A.launches(), a, sa, na, njobs, b, nb, out, so);
+            return;
+        }
+        for (uint64_t j = 0; j < njobs; ++j) A.mul_limbs(a + j * sa, na, b, nb, out + j * so);
+    };
 
     Timer tm("divide-and-conquer levels and leaves");
     const uint64_t* cur = x.d;
@@ -567,25 +662,30 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         const DevNum& Ij = iv(j);
         const size_t ni = Ij.n, np = Pj.n;
         if (cur_n == 0) cur_n = 1;
-        // T = c * inv, q = T >> 2K into the even slots of the next level
-        const size_t sT = even(cur_n + ni);
+        // T = (c >> 64 s) * inv, q = T >> (2K - 64 s) into the even slots of the next level. The
+        // chunk's low 64 s <= K - 2 bits are dropped (an even limb count, so the operand stays
+        // 16-byte aligned): that lowers c inv / 2^(2K) by less than 2^(64 s + 1 - K) <= 1/2, so q
+        // undershoots floor(c / P) by at most 3 and the product is about 2K bits, not 3K.
+        const size_t s64 = std::min<size_t>(kb(j) >= 66 ? ((kb(j) - 2) / 64) & ~(size_t)1 : 0, (cur_n - 1) & ~(size_t)1);
+        const size_t nct = cur_n - s64;
+        const size_t sT = even(nct + ni);
         A.reserve(Tbuf, sT * njobs);
-        sp.run(A.tables(), st, A.launches(), cur, cur_s, cur_n, njobs, Ij.d, ni, Tbuf.v.d, sT);
+        shared_mul(cur + s64, cur_s, nct, njobs, Ij.d, ni, Tbuf.v.d, sT);
         A.reserve(*next, 2 * cap * njobs);
-        A.batch_shr(Tbuf.v.d, sT, cur_n + ni, next->d, 2 * cap, cap, 2 * kb(j), njobs);
+        A.batch_shr(Tbuf.v.d, sT, nct + ni, next->d, 2 * cap, cap, 2 * kb(j) - 64 * s64, njobs);
         // U = q * P, r = c - U (< 3 P) into the odd slots
         const size_t sU = even(cap + np);
         A.reserve(Ubuf, sU * njobs);
-        sp.run(A.tables(), st, A.launches(), next->d, 2 * cap, cap, njobs, Pj.d, np, Ubuf.v.d, sU);
+        shared_mul(next->d, 2 * cap, cap, njobs, Pj.d, np, Ubuf.v.d, sU);
         A.reserve(Rbuf, cur_s * njobs);
         A.batch_add(cur, cur_s, cur_n, Ubuf.v.d, sU, std::min(cap + np, cur_n), Rbuf.v.d, cur_s, cur_n, true, 0,
                     nullptr, njobs);
         A.batch_shr(Rbuf.v.d, cur_s, cur_n, next->d + cap, 2 * cap, cap, 0, njobs);
-        // corrections: while r >= P: r -= P, q += 1 (at most twice)
+        // corrections: while r >= P: r -= P, q += 1 (at most three times)
         A.reserve(Ppad, cap);
         cudaMemsetAsync(Ppad.v.d, 0, cap * 8, st);
         cudaMemcpyAsync(Ppad.v.d, Pj.d, np * 8, cudaMemcpyDeviceToDevice, st);
-        for (int round = 0; round < 2; ++round) {
+        for (int round = 0; round < 3; ++round) {
             A.batch_ge(next->d + cap, 2 * cap, Ppad.v.d, 0, cap, ge, njobs);
             A.batch_add(next->d + cap, 2 * cap, cap, Ppad.v.d, 0, np, next->d + cap, 2 * cap, cap, true, 0, ge, njobs);
             A.batch_add(next->d, 2 * cap, cap, nullptr, 0, 0, next->d, 2 * cap, cap, false, 1, ge, njobs);
@@ -721,12 +821,14 @@ bool load_node(const std::string& path, DevArith& A, CkptStaging& S, Node& x) {
 // file lies on a node below it, its halves are resolved and merged on the device
 // (P = Pl Pr, Q = Ql Qr, R = Qr Rl + Pl Rr, binary_splitting.cpp:161-293); otherwise the whole
 // range is one level-batched device splitting. A file that does not load (short or unreadable)
-// counts as absent, as in the reference's load_bs_result.
+// counts as absent, as in the reference's load_bs_result. A range whose top merges need
+// transforms longer than split_logL() is split the same way (with no directory this is how
+// pi beyond ~300M digits runs: level-batched subtrees below, block products above).
 class CkptSplit {
 public:
     CkptSplit(pg_ctx* ctx, DevArith& A, CkptStaging& S, const std::string& dir, pg_ckpt_report& rep)
         : ctx_(ctx), A_(A), S_(S), dir_(dir), rep_(rep) {
-        if (DIR* d = opendir(dir.c_str())) {
+        if (DIR* d = dir.empty() ? nullptr : opendir(dir.c_str())) {
             while (dirent* e = readdir(d)) {
                 unsigned long fa = 0, fb = 0;
                 int used = 0;
@@ -745,23 +847,20 @@ public:
             ++rep_.nodes_loaded;
             return true;
         }
-        const unsigned long m = a + (b - a) / 2;
         if (b - a > 1 && has_inner(a, b)) {
-            Node L(A_), Rn(A_);
-            resolve(a, m, L);
-            resolve(m, b, Rn);
-            A_.mul(x.P, L.P, Rn.P);
-            A_.mul(x.Q, L.Q, Rn.Q);
-            Num t(A_), u(A_);
-            A_.mul(t, Rn.Q, L.R);
-            A_.mul(u, L.P, Rn.R);
-            A_.add(x.R, t, u);
-            ++rep_.merges;
+            merge_halves(a, b, x);
             return false;
         }
         LevelView root;
         uint32_t hl[3];
         const pg_status s = bs_run_locked(ctx_, a, b, root, hl);
+        if (s == PG_ERR_TOO_LARGE && b - a > 1) {
+            // the top merges of [a, b) need longer transforms than one product may use: its
+            // halves, merged with the device arithmetic (block products)
+            ctx_set_error(ctx_, "");
+            merge_halves(a, b, x);
+            return false;
+        }
         if (s != PG_OK) throw DevError(s, pg_last_error(ctx_));
         // signs over the series: P(a,b) = (-1)^(#k >= 1), Q > 0, R(a,b) has the sign of R(a, a+1)
         const unsigned long neg_terms = (b - a) - (a == 0 ? 1 : 0);
@@ -778,6 +877,20 @@ public:
     }
 
 private:
+    void merge_halves(unsigned long a, unsigned long b, Node& x) {
+        const unsigned long m = a + (b - a) / 2;
+        Node L(A_), Rn(A_);
+        resolve(a, m, L);
+        resolve(m, b, Rn);
+        A_.mul(x.P, L.P, Rn.P);
+        A_.mul(x.Q, L.Q, Rn.Q);
+        Num t(A_), u(A_);
+        A_.mul(t, Rn.Q, L.R);
+        A_.mul(u, L.P, Rn.R);
+        A_.add(x.R, t, u);
+        ++rep_.merges;
+    }
+
     // Is [fa, fb) a node of the tree rooted at [a, b)?
     static bool is_node(unsigned long a, unsigned long b, unsigned long fa, unsigned long fb) {
         while (true) {
@@ -864,6 +977,27 @@ pg_status guarded(pg_ctx* ctx, F&& f) {
 }
 
 }  // namespace
+
+pg_status bs_split_to_host(pg_ctx* ctx, unsigned long a, unsigned long b, uint64_t* P, uint64_t* Q, uint64_t* R,
+                           size_t cap, size_t* len, int* sign) {
+    return guarded(ctx, [&] {
+        FinishState& fs = *ctx_finish(ctx);
+        DevArith A(ctx_tables(ctx), ctx_workspace(ctx), ctx_stream(ctx), ctx_launches(ctx), fs.pool);
+        Node x(A);
+        pg_ckpt_report rep{};
+        CkptSplit split(ctx, A, fs.stage, "", rep);
+        split.resolve(a, b, x);
+        uint64_t* dst[3] = {P, Q, R};
+        for (int k = 0; k < 3; ++k)
+            if (dst[k] && x.at(k).n > cap) throw DevError(PG_ERR_BAD_ARG, "output buffers smaller than the result");
+        for (int k = 0; k < 3; ++k) {
+            len[k] = x.at(k).n;
+            sign[k] = x.at(k).sign;
+            if (dst[k]) A.download(x.at(k), dst[k]);
+        }
+    });
+}
+
 }  // namespace pg
 
 extern "C" {
@@ -882,6 +1016,27 @@ pg_status pg_recip_floor(pg_ctx* ctx, const uint64_t* r, size_t nr, uint64_t* z,
         if (Z.v.n > zcap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_recip_floor: output buffer too small");
         A.download(Z, z);
         *zlen = Z.v.n;
+    });
+}
+
+pg_status pg_mul_wrap(pg_ctx* ctx, const uint64_t* a, size_t na, const uint64_t* b, size_t nb, int logL, uint64_t* out,
+                      size_t cap, size_t* len) {
+    if (!ctx || !out || !len || (na && !a) || (nb && !b) || logL < pg::kMinLogL || logL > pg::kMaxLogL)
+        return PG_ERR_BAD_ARG;
+    const size_t half = (size_t)1 << (logL - 1);
+    if (na > half || nb > half) return PG_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaSetDevice(pg::ctx_device(ctx));
+    return pg::guarded(ctx, [&] {
+        pg::FinishState& fs = *pg::ctx_finish(ctx);
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        pg::Num X(A), Y(A), Z(A);
+        A.upload(X, a, na, 1);
+        A.upload(Y, b, nb, 1);
+        A.mul_wrap(Z, X, Y, logL);
+        if (Z.v.n > cap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_mul_wrap: output buffer too small");
+        A.download(Z, out);
+        *len = Z.v.n;
     });
 }
 
@@ -949,23 +1104,36 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
     pg::LevelView root;
     uint32_t hl[3];
     pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl);
-    if (s != PG_OK) return s;
-    const double t_bs = secs(t0);
-    const auto t1 = std::chrono::steady_clock::now();
-    double t_final = 0;
+    const bool big = (s == PG_ERR_TOO_LARGE);  // split into subtrees below, merged on the device
+    if (s != PG_OK && !big) return s;
+    if (big) pg::ctx_set_error(ctx, "");
+    double t_bs = secs(t0), t_final = 0;
+    auto t1 = std::chrono::steady_clock::now();
     s = pg::guarded(ctx, [&] {
         pg::FinishState& fs = *pg::ctx_finish(ctx);
         pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
-        // Q, R of the root (both positive for a = 0), copied out of the splitting buffers
+        // Q, R of the root (both positive for a = 0)
         pg::Num Q(A), R(A), X(A);
-        A.reserve(Q, hl[1]);
-        A.reserve(R, hl[2]);
-        cudaMemcpyAsync(Q.v.d, root.X[1], (size_t)hl[1] * 8, cudaMemcpyDeviceToDevice, A.stream());
-        cudaMemcpyAsync(R.v.d, root.X[2], (size_t)hl[2] * 8, cudaMemcpyDeviceToDevice, A.stream());
-        Q.v.n = hl[1];
-        Q.v.sign = hl[1] ? 1 : 0;
-        R.v.n = hl[2];
-        R.v.sign = hl[2] ? 1 : 0;
+        if (big) {
+            pg::Node x(A);
+            pg_ckpt_report rep{};
+            pg::CkptSplit split(ctx, A, fs.stage, "", rep);
+            split.resolve(0, terms, x);
+            std::swap(Q.v, x.Q.v);
+            std::swap(R.v, x.R.v);
+            A.sync();
+            t_bs = secs(t0);
+            t1 = std::chrono::steady_clock::now();
+        } else {  // copied out of the splitting buffers
+            A.reserve(Q, hl[1]);
+            A.reserve(R, hl[2]);
+            cudaMemcpyAsync(Q.v.d, root.X[1], (size_t)hl[1] * 8, cudaMemcpyDeviceToDevice, A.stream());
+            cudaMemcpyAsync(R.v.d, root.X[2], (size_t)hl[2] * 8, cudaMemcpyDeviceToDevice, A.stream());
+            Q.v.n = hl[1];
+            Q.v.sign = hl[1] ? 1 : 0;
+            R.v.n = hl[2];
+            R.v.sign = hl[2] ? 1 : 0;
+        }
         pg::final_formula(A, X, Q, R, digits);
         t_final = secs(t1);
         char* body = out + 1;  // the integer's digits: "3" then the fraction digits

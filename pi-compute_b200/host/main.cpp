@@ -20,6 +20,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <unistd.h>
 #include <stdexcept>
 #include <string>
 
@@ -124,7 +125,12 @@ int main(int argc, char** argv) {
         if (auto* b = dynamic_cast<pi::B200Multiplier*>(mult.get())) {
             if (cfg.verbose) b->print_stats();
         }
-        return 0;
+        // The output file is closed and checked: leave without tearing the device context down
+        // (freeing gigabytes of device buffers one by one takes longer than the driver's own
+        // clean-up of an exiting process).
+        std::fflush(stdout);
+        std::fflush(stderr);
+        _exit(0);
     } catch (const std::exception& e) {
         std::fprintf(stderr, "Error: %s\n", e.what());
         return 1;

@@ -9,7 +9,8 @@ without them):
 Outputs
   pi_1000.txt        "3." + 1000 digits from the reference program (checked byte-for-byte
                      against the reference's own tests/data/pi_1000.txt when it is mounted)
-  pi_golden.json     sha256 / head / tail of the reference program's 1M and 10M digit files
+  pi_golden.json     sha256 / head / tail of the reference program's 1M, 10M and 100M digit files
+                     (and 1B with --1b: `python tests/golden/make_golden.py --1b`)
   bs_golden.json     P, Q, R (hex) of the reference's BinarySplitting for small ranges, and
                      sha256 of P/Q/R for the 1M-digit term range
   products.json      sha256 of seeded random products computed by libgmp's mpz_mul
@@ -64,12 +65,19 @@ def main() -> None:
         assert pi1000 == open(REF_DATA, "rb").read().rstrip(b"\r\n "), "reference build disagrees with pi_1000.txt"
     open(os.path.join(HERE, "pi_1000.txt"), "wb").write(pi1000)
 
+    path = os.path.join(HERE, "pi_golden.json")
+    old = json.load(open(path)) if os.path.exists(path) else {}
     pig = {}
-    for d in (1_000_000, 10_000_000, 100_000_000):
+    # 1B digits (config 5) takes the reference ~15 minutes on 6 cores and 6.5 GB: only with --1b,
+    # otherwise an earlier entry is kept
+    sizes = [1_000_000, 10_000_000, 100_000_000] + ([1_000_000_000] if "--1b" in sys.argv else [])
+    for d in sizes:
         s = run_ref(d, os.cpu_count() or 1)
         pig[str(d)] = {"sha256": hashlib.sha256(s).hexdigest(), "bytes": len(s), "head": s[:66].decode(),
                        "tail": s[-64:].decode()}
-    json.dump(pig, open(os.path.join(HERE, "pi_golden.json"), "w"), indent=1)
+    if "1000000000" not in pig and "1000000000" in old:
+        pig["1000000000"] = old["1000000000"]
+    json.dump(pig, open(path, "w"), indent=1)
 
     bsg = {"ranges": {}, "hash_ranges": {}}
     for a, b in [(0, 1), (1, 2), (2, 3), (0, 2), (0, 8), (3, 11), (0, 79), (100, 357), (0, 1000)]:

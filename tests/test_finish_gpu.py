@@ -48,6 +48,28 @@ def test_recip_floor_exact(eng, bits):
     assert eng.recip_floor((1 << k) - 1) == (1 << (2 * k)) // ((1 << k) - 1)  # all ones
 
 
+def mod_mersenne(x: int, n: int) -> int:
+    """x mod 2^n - 1 by folding (Python's % would divide in quadratic time)."""
+    m = (1 << n) - 1
+    while x > m:
+        x = (x & m) + (x >> n)
+    return 0 if x == m else x
+
+
+@pytest.mark.parametrize("logl", [6, 7, 10, 13, 14, 16])
+def test_mul_wrap_is_the_product_modulo_2_32L_minus_1(eng, logl):
+    L = 1 << logl
+    M = (1 << (32 * L)) - 1
+    half = L // 2
+    full = [rnd_bits(64 * half, 7 * logl + i) for i in range(2)]
+    cases = [(full[0], full[1]), (M, full[0]), (M, M), (1, 1), (1 << (32 * L - 1), 2), (0, full[1]),
+             (rnd_bits(64, logl), full[1]), (M - 1, M - 1), (full[0], full[0])]
+    for a, b in cases:
+        got = eng.mul_wrap(a, b, logl)
+        assert 0 <= got <= M, (logl, a.bit_length(), b.bit_length())
+        assert mod_mersenne(got, 32 * L) == mod_mersenne(a * b, 32 * L), (logl, a.bit_length(), b.bit_length())
+
+
 @pytest.mark.parametrize("s", [0, 1, 60, 64, 65, 200, 5000, 100_000, 1_000_003])
 def test_sqrt_scaled_exact(eng, s):
     for a in (10005, 2, 3):
