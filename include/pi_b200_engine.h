@@ -42,6 +42,14 @@ int pib_pi(size_t digits, int mode, unsigned threads, size_t threshold, int devi
 int pib_bs(unsigned long a, unsigned long b, int mode, size_t threshold, int device, uint64_t* P, uint64_t* Q,
            uint64_t* R, size_t cap, size_t* len, int* sign);
 
+/* r = a * b through the drop-in pi::B200Multiplier::multiply on mpz_t (threshold routing like the
+ * reference's should_use_gpu; products longer than one transform as block products of pg_mul
+ * calls). Magnitudes are little-endian limbs with signs sa, sb; out (out_cap limbs) receives |r|,
+ * out_len its length and out_sign its sign. Replaces GpuNttMultiplier::multiply
+ * (src/arithmetic/gpu_ntt_multiplier.cpp:144-210) for callers outside C++. */
+int pib_mul(const uint64_t* a, size_t na, int sa, const uint64_t* b, size_t nb, int sb, size_t threshold, int device,
+            uint64_t* out, size_t out_cap, size_t* out_len, int* out_sign);
+
 /* Message of the last failing call in this thread. */
 const char* pib_last_error(void);
 

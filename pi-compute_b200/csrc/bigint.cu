@@ -45,6 +45,12 @@ __device__ __forceinline__ uint32_t gp_warp_scan(uint32_t gp, int lane) {
     return gp;
 }
 
+// *p = v (a single word written by the device, so the host does not wait to reuse a pinned word)
+__global__ void set_word_kernel(uint64_t* p, uint64_t v) { *p = v; }
+
+// *out = (*in == 0): the enable flag of a negation that runs only after a borrow
+__global__ void not_flag_kernel(const uint32_t* in, uint32_t* out) { *out = (*in & 1u) ? 0u : 1u; }
+
 // Short numbers: one warp per job, K = ceil(n / 32) <= 8 limbs per lane.
 template <AddForm F>
 __global__ void add_warp_kernel(AddArgs A) {
@@ -436,6 +442,7 @@ void DevArith::release(DevNum& x) {
     x.d = nullptr;
     x.cap = x.n = 0;
     x.sign = 0;
+    x.slack = 0;
 }
 
 uint64_t* DevArith::scratch(size_t limbs) {
@@ -524,26 +531,29 @@ void DevArith::normalize(DevNum& x) {
     sync();
     x.n = (size_t)host_word_[0];
     if (x.n == 0) x.sign = 0;
+    x.slack = 0;
 }
 
 void DevArith::set_ui(DevNum& x, uint64_t v) {
     reserve(x, 2);
-    host_word_[1] = v;
-    check(cudaMemcpyAsync(x.d, host_word_ + 1, 8, cudaMemcpyHostToDevice, st_), "set_ui");
-    sync();  // the pinned word is reused
+    set_word_kernel<<<1, 1, 0, st_>>>(x.d, v);  // a launch, not a copy from a reused pinned word
+    check(cudaGetLastError(), "set_ui");
+    ++*launches_;
     x.n = v ? 1 : 0;
     x.sign = v ? 1 : 0;
+    x.slack = 0;
 }
 
 void DevArith::set_pow2(DevNum& x, size_t e) {
     const size_t n = e / 64 + 1;
     reserve(x, n);
-    check(cudaMemsetAsync(x.d, 0, n * 8, st_), "set_pow2");
-    host_word_[1] = 1ull << (e % 64);
-    check(cudaMemcpyAsync(x.d + n - 1, host_word_ + 1, 8, cudaMemcpyHostToDevice, st_), "set_pow2");
-    sync();
+    if (n > 1) check(cudaMemsetAsync(x.d, 0, (n - 1) * 8, st_), "set_pow2");
+    set_word_kernel<<<1, 1, 0, st_>>>(x.d + n - 1, 1ull << (e % 64));
+    check(cudaGetLastError(), "set_pow2");
+    ++*launches_;
     x.n = n;
     x.sign = 1;
+    x.slack = 0;
 }
 
 void DevArith::copy(DevNum& z, const DevNum& x) {
@@ -552,6 +562,7 @@ void DevArith::copy(DevNum& z, const DevNum& x) {
     if (x.n) check(cudaMemcpyAsync(z.d, x.d, x.n * 8, cudaMemcpyDeviceToDevice, st_), "copy");
     z.n = x.n;
     z.sign = x.sign;
+    z.slack = x.slack;
 }
 
 void DevArith::upload(DevNum& x, const uint64_t* host, size_t n, int sign) {
@@ -560,15 +571,18 @@ void DevArith::upload(DevNum& x, const uint64_t* host, size_t n, int sign) {
     if (n) check(cudaMemcpyAsync(x.d, host, n * 8, cudaMemcpyHostToDevice, st_), "upload");
     sync();
     x.n = n;
+    x.slack = 0;
     x.sign = n ? (sign < 0 ? -1 : 1) : 0;
 }
 
 void DevArith::download(const DevNum& x, uint64_t* host) {
+    exact(const_cast<DevNum&>(x));  // the value is unchanged; only its recorded length
     if (x.n) check(cudaMemcpyAsync(host, x.d, x.n * 8, cudaMemcpyDeviceToHost, st_), "download");
     sync();
 }
 
 size_t DevArith::bits(const DevNum& x) {
+    exact(const_cast<DevNum&>(x));
     if (x.n == 0) return 0;
     check(cudaMemcpyAsync(host_word_, x.d + x.n - 1, 8, cudaMemcpyDeviceToHost, st_), "bits");
     sync();
@@ -577,6 +591,8 @@ size_t DevArith::bits(const DevNum& x) {
 }
 
 int DevArith::cmp_abs(const DevNum& x, const DevNum& y) {
+    exact(const_cast<DevNum&>(x));
+    exact(const_cast<DevNum&>(y));
     if (x.n != y.n) return x.n < y.n ? -1 : 1;
     if (x.n == 0) return 0;
     unsigned long long* diff = reinterpret_cast<unsigned long long*>(flags(2));
@@ -594,6 +610,8 @@ int DevArith::cmp_abs(const DevNum& x, const DevNum& y) {
 }
 
 int DevArith::cmp(const DevNum& x, const DevNum& y) {
+    exact(const_cast<DevNum&>(x));  // a zero value gets sign 0
+    exact(const_cast<DevNum&>(y));
     if (x.sign != y.sign) return x.sign < y.sign ? -1 : 1;
     const int c = cmp_abs(x, y);
     return x.sign >= 0 ? c : -c;
@@ -617,7 +635,7 @@ void DevArith::add_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign) {
     run_add(a, 0);
     out.n = n;
     out.sign = sign;
-    normalize(out);
+    out.slack = std::max(x.slack, y.slack) + 1;
     if (alias) {
         std::swap(z, t);
         release(t);
@@ -631,7 +649,10 @@ void DevArith::sub_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign_if_
     const bool alias = (&z == &x) || (&z == &y);
     DevNum& out = alias ? t : z;
     reserve(out, n);
-    uint32_t* co = flags(1);
+    // f[0]: carry out of x - y (0 <=> |x| < |y|), f[1]: 1 - f[0], f[2..3]: exact length
+    uint32_t* f = flags(4);
+    unsigned long long* top = reinterpret_cast<unsigned long long*>(f + 2);
+    check(cudaMemsetAsync(f, 0, 16, st_), "sub");
     AddArgs a{};
     a.x = x.d;
     a.nx = x.n;
@@ -642,26 +663,29 @@ void DevArith::sub_mag(DevNum& z, const DevNum& x, const DevNum& y, int sign_if_
     a.z = out.d;
     a.n = n;
     a.njobs = 1;
-    a.carry_out = co;
+    a.carry_out = f;
     run_add(a, 0);
-    check(cudaMemcpyAsync(host_word_, co, 4, cudaMemcpyDeviceToHost, st_), "sub");
+    not_flag_kernel<<<1, 1, 0, st_>>>(f, f + 1);
+    ++*launches_;
+    AddArgs b{};  // on a borrow, two's complement in place: magnitude = ~out + 1
+    b.x = out.d;
+    b.nx = n;
+    b.mx = ~0ull;
+    b.cin = 1;
+    b.z = out.d;
+    b.n = n;
+    b.enable = f + 1;
+    b.njobs = 1;
+    run_add(b, 0);
+    top_kernel<<<grid_for(n), 256, 0, st_>>>(out.d, n, top);
+    ++*launches_;
+    // the borrow and the exact length come back together: the one host wait of a subtraction
+    check(cudaMemcpyAsync(host_word_, f, 16, cudaMemcpyDeviceToHost, st_), "sub");
     sync();
-    const bool borrow = (host_word_[0] & 1u) == 0;  // carry out 0 <=> |x| < |y|
-    out.n = n;
-    out.sign = sign_if_pos;
-    if (borrow) {  // two's complement: magnitude = ~out + 1
-        AddArgs b{};
-        b.x = out.d;
-        b.nx = n;
-        b.mx = ~0ull;
-        b.cin = 1;
-        b.z = out.d;
-        b.n = n;
-        b.njobs = 1;
-        run_add(b, 0);
-        out.sign = -sign_if_pos;
-    }
-    normalize(out);
+    const bool borrow = (host_word_[0] & 1u) == 0;
+    out.n = (size_t)host_word_[1];
+    out.sign = out.n ? (borrow ? -sign_if_pos : sign_if_pos) : 0;
+    out.slack = 0;
     if (alias) {
         std::swap(z, t);
         release(t);
@@ -701,12 +725,16 @@ void DevArith::mul(DevNum& z, const DevNum& x, const DevNum& y) {
         z.sign = 0;
         return;
     }
+    // upper-bound lengths compound through chains of products (a squaring doubles the slack):
+    // operands more than a few limbs over their exact length are measured first
+    if (x.slack > 4) exact(const_cast<DevNum&>(x));
+    if (y.slack > 4) exact(const_cast<DevNum&>(y));
     DevNum t;
     reserve(t, x.n + y.n);
     mul_limbs(x.d, x.n, y.d, y.n, t.d);
     t.n = x.n + y.n;
     t.sign = x.sign * y.sign;
-    normalize(t);
+    t.slack = x.slack + y.slack + 1;
     std::swap(z, t);
     release(t);
 }
@@ -762,16 +790,18 @@ void DevArith::fold(DevNum& z, const DevNum& x, int logL) {
     if (x.n <= half) return copy(z, x);
     if (x.n > half + 2) throw DevError(3, "fold: value too long");
     const int sign = x.sign;
-    DevNum lo, hi;  // views of x (never released)
+    DevNum lo, hi;  // views of x (never released); lo may have zero top limbs, which add() allows
     lo.d = x.d;
     lo.n = half;
     lo.sign = 1;
-    normalize(lo);
+    lo.slack = half;
     hi.d = x.d + half;
     hi.n = x.n - half;
     hi.sign = 1;
+    hi.slack = hi.n;
     DevNum t;
     add(t, lo, hi);  // < 2^(32 L) + 2^128
+    exact(t);
     if (t.n > half) {  // 2^(32 L) = M + 1: drop it and add one
         tdiv_r_2exp(t, t, 64 * half);
         add_si(t, t, 1);
@@ -794,9 +824,9 @@ void DevArith::mul_wrap(DevNum& z, const DevNum& x, const DevNum& y, int logL) {
     reserve(t, half + 1);
     const bool sq = (&x == &y || x.d == y.d);
     check(enqueue_product_wrap(T_, W_, x.d, x.n, sq ? nullptr : y.d, y.n, logL, t.d, st_, launches_), "wrapped product");
-    t.n = half + 1;
+    t.n = half + 1;  // an upper bound: fold() adds the top limb in whether or not it is zero
     t.sign = 1;
-    normalize(t);
+    t.slack = half + 1;
     fold(z, t, logL);
     release(t);
     if (z.n) z.sign = x.sign * y.sign;
@@ -821,7 +851,7 @@ void DevArith::mul_ui(DevNum& z, const DevNum& x, uint64_t c) {
     run_add(a, 1);
     t.n = x.n + 1;
     t.sign = x.sign;
-    normalize(t);
+    t.slack = x.slack + 1;
     std::swap(z, t);
     release(t);
 }
@@ -836,7 +866,7 @@ void DevArith::shl(DevNum& z, const DevNum& x, size_t s) {
     ++*launches_;
     t.n = n;
     t.sign = x.sign;
-    normalize(t);
+    t.slack = x.slack + 1;
     std::swap(z, t);
     release(t);
 }
@@ -856,30 +886,42 @@ void DevArith::tdiv_q_2exp(DevNum& z, const DevNum& x, size_t s) {
     ++*launches_;
     t.n = n;
     t.sign = x.sign;
-    normalize(t);
+    t.slack = x.slack + 1;
     std::swap(z, t);
     release(t);
 }
 
 void DevArith::fdiv_q_2exp(DevNum& z, const DevNum& x, size_t s) {
-    if (x.sign >= 0) return tdiv_q_2exp(z, x, s);
-    // floor of a negative quotient: -(ceil(|x| / 2^s)) = -(trunc + (any low bit set))
+    if (x.sign >= 0 || x.n == 0) return tdiv_q_2exp(z, x, s);
+    // floor of a negative quotient: -(trunc(|x| / 2^s) + (any low bit set)); the +1 is applied on
+    // the device under the sticky flag, so the host does not wait for it
+    const size_t q = s / 64;
+    const size_t n = x.n > q ? x.n - q : 0;
+    DevNum t;
+    reserve(t, n + 1);
     uint32_t* f = flags(1);
     check(cudaMemsetAsync(f, 0, 4, st_), "fdiv");
-    sticky_kernel<<<grid_for(std::min<uint64_t>(x.n, s / 64 + 1)), 256, 0, st_>>>(x.d, x.n, s, f);
+    sticky_kernel<<<grid_for(std::min<uint64_t>(x.n, q + 1)), 256, 0, st_>>>(x.d, x.n, s, f);
     ++*launches_;
-    check(cudaMemcpyAsync(host_word_, f, 4, cudaMemcpyDeviceToHost, st_), "fdiv");
-    sync();
-    const bool sticky = (host_word_[0] & 1u) != 0;
-    tdiv_q_2exp(z, x, s);
-    if (sticky) {
-        if (z.sign == 0) {
-            set_ui(z, 1);
-            z.sign = -1;
-        } else {
-            add_si(z, z, -1);  // z is negative: -1 grows its magnitude
-        }
+    if (n) {
+        shr_kernel<<<grid_for(n), 256, 0, st_>>>(x.d, 0, x.n, t.d, 0, n, s, 1);
+        ++*launches_;
     }
+    check(cudaMemsetAsync(t.d + n, 0, 8, st_), "fdiv");
+    AddArgs a{};
+    a.x = t.d;
+    a.nx = n + 1;
+    a.cin = 1;
+    a.z = t.d;
+    a.n = n + 1;
+    a.enable = f;  // in place, only when a dropped bit was set
+    a.njobs = 1;
+    run_add(a, 0);
+    t.n = n + 1;
+    t.sign = -1;
+    t.slack = x.slack + 2;
+    std::swap(z, t);
+    release(t);
 }
 
 void DevArith::tdiv_r_2exp(DevNum& z, const DevNum& x, size_t s) {
@@ -893,7 +935,7 @@ void DevArith::tdiv_r_2exp(DevNum& z, const DevNum& x, size_t s) {
     }
     t.n = n;
     t.sign = x.sign;
-    normalize(t);
+    t.slack = n;  // the low bits may have zero limbs on top: length unknown
     std::swap(z, t);
     release(t);
 }

@@ -1,8 +1,9 @@
 // DevArith: signed multi-limb integers in device memory with mpz-like operations, for the
 // pieces of the pi pipeline that follow binary splitting (Newton reciprocal, square root,
 // final products, radix conversion). Magnitudes are little-endian 64-bit limb arrays in HBM;
-// the sign and the exact limb count are kept on the host (operations whose result length or
-// sign depends on the data read one small word back, which waits for the stream).
+// the sign and the limb count are kept on the host. Operations leave an upper bound on the limb
+// count without waiting; the exact count is read back (a host wait) only where it is needed:
+// bit lengths, comparisons, the sign of a difference, downloads.
 //
 // Products go through the NTT engine (enqueue_product); additions, shifts, comparisons and
 // small multiples through the carry-chain kernels of bigint.cuh.
@@ -22,8 +23,9 @@ namespace pg {
 struct DevNum {
     uint64_t* d = nullptr;
     size_t cap = 0;   // limbs allocated
-    size_t n = 0;     // limbs in use (top limb non-zero when n > 0)
-    int sign = 0;     // -1, 0, +1
+    size_t n = 0;     // limbs in use: exact (top limb non-zero when n > 0), or an upper bound
+    int sign = 0;     // -1, 0, +1; with an upper-bound length a zero value may still carry +-1
+    size_t slack = 0;   // n may exceed the exact length by at most this many limbs (0: exact)
 };
 
 class DevError : public std::runtime_error {
@@ -66,7 +68,14 @@ public:
     void set_pow2(DevNum& x, size_t e);
     void copy(DevNum& z, const DevNum& x);
     void upload(DevNum& x, const uint64_t* host, size_t n, int sign);
-    void download(const DevNum& x, uint64_t* host);  // x.n limbs
+    void download(const DevNum& x, uint64_t* host);  // x.n limbs (exact length first)
+    // Makes x.n exact (and the sign 0 for a zero value), reading the length back from the device
+    // when an operation left an upper bound. Products, additions, shifts and small multiples leave
+    // upper bounds, so a chain of them runs without host waits; comparisons, bit lengths and
+    // downloads call this.
+    void exact(DevNum& x) {
+        if (x.slack) normalize(x);
+    }
 
     size_t bits(const DevNum& x);             // bit length of |x|
     int cmp_abs(const DevNum& x, const DevNum& y);

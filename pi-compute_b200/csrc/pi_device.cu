@@ -251,6 +251,7 @@ void upload_u128(DevArith& A, DevNum& x, u128 v) {
 }
 
 u128 download_u128(DevArith& A, const DevNum& x) {
+    A.exact(const_cast<DevNum&>(x));
     if (x.n > 2) throw DevError(PG_ERR_INTERNAL, "download_u128: value too long");
     uint64_t w[2] = {0, 0};
     if (x.n) A.download(x, w);
@@ -278,6 +279,8 @@ u128 isqrt128(u128 v) {
 // leaves room for a value of `bits` bits and a sign (32 L >= bits + 2), with operands of na, nb
 // limbs fitting the transform; 0 when that is not shorter than the full product's transform.
 int wrap_logL(size_t bits, size_t na, size_t nb) {
+    // below 2^17 points the product is cheaper than the fold's and centring's extra host waits
+    if (product_logL(na, nb) <= 17) return 0;
     int l = kMinLogL;
     while (((uint64_t)32 << l) < (uint64_t)bits + 2 || ((uint64_t)1 << l) < 2 * (uint64_t)std::max(na, nb)) ++l;
     if (l > split_logL() || l >= product_logL(na, nb)) return 0;
@@ -498,6 +501,7 @@ void final_formula(DevArith& A, DevNum& pi_int, const DevNum& Q, const DevNum& R
         const u128 tv = download_u128(A, top);
         const u128 all_ones = ((u128)1 << 100) - 1;
         const bool below = tv == 0;                          // fr < 2^(fb-100)
+        A.exact(low);  // a zero low part has sign 0 only with its exact length
         const bool above = tv == all_ones && low.v.sign != 0;  // fr > 2^fb - 2^(fb-100)
         if (!below && !above) {
             A.tdiv_q_2exp(pi_int, X, fb);
@@ -559,8 +563,8 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         for (int j = 0; j < J; ++j) {
             if (j >= kLeafLog) {
                 P.push_back(new Num(A));
+                K.push_back(A.bits(p));  // makes p's length exact before the copy
                 A.copy(*P.back(), p);
-                K.push_back(A.bits(p));
                 inv.push_back(new Num(A));
             }
             if (j + 1 < J) A.sqr(p, p);
@@ -788,6 +792,7 @@ bool read_dev(ckpt::File& f, DevArith& A, CkptStaging& S, DevNum& x, bool with_s
     if (!ok) return false;
     x.n = (used + 7) / 8;
     x.sign = x.n ? (sign < 0 ? -1 : 1) : 0;
+    x.slack = 0;
     return true;
 }
 
@@ -871,6 +876,7 @@ public:
             if (hl[k]) cudaMemcpyAsync(v.d, root.X[k], (size_t)hl[k] * 8, cudaMemcpyDeviceToDevice, A_.stream());
             v.n = hl[k];
             v.sign = hl[k] ? sg[k] : 0;
+            v.slack = 0;
         }
         ++rep_.subtrees_computed;
         return false;
@@ -988,6 +994,7 @@ pg_status bs_split_to_host(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
         CkptSplit split(ctx, A, fs.stage, "", rep);
         split.resolve(a, b, x);
         uint64_t* dst[3] = {P, Q, R};
+        for (int k = 0; k < 3; ++k) A.exact(x.at(k));
         for (int k = 0; k < 3; ++k)
             if (dst[k] && x.at(k).n > cap) throw DevError(PG_ERR_BAD_ARG, "output buffers smaller than the result");
         for (int k = 0; k < 3; ++k) {
@@ -1013,6 +1020,7 @@ pg_status pg_recip_floor(pg_ctx* ctx, const uint64_t* r, size_t nr, uint64_t* z,
         A.upload(R, r, nr, 1);
         if (R.v.sign == 0) throw pg::DevError(PG_ERR_BAD_ARG, "pg_recip_floor: R is zero");
         pg::recip_floor(A, Z, R);
+        A.exact(Z);
         if (Z.v.n > zcap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_recip_floor: output buffer too small");
         A.download(Z, z);
         *zlen = Z.v.n;
@@ -1034,6 +1042,7 @@ pg_status pg_mul_wrap(pg_ctx* ctx, const uint64_t* a, size_t na, const uint64_t*
         A.upload(X, a, na, 1);
         A.upload(Y, b, nb, 1);
         A.mul_wrap(Z, X, Y, logL);
+        A.exact(Z);
         if (Z.v.n > cap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_mul_wrap: output buffer too small");
         A.download(Z, out);
         *len = Z.v.n;
@@ -1049,6 +1058,7 @@ pg_status pg_sqrt_scaled(pg_ctx* ctx, uint64_t a, size_t s, uint64_t* out, size_
         pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
         pg::Num S(A);
         pg::sqrt_scaled(A, S, a, s);
+        A.exact(S);
         if (S.v.n > cap) throw pg::DevError(PG_ERR_BAD_ARG, "pg_sqrt_scaled: output buffer too small");
         A.download(S, out);
         *len = S.v.n;
@@ -1133,6 +1143,7 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
             Q.v.sign = hl[1] ? 1 : 0;
             R.v.n = hl[2];
             R.v.sign = hl[2] ? 1 : 0;
+            Q.v.slack = R.v.slack = 0;
         }
         pg::final_formula(A, X, Q, R, digits);
         t_final = secs(t1);
@@ -1162,6 +1173,7 @@ pg_status pg_bs_checkpointed(pg_ctx* ctx, unsigned long a, unsigned long b, cons
         pg::Node x(A);
         pg::split_checkpointed(ctx, A, fs.stage, dir, a, b, x, rep);
         uint64_t* dst[3] = {P, Q, R};
+        for (int k = 0; k < 3; ++k) A.exact(x.at(k));
         for (int k = 0; k < 3; ++k)
             if (dst[k] && x.at(k).n > cap) throw pg::DevError(PG_ERR_BAD_ARG, "output buffers smaller than the result");
         for (int k = 0; k < 3; ++k) {

@@ -8,6 +8,7 @@
 #include <map>
 #include <mutex>
 #include <stdexcept>
+#include <vector>
 
 namespace pi {
 
@@ -66,11 +67,13 @@ void B200Multiplier::product(mpz_t result, const mpz_t a, const mpz_t b, bool sq
     size_t len = 0;
     pg_status s;
     const uint64_t* ap = reinterpret_cast<const uint64_t*>(mpz_limbs_read(a));
-    if (sq)
+    const uint64_t* bp = reinterpret_cast<const uint64_t*>(mpz_limbs_read(b));
+    if (na + nb > pg_mul_max_limbs())
+        s = block_product(ap, na, bp, nb, sq, reinterpret_cast<uint64_t*>(out), &len);
+    else if (sq)
         s = pg_sqr(ctx_, ap, na, reinterpret_cast<uint64_t*>(out), na + nb, &len);
     else
-        s = pg_mul(ctx_, ap, na, reinterpret_cast<const uint64_t*>(mpz_limbs_read(b)), nb,
-                   reinterpret_cast<uint64_t*>(out), na + nb, &len);
+        s = pg_mul(ctx_, ap, na, bp, nb, reinterpret_cast<uint64_t*>(out), na + nb, &len);
     if (s != PG_OK) {
         mpz_limbs_finish(dst, 0);
         if (alias) mpz_clear(tmp);
@@ -86,6 +89,45 @@ void B200Multiplier::product(mpz_t result, const mpz_t a, const mpz_t b, bool sq
     stats_.gpu_limbs.fetch_add(na + nb);
     stats_.gpu_ns.fetch_add(
         (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count());
+}
+
+// A product longer than one transform (pg_mul_max_limbs): products of blocks of at most half that
+// many limbs each, one pg_mul call per pair, added into out at their limb offsets.
+pg_status B200Multiplier::block_product(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, bool sq,
+                                        uint64_t* out, size_t* len) {
+    const size_t cap = pg_mul_max_limbs() / 2;
+    const size_t ka = (na + cap - 1) / cap, kb = (nb + cap - 1) / cap;
+    const size_t Ba = (na + ka - 1) / ka, Bb = (nb + kb - 1) / kb, total = na + nb;
+    std::fill(out, out + total, (uint64_t)0);
+    std::vector<uint64_t> buf(Ba + Bb);
+    for (size_t i = 0; i < ka && i * Ba < na; ++i) {
+        const size_t la = std::min(Ba, na - i * Ba);
+        for (size_t j = sq ? i : 0; j < kb && j * Bb < nb; ++j) {
+            const size_t lb = std::min(Bb, nb - j * Bb);
+            size_t n = 0;
+            const pg_status s = (sq && i == j) ? pg_sqr(ctx_, a + i * Ba, la, buf.data(), la + lb, &n)
+                                               : pg_mul(ctx_, a + i * Ba, la, b + j * Bb, lb, buf.data(), la + lb, &n);
+            if (s != PG_OK) return s;
+            for (int rep = 0; rep < ((sq && i != j) ? 2 : 1); ++rep) {  // off-diagonal blocks of a square twice
+                unsigned __int128 c = 0;
+                size_t k = i * Ba + j * Bb;
+                for (size_t t = 0; t < n; ++t, ++k) {
+                    c += (unsigned __int128)out[k] + buf[t];
+                    out[k] = (uint64_t)c;
+                    c >>= 64;
+                }
+                for (; c && k < total; ++k) {
+                    c += out[k];
+                    out[k] = (uint64_t)c;
+                    c >>= 64;
+                }
+            }
+        }
+    }
+    size_t n = total;
+    while (n && out[n - 1] == 0) --n;
+    *len = n;
+    return PG_OK;
 }
 
 void B200Multiplier::multiply(mpz_t result, const mpz_t a, const mpz_t b) { product(result, a, b, a == b); }

@@ -55,6 +55,8 @@ public:
 
 private:
     void product(mpz_t result, const mpz_t a, const mpz_t b, bool square);
+    pg_status block_product(const uint64_t* a, size_t na, const uint64_t* b, size_t nb, bool square, uint64_t* out,
+                            size_t* len);
     pg_ctx* ctx_ = nullptr;
     bool owned_ = true;
     size_t threshold_;

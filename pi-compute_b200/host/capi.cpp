@@ -104,6 +104,38 @@ int pib_bs(unsigned long a, unsigned long b, int mode, size_t threshold, int dev
     }
 }
 
+int pib_mul(const uint64_t* a, size_t na, int sa, const uint64_t* b, size_t nb, int sb, size_t threshold, int device,
+            uint64_t* out, size_t out_cap, size_t* out_len, int* out_sign) {
+    try {
+        if ((na && !a) || (nb && !b) || !out || !out_len || !out_sign) throw std::invalid_argument("null argument");
+        pi::B200Multiplier m(threshold, device);
+        mpz_t x, y, r;
+        mpz_init(x);
+        mpz_init(y);
+        mpz_init(r);
+        if (na) mpz_import(x, na, -1, sizeof(uint64_t), 0, 0, a);
+        if (nb) mpz_import(y, nb, -1, sizeof(uint64_t), 0, 0, b);
+        if (sa < 0) mpz_neg(x, x);
+        if (sb < 0) mpz_neg(y, y);
+        try {
+            m.multiply(r, x, y);
+            export_signed(r, out, out_cap, out_len, out_sign);
+        } catch (...) {
+            mpz_clear(x);
+            mpz_clear(y);
+            mpz_clear(r);
+            throw;
+        }
+        mpz_clear(x);
+        mpz_clear(y);
+        mpz_clear(r);
+        return 0;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 1;
+    }
+}
+
 const char* pib_last_error(void) { return g_err.c_str(); }
 
 }  // extern "C"

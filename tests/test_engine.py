@@ -28,8 +28,25 @@ def lib():
     L.pib_bs.argtypes = [ctypes.c_ulong, ctypes.c_ulong, ctypes.c_int, ctypes.c_size_t, ctypes.c_int, P, P, P,
                          ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
     L.pib_bs.restype = ctypes.c_int
+    L.pib_mul.argtypes = [P, ctypes.c_size_t, ctypes.c_int, P, ctypes.c_size_t, ctypes.c_int, ctypes.c_size_t,
+                          ctypes.c_int, P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t),
+                          ctypes.POINTER(ctypes.c_int)]
+    L.pib_mul.restype = ctypes.c_int
     L.pib_last_error.restype = ctypes.c_char_p
     return L
+
+
+def drop_in_mul(lib, a, sa, b, sb, threshold=1):
+    """a * b through pib_mul (pi::B200Multiplier::multiply on mpz_t); returns (limbs, sign)."""
+    P = ctypes.POINTER(ctypes.c_uint64)
+    cap = len(a) + len(b) + 1
+    out = np.zeros(cap, dtype=np.uint64)
+    n = ctypes.c_size_t()
+    sg = ctypes.c_int()
+    st = lib.pib_mul(a.ctypes.data_as(P), len(a), sa, b.ctypes.data_as(P), len(b), sb, threshold, 0,
+                     out.ctypes.data_as(P), cap, ctypes.byref(n), ctypes.byref(sg))
+    assert st == 0, lib.pib_last_error()
+    return out[: n.value], sg.value
 
 
 def pi_digits(lib, digits, mode, threshold=1024, threads=1):
@@ -207,3 +224,27 @@ def test_newton_finish_1m_cpu_hash(lib):
     s, _ = pi_digits(lib, 1_000_000, GMP_NEWTON, threads=8)
     g = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
     assert hashlib.sha256(s.encode()).hexdigest() == g["sha256"]
+
+
+@pytest.mark.gpu
+def test_drop_in_multiply_signs_and_routing(lib):
+    a, b = pkg.random_operand(5000, 11), pkg.random_operand(4000, 12)
+    for sa, sb in ((1, 1), (-1, 1), (1, -1), (-1, -1)):
+        got, sg = drop_in_mul(lib, a, sa, b, sb)
+        assert sg == sa * sb and np.array_equal(got, oracle.mul_gmp(a, b))
+    got, sg = drop_in_mul(lib, a, 1, b, 1, threshold=10_000)  # routed to GMP below the threshold
+    assert np.array_equal(got, oracle.mul_gmp(a, b))
+
+
+@pytest.mark.gpu
+def test_drop_in_multiply_beyond_one_transform(lib):
+    """Products longer than pg_mul_max_limbs go through block products of pg_mul calls."""
+    n = (1 << 25) - 5
+    a, b = pkg.random_operand(n, 21), pkg.random_operand(12, 22)
+    got, _ = drop_in_mul(lib, a, 1, b, 1)
+    assert np.array_equal(got, oracle.mul_gmp(a, b))
+    c = pkg.random_operand((1 << 24) + 3, 23)  # two blocks per operand: checked modulo three primes
+    got, _ = drop_in_mul(lib, c, 1, c, 1)
+    C, G = pkg.limbs_to_int(c), pkg.limbs_to_int(got)
+    for q in (2**61 - 1, 1000000007, 998244353):
+        assert (C % q) * (C % q) % q == G % q
