@@ -295,43 +295,6 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
     }
 }
 
-// Pointwise combination for every merge of an NTT level: operands at base + (6m + o) * stride
-// (o = Pl Ql Rl Pr Qr Rr); writes P^ -> slot 3, Q^ -> slot 4, R^ -> slot 5.
-__global__ void bs_combine_kernel(uint32_t* base, uint64_t stride, uint64_t L, uint64_t merges, uint64_t a0,
-                                  uint64_t b0, int depth) {
-    const uint64_t m = blockIdx.y + (uint64_t)blockIdx.z * 65535;
-    if (m >= merges) return;
-    uint64_t a, b;
-    node_range(a0, b0, depth, m, a, b);
-    const int sgn = merge_r_sign(a, b);
-    uint32_t* g = base + 6 * m * stride;
-    for (uint64_t e = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; e < 3 * L;
-         e += (uint64_t)gridDim.x * blockDim.x * 4) {
-        const int j = (int)(e / L);
-        const uint32_t p = kPrime(j), pinv = inv_mod_2_32(p);
-        const uint4 pl = *reinterpret_cast<const uint4*>(g + 0 * stride + e);
-        const uint4 ql = *reinterpret_cast<const uint4*>(g + 1 * stride + e);
-        const uint4 rl = *reinterpret_cast<const uint4*>(g + 2 * stride + e);
-        const uint4 pr = *reinterpret_cast<const uint4*>(g + 3 * stride + e);
-        const uint4 qr = *reinterpret_cast<const uint4*>(g + 4 * stride + e);
-        const uint4 rr = *reinterpret_cast<const uint4*>(g + 5 * stride + e);
-        uint4 P, Q, R;
-#define PG_COMB(f)                                                             \
-    P.f = mul_mont(pl.f, pr.f, p, pinv);                                       \
-    Q.f = mul_mont(ql.f, qr.f, p, pinv);                                       \
-    {                                                                          \
-        const uint32_t u = mul_mont(qr.f, rl.f, p, pinv);                      \
-        const uint32_t v = mul_mont(pl.f, rr.f, p, pinv);                      \
-        R.f = sgn > 0 ? add_mod(u, v, p) : sub_mod(u, v, p);                   \
-    }
-        PG_COMB(x) PG_COMB(y) PG_COMB(z) PG_COMB(w)
-#undef PG_COMB
-        *reinterpret_cast<uint4*>(g + 3 * stride + e) = P;
-        *reinterpret_cast<uint4*>(g + 4 * stride + e) = Q;
-        *reinterpret_cast<uint4*>(g + 5 * stride + e) = R;
-    }
-}
-
 // ------------------------------------------------------------------ host side
 namespace {
 
@@ -662,20 +625,12 @@ struct DeviceBS {
             if (e != cudaSuccess) return e;
             if (launches) ++*launches;
         }
-        // pointwise combination
-        {
-            const uint64_t per = std::max<uint64_t>(1, std::min<uint64_t>((3 * L / 4 + 255) / 256, 64));
-            dim3 grid((unsigned)per, (unsigned)std::min<uint64_t>(M, 65535), (unsigned)((M + 65534) / 65535));
-            bs_combine_kernel<<<grid, 256, 0, st>>>(res, stride, L, M, a0, b0, depth);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return e;
-            if (launches) ++*launches;
-        }
-        // inverse transforms of the 3M outputs (slots 3..5 of every merge): as a batch of
-        // 2M jobs of stride 3*stride starting at slot 3 would skip slots; run them as 6M jobs
-        // over the whole workspace instead would transform inputs too. Use jobs with stride
-        // `stride` over slots [3, 6) of each merge: three launches of M jobs each.
-        for (int k = 0; k < 3; ++k) {
+        // inverse transforms of the 3M outputs, written over operand slots 3..5 of every merge (jobs
+        // of stride 6*stride, three launches of M jobs per pass). The first inverse pass (the
+        // contiguous one) forms its tiles from the operands on load: P^ = Pl Pr, R^ = Qr Rl +- Pl Rr,
+        // Q^ = Ql Qr, in that order, since R^ still reads Qr (slot 4) after P^ overwrote Pr (slot 3)
+        // and Q^ overwrites Qr last (no separate pointwise kernel and no pass over the products).
+        for (int k : {0, 2, 1}) {
             PassParams q{};
             q.data = res + (3 + k) * stride;
             q.out = q.data;
@@ -684,9 +639,15 @@ struct DeviceBS {
             q.job_stride = 6 * stride;
             q.njobs = (uint32_t)M;
             q.merge = 0;
+            q.comb_k = k;
+            q.comb_slot = stride;
+            q.comb_a0 = a0;
+            q.comb_b0 = b0;
+            q.comb_depth = depth;
             for (int i = plan.npass - 1; i >= 0; --i) {
                 set_pass(q, plan, i);
-                e = launch_pass(plan, i, true, Source::Residues, Fuse::None, q, T->tw, st);
+                e = launch_pass(plan, i, true, Source::Residues, i == plan.npass - 1 ? Fuse::Combine : Fuse::None, q,
+                                T->tw, st);
                 if (e != cudaSuccess) return e;
                 if (launches) ++*launches;
             }

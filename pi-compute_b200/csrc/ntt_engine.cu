@@ -179,6 +179,8 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cuda
 
 #define PG_CONTIG_CASE(N)                                                                                    \
     case N:                                                                                                  \
+        if (inverse && fuse == Fuse::Combine)                                                                \
+            return run_pass<Layout::Contig, N, true, Source::Residues, Fuse::Combine>(prm, tw, st);          \
         if (inverse) return run_pass<Layout::Contig, N, true, Source::Residues, Fuse::None>(prm, tw, st);   \
         if (src == Source::Limbs) {                                                                          \
             if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::None>(prm, tw, st); \
@@ -206,7 +208,8 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
         if (!prm.rowB) return cudaErrorInvalidValue;  // no four-step table for this split
     }
     if (contig) {
-        if (inverse && (src != Source::Residues || fuse != Fuse::None)) return cudaErrorInvalidValue;
+        if (inverse && (src != Source::Residues || (fuse != Fuse::None && fuse != Fuse::Combine)))
+            return cudaErrorInvalidValue;
         switch (logN) {
             PG_CONTIG_CASE(6)
             PG_CONTIG_CASE(7)

@@ -25,6 +25,7 @@
 #include <cstdint>
 
 #include "modarith.cuh"
+#include "series.cuh"
 #include "types.cuh"
 
 namespace pg {
@@ -333,6 +334,11 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         if constexpr (INV) __syncthreads();  // used by the load loop below
     }
 
+    // A strided tile belongs to one job: its source words are looked up once, not per element.
+    const uint32_t* swords = nullptr;
+    uint64_t sncoef = 0;
+    if constexpr (SRC == Source::Limbs && LAY == Layout::Strided) job_source(P, sjob, swords, sncoef);
+
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
     for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
         uint32_t m, c;
@@ -355,9 +361,9 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         }
         uint4 x;
         if constexpr (SRC == Source::Limbs) {
-            const uint32_t* words;
-            uint64_t ncoef;
-            job_source(P, job, words, ncoef);
+            const uint32_t* words = swords;
+            uint64_t ncoef = sncoef;
+            if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
             const uint32_t one_p = (uint32_t)(0x100000000ull / p);
             uint32_t w[4];
             if (g + 4 <= ncoef) {
@@ -369,6 +375,28 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
             }
             x = make_uint4(reduce_u32(w[0], p, one_p), reduce_u32(w[1], p, one_p), reduce_u32(w[2], p, one_p),
                            reduce_u32(w[3], p, one_p));
+        } else if constexpr (FUSE == Fuse::Combine) {
+            // the merge's products in the transform domain (Montgomery: the 2^-32 is in the CRT scale)
+            const uint32_t* slot0 =
+                P.data + job * P.job_stride + prime_off + g - (uint64_t)(3 + P.comb_k) * P.comb_slot;
+            auto at = [&](int o) { return *reinterpret_cast<const uint4*>(slot0 + (uint64_t)o * P.comb_slot); };
+            if (P.comb_k == 2) {
+                uint64_t a, b;
+                node_range(P.comb_a0, P.comb_b0, P.comb_depth, job, a, b);
+                const int sgn = merge_r_sign(a, b);
+                const uint4 pl = at(0), rl = at(2), qr = at(4), rr = at(5);
+                uint32_t u, v;
+#define PG_RCOMB(f)                                         \
+    u = mul_mont(qr.f, rl.f, p, pinv);                      \
+    v = mul_mont(pl.f, rr.f, p, pinv);                      \
+    x.f = sgn > 0 ? add_mod(u, v, p) : sub_mod(u, v, p);
+                PG_RCOMB(x) PG_RCOMB(y) PG_RCOMB(z) PG_RCOMB(w)
+#undef PG_RCOMB
+            } else {
+                const uint4 l = at(P.comb_k), r = at(P.comb_k + 3);  // Pl Pr or Ql Qr
+                x = make_uint4(mul_mont(l.x, r.x, p, pinv), mul_mont(l.y, r.y, p, pinv), mul_mont(l.z, r.z, p, pinv),
+                               mul_mont(l.w, r.w, p, pinv));
+            }
         } else {
             x = *reinterpret_cast<const uint4*>(P.data + job * P.job_stride + prime_off + g);
         }
@@ -380,7 +408,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
     }
     __syncthreads();
 
-    if constexpr (FUSE == Fuse::None) {
+    if constexpr (FUSE == Fuse::None || FUSE == Fuse::Combine) {
         tile_transform<LAY, LOGN, LOGE, NTHREADS, INV>(sm, T.stage[dir][j], p);
     } else {
         // Forward rounds but the last; then, per 16-word group, the last forward round (stride 1),

@@ -58,7 +58,9 @@ inline const uint2* row_table(const TwiddleTables& T, int logNp, int logN, int d
 
 enum class Layout : int { Strided = 0, Contig = 1 };
 enum class Source : int { Residues = 0, Limbs = 1 };
-enum class Fuse : int { None = 0, MulInverse = 1, SqrInverse = 2 };
+// Combine (inverse contiguous pass of a binary-splitting level only): the tile is formed on load
+// from the merge's forward-transformed operands, P^ = Pl Pr, Q^ = Ql Qr or R^ = Qr Rl +- Pl Rr.
+enum class Fuse : int { None = 0, MulInverse = 1, SqrInverse = 2, Combine = 3 };
 
 // Table-driven batch (merge == 2): operand j of a pass launch comes from src[j], CRT job j
 // writes dst[j].
@@ -108,6 +110,12 @@ struct PassParams {
     MergeSrc ms;
     const SrcEntry* src;
     const uint2* rowB;       // strided passes: four-step factor table of prime 0 (set by launch_pass)
+    // Fuse::Combine: output k (0 P^, 1 Q^, 2 R^) of merge `job`, written over operand slot 3 + k;
+    // operand o (Pl Ql Rl Pr Qr Rr) of that merge lies (o - 3 - k) * comb_slot words from it
+    int comb_k;
+    uint64_t comb_slot;
+    uint64_t comb_a0, comb_b0;  // the splitting's range and this level's depth (R's sign per merge)
+    int comb_depth;
 };
 
 struct CrtConsts {
