@@ -135,6 +135,14 @@ __device__ __forceinline__ void dit_round(uint32_t (&v)[1 << LR], uint32_t tp, i
 // Every pattern above touches each bank once per 128 bytes moved.
 __device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ ((((x >> 5) ^ ((x >> 8) << 2)) & 7u) << 2); }
 
+// 16-byte asynchronous copy global -> shared (no register staging, so every copy of a thread is in
+// flight at once); both addresses 16-byte aligned.
+__device__ __forceinline__ void cp_async16(uint32_t* smem, const uint32_t* gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // Shared-memory address of tile element (m, c).
 template <Layout LAY, int LOGN, int LOGE>
 __device__ __forceinline__ uint32_t sidx(uint32_t m, uint32_t c) {
@@ -359,52 +367,65 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
             job = R >> logRows;
             g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);
         }
-        uint4 x;
-        if constexpr (SRC == Source::Limbs) {
-            const uint32_t* words = swords;
-            uint64_t ncoef = sncoef;
-            if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
-            const uint32_t one_p = (uint32_t)(0x100000000ull / p);
-            uint32_t w[4];
-            if (g + 4 <= ncoef) {
-                uint4 raw = __ldg(reinterpret_cast<const uint4*>(words + g));
-                w[0] = raw.x; w[1] = raw.y; w[2] = raw.z; w[3] = raw.w;
-            } else {
+        if constexpr (SRC == Source::Residues && FUSE != Fuse::Combine) {
+            // residues: an asynchronous copy straight into shared memory (the inverse strided
+            // twiddle, if any, is applied below once the copies have landed)
+            cp_async16(sm + swz(e4), P.data + job * P.job_stride + prime_off + g);
+        } else {
+            uint4 x;
+            if constexpr (SRC == Source::Limbs) {
+                const uint32_t* words = swords;
+                uint64_t ncoef = sncoef;
+                if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
+                const uint32_t one_p = (uint32_t)(0x100000000ull / p);
+                uint32_t w[4];
+                if (g + 4 <= ncoef) {
+                    uint4 raw = __ldg(reinterpret_cast<const uint4*>(words + g));
+                    w[0] = raw.x; w[1] = raw.y; w[2] = raw.z; w[3] = raw.w;
+                } else {
 #pragma unroll
-                for (int u = 0; u < 4; ++u) w[u] = (g + u < ncoef) ? __ldg(words + g + u) : 0u;
-            }
-            x = make_uint4(reduce_u32(w[0], p, one_p), reduce_u32(w[1], p, one_p), reduce_u32(w[2], p, one_p),
-                           reduce_u32(w[3], p, one_p));
-        } else if constexpr (FUSE == Fuse::Combine) {
-            // the merge's products in the transform domain (Montgomery: the 2^-32 is in the CRT scale)
-            const uint32_t* slot0 =
-                P.data + job * P.job_stride + prime_off + g - (uint64_t)(3 + P.comb_k) * P.comb_slot;
-            auto at = [&](int o) { return *reinterpret_cast<const uint4*>(slot0 + (uint64_t)o * P.comb_slot); };
-            if (P.comb_k == 2) {
-                uint64_t a, b;
-                node_range(P.comb_a0, P.comb_b0, P.comb_depth, job, a, b);
-                const int sgn = merge_r_sign(a, b);
-                const uint4 pl = at(0), rl = at(2), qr = at(4), rr = at(5);
-                uint32_t u, v;
+                    for (int u = 0; u < 4; ++u) w[u] = (g + u < ncoef) ? __ldg(words + g + u) : 0u;
+                }
+                x = make_uint4(reduce_u32(w[0], p, one_p), reduce_u32(w[1], p, one_p), reduce_u32(w[2], p, one_p),
+                               reduce_u32(w[3], p, one_p));
+            } else if constexpr (FUSE == Fuse::Combine) {
+                // the merge's products in the transform domain (Montgomery: the 2^-32 is in the CRT scale)
+                const uint32_t* slot0 =
+                    P.data + job * P.job_stride + prime_off + g - (uint64_t)(3 + P.comb_k) * P.comb_slot;
+                auto at = [&](int o) { return *reinterpret_cast<const uint4*>(slot0 + (uint64_t)o * P.comb_slot); };
+                if (P.comb_k == 2) {
+                    uint64_t a, b;
+                    node_range(P.comb_a0, P.comb_b0, P.comb_depth, job, a, b);
+                    const int sgn = merge_r_sign(a, b);
+                    const uint4 pl = at(0), rl = at(2), qr = at(4), rr = at(5);
+                    uint32_t u, v;
 #define PG_RCOMB(f)                                         \
     u = mul_mont(qr.f, rl.f, p, pinv);                      \
     v = mul_mont(pl.f, rr.f, p, pinv);                      \
     x.f = sgn > 0 ? add_mod(u, v, p) : sub_mod(u, v, p);
-                PG_RCOMB(x) PG_RCOMB(y) PG_RCOMB(z) PG_RCOMB(w)
+                    PG_RCOMB(x) PG_RCOMB(y) PG_RCOMB(z) PG_RCOMB(w)
 #undef PG_RCOMB
-            } else {
-                const uint4 l = at(P.comb_k), r = at(P.comb_k + 3);  // Pl Pr or Ql Qr
-                x = make_uint4(mul_mont(l.x, r.x, p, pinv), mul_mont(l.y, r.y, p, pinv), mul_mont(l.z, r.z, p, pinv),
-                               mul_mont(l.w, r.w, p, pinv));
+                } else {
+                    const uint4 l = at(P.comb_k), r = at(P.comb_k + 3);  // Pl Pr or Ql Qr
+                    x = make_uint4(mul_mont(l.x, r.x, p, pinv), mul_mont(l.y, r.y, p, pinv), mul_mont(l.z, r.z, p, pinv),
+                                   mul_mont(l.w, r.w, p, pinv));
+                }
             }
-        } else {
-            x = *reinterpret_cast<const uint4*>(P.data + job * P.job_stride + prime_off + g);
+            *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
         }
+    }
+    if constexpr (SRC == Source::Residues && FUSE != Fuse::Combine) {
+        cp_async_wait_all();  // this thread's copies (the barrier below publishes them to the block)
         if constexpr (INV && LAY == Layout::Strided) {
-            // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m))
-            fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
+            // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m)), on the
+            // same elements this thread copied
+            for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
+                const uint32_t m = e4 >> LOGC, c = e4 & ((1u << LOGC) - 1);
+                uint4 x = *reinterpret_cast<uint4*>(sm + swz(e4));
+                fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
+                *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
+            }
         }
-        *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
     }
     __syncthreads();
 
