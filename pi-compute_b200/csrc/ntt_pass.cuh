@@ -371,24 +371,23 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
             // residues: an asynchronous copy straight into shared memory (the inverse strided
             // twiddle, if any, is applied below once the copies have landed)
             cp_async16(sm + swz(e4), P.data + job * P.job_stride + prime_off + g);
+        } else if constexpr (SRC == Source::Limbs) {
+            // operand words: whole 16-byte groups copied asynchronously, the ragged end (and the
+            // zero padding) written directly; reduced modulo p below once landed
+            const uint32_t* words = swords;
+            uint64_t ncoef = sncoef;
+            if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
+            if (g + 4 <= ncoef) {
+                cp_async16(sm + swz(e4), words + g);
+            } else {
+                uint32_t w[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) w[u] = (g + u < ncoef) ? __ldg(words + g + u) : 0u;
+                *reinterpret_cast<uint4*>(sm + swz(e4)) = make_uint4(w[0], w[1], w[2], w[3]);
+            }
         } else {
             uint4 x;
-            if constexpr (SRC == Source::Limbs) {
-                const uint32_t* words = swords;
-                uint64_t ncoef = sncoef;
-                if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
-                const uint32_t one_p = (uint32_t)(0x100000000ull / p);
-                uint32_t w[4];
-                if (g + 4 <= ncoef) {
-                    uint4 raw = __ldg(reinterpret_cast<const uint4*>(words + g));
-                    w[0] = raw.x; w[1] = raw.y; w[2] = raw.z; w[3] = raw.w;
-                } else {
-#pragma unroll
-                    for (int u = 0; u < 4; ++u) w[u] = (g + u < ncoef) ? __ldg(words + g + u) : 0u;
-                }
-                x = make_uint4(reduce_u32(w[0], p, one_p), reduce_u32(w[1], p, one_p), reduce_u32(w[2], p, one_p),
-                               reduce_u32(w[3], p, one_p));
-            } else if constexpr (FUSE == Fuse::Combine) {
+            if constexpr (FUSE == Fuse::Combine) {
                 // the merge's products in the transform domain (Montgomery: the 2^-32 is in the CRT scale)
                 const uint32_t* slot0 =
                     P.data + job * P.job_stride + prime_off + g - (uint64_t)(3 + P.comb_k) * P.comb_slot;
@@ -412,6 +411,16 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
                 }
             }
             *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
+        }
+    }
+    if constexpr (SRC == Source::Limbs) {
+        cp_async_wait_all();  // this thread's copies; each word of its elements reduced modulo p
+        const uint32_t one_p = (uint32_t)(0x100000000ull / p);
+        for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
+            uint4 w = *reinterpret_cast<uint4*>(sm + swz(e4));
+            w = make_uint4(reduce_u32(w.x, p, one_p), reduce_u32(w.y, p, one_p), reduce_u32(w.z, p, one_p),
+                           reduce_u32(w.w, p, one_p));
+            *reinterpret_cast<uint4*>(sm + swz(e4)) = w;
         }
     }
     if constexpr (SRC == Source::Residues && FUSE != Fuse::Combine) {
