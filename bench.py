@@ -21,7 +21,7 @@ fixed algorithmic bytes B_mul = 400 * (na + nb) and the measured HBM copy bandwi
 from its sources) on every host core, bounded sample: pi to 10M digits. `--impl reference`
 runs that program at the full D digits once (about a minute on 16 cores) and reports digits/s.
 
-Multi-GPU (torchrun): each rank computes pi independently (replicas only: the north star is
+Multi-GPU (torchrun): each rank computes pi independently (replicas only: the computation runs on
 one GPU and the path has no exchange step); value = total digits / max rank time.
 """
 from __future__ import annotations
@@ -41,6 +41,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 METRIC = "pi digits/s at 100M (batched vs per-call GPU, bit-exact); mul GB/s vs HBM"
+PIB_MODE_PER_CALL = 1
 PIB_MODE_BATCHED = 2
 PI_COMPUTE_REF = os.path.join(ROOT, "oracle", "_ref", "pi_compute_ref")
 
@@ -266,11 +267,14 @@ def run_b200(args):
     lib.pib_last_error.restype = ctypes.c_char_p
     D = args.digits
     threads = os.cpu_count() or 1
+    # batched: the device pipeline (pg_pi); per-call: the reference's BinarySplitting and mpf finish
+    # with every product of at least --threshold limbs sent to the B200 one call at a time
+    mode = PIB_MODE_PER_CALL if args.mode == "per-call" else PIB_MODE_BATCHED
     buf = ctypes.create_string_buffer(D + 2)
     stats = (ctypes.c_double * 8)()
 
     def step():
-        st = lib.pib_pi(D, PIB_MODE_BATCHED, threads, args.threshold, local, buf, D + 2, stats)
+        st = lib.pib_pi(D, mode, threads, args.threshold, local, buf, D + 2, stats)
         if st != 0:
             raise RuntimeError(lib.pib_last_error().decode())
         return list(stats)
@@ -313,13 +317,14 @@ def run_b200(args):
         # end to end through the command-line program, like the reference's pi_compute
         e2e = None
         if not args.no_e2e:
-            # three fresh processes (CUDA start-up dominates and varies from run to run): the median
+            # five fresh processes (CUDA start-up dominates and varies from run to run): the median
             runs, sha = [], None
             with tempfile.TemporaryDirectory() as td:
                 out = os.path.join(td, "pi.txt")
-                for _ in range(3):
+                for _ in range(5):
                     t0 = time.perf_counter()
-                    subprocess.run([pkg.PI_B200_BIN, "--batched", "--digits", str(D), "--threads", str(threads),
+                    flags = ["--batched"] if mode == PIB_MODE_BATCHED else ["--gpu", "--gpu-threshold", str(args.threshold)]
+                    subprocess.run([pkg.PI_B200_BIN, *flags, "--digits", str(D), "--threads", str(threads),
                                     "--device", str(local), "--output", out], check=True, stdout=subprocess.DEVNULL)
                     runs.append(time.perf_counter() - t0)
                     got_sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
@@ -328,15 +333,19 @@ def run_b200(args):
             e2e = {"value": round(D / e2e_s, 1), "unit": "digits/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": D + 2, "seconds": round(e2e_s, 3),
                    "runs_s": [round(x, 3) for x in runs],
-                   "path": "pi_b200 --batched (process start, CUDA context, output file)",
+                   "path": ("pi_b200 --batched" if mode == PIB_MODE_BATCHED else "pi_b200 --gpu")
+                           + " (process start, CUDA context, output file)",
                    "sha256_matches_reference": (sha == want) if want else None}
         ph = np.mean(np.array(phases), axis=0)
         line = {
             "metric": METRIC, "value": round(value, 1), "unit": "digits/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * total / args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32 mod p (NTT), u64 limbs", "data": "none (pi)",
-            "config": {"workload": f"pi to {D:,} digits: level-batched device binary splitting + Newton finish "
-                                   f"+ D&C decimal conversion on B200 products",
+            "config": {"workload": (f"pi to {D:,} digits: level-batched device binary splitting + Newton finish "
+                                    f"+ D&C decimal conversion on B200 products") if mode == PIB_MODE_BATCHED else
+                                   (f"pi to {D:,} digits: the reference's splitting and mpf finish, every product of "
+                                    f">= {args.threshold} limbs on the B200 one call at a time (per-call drop-in)"),
+                       "mode": args.mode,
                        "digits": D, "terms": None, "parallelism": f"replicas x{world}",
                        "l2": "every product of the top tree levels moves GBs through HBM (far above the 126 MB L2)",
                        "phases_s": {"binary_splitting": round(ph[0], 3), "final_formula": round(ph[1], 3),
@@ -569,6 +578,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="pi", choices=["pi", "mul", "batch", "sweep"])
+    ap.add_argument("--mode", default="batched", choices=["batched", "per-call"],
+                    help="pi workload: device pipeline (default) or the per-call drop-in multiplier")
     ap.add_argument("--trials", type=int, default=5, help="timed runs per size and shape (sweep)")
     ap.add_argument("--batch-jobs", type=int, default=4096)
     args = ap.parse_args()
