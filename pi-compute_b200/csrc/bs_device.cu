@@ -710,6 +710,33 @@ struct DeviceBS {
             dp[0].kind = 0;
             D = 1;
         }
+        // Every buffer at its largest size for this range before the first launch: growing them
+        // depth by depth would free and reallocate (each cudaFree waits for the device) up to the
+        // root on a range's first run.
+        {
+            uint64_t lev_need[2][3] = {{0}}, len_need[2] = {0, 0}, res_need = 0, sync_need = 0;
+            for (int d = D - 1; d >= 0; --d) {
+                const DepthPlan& P = dp[d];
+                const int s = (D - 1 - d) & 1;
+                for (int k = 0; k < 3; ++k) lev_need[s][k] = std::max<uint64_t>(lev_need[s][k], P.nodes * P.cap[k] * 8);
+                len_need[s] = std::max<uint64_t>(len_need[s], P.nodes * 3 * 4);
+                if (P.kind == 2) {
+                    const uint64_t L = 1ull << P.logL, M = P.nodes;
+                    res_need = std::max<uint64_t>(res_need, 6 * M * 3 * L * 4);
+                    const uint64_t maxw = 2ull * std::max({P.cap[0], P.cap[1], P.cap[2]});
+                    const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+                    sync_need = std::max<uint64_t>(sync_need, (3 * M + 3 * M * bpj) * 4);
+                }
+            }
+            for (int s = 0; s < 2; ++s) {
+                for (int k = 0; k < 3; ++k)
+                    if (lev_need[s][k] && (e = grow((void**)&lev[s][k], lev_cap[s][k], lev_need[s][k])) != cudaSuccess)
+                        return e;
+                if (len_need[s] && (e = grow((void**)&lev_len[s], lev_len_cap[s], len_need[s])) != cudaSuccess) return e;
+            }
+            if (res_need && (e = grow((void**)&res, res_cap, res_need)) != cudaSuccess) return e;
+            if (sync_need && (e = grow((void**)&sync, sync_cap, sync_need)) != cudaSuccess) return e;
+        }
         auto view = [&](int slot, const DepthPlan& P) {
             LevelView v;
             for (int k = 0; k < 3; ++k) {
