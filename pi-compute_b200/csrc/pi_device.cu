@@ -308,7 +308,11 @@ void residue_diff(DevArith& A, DevNum& e, size_t p, const DevNum& xm, int logL) 
     centre(A, e, logL);
 }
 
-void recip_floor(DevArith& A, DevNum& Z, const DevNum& R) {
+// Z = floor(2^(2k) / R), k = bits(R). With exact == false the top step's correction is skipped:
+// then |Z - 2^(2k)/R| < 2. The ideal Newton update Z0 + Z0 E / 2^(2k) has error eps^2 / z* with
+// eps = z* - Z0, |eps| <= 2^(k-h+2) and z* = 2^(2k)/R > 2^k, i.e. below 2^(k - 2h + 4) = 2^-60;
+// dropping E's low bits costs < 1/2 and the floor < 1 (the lower levels stay exact).
+void recip_floor(DevArith& A, DevNum& Z, const DevNum& R, bool exact = true) {
     const size_t k = A.bits(R);
     if (k == 0 || R.sign < 0) throw DevError(PG_ERR_BAD_ARG, "recip_floor: R must be positive");
     if (k <= 64) {
@@ -346,6 +350,7 @@ void recip_floor(DevArith& A, DevNum& Z, const DevNum& R) {
     A.mul(D, Zh, T);
     A.fdiv_q_2exp(D, D, k + h - s);
     A.add(Z, Z0, D);
+    if (!exact) return;
     A.mul(T, R, D);
     A.sub(E, E, T);                 // E = 2^(2k) - R Z
     int steps = 0;
@@ -397,13 +402,16 @@ void rsqrt_approx(DevArith& A, DevNum& u, uint64_t a, size_t q) {
     A.add(u, u0, D);
 }
 
-// S = floor(sqrt(a) 2^s), exactly.
-void sqrt_scaled(DevArith& A, DevNum& S, uint64_t a, size_t s) {
+// S = floor(sqrt(a) 2^s), exactly; with exact == false |S - sqrt(a) 2^s| < 2 (u is within a few
+// units of 2^q / sqrt(a), so a u / 2^(q-s) is within a few a / 2^64 units of sqrt(a) 2^s, plus the
+// floor) and the square check is skipped.
+void sqrt_scaled(DevArith& A, DevNum& S, uint64_t a, size_t s, bool exact = true) {
     const size_t q = s + 64;
     Num u(A), N(A), V(A), t(A);
     rsqrt_approx(A, u, a, q);
     A.mul_ui(S, u, a);              // a 2^q / sqrt(a)
     A.tdiv_q_2exp(S, S, q - s);
+    if (!exact) return;
     // V = N - S^2 with N = a 2^(2s); S is within a few units of sqrt(N), so |V| is about
     // 2 S c < 2^(s + 40) for a < 2^64: S^2 modulo 2^(32 L) - 1 is enough
     const int lw = wrap_logL(s + 40, S.n, S.n);
@@ -463,11 +471,11 @@ void final_formula(DevArith& A, DevNum& pi_int, const DevNum& Q, const DevNum& R
         if (eR >= 0) A.tdiv_q_2exp(Rt, R, (size_t)eR); else A.shl(Rt, R, (size_t)-eR);
         {
             Timer tm("reciprocal of R");
-            recip_floor(A, Z, Rt);      // 2^(2k) / Rt
+            recip_floor(A, Z, Rt, false);  // 2^(2k) / Rt within 2 units
         }
         {
             Timer tm("sqrt(10005)");
-            sqrt_scaled(A, S, 10005, k);
+            sqrt_scaled(A, S, 10005, k, false);  // within 2 units
         }
         {
             Timer tm("5^digits");
@@ -491,9 +499,11 @@ void final_formula(DevArith& A, DevNum& pi_int, const DevNum& Q, const DevNum& R
         mul_trunc(F);
         if (e >= -160) throw DevError(PG_ERR_INTERNAL, "final formula: not enough fraction bits");
         const size_t fb = (size_t)(-e);
-        // Relative error < 8 * 2^-(k-1) and pi 10^d < 2^(P - guard): absolute error below
-        // 2^-(guard + 60); the floor is certain unless the fraction is within 2^-100 of an
-        // integer. fr = X mod 2^fb; top = fr >> (fb - 100) (100 bits), low = fr mod 2^(fb-100).
+        // Z and S are within 2 units of their exact values (>= 2^(k-1)), the truncations of Qt,
+        // Rt and the three products within 1 unit each: relative error < 16 * 2^-(k-1), and
+        // pi 10^d < 2^(P - guard), so the absolute error is below 2^-(guard + 59); the floor is
+        // certain unless the fraction is within 2^-100 of an integer (guard >= 128).
+        // fr = X mod 2^fb; top = fr >> (fb - 100) (100 bits), low = fr mod 2^(fb-100).
         Num fr(A), top(A), low(A);
         A.tdiv_r_2exp(fr, X, fb);
         A.tdiv_q_2exp(top, fr, fb - 100);
