@@ -313,6 +313,31 @@ def run_b200(args):
     roof = product_roofline(pkg, eng, torch, local, logn=args.logn)
     eng.close()
 
+    # The metric's other half: the same digits with the per-call drop-in (the reference's
+    # BinarySplitting and mpf finish, every product of >= --threshold limbs sent to the B200 one
+    # pi::Multiplier call at a time), once, after the timed batched steps; every rank runs it so the
+    # ranks stay in step.
+    per_call = None
+    if mode == PIB_MODE_BATCHED and not args.no_per_call:
+        t0 = time.perf_counter()
+        st = lib.pib_pi(D, PIB_MODE_PER_CALL, threads, args.threshold, local, buf, D + 2, stats)
+        dt = time.perf_counter() - t0
+        if st != 0:
+            raise RuntimeError(lib.pib_last_error().decode())
+        pc = list(stats)
+        pc_sha = hashlib.sha256(buf.raw[: D + 2]).hexdigest()
+        bs_batched = float(np.mean([p[0] for p in phases]))
+        per_call = {"seconds": round(dt, 3), "value": round(D / dt, 1), "unit": "digits/s",
+                    "threshold_limbs": args.threshold, "host_threads": threads,
+                    "phases_s": {"binary_splitting": round(pc[0], 3), "final_formula": round(pc[1], 3),
+                                 "decimal_conversion": round(pc[2], 3)},
+                    "gpu_products": int(pc[5]), "gmp_products": int(pc[6]), "gpu_launches": int(pc[4]),
+                    "digits_sha256": pc_sha, "matches_reference": (pc_sha == want) if want else None,
+                    "batched_over_per_call": round(dt / (total / args.steps), 2),
+                    "batched_over_per_call_bs": round(pc[0] / bs_batched, 2) if bs_batched > 0 else None,
+                    "how": "pib_pi(PIB_MODE_PER_CALL): the reference's BinarySplitting and mpf finish over "
+                           "pi::B200Multiplier, one run after the timed batched steps, host wall clock"}
+
     if rank == 0:
         # end to end through the command-line program, like the reference's pi_compute
         e2e = None
@@ -354,6 +379,7 @@ def run_b200(args):
                        "step_phases_s": [[round(v, 4) for v in s3[:3]] for s3 in phases],
                        "digits_sha256": got, "matches_reference": (got == want) if want else None},
             "roofline": roof,
+            "per_call": per_call,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
@@ -387,9 +413,10 @@ def run_mul(args):
 
 
 def run_sweep(args):
-    """Workload "sweep": the standalone multiply sweep. Seeded operands (splitmix64, a seed per size,
-    shape and trial) of n = 2^j and 3*2^(j-1) limbs, j = 10..24; balanced a*b, 1:4, 1:16 and
-    squares; every product's first run checked modulo three primes, then `--trials` timed runs
+    """Workload "sweep": the standalone multiply sweep. Seeded operands (splitmix64, a seed per size
+    and shape) of n = 2^j and 3*2^(j-1) limbs, j = 10..24; balanced a*b, 1:4, 1:16 and squares;
+    every product's first run checked (word for word against mpz_mul's sha256 where tests/golden
+    holds the case, 2^24 included; modulo three primes otherwise), then `--trials` timed runs
     (CUDA events on the context's stream, operands in HBM). Reports median ms, GB/s of
     B_mul = 400 (na + nb) / B_sqr = 536 n and the fraction of measured HBM bandwidth; GMP's mpz_mul
     (the reference's GmpMultiplier, one core) beside it up to 2^20 limbs."""
@@ -409,12 +436,19 @@ def run_sweep(args):
         if j < 24:
             sizes.append(3 << (j - 1))
     rows = []
+    # products with a committed mpz_mul hash (tests/golden) use that case's seeds and are compared
+    # word for word; the others are checked modulo three primes
+    golden = {}
+    for fn in ("products.json", "products_top.json"):
+        for c in json.load(open(os.path.join(ROOT, "tests", "golden", fn))):
+            golden[(c["na"], c["nb"])] = c
     launches0 = lib.pg_launch_count(eng.ctx)
     for n in sizes:
         for shape, nb in (("balanced", n), ("1:4", n // 4), ("1:16", n // 16), ("square", 0)):
-            seed = n * 8 + len(rows) % 4
+            g = golden.get((n, nb))
+            seed = g["seed"] if g else n * 8 + len(rows) % 4
             a_h = pkg.random_operand(n, seed)
-            b_h = pkg.random_operand(nb, seed + 1) if nb else a_h
+            b_h = pkg.random_operand(nb, seed + 7) if nb else a_h
             a_d = torch.from_numpy(a_h.view(np.int64)).to(dev)
             b_d = torch.from_numpy(b_h.view(np.int64)).to(dev) if nb else a_d
             m = n + (nb if nb else n)
@@ -431,9 +465,15 @@ def run_sweep(args):
             step()
             if lib.pg_sync(eng.ctx) != 0:
                 raise pkg.PgError(-1, eng.last_error())
-            A, B = pkg.limbs_to_int(a_h), pkg.limbs_to_int(b_h)
-            R = pkg.limbs_to_int(out_d.cpu().numpy().view(np.uint64))
-            ok = all((A % q) * (B % q) % q == R % q for q in (2**61 - 1, 1000000007, 998244353))
+            r_h = out_d.cpu().numpy().view(np.uint64)
+            if g:
+                r_t = r_h[: int(np.max(np.nonzero(r_h)[0])) + 1] if r_h.any() else r_h[:0]
+                ok = len(r_t) == g["len"] and hashlib.sha256(r_t.astype("<u8").tobytes()).hexdigest() == g["sha256"]
+                checked = "sha256 = mpz_mul's (tests/golden)"
+            else:
+                A, B, R = pkg.limbs_to_int(a_h), pkg.limbs_to_int(b_h), pkg.limbs_to_int(r_h)
+                ok = all((A % q) * (B % q) % q == R % q for q in (2**61 - 1, 1000000007, 998244353))
+                checked = "mod 2^61-1, 1e9+7, 998244353"
             if not ok:
                 raise RuntimeError(f"product check failed at n={n} shape={shape}")
             step()
@@ -448,7 +488,7 @@ def run_sweep(args):
             balg = 400 * (n + nb) if nb else 536 * n
             gbs = balg / (ms / 1e3) / 1e9
             rows.append({"na": n, "nb": nb if nb else n, "shape": shape, "ms": round(ms, 4), "gbs": round(gbs, 1),
-                         "frac": round(gbs / peaks["hbm_gbs"], 4), "checked": "mod 2^61-1, 1e9+7, 998244353"})
+                         "frac": round(gbs / peaks["hbm_gbs"], 4), "checked": checked})
             del a_d, b_d, out_d
     launches = lib.pg_launch_count(eng.ctx) - launches0
     eng.close()
@@ -577,6 +617,8 @@ def main():
     ap.add_argument("--logn", type=int, default=24)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-per-call", action="store_true",
+                    help="pi workload: skip the one per-call drop-in run after the timed batched steps")
     ap.add_argument("--workload", default="pi", choices=["pi", "mul", "batch", "sweep"])
     ap.add_argument("--mode", default="batched", choices=["batched", "per-call"],
                     help="pi workload: device pipeline (default) or the per-call drop-in multiplier")

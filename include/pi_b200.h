@@ -248,8 +248,8 @@ pg_status pg_tune_load(pg_ctx* ctx, const char* path);
  * Limit: na + nb <= 16384 limbs; larger products return PG_ERR_TOO_LARGE without touching
  * any memory. Pointers are device addresses on the CURRENT device, 16-byte aligned; d_out
  * receives exactly na + nb limbs and must not overlap d_a or d_b (d_a == d_b is allowed).
- * `stream` is a cudaStream_t (NULL = the legacy default stream); the call returns after the
- * product is complete and reports device-side errors like pg_sync.
+ * `stream` is a cudaStream_t (NULL = the legacy default stream). Every call synchronises that
+ * stream: it returns after the product is complete and reports device-side errors like pg_sync.
  *
  * The first call on a device sets that device up (looks up the arrays and fills the tables,
  * waiting for it); make it before any stream capture. All calls share the same arrays, so

@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "bigint.cuh"
+#include "dev_alloc.h"
 #include "devnum.h"
 
 namespace pg {
@@ -431,7 +432,7 @@ void DevArith::reserve(DevNum& x, size_t limbs) {
         x.d = it->second;
         pool_.erase(it);
     } else {
-        check(cudaMalloc((void**)&x.d, cap * 8), "DevArith allocation");
+        check(pg::dev_malloc((void**)&x.d, cap * 8), "DevArith allocation");
         all_.push_back({x.d, cap});
     }
     x.cap = cap;
@@ -454,7 +455,7 @@ uint64_t* DevArith::scratch(size_t limbs) {
         scratch_ = nullptr;
         scratch_cap_ = 0;
         const size_t cap = std::max(limbs, scratch_cap_ * 3 / 2);
-        check(cudaMalloc((void**)&scratch_, cap * 8), "DevArith scratch");
+        check(pg::dev_malloc((void**)&scratch_, cap * 8), "DevArith scratch");
         scratch_cap_ = cap;
     }
     return scratch_;
@@ -468,7 +469,7 @@ uint32_t* DevArith::flags(size_t n) {
         }
         flags_ = nullptr;
         const size_t cap = std::max<size_t>(n, 1024);
-        check(cudaMalloc((void**)&flags_, cap * 8), "DevArith flags");
+        check(pg::dev_malloc((void**)&flags_, cap * 8), "DevArith flags");
         flags_cap_ = cap;
     }
     return flags_;
@@ -500,7 +501,7 @@ void DevArith::run_add(const AddArgs& a0, int form) {
         }
         seg_ = nullptr;
         const size_t cap = std::max<size_t>(a.njobs * nseg, 4096);
-        check(cudaMalloc((void**)&seg_, cap * 4), "DevArith segments");
+        check(pg::dev_malloc((void**)&seg_, cap * 4), "DevArith segments");
         seg_cap_ = cap;
     }
     a.seg = seg_;

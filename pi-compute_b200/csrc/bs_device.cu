@@ -393,7 +393,7 @@ struct DeviceBS {
         if (*p) cudaFree(*p);
         *p = nullptr;
         cap = 0;
-        cudaError_t e = cudaMalloc(p, need);
+        cudaError_t e = pg::dev_malloc(p, need);
         if (e == cudaSuccess) cap = need;
         return e;
     }

@@ -16,8 +16,9 @@
 // entries of (carry + 1). Functions compose associatively, so a warp scan, a block scan
 // and a decoupled look-back across blocks (single pass, CTA order fixed by an atomic
 // ticket so every predecessor is resident; one warp inspects 32 predecessors per step)
-// give each thread its exact carry in. Every spin in the look-back has an iteration limit;
-// running out sets an error word the host checks, and the kernel finishes without hanging.
+// give each thread its exact carry in. Every spin in the look-back has an iteration limit
+// (kSpinLimit polls, or CrtParams::spin_limit); running out sets an error word the host checks,
+// and the kernel finishes without hanging.
 //
 // One launch can recombine many products (the three outputs of every merge of a
 // binary-splitting level); each has its own ticket and status words.
@@ -259,10 +260,12 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
         // base - l). The window's functions compose into one; the nearest block that already
         // knows its carry out ends the walk. Carries are stored as u = carry + 1.
         uint32_t u_in = 1;
+        const bool publish = bid + 1 != P.withhold1;  // false only under the test hook
+        const uint32_t spin_limit = P.spin_limit ? P.spin_limit : kSpinLimit;
         if (bid == 0) {
-            if (lane == 0) st[0] = kStIncl | (fapply(blk, 1) << 8);
+            if (lane == 0 && publish) st[0] = kStIncl | (fapply(blk, 1) << 8);
         } else {
-            if (lane == 0) {
+            if (lane == 0 && publish) {
                 __threadfence();
                 st[bid] = kStAgg | (blk << 8);
             }
@@ -278,7 +281,7 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
                 const int first = incl_mask ? (__ffs(incl_mask) - 1) : 32;
                 const unsigned upto = (first >= 31) ? 0xffffffffu : ((2u << first) - 1u);
                 if (none_mask & upto) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spin_limit) {
                         if (lane == 0) atomicExch(P.error, 1u);
                         break;
                     }
@@ -301,7 +304,7 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
                 }
                 base -= 32;
             }
-            if (lane == 0) {
+            if (lane == 0 && publish) {
                 __threadfence();
                 st[bid] = kStIncl | (fapply(blk, u_in) << 8);
             }

@@ -83,7 +83,7 @@ cudaError_t DeviceTables::build(int device) {
             for (int j = 0; j < kNumPrimes; ++j) th.emplace_back(fill, dir, j);
         for (auto& t : th) t.join();
     }
-    cudaError_t e = cudaMalloc(&base, h.size() * sizeof(uint2));
+    cudaError_t e = pg::dev_malloc(&base, h.size() * sizeof(uint2));
     if (e != cudaSuccess) return e;
     e = cudaMemcpy(base, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
@@ -106,7 +106,7 @@ void DeviceTables::release() {
 static cudaError_t grow(void** ptr, uint64_t bytes) {
     if (*ptr) cudaFree(*ptr);
     *ptr = nullptr;
-    return cudaMalloc(ptr, bytes);
+    return pg::dev_malloc(ptr, bytes);
 }
 
 cudaError_t Workspace::ensure_res(uint64_t n) {
@@ -236,7 +236,18 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
     }
 }
 
-cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st, uint64_t max_words) {
+// Test hooks of the look-back wait, read on every launch so that a test can set and clear them
+// around one product: PG_TEST_CRT_SPIN_LIMIT=n ends each wait after n polls, and
+// PG_TEST_CRT_WITHHOLD=b keeps the block with ticket b from publishing its carry, so that the
+// next block's wait runs out (PG_ERR_TIMEOUT, no GPU fault). Unset: the built-in limit, no hook.
+static void crt_test_hooks(CrtParams& c) {
+    if (const char* e = std::getenv("PG_TEST_CRT_SPIN_LIMIT")) c.spin_limit = (uint32_t)std::strtoul(e, nullptr, 10);
+    if (const char* e = std::getenv("PG_TEST_CRT_WITHHOLD")) c.withhold1 = (uint32_t)std::strtoul(e, nullptr, 10) + 1;
+}
+
+cudaError_t launch_crt(const CrtParams& c0, uint64_t blocks, cudaStream_t st, uint64_t max_words) {
+    CrtParams c = c0;
+    crt_test_hooks(c);
     if (max_words && max_words <= kCrtWarpWords && c.blocks_per_job == 1) {
         // blocks == jobs here: one warp per job
         crt_warp_kernel<<<(unsigned)((blocks * 32 + 255) / 256), 256, 0, st>>>(c, blocks);

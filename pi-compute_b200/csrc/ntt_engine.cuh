@@ -7,6 +7,7 @@
 #include <mutex>
 #include <string>
 
+#include "dev_alloc.h"
 #include "plan.h"
 #include "types.cuh"
 

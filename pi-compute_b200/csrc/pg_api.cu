@@ -100,8 +100,8 @@ pg_status host_product(pg_ctx* c, const uint64_t* a, size_t na, const uint64_t* 
                        uint64_t* out, size_t out_cap, size_t* out_len) {
     if (!c || !out_len || (na && !a) || (!square && nb && !b)) return fail(c, PG_ERR_BAD_ARG, "null argument");
     if (square) nb = na, b = a;
-    // Reject by buffer length before reading the operands.
-    if (na + nb > pg_mul_max_limbs()) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
+    // Reject by buffer length before reading the operands (each length on its own: no wrap-around).
+    if (na > pg_mul_max_limbs() || nb > pg_mul_max_limbs() - na) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
     na = trimmed(a, na);
     nb = trimmed(b, nb);
     if (na == 0 || nb == 0) {
@@ -255,7 +255,8 @@ pg_status pg_mul_device(pg_ctx* c, const uint64_t* d_a, size_t na, const uint64_
     if (!c || !d_out || (na && !d_a) || (nb && !d_b)) return fail(c, PG_ERR_BAD_ARG, "null argument");
     if (((uintptr_t)d_a | (uintptr_t)d_b | (uintptr_t)d_out) & 15)
         return fail(c, PG_ERR_BAD_ARG, "device pointers must be 16-byte aligned");
-    if (na + nb > pg_mul_max_limbs()) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
+    if (na > pg_mul_max_limbs() || nb > pg_mul_max_limbs() - na)
+        return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
     std::lock_guard<std::mutex> lock(c->mu);
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
@@ -270,7 +271,7 @@ pg_status pg_mul_device(pg_ctx* c, const uint64_t* d_a, size_t na, const uint64_
 pg_status pg_sqr_device(pg_ctx* c, const uint64_t* d_a, size_t na, uint64_t* d_out) {
     if (!c || !d_out || (na && !d_a)) return fail(c, PG_ERR_BAD_ARG, "null argument");
     if (((uintptr_t)d_a | (uintptr_t)d_out) & 15) return fail(c, PG_ERR_BAD_ARG, "device pointers must be 16-byte aligned");
-    if (2 * na > pg_mul_max_limbs()) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
+    if (na > pg_mul_max_limbs() / 2) return fail(c, PG_ERR_TOO_LARGE, "product exceeds the transform range");
     std::lock_guard<std::mutex> lock(c->mu);
     cudaError_t e = cudaSetDevice(c->device);
     if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");

@@ -75,7 +75,7 @@ cudaError_t grow_dev(T** p, uint64_t& cap, uint64_t n) {
     if (*p) cudaFree(*p);
     *p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
+    cudaError_t e = pg::dev_malloc((void**)p, n * sizeof(T));
     if (e == cudaSuccess) cap = n;
     return e;
 }
@@ -165,7 +165,7 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
             nc = J.nc;
             nd = J.d ? J.nd : J.nc;
         }
-        if (J.na + nb > maxl || nc + nd > maxl)
+        if (J.na > maxl || nb > maxl - J.na || nc > maxl || nd > maxl - nc)
             return fail(ctx, PG_ERR_TOO_LARGE, job_msg(i, "product exceeds the transform range"));
         const size_t top = std::max(J.na + nb, nc + nd) + (J.acc > 0 ? 1 : 0);
         if (J.out_cap < top) return fail(ctx, PG_ERR_BAD_ARG, job_msg(i, "out_cap below the result length"));
@@ -232,7 +232,7 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
     e = grow_dev(&W->d_src, W->src_cap, 4 * n);
     if (e == cudaSuccess) e = grow_dev(&W->d_dst, W->dst_cap, n);
     if (e == cudaSuccess && !W->errw) {
-        e = cudaMalloc((void**)&W->errw, 4);
+        e = pg::dev_malloc((void**)&W->errw, 4);
         if (e == cudaSuccess) e = cudaMemsetAsync(W->errw, 0, 4, st);
     }
     if (e != cudaSuccess) return cuda_fail(ctx, e, "batch tables");
@@ -263,7 +263,7 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
             }
             W->res_cap = 0;
             for (auto*& r : W->res) {
-                e = cudaMalloc((void**)&r, want * 4);
+                e = pg::dev_malloc((void**)&r, want * 4);
                 if (e != cudaSuccess) {
                     for (auto*& q : W->res) {
                         if (q) cudaFree(q);
@@ -389,7 +389,7 @@ pg_status pg_buf_alloc(pg_ctx* ctx, size_t cap, pg_buf** out) {
     b->device = pg::ctx_device(ctx);
     b->cap = cap;
     cudaError_t e = cudaSetDevice(b->device);
-    if (e == cudaSuccess && cap) e = cudaMalloc((void**)&b->d, cap * 8);
+    if (e == cudaSuccess && cap) e = pg::dev_malloc((void**)&b->d, cap * 8);
     if (e == cudaSuccess && cap) e = cudaMemsetAsync(b->d, 0, cap * 8, pg::ctx_stream(ctx));
     if (e != cudaSuccess) {
         if (b->d) cudaFree(b->d);

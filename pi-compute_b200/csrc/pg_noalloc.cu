@@ -16,7 +16,8 @@
 // Set-up: the first call on a device (with that device current) looks up the arrays'
 // device addresses with cudaGetSymbolAddress and fills the tables with a kernel on the
 // caller's stream, then waits for it. Make that first call before any stream capture.
-// Later calls only enqueue the product kernels and wait for them.
+// Every call, the first and all later ones, waits for the caller's stream before it returns:
+// it reads the product's error word back with cudaMemcpyAsync and cudaStreamSynchronize.
 //
 // All calls share the arrays and the arrays keep the previous call's contents: the carry
 // look-back words are cleared at the start of every call (the residues are overwritten in
@@ -135,21 +136,29 @@ pg_status setup_device(int dev, cudaStream_t st) {
 
 }  // namespace
 
+// Every failure of a CUDA call leaves through here: the runtime's sticky last error is read
+// (and so cleared), so that it does not surface later in the caller's own error checks.
+static pg_status device_failure(cudaError_t e) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
+}
+
 extern "C" pg_status pg_mul_noalloc(const uint64_t* d_a, size_t na, const uint64_t* d_b, size_t nb,
                                     uint64_t* d_out, void* stream) {
-    if (na + nb > kNoAllocMaxLimbs) return PG_ERR_TOO_LARGE;
+    // each operand on its own, so that na + nb cannot wrap around
+    if (na > kNoAllocMaxLimbs || nb > kNoAllocMaxLimbs - na) return PG_ERR_TOO_LARGE;
     if (!d_out || (na && !d_a) || (nb && !d_b)) return PG_ERR_BAD_ARG;
     if (((uintptr_t)d_a | (uintptr_t)d_b | (uintptr_t)d_out) & 15) return PG_ERR_BAD_ARG;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     std::lock_guard<std::mutex> lock(g_mu);
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        cudaGetLastError();
-        return PG_ERR_DEVICE;
-    }
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return device_failure(e);
+    if (dev < 0 || dev >= kMaxDevices) return PG_ERR_DEVICE;
     if (na == 0 || nb == 0) {
-        if (na + nb && cudaMemsetAsync(d_out, 0, (na + nb) * 8, st) != cudaSuccess) return PG_ERR_DEVICE;
-        return cudaStreamSynchronize(st) == cudaSuccess ? PG_OK : PG_ERR_DEVICE;
+        if (na + nb && (e = cudaMemsetAsync(d_out, 0, (na + nb) * 8, st)) != cudaSuccess) return device_failure(e);
+        e = cudaStreamSynchronize(st);
+        return e == cudaSuccess ? PG_OK : device_failure(e);
     }
     pg_status s = setup_device(dev, st);
     if (s != PG_OK) {
@@ -167,15 +176,11 @@ extern "C" pg_status pg_mul_noalloc(const uint64_t* d_a, size_t na, const uint64
     w.sync_cap = kSyncWords;
     pg::DeviceTables t;
     t.tw = d.tw;
-    if (cudaMemsetAsync(w.sync, 0, 4, st) != cudaSuccess) return PG_ERR_DEVICE;  // error word
-    cudaError_t e = pg::enqueue_product(t, w, d_a, na, d_b, nb, d_out, st);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
-    }
+    if ((e = cudaMemsetAsync(w.sync, 0, 4, st)) != cudaSuccess) return device_failure(e);  // error word
+    if ((e = pg::enqueue_product(t, w, d_a, na, d_b, nb, d_out, st)) != cudaSuccess) return device_failure(e);
     uint32_t err = 0;
-    if (cudaMemcpyAsync(&err, w.sync, 4, cudaMemcpyDeviceToHost, st) != cudaSuccess) return PG_ERR_DEVICE;
-    if (cudaStreamSynchronize(st) != cudaSuccess) return PG_ERR_DEVICE;
+    if ((e = cudaMemcpyAsync(&err, w.sync, 4, cudaMemcpyDeviceToHost, st)) != cudaSuccess) return device_failure(e);
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return device_failure(e);
     if (err == 1) return PG_ERR_TIMEOUT;
     if (err != 0) return PG_ERR_INTERNAL;
     return PG_OK;

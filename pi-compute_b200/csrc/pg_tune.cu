@@ -98,11 +98,11 @@ pg_status pg_tune(pg_ctx* ctx, int lo, int hi, double* best_us) {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     pg_status status = PG_OK;
     std::string msg;
-    e = cudaMalloc(&a, nmax * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&b, nmax * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&ref, 2 * nmax * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&out, 2 * nmax * 8);
-    if (e == cudaSuccess) e = cudaMalloc(&cnt, sizeof(unsigned long long));
+    e = pg::dev_malloc(&a, nmax * 8);
+    if (e == cudaSuccess) e = pg::dev_malloc(&b, nmax * 8);
+    if (e == cudaSuccess) e = pg::dev_malloc(&ref, 2 * nmax * 8);
+    if (e == cudaSuccess) e = pg::dev_malloc(&out, 2 * nmax * 8);
+    if (e == cudaSuccess) e = pg::dev_malloc(&cnt, sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaEventCreate(&ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&ev1);
     if (e == cudaSuccess) {

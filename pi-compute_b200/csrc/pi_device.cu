@@ -82,7 +82,7 @@ struct SharedProduct {
         *p = nullptr;
         cap = 0;
         const uint64_t want = std::max(words, cap + cap / 2);
-        cudaError_t e = cudaMalloc((void**)p, want * 4);
+        cudaError_t e = pg::dev_malloc((void**)p, want * 4);
         if (e != cudaSuccess) {
             cudaGetLastError();
             throw DevError(e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE, "batched product buffers");
@@ -96,7 +96,7 @@ struct SharedProduct {
         if (product_logL(na, nb) > split_logL()) throw DevError(PG_ERR_TOO_LARGE, "batched product too long");
         if ((sa | so) & 1) throw DevError(PG_ERR_INTERNAL, "batched product strides must be even");
         if (!errw) {
-            if (cudaMalloc((void**)&errw, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "error word");
+            if (pg::dev_malloc((void**)&errw, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "error word");
             cudaMemsetAsync(errw, 0, 4, st);
         }
         const int logL = product_logL(na, nb);
@@ -550,7 +550,7 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         if (sp.digits) cudaFree(sp.digits);
         sp.digits = nullptr;
         sp.digits_cap = 0;
-        if (cudaMalloc((void**)&sp.digits, nd) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
+        if (pg::dev_malloc((void**)&sp.digits, nd) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
         sp.digits_cap = nd;
     }
     char* d_out = sp.digits;
@@ -660,7 +660,7 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
             if (sp.flags) cudaFree(sp.flags);
             sp.flags = nullptr;
             sp.flags_cap = 0;
-            if (cudaMalloc((void**)&sp.flags, (most + 1) * 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
+            if (pg::dev_malloc((void**)&sp.flags, (most + 1) * 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
             sp.flags_cap = most + 1;
         }
         bad = sp.flags + most;

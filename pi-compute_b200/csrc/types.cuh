@@ -157,6 +157,11 @@ struct CrtParams {
     int depth;
     // table batch (merge == 2): job i's residues at res + i * res_stride, output per dtab[i]
     const DstEntry* dtab;
+    // Look-back wait limit in polls (0: kSpinLimit) and a test hook: when withhold1 = b + 1, the
+    // block with ticket b never publishes its status, so its successor's wait runs out (0: none).
+    // launch_crt fills both from the environment (PG_TEST_CRT_SPIN_LIMIT, PG_TEST_CRT_WITHHOLD).
+    uint32_t spin_limit;
+    uint32_t withhold1;
 };
 
 constexpr int kCrtThreads = 256;

@@ -1,10 +1,11 @@
 """Regenerate the golden fixtures in tests/golden/ from the reference build and the oracle.
 
 Run from the repository root after `make -C oracle` (needs the reference sources mounted
-for the reference build; the fixtures it writes are committed and used on machines
-without them):
+for the reference build, at the directory named by the environment variable PI_REF; the
+fixtures it writes are committed and used on machines without them):
 
-    python tests/golden/make_golden.py
+    PI_REF=<reference checkout> python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --top     # only the top-size product hashes (products_top.json)
 
 Outputs
   pi_1000.txt        "3." + 1000 digits from the reference program (checked byte-for-byte
@@ -14,6 +15,8 @@ Outputs
   bs_golden.json     P, Q, R (hex) of the reference's BinarySplitting for small ranges, and
                      sha256 of P/Q/R for the 1M-digit term range
   products.json      sha256 of seeded random products computed by libgmp's mpz_mul
+  products_top.json  the same for the largest products one transform takes (2^24-limb operands:
+                     balanced, 3*2^23 x 2^23, 1:4, 1:16 and the square; about 10 s of mpz_mul each)
 """
 from __future__ import annotations
 
@@ -29,7 +32,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 from helpers import oracle, pkg  # noqa: E402
 
-REF_DATA = "/root/reference/tests/data/pi_1000.txt"
+REF_DATA = os.path.join(os.environ.get("PI_REF", ""), "tests", "data", "pi_1000.txt")
 
 
 def run_ref(digits: int, threads: int) -> bytes:
@@ -56,7 +59,31 @@ for n in [1, 2, 3, 7, 16, 31, 32, 33, 100, 1000, 1024, 1536, 4096, 6144, 16384, 
     PRODUCT_CASES.append((n, 0, 4000 + n))  # nb == 0 encodes a square
 
 
+# The largest products one transform takes (na + nb = 2^25 limbs, L = 2^26 points): the sizes the
+# multiply's roofline is quoted on. (na, nb, seed), nb == 0 a square.
+TOP_CASES = [(1 << 24, 1 << 24, 71), (3 << 23, 1 << 23, 72), (1 << 24, 1 << 22, 73), (1 << 24, 1 << 20, 74),
+             (1 << 24, 0, 75)]
+
+
+def product_entry(na: int, nb: int, seed: int) -> dict:
+    a = pkg.random_operand(na, seed)
+    r = oracle.mul_gmp(a, a) if nb == 0 else oracle.mul_gmp(a, pkg.random_operand(nb, seed + 7))
+    return {"na": na, "nb": nb, "seed": seed, "len": int(len(r)), "sha256": limb_hash(r)}
+
+
+def main_top() -> None:
+    oracle.build()
+    out = [product_entry(na, nb, seed) for na, nb, seed in TOP_CASES]
+    json.dump(out, open(os.path.join(HERE, "products_top.json"), "w"), indent=1)
+    print("top-size product hashes written to", HERE)
+
+
 def main() -> None:
+    if "--top" in sys.argv:
+        main_top()
+        return
+    if not os.path.isdir(os.environ.get("PI_REF", "")):
+        sys.exit("set PI_REF to the reference checkout (its tests/data/pi_1000.txt pins the reference build)")
     oracle.build()
     os.makedirs(HERE, exist_ok=True)
 
@@ -88,15 +115,7 @@ def main() -> None:
         bsg["hash_ranges"][f"{a},{b}"] = [hashlib.sha256(hex(v).encode()).hexdigest() for v in (P, Q, R)]
     json.dump(bsg, open(os.path.join(HERE, "bs_golden.json"), "w"), indent=1)
 
-    prods = []
-    for na, nb, seed in PRODUCT_CASES:
-        a = pkg.random_operand(na, seed)
-        if nb == 0:
-            r = oracle.mul_gmp(a, a)
-        else:
-            b = pkg.random_operand(nb, seed + 7)
-            r = oracle.mul_gmp(a, b)
-        prods.append({"na": na, "nb": nb, "seed": seed, "len": int(len(r)), "sha256": limb_hash(r)})
+    prods = [product_entry(na, nb, seed) for na, nb, seed in PRODUCT_CASES]
     json.dump(prods, open(os.path.join(HERE, "products.json"), "w"), indent=1)
     print("golden fixtures written to", HERE)
 

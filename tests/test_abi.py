@@ -52,3 +52,16 @@ def test_limb_helpers_roundtrip():
     a = pkg.random_operand(5, 3)
     assert int(a[-1]) >> 63 == 1
     assert list(pkg.splitmix64(0, 1)) == [0xE220A8397B1DCDAF]
+
+
+def test_size_checks_do_not_wrap_around():
+    # na + nb would wrap around size_t: pg_mul_noalloc must still reject the lengths before it
+    # touches memory or the device (these calls return before any CUDA call)
+    lib = pkg.load_library()
+    big = ctypes.c_size_t(-1).value
+    f = lib.pg_mul_noalloc
+    f.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p,
+                  ctypes.c_void_p]
+    f.restype = ctypes.c_int
+    for na, nb in [(big, 1), (big, 2), (1, big), (big, big), (16384, 1)]:
+        assert f(16, na, 16, nb, 16, None) == pkg.PG_ERR_TOO_LARGE, (na, nb)

@@ -2,8 +2,8 @@
 
 Every product is compared bit-exactly with the oracle (libgmp's mpz_mul, the call the
 reference's GmpMultiplier makes, gmp_multiplier.cpp:10-19) or with committed golden
-hashes of oracle products; the largest sizes use size-independent properties (residues
-modulo independent primes, square vs product of equal operands).
+hashes of oracle products, up to the largest products one transform takes (2^24-limb
+operands, tests/golden/products_top.json).
 Cases follow the reference's GPU suite (tests/test_gpu_ntt_multiplier.cpp:65-166) and
 extend it with transform-length boundaries, uneven shapes, carry-chain stress and errors.
 """
@@ -162,23 +162,23 @@ def test_golden_product_hashes(eng):
         assert hashlib.sha256(r.astype("<u8").tobytes()).hexdigest() == c["sha256"], c
 
 
-def residues_agree(a, b, r, primes=(2**61 - 1, 2**31 - 1, 1000000007, 998244353, 0xFFFFFFFB)):
-    A, B, R = pkg.limbs_to_int(a), pkg.limbs_to_int(b), pkg.limbs_to_int(r)
-    return all((A % q) * (B % q) % q == R % q for q in primes)
-
-
 @pytest.mark.parametrize("logn", [20, 22])
 def test_large_balanced_vs_oracle(eng, logn):
     n = 1 << logn
     check(eng, pkg.random_operand(n, 900 + logn), pkg.random_operand(n, 901 + logn))
 
 
-@pytest.mark.parametrize("na,nb", [(1 << 24, 1 << 24), (3 << 23, 1 << 23), (1 << 24, 1 << 20)])
-def test_max_size_products(eng, na, nb):
-    a = pkg.random_operand(na, 7 + na)
-    b = pkg.random_operand(nb, 9 + nb)
-    r = eng.mul_limbs(a, b)
-    assert len(r) in (na + nb, na + nb - 1)
-    assert residues_agree(a, b, r)
-    s = eng.sqr_limbs(b)
-    assert residues_agree(b, b, s)
+TOP = json.load(open(os.path.join(GOLDEN, "products_top.json")))
+
+
+@pytest.mark.parametrize("case", TOP, ids=[f"{c['na']}x{c['nb'] or 'sq'}" for c in TOP])
+def test_max_size_products_bit_exact(eng, case):
+    # the largest products one transform takes (na + nb = 2^25 limbs, L = 2^26 points), where the
+    # roofline is quoted: compared word for word with mpz_mul through sha256 of the limbs
+    a = pkg.random_operand(case["na"], case["seed"])
+    if case["nb"] == 0:
+        r = eng.sqr_limbs(a)
+    else:
+        r = eng.mul_limbs(a, pkg.random_operand(case["nb"], case["seed"] + 7))
+    assert len(r) == case["len"]
+    assert hashlib.sha256(r.astype("<u8").tobytes()).hexdigest() == case["sha256"]

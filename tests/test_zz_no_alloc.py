@@ -6,7 +6,8 @@ the library. The test calls it through the C ABI twice in a row and checks each 
 against the existing entry point pg_mul_device, bit for bit (integer products: the
 tolerance is zero), and against the oracle. This file sorts last so that a run stopping at
 the first failure has run every other test already; it also passes alone in a fresh process
-(the first call on the device does the set-up).
+(the first call on the device does the set-up). Shapes cover the one-pass plans (na + nb <= 4096
+limbs), the two-pass plans and an empty operand.
 """
 import ctypes
 
@@ -35,12 +36,15 @@ def test_noalloc_matches_existing_entry_point_twice():
     stream = torch.cuda.current_stream().cuda_stream
     eng = pkg.Engine(0)
     try:
-        # two calls in a row, different shapes; the second is the largest size accepted
-        for na, nb, seed in [(5000, 3001, 1), (8192, 8192, 2)]:
+        # calls in a row, different shapes: two-pass plans (L = 2^14, and 2^15 at the largest size
+        # accepted), one-pass plans (na + nb <= 4096: L = 2^6, 2^9, 2^13) and an empty operand
+        for na, nb, seed in [(5000, 3001, 1), (8192, 8192, 2), (1, 1, 3), (100, 37, 4), (3000, 1096, 5),
+                             (0, 5, 6), (4096, 4096, 7)]:
             a = pkg.random_operand(na, seed)
             b = pkg.random_operand(nb, seed + 100)
-            da = torch.from_numpy(a.view(np.int64)).cuda()
-            db = torch.from_numpy(b.view(np.int64)).cuda()
+            # an empty operand still gets a valid (16-byte aligned) device address
+            da = torch.from_numpy(a.view(np.int64)).cuda() if na else torch.zeros(2, dtype=torch.int64, device="cuda")
+            db = torch.from_numpy(b.view(np.int64)).cuda() if nb else torch.zeros(2, dtype=torch.int64, device="cuda")
             out_new = torch.full((na + nb,), -1, dtype=torch.int64, device="cuda")
             out_ref = torch.zeros(na + nb, dtype=torch.int64, device="cuda")
             torch.cuda.synchronize()
@@ -51,7 +55,7 @@ def test_noalloc_matches_existing_entry_point_twice():
             got = out_new.cpu().numpy().view(np.uint64)
             ref = out_ref.cpu().numpy().view(np.uint64)
             assert np.array_equal(got, ref)
-            exp = oracle.mul_gmp(a, b)
+            exp = oracle.mul_gmp(a, b) if na and nb else np.zeros(0, dtype=np.uint64)
             assert np.array_equal(got[: len(exp)], exp) and not got[len(exp):].any()
         # beyond the stated maximum: rejected with a clear status, nothing touched
         assert noalloc(da.data_ptr(), 8192, db.data_ptr(), 8193, out_new.data_ptr(), stream) == pkg.PG_ERR_TOO_LARGE
