@@ -148,6 +148,22 @@ typedef struct pg_job {
 } pg_job;
 pg_status pg_mul_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs);
 
+/* ---- A tree level as a CUDA graph. pg_graph_capture_level validates `jobs` like pg_mul_batch,
+ * sizes buffers of its own for them, uploads their tables and captures the level's launches (one
+ * per pass per transform-length group, the pointwise steps, one CRT + carry per group) into a CUDA
+ * graph on the context's stream; nothing runs yet. pg_graph_launch replays it: the same products
+ * over whatever the operand buffers hold at that moment, written to the same outputs, and returns
+ * when they are complete (errors as pg_mul_batch). The pointers in `jobs` must stay valid while the
+ * graph lives; the graph's buffers are its own, so products and batches on the same context may run
+ * between replays. pg_graph_destroy waits for the context's stream and frees the graph.
+ * The reference's level is a sequence of Multiplier calls issued from threads
+ * (src/engine/binary_splitting.cpp:183-238); a caller that splits level by level captures each
+ * level shape once and replays it with one launch call. */
+typedef struct pg_graph pg_graph;
+pg_status pg_graph_capture_level(pg_ctx* ctx, const pg_job* jobs, size_t njobs, pg_graph** out);
+pg_status pg_graph_launch(pg_graph* g);
+void pg_graph_destroy(pg_graph* g);
+
 /* ---- Device-resident finish of a pi computation. Every operand stays in HBM; products run
  * on the transform above, additions, shifts and comparisons on carry-chain kernels.
  *

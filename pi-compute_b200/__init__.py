@@ -113,6 +113,12 @@ def load_library(path: str = LIBPIGPU) -> ctypes.CDLL:
     lib.pg_buf_set_len.restype = ctypes.c_int
     lib.pg_mul_batch.argtypes = [vp, ctypes.POINTER(PgJob), sz]
     lib.pg_mul_batch.restype = ctypes.c_int
+    lib.pg_graph_capture_level.argtypes = [vp, ctypes.POINTER(PgJob), sz, ctypes.POINTER(vp)]
+    lib.pg_graph_capture_level.restype = ctypes.c_int
+    lib.pg_graph_launch.argtypes = [vp]
+    lib.pg_graph_launch.restype = ctypes.c_int
+    lib.pg_graph_destroy.argtypes = [vp]
+    lib.pg_graph_destroy.restype = None
     lib.pg_recip_floor.argtypes = [vp, _u64p, sz, _u64p, sz, _sizep]
     lib.pg_recip_floor.restype = ctypes.c_int
     lib.pg_mul_wrap.argtypes = [vp, _u64p, sz, _u64p, sz, ctypes.c_int, _u64p, sz, _sizep]

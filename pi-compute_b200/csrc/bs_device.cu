@@ -363,7 +363,6 @@ struct DeviceBS {
     // CUDA graph of the last range's launch sequence (replayed when the same range comes back
     // and no buffer moved since it was captured)
     uint64_t moves = 0;           // buffer reallocations so far
-    uint64_t seen_a0 = ~0ull, seen_b0 = 0, seen_moves = ~0ull;  // last range run directly
     cudaGraphExec_t gexec = nullptr;  // captured for [g_a0, g_b0); destroyed when a buffer moves
     uint64_t g_a0 = ~0ull, g_b0 = 0;
     LevelView groot{};
@@ -398,9 +397,9 @@ struct DeviceBS {
         return e;
     }
 
-    // run() through a CUDA graph: the first call on a range runs directly (and sizes the buffers);
-    // a second call on the same range with no buffer moved since captures the launch sequence
-    // (it has no host waits and, the buffers being sized, no allocation); later calls replay it.
+    // run() through a CUDA graph: the range is planned and every buffer sized first (host work
+    // and allocations, outside any capture), then its launch sequence is captured and replayed; a
+    // later call on the same range, with no buffer moved since, replays the graph alone.
     cudaError_t run_graph(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
         if (trace_on()) return run(a0, b0, root, err);  // tracing waits between depths
         if (gexec && g_a0 == a0 && g_b0 == b0) {  // no buffer moved since the capture
@@ -408,67 +407,46 @@ struct DeviceBS {
             if (launches) *launches += glaunches;
             return cudaGraphLaunch(gexec, st);
         }
-        const bool same = seen_a0 == a0 && seen_b0 == b0 && seen_moves == moves;
-        if (!same) {
-            cudaError_t e = run(a0, b0, root, err);
-            seen_a0 = a0;
-            seen_b0 = b0;
-            seen_moves = (e == cudaSuccess && err.empty()) ? moves : ~0ull;
-            return e;
-        }
-        // capture
         if (gexec) {
             cudaGraphExecDestroy(gexec);
             gexec = nullptr;
         }
+        std::vector<DepthPlan> dp;
+        int D = 0;
+        cudaError_t e = prepare(a0, b0, dp, D, err);
+        if (e != cudaSuccess) return e;
         uint64_t* saved = launches;
         uint64_t counted = 0;
         launches = &counted;
         cudaGraph_t g = nullptr;
-        cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
-#ifdef PG_GRAPH_DEBUG
-        std::fprintf(stderr, "[graph] begin capture: %s\n", cudaGetErrorString(e));
-#endif
+        e = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
         if (e != cudaSuccess) {
             launches = saved;
             cudaGetLastError();
-            return run(a0, b0, root, err);
+            return enqueue(a0, b0, dp, D, root);  // run directly instead
         }
         const uint64_t m0 = moves;
-        cudaError_t er = run(a0, b0, root, err);
+        cudaError_t er = enqueue(a0, b0, dp, D, root);
         e = cudaStreamEndCapture(st, &g);
         launches = saved;
-#ifdef PG_GRAPH_DEBUG
-        std::fprintf(stderr, "[graph] run in capture: %s, end capture: %s, moves %llu -> %llu\n",
-                     cudaGetErrorString(er), cudaGetErrorString(e), (unsigned long long)m0, (unsigned long long)moves);
-#endif
-        if (er != cudaSuccess || e != cudaSuccess || !err.empty() || moves != m0) {
+        if (er != cudaSuccess || e != cudaSuccess || moves != m0) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
-            seen_moves = ~0ull;
-            if (!err.empty()) return cudaErrorInvalidValue;
-            return run(a0, b0, root, err);  // run directly instead
+            return enqueue(a0, b0, dp, D, root);
         }
         e = cudaGraphInstantiate(&gexec, g, 0);
         cudaGraphDestroy(g);
-#ifdef PG_GRAPH_DEBUG
-        std::fprintf(stderr, "[graph] instantiate: %s\n", cudaGetErrorString(e));
-#endif
         if (e != cudaSuccess) {
             gexec = nullptr;
             cudaGetLastError();
-            return run(a0, b0, root, err);
+            return enqueue(a0, b0, dp, D, root);
         }
         groot = root;
         g_a0 = a0;
         g_b0 = b0;
         glaunches = counted;
         if (launches) *launches += counted;
-        e = cudaGraphLaunch(gexec, st);
-#ifdef PG_GRAPH_DEBUG
-        std::fprintf(stderr, "[graph] first launch: %s\n", cudaGetErrorString(e));
-#endif
-        return e;
+        return cudaGraphLaunch(gexec, st);
     }
 
     std::vector<DepthPlan> plan(uint64_t a0, uint64_t b0, int& D, std::string& err) {
@@ -625,21 +603,21 @@ struct DeviceBS {
             if (e != cudaSuccess) return e;
             if (launches) ++*launches;
         }
-        // inverse transforms of the 3M outputs, written over operand slots 3..5 of every merge (jobs
-        // of stride 6*stride, three launches of M jobs per pass). The first inverse pass (the
-        // contiguous one) forms its tiles from the operands on load: P^ = Pl Pr, R^ = Qr Rl +- Pl Rr,
-        // Q^ = Ql Qr, in that order, since R^ still reads Qr (slot 4) after P^ overwrote Pr (slot 3)
-        // and Q^ overwrites Qr last (no separate pointwise kernel and no pass over the products).
-        for (int k : {0, 2, 1}) {
+        // inverse transforms of the 3M outputs, one launch per pass over all of them: output k of
+        // merge m (P^ = Pl Pr, Q^ = Ql Qr, R^ = Qr Rl +- Pl Rr) is formed on load by the first
+        // (contiguous) inverse pass and written over operand slot comb_out_slot(k) (Pr, Ql, Rr),
+        // which no other output reads, so the three outputs need no order among themselves (no
+        // separate pointwise kernel and no pass over the products).
+        {
             PassParams q{};
-            q.data = res + (3 + k) * stride;
-            q.out = q.data;
+            q.data = res;
+            q.out = res;
             q.L = L;
             q.logL = P.logL;
-            q.job_stride = 6 * stride;
-            q.njobs = (uint32_t)M;
+            q.job_stride = 0;
+            q.njobs = (uint32_t)(3 * M);
             q.merge = 0;
-            q.comb_k = k;
+            q.comb3 = 1;
             q.comb_slot = stride;
             q.comb_a0 = a0;
             q.comb_b0 = b0;
@@ -687,18 +665,17 @@ struct DeviceBS {
     }
 
     // Computes P, Q, R of [a0, b0); results stay in the final level buffers (root = node 0).
-    cudaError_t run(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
-        int D = 0;
+    // Plans [a0, b0) and sizes every buffer for it (allocations and host work only, nothing enqueued).
+    cudaError_t prepare(uint64_t a0, uint64_t b0, std::vector<DepthPlan>& dp, int& D, std::string& err) {
+        D = 0;
         const bool tr = trace_on();
         auto tp0 = std::chrono::steady_clock::now();
-        std::vector<DepthPlan> dp = plan(a0, b0, D, err);
+        dp = plan(a0, b0, D, err);
         if (tr)
             std::fprintf(stderr, "[pg_bs] plan %.3f ms, %d depths\n",
                          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp0).count(), D);
         if (!err.empty()) return cudaErrorInvalidValue;
         cudaError_t e = grow((void**)&errw, errw_cap, 256);
-        if (e != cudaSuccess) return e;
-        e = cudaMemsetAsync(errw, 0, 4, st);
         if (e != cudaSuccess) return e;
         if (D == 0) {
             // single term: the root is a leaf; treat it as a "pair level" of one node of size 1
@@ -737,6 +714,15 @@ struct DeviceBS {
             if (res_need && (e = grow((void**)&res, res_cap, res_need)) != cudaSuccess) return e;
             if (sync_need && (e = grow((void**)&sync, sync_cap, sync_need)) != cudaSuccess) return e;
         }
+        return cudaSuccess;
+    }
+
+    // Enqueues the splitting of [a0, b0) planned and sized by prepare(): kernels and memsets only
+    // (no allocation, no host wait), so it may run inside a stream capture.
+    cudaError_t enqueue(uint64_t a0, uint64_t b0, std::vector<DepthPlan>& dp, int D, LevelView& root) {
+        const bool tr = trace_on();
+        cudaError_t e = cudaMemsetAsync(errw, 0, 4, st);
+        if (e != cudaSuccess) return e;
         auto view = [&](int slot, const DepthPlan& P) {
             LevelView v;
             for (int k = 0; k < 3; ++k) {
@@ -807,6 +793,14 @@ struct DeviceBS {
         }
         root = view(slot, dp[0]);
         return cudaSuccess;
+    }
+
+    cudaError_t run(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
+        std::vector<DepthPlan> dp;
+        int D = 0;
+        cudaError_t e = prepare(a0, b0, dp, D, err);
+        if (e != cudaSuccess) return e;
+        return enqueue(a0, b0, dp, D, root);
     }
 };
 

@@ -107,7 +107,7 @@ __device__ __forceinline__ CrtJob crt_job(const CrtParams& P, uint64_t job) {
     }
     const uint64_t m = job / 3;
     const int which = (int)(job % 3);
-    J.res = P.res + (6 * m + 3 + which) * P.res_stride;
+    J.res = P.res + (6 * m + comb_out_slot(which)) * P.res_stride;
     J.out = reinterpret_cast<uint32_t*>(P.dst[which] + m * P.dcap[which]);
     J.nwords = 2ull * P.dcap[which];
     J.len = P.dlen + 3 * m + which;

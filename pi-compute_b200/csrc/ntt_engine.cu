@@ -26,75 +26,108 @@ uint32_t inv_mod(uint32_t a, uint32_t p) { return pow_mod(a, p - 2, p); }
 uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
 
 // ---------------------------------------------------------------- tables
-// Layout of the single table allocation, in uint2 entries, 2^13 per table:
-//   [dir][prime] stage  : entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
-//   [dir][prime] fs_lo  : w_{2^26}^j
-//   [dir][prime] fs_hi  : w_{2^26}^(2^13 j)
-//   [n][l][dir][prime] row : w_{2^n}^(c bitrev_l(m)) at m * 2^(13-l) + c, for four-step blocks of
-//                            2^n points (n = 14..26) and strided sub-transforms of 2^l points (l = 5..10)
+// Layout of the single table allocation, in uint2 entries:
+//   [dir][prime] stage  (2^14 each): entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
+//   [dir][prime] fs_lo  (2^13 each): w_{2^26}^j
+//   [dir][prime] fs_hi  (2^13 each): w_{2^26}^(2^13 j)
+//   [n][l][dir][prime] row (2^13 each): w_{2^n}^(c bitrev_l(m)) at m * 2^(13-l) + c, for four-step
+//                       blocks of 2^n points (n = 14..26) and strided sub-transforms of 2^l points
+//                       (l = 5..10, tiles of 2^13)
+//   [n][l][dir][prime] row_big (2^14 each): the same for l = 11, 12 in tiles of 2^14 (m * 2^(14-l) + c)
+// The host computes the stage and fs tables (1.5 MB); a kernel derives every row table from fs_lo and
+// fs_hi on the device (w_{2^26}^e = lo[e mod 2^13] * hi[e / 2^13]), so a context's 50 MB of tables
+// cost no host arithmetic and no upload.
+namespace {
+constexpr size_t kFsEnt = 1u << kFsLog;
+constexpr size_t kSmallTables = (size_t)2 * kNumPrimes * (kStageEnt + 2 * kFsEnt);  // entries
+constexpr size_t kRowEnt = (size_t)kRowTables * 2 * kNumPrimes * kFsEnt;
+constexpr size_t kRowBigEnt = (size_t)kRowTablesBig * 2 * kNumPrimes * (1u << 14);
+
+__global__ void fill_row_tables_kernel(uint2* row, uint2* row_big, TwiddleTables tw) {
+    const uint64_t total = kRowEnt + kRowBigEnt;
+    for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (uint64_t)gridDim.x * blockDim.x) {
+        const bool big = idx >= kRowEnt;
+        const uint64_t k = big ? idx - kRowEnt : idx;
+        const int logE = big ? 14 : 13;
+        const uint32_t i = (uint32_t)(k & ((1u << logE) - 1));  // entry in its table
+        const uint64_t t = k >> logE;                            // ((n, l) * 2 + dir) * primes + prime
+        const int j = (int)(t % kNumPrimes);
+        const int dir = (int)((t / kNumPrimes) & 1);
+        const uint64_t nl = t / (2 * kNumPrimes);
+        const int nls = big ? (kRowNBigMax - kRowNBigMin + 1) : (kRowNMax - kRowNMin + 1);
+        const int n = kRowLogMin + (int)(nl / nls);
+        const int l = (big ? kRowNBigMin : kRowNMin) + (int)(nl % nls);
+        const uint32_t m = i >> (logE - l), c = i & ((1u << (logE - l)) - 1);
+        const uint32_t kr = __brev(m) >> (32 - l);  // bitrev_l(m)
+        const uint32_t e = (c * kr) << (kMaxLogL - n);  // c * kr < 2^logE <= 2^n: e < 2^26
+        const uint32_t p = kPrime(j);
+        const uint2 a = tw.fs_lo[dir][j][e & (kFsEnt - 1)];
+        const uint2 b = tw.fs_hi[dir][j][e >> kFsLog];
+        const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
+        (big ? row_big : row)[k] = make_uint2(w, shoup_companion_dev(w, p, kRecip64(j)));
+    }
+}
+}  // namespace
+
+static cudaError_t allow_big_tiles();
+
 cudaError_t DeviceTables::build(int device) {
     (void)device;
-    constexpr size_t kEnt = 1u << 13;
-    constexpr size_t kTables = (3 + kRowTables) * 2 * kNumPrimes;
-    std::vector<uint2> h(kTables * kEnt);
-    // one host thread per (direction, prime): the tables of each pair are independent
-    auto fill = [&](int dir, int j) {
-        {
+    std::vector<uint2> h(kSmallTables);
+    auto stage_at = [&](int dir, int j) { return h.data() + (size_t)(dir * kNumPrimes + j) * kStageEnt; };
+    auto fs_at = [&](int which, int dir, int j) {
+        return h.data() + (size_t)2 * kNumPrimes * kStageEnt + ((size_t)(which * 2 + dir) * kNumPrimes + j) * kFsEnt;
+    };
+    for (int dir = 0; dir < 2; ++dir)
+        for (int j = 0; j < kNumPrimes; ++j) {
             const uint32_t p = kPrime(j);
             uint32_t w26 = pow_mod(kGenerator(j), (uint64_t)(p - 1) >> kMaxLogL, p);  // primitive 2^26-th root
             if (dir == 1) w26 = inv_mod(w26, p);
             const uint32_t w14 = pow_mod(w26, 1ull << (kMaxLogL - kStageLog), p);
             const uint32_t w26hi = pow_mod(w26, 1ull << kFsLog, p);
-            uint2* st = h.data() + ((0 * 2 + dir) * kNumPrimes + j) * kEnt;
-            uint2* lo = h.data() + ((1 * 2 + dir) * kNumPrimes + j) * kEnt;
-            uint2* hi = h.data() + ((2 * 2 + dir) * kNumPrimes + j) * kEnt;
+            uint2* st = stage_at(dir, j);
+            uint2* lo = fs_at(0, dir, j);
+            uint2* hi = fs_at(1, dir, j);
+            // stage entries by level: entry 2^k + x = w_{2^(k+1)}^x = w14^(x 2^(13-k))
+            st[0] = make_uint2(1, shoup_companion(1, p));
+            for (int k = 0; k < kStageLog; ++k) {
+                const uint64_t step = pow_mod(w14, 1ull << (kStageLog - 1 - k), p);
+                uint64_t r = 1;
+                for (uint32_t x = 0; x < (1u << k); ++x) {
+                    st[(1u << k) + x] = make_uint2((uint32_t)r, shoup_companion((uint32_t)r, p));
+                    r = r * step % p;
+                }
+            }
             uint64_t b = 1, c = 1;
-            for (size_t i = 0; i < kEnt; ++i) {
-                const uint32_t a = pow_mod(w14, stage_exponent((uint32_t)i), p);
-                st[i] = make_uint2(a, shoup_companion(a, p));
+            for (size_t i = 0; i < kFsEnt; ++i) {
                 lo[i] = make_uint2((uint32_t)b, shoup_companion((uint32_t)b, p));
                 hi[i] = make_uint2((uint32_t)c, shoup_companion((uint32_t)c, p));
                 b = b * w26 % p;
                 c = c * w26hi % p;
             }
-            for (int n = kRowLogMin; n <= kMaxLogL; ++n) {
-                const uint64_t wn = pow_mod(w26, 1ull << (kMaxLogL - n), p);  // w_{2^n}
-                for (int l = kRowNMin; l <= kRowNMax; ++l) {
-                    const int t = ((n - kRowLogMin) * (kRowNMax - kRowNMin + 1) + (l - kRowNMin)) * 2 + dir;
-                    uint2* row = h.data() + ((size_t)(3 * 2 * kNumPrimes) + (size_t)t * kNumPrimes + j) * kEnt;
-                    const uint32_t C = 1u << (kTileLog - l);
-                    for (uint32_t m = 0; m < (1u << l); ++m) {
-                        uint32_t k = 0;  // bitrev_l(m)
-                        for (int b = 0; b < l; ++b) k |= ((m >> b) & 1u) << (l - 1 - b);
-                        const uint64_t step = pow_mod((uint32_t)wn, k, p);
-                        uint64_t r = 1;
-                        for (uint32_t c = 0; c < C; ++c) {
-                            row[m * C + c] = make_uint2((uint32_t)r, shoup_companion((uint32_t)r, p));
-                            r = r * step % p;
-                        }
-                    }
-                }
-            }
         }
-    };
-    {
-        std::vector<std::thread> th;
-        for (int dir = 0; dir < 2; ++dir)
-            for (int j = 0; j < kNumPrimes; ++j) th.emplace_back(fill, dir, j);
-        for (auto& t : th) t.join();
-    }
-    cudaError_t e = pg::dev_malloc(&base, h.size() * sizeof(uint2));
+    cudaError_t e = pg::dev_malloc(&base, (kSmallTables + kRowEnt + kRowBigEnt) * sizeof(uint2));
     if (e != cudaSuccess) return e;
     e = cudaMemcpy(base, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
     for (int dir = 0; dir < 2; ++dir)
         for (int j = 0; j < kNumPrimes; ++j) {
-            tw.stage[dir][j] = base + ((0 * 2 + dir) * kNumPrimes + j) * kEnt;
-            tw.fs_lo[dir][j] = base + ((1 * 2 + dir) * kNumPrimes + j) * kEnt;
-            tw.fs_hi[dir][j] = base + ((2 * 2 + dir) * kNumPrimes + j) * kEnt;
+            tw.stage[dir][j] = base + (size_t)(dir * kNumPrimes + j) * kStageEnt;
+            tw.fs_lo[dir][j] = base + (size_t)2 * kNumPrimes * kStageEnt + ((size_t)(0 * 2 + dir) * kNumPrimes + j) * kFsEnt;
+            tw.fs_hi[dir][j] = base + (size_t)2 * kNumPrimes * kStageEnt + ((size_t)(1 * 2 + dir) * kNumPrimes + j) * kFsEnt;
         }
-    tw.row = base + (size_t)3 * 2 * kNumPrimes * kEnt;
-    return cudaSuccess;
+    uint2* row = base + kSmallTables;
+    uint2* row_big = row + kRowEnt;
+    tw.row = row;
+    tw.row_big = row_big;
+    tw.row_layout = 0;
+    e = allow_big_tiles();
+    if (e != cudaSuccess) return e;
+    fill_row_tables_kernel<<<148 * 8, 256>>>(row, row_big, tw);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    return e;
 }
 
 void DeviceTables::release() {
@@ -158,9 +191,16 @@ void Workspace::release() {
 }
 
 // ---------------------------------------------------------------- pass dispatch
+// Dynamic shared memory of a pass: the tile, plus the four-step row factors of a strided tile.
+template <Layout LAY, int LOGN>
+constexpr size_t pass_smem() {
+    return ((size_t)4 << tile_log(LAY == Layout::Strided, LOGN)) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
+}
+
 template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
 static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cudaStream_t st) {
-    constexpr int LOGE = kTileLog;
+    constexpr int LOGE = tile_log(LAY == Layout::Strided, LOGN);
+    constexpr int NT = pass_threads(LOGE);
     uint64_t tiles;
     if constexpr (LAY == Layout::Strided) {
         tiles = (uint64_t)prm.njobs << (prm.logL - LOGE);
@@ -169,12 +209,51 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cuda
         const uint64_t per = 1ull << (LOGE - LOGN);
         tiles = (rows + per - 1) / per;
     }
-    auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, kPassThreads, INV, SRC, FUSE>;
-    // the tile, plus the four-step row factors of a strided tile
-    const size_t smem = ((size_t)4 << LOGE) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
+    auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, NT, INV, SRC, FUSE>;
+    constexpr size_t smem = pass_smem<LAY, LOGN>();
     dim3 grid((unsigned)tiles, kNumPrimes);
-    kern<<<grid, kPassThreads, smem, st>>>(prm, tw);
+    kern<<<grid, NT, smem, st>>>(prm, tw);
     return cudaGetLastError();
+}
+
+// Kernels whose tiles need more than the default 48 KB of dynamic shared memory opt in on the
+// current device; done for every such kernel when a context's tables are built, so that no
+// attribute is set in the middle of a stream capture.
+template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
+static cudaError_t allow_smem() {
+    constexpr int LOGE = tile_log(LAY == Layout::Strided, LOGN);
+    constexpr size_t smem = pass_smem<LAY, LOGN>();
+    if constexpr (smem <= 48 * 1024) return cudaSuccess;
+    return cudaFuncSetAttribute(ntt_pass_kernel<LAY, LOGN, LOGE, pass_threads(LOGE), INV, SRC, FUSE>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <int N>
+static cudaError_t allow_smem_contig() {
+    cudaError_t e = allow_smem<Layout::Contig, N, true, Source::Residues, Fuse::Combine>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, true, Source::Residues, Fuse::None>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Limbs, Fuse::None>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Limbs, Fuse::MulInverse>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Limbs, Fuse::SqrInverse>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Residues, Fuse::None>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Residues, Fuse::MulInverse>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Residues, Fuse::SqrInverse>();
+    return e;
+}
+
+template <int N>
+static cudaError_t allow_smem_strided() {
+    cudaError_t e = allow_smem<Layout::Strided, N, true, Source::Residues, Fuse::None>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Strided, N, false, Source::Limbs, Fuse::None>();
+    if (e == cudaSuccess) e = allow_smem<Layout::Strided, N, false, Source::Residues, Fuse::None>();
+    return e;
+}
+
+static cudaError_t allow_big_tiles() {
+    cudaError_t e = allow_smem_contig<14>();
+    if (e == cudaSuccess) e = allow_smem_strided<11>();
+    if (e == cudaSuccess) e = allow_smem_strided<12>();
+    return e;
 }
 
 #define PG_CONTIG_CASE(N)                                                                                    \
@@ -219,6 +298,7 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
             PG_CONTIG_CASE(11)
             PG_CONTIG_CASE(12)
             PG_CONTIG_CASE(13)
+            PG_CONTIG_CASE(14)
             default:
                 return cudaErrorInvalidValue;
         }
@@ -230,6 +310,8 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
             PG_STRIDED_CASE(8)
             PG_STRIDED_CASE(9)
             PG_STRIDED_CASE(10)
+            PG_STRIDED_CASE(11)
+            PG_STRIDED_CASE(12)
             default:
                 return cudaErrorInvalidValue;
         }

@@ -30,7 +30,9 @@ inline int split_logL() {
     return v;
 }
 
-constexpr int kPassThreads = 256;
+// Threads of a pass kernel's CTA: 256 for tiles of 2^13 residues (4 CTAs per SM), 512 for tiles of
+// 2^14 (2 CTAs per SM): 32 resident warps and <= 64 registers per thread either way.
+constexpr int pass_threads(int logE) { return logE > kTileLog ? 512 : 256; }
 
 // Launch one forward/inverse pass. Returns cudaGetLastError().
 cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm,

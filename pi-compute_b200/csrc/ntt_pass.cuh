@@ -39,9 +39,9 @@ namespace pg {
 #ifndef PG_FUSED_MINB
 #define PG_FUSED_MINB 4
 #endif
-template <Layout LAY, Fuse FUSE>
+template <Layout LAY, Fuse FUSE, int LOGE>
 constexpr int pass_min_blocks() {
-    return LAY == Layout::Strided ? PG_STRIDED_MINB : (FUSE == Fuse::None ? 4 : PG_FUSED_MINB);
+    return LOGE > 13 ? 2 : (LAY == Layout::Strided ? PG_STRIDED_MINB : (FUSE == Fuse::None ? 4 : PG_FUSED_MINB));
 }
 
 __device__ __forceinline__ uint32_t bitrev_n(uint32_t x, int logn) {
@@ -125,15 +125,20 @@ __device__ __forceinline__ void dit_round(uint32_t (&v)[1 << LR], uint32_t tp, i
 }
 
 // Shared-memory address of linear tile index x: the eight 16-byte chunks of each 128-byte
-// line are permuted by f = ((x >> 5) ^ (x >> 8 << 2)) & 7. The access patterns of a warp:
+// line are permuted by f = ((x >> 5) ^ (x >> 7) ^ (x >> 8 << 2)) & 7 (bits 5-9 of x select the
+// permutation, bits 2-4 are permuted, bits 0-1 stay: 16-byte vectors stay whole). The access
+// patterns of a warp:
 //   global<->shared copies, 16-byte vectors of consecutive chunks: one line per 8 lanes;
-//   stride-1 rounds (contiguous tiles), 16-byte vectors at a 64-byte lane stride: lanes
-//     2i and 2i+1 share a line and differ in chunk bit 2, f walks through the lines;
-//   stride-16 rounds, 16 lanes on consecutive words and the other 16 lanes 256 words
-//     further: bit 2 of f flips with bit 8 of x, so the halves take opposite bank halves;
-//   stride >= 256 rounds: 32 consecutive words.
-// Every pattern above touches each bank once per 128 bytes moved.
-__device__ __forceinline__ uint32_t swz(uint32_t x) { return x ^ ((((x >> 5) ^ ((x >> 8) << 2)) & 7u) << 2); }
+//   stride-1 rounds of contiguous tiles, 16-byte vectors at a 64-byte lane stride;
+//   stride-16 rounds of contiguous tiles, 16 lanes on consecutive words and the other 16 lanes
+//     256 words further;
+//   stride-1 rounds of strided tiles with C = 4 or 8 columns: 32 / C row groups, 16 C words apart;
+//   every other round: 32 consecutive words.
+// Every pattern above touches each bank once per 128 bytes moved, for every tile shape the passes
+// use except the radix-2 remainder round of a 64-point contiguous transform (2 ways).
+__device__ __forceinline__ uint32_t swz(uint32_t x) {
+    return x ^ ((((x >> 5) ^ (x >> 7) ^ ((x >> 8) << 2)) & 7u) << 2);
+}
 
 // 16-byte asynchronous copy global -> shared (no register staging, so every copy of a thread is in
 // flight at once); both addresses 16-byte aligned.
@@ -143,14 +148,16 @@ __device__ __forceinline__ void cp_async16(uint32_t* smem, const uint32_t* gmem)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Shared-memory address of tile element (m, c).
-template <Layout LAY, int LOGN, int LOGE>
-__device__ __forceinline__ uint32_t sidx(uint32_t m, uint32_t c) {
-    if constexpr (LAY == Layout::Strided) {
-        return swz((m << (LOGE - LOGN)) + c);
-    } else {
-        return swz((c << LOGN) + m);
-    }
+// swz is linear over GF(2) (shifts, XOR and a constant mask), so for index bits that do not
+// overlap, swz(x0 | y) = swz(x0) ^ swz(y). A round's group of R elements sits at
+// x0 | (q << qb) for q < R, with x0's bits [qb, qb + log2 R) zero: one swizzle per group and a
+// compile-time constant per element (the rounds are unrolled, so qb and q are constants).
+// The constant splits into bits 0-4 (XORed into the group's base: at most 8 distinct bases per
+// group, since only bits 2-4 can be set) and bits >= 5, which are zero in b0 (they are x0's bits,
+// zero in [qb, qb + log2 R)) and so add: a register base plus an immediate offset per element.
+__device__ __forceinline__ uint32_t swz_elem(uint32_t b0, uint32_t q, int qb) {
+    const uint32_t k = swz(q << qb);
+    return (b0 ^ (k & 31u)) + (k & ~31u);
 }
 
 // Run the radix rounds of one sub-transform direction over the whole tile.
@@ -178,7 +185,10 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
         if (LRr == 4) {
             constexpr int R = 16;
             constexpr int NG = (1 << LOGE) / R;
-            for (int g = threadIdx.x; g < NG; g += NTHREADS) {
+            static_assert(NG % NTHREADS == 0, "whole groups per thread");
+#pragma unroll 1
+            for (int it = 0; it < NG / NTHREADS; ++it) {
+                const int g = threadIdx.x + it * NTHREADS;
                 uint32_t c, tp, blk;
                 const uint32_t s = 1u << logs;
                 if constexpr (LAY == Layout::Strided) {
@@ -192,15 +202,18 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                     blk = rest & ((1u << (LOGN - logs - 4)) - 1);
                     c = rest >> (LOGN - logs - 4);
                 }
-                uint32_t m0 = blk * (R << logs) + tp;
+                // m0's bits [logs, logs + 4) are zero (tp < s), so element q is at x0 | (q << qb)
+                const uint32_t m0 = (blk << (logs + 4)) | tp;
+                const uint32_t x0 = (LAY == Layout::Strided) ? ((m0 << LOGC) | c) : ((c << LOGN) | m0);
+                const int qb = (LAY == Layout::Strided) ? logs + LOGC : logs;
+                const uint32_t b0 = swz(x0);
                 uint32_t v[R];
                 // A contiguous tile's stride-1 round reads 16 consecutive words: 4 vectors.
                 const bool vec = (LAY == Layout::Contig) && logs == 0;
                 if (vec) {
-                    const uint32_t x0 = (c << LOGN) + m0;
 #pragma unroll
                     for (int q4 = 0; q4 < R / 4; ++q4) {
-                        const uint4 t = *reinterpret_cast<const uint4*>(sm + swz(x0 + 4 * q4));
+                        const uint4 t = *reinterpret_cast<const uint4*>(sm + swz_elem(b0, 4 * q4, 0));
                         v[4 * q4] = t.x;
                         v[4 * q4 + 1] = t.y;
                         v[4 * q4 + 2] = t.z;
@@ -208,21 +221,20 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                     }
                 } else {
 #pragma unroll
-                    for (int q = 0; q < R; ++q) v[q] = sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)];
+                    for (int q = 0; q < R; ++q) v[q] = sm[swz_elem(b0, q, qb)];
                 }
                 if (INV)
                     dit_round<4>(v, tp, logs, stw, p);
                 else
                     dif_round<4>(v, tp, logs, stw, p);
                 if (vec) {
-                    const uint32_t x0 = (c << LOGN) + m0;
 #pragma unroll
                     for (int q4 = 0; q4 < R / 4; ++q4)
-                        *reinterpret_cast<uint4*>(sm + swz(x0 + 4 * q4)) =
+                        *reinterpret_cast<uint4*>(sm + swz_elem(b0, 4 * q4, 0)) =
                             make_uint4(v[4 * q4], v[4 * q4 + 1], v[4 * q4 + 2], v[4 * q4 + 3]);
                 } else {
 #pragma unroll
-                    for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(m0 + (q << logs), c)] = v[q];
+                    for (int q = 0; q < R; ++q) sm[swz_elem(b0, q, qb)] = v[q];
                 }
             }
         } else {
@@ -230,8 +242,11 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
             constexpr int LRX = (REM == 0) ? 1 : REM;
             constexpr int R = 1 << LRX;
             constexpr int NG = (1 << LOGE) / R;
+            static_assert(NG % NTHREADS == 0, "whole groups per thread");
             constexpr int LOGSR = LOGN - LRX;
-            for (int g = threadIdx.x; g < NG; g += NTHREADS) {
+#pragma unroll 2
+            for (int it = 0; it < NG / NTHREADS; ++it) {
+                const int g = threadIdx.x + it * NTHREADS;
                 uint32_t c, tp;
                 if constexpr (LAY == Layout::Strided) {
                     c = g & ((1u << LOGC) - 1);
@@ -240,15 +255,19 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                     tp = g & ((1u << LOGSR) - 1);
                     c = g >> LOGSR;
                 }
+                // tp < 2^LOGSR: element q is at x0 | (q << qb)
+                const uint32_t x0 = (LAY == Layout::Strided) ? ((tp << LOGC) | c) : ((c << LOGN) | tp);
+                constexpr int qb = (LAY == Layout::Strided) ? LOGSR + LOGC : LOGSR;
+                const uint32_t b0 = swz(x0);
                 uint32_t v[R];
 #pragma unroll
-                for (int q = 0; q < R; ++q) v[q] = sm[sidx<LAY, LOGN, LOGE>(tp + ((uint32_t)q << LOGSR), c)];
+                for (int q = 0; q < R; ++q) v[q] = sm[swz_elem(b0, q, qb)];
                 if (INV)
                     dit_round<LRX>(v, tp, LOGSR, stw, p);
                 else
                     dif_round<LRX>(v, tp, LOGSR, stw, p);
 #pragma unroll
-                for (int q = 0; q < R; ++q) sm[sidx<LAY, LOGN, LOGE>(tp + ((uint32_t)q << LOGSR), c)] = v[q];
+                for (int q = 0; q < R; ++q) sm[swz_elem(b0, q, qb)] = v[q];
             }
         }
         __syncthreads();
@@ -279,6 +298,15 @@ __device__ __forceinline__ uint32_t tcol(uint64_t tile, uint32_t c, int logS) {
     return (uint32_t)(((tile & ((1ull << logTpb) - 1)) << LOGC) + c);
 }
 
+// Residue words from the launch's data (or out) pointer to job `job`'s arrays.
+__device__ __forceinline__ uint64_t job_offset(const PassParams& P, uint64_t job) {
+    if (P.comb3) {
+        const uint64_t m = job / 3;
+        return (6 * m + comb_out_slot((int)(job - 3 * m))) * P.comb_slot;
+    }
+    return job * P.job_stride;
+}
+
 // Source limbs of job `job` (first forward pass).
 __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, const uint32_t*& words,
                                            uint64_t& ncoef) {
@@ -301,10 +329,11 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
 template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE>
-__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
+__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
     extern __shared__ uint32_t sm[];
     constexpr int LOGC = LOGE - LOGN;
     constexpr uint32_t E = 1u << LOGE;
+    static_assert(E % (4 * NTHREADS) == 0, "tile copies: whole 16-byte chunks per thread");
     const int j = blockIdx.y;
     const uint32_t p = kPrime(j);
     const int dir = INV ? 1 : 0;
@@ -326,7 +355,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
     uint2* smA = reinterpret_cast<uint2*>(sm + E);
     const uint2* rowB = nullptr;
     if constexpr (LAY == Layout::Strided) {
-        rowB = P.rowB + (size_t)j * (1u << kFsLog);
+        rowB = P.rowB + ((size_t)j << LOGE);  // one table per prime, an entry per tile element
         const uint32_t t0 = tcol<LAY, LOGN, LOGE>(stile, 0, P.logS);
         const int sh = kMaxLogL - P.logNp;
         const uint2* lo = T.fs_lo[dir][j];
@@ -342,20 +371,32 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         if constexpr (INV) __syncthreads();  // used by the load loop below
     }
 
+    // Strided tiles: this thread's chunk `it` is row m_0 + it * (4 NTHREADS / C), column c_0, so its
+    // element index moves by a fixed step per chunk.
+    static_assert(LAY != Layout::Strided || (4 * NTHREADS) % (1u << LOGC) == 0, "chunk rows advance evenly");
+    uint64_t sg0 = 0, sgstep = 0;
+    if constexpr (LAY == Layout::Strided) {
+        const uint32_t e0 = threadIdx.x * 4;
+        sg0 = gidx<LAY, LOGN, LOGE>(stile, e0 >> LOGC, e0 & ((1u << LOGC) - 1), P.logS);
+        sgstep = (uint64_t)((4 * NTHREADS) >> LOGC) << P.logS;
+    }
+
     // A strided tile belongs to one job: its source words are looked up once, not per element.
     const uint32_t* swords = nullptr;
     uint64_t sncoef = 0;
     if constexpr (SRC == Source::Limbs && LAY == Layout::Strided) job_source(P, sjob, swords, sncoef);
 
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
-    for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
+#pragma unroll(LAY == Layout::Strided ? E / (4 * NTHREADS) : 1)
+    for (uint32_t it = 0; it < E / (4 * NTHREADS); ++it) {
+        const uint32_t e4 = threadIdx.x * 4 + it * (NTHREADS * 4);
         uint32_t m, c;
         uint64_t job, g;
         if constexpr (LAY == Layout::Strided) {
             m = e4 >> LOGC;
             c = e4 & ((1u << LOGC) - 1);
             job = sjob;
-            g = gidx<LAY, LOGN, LOGE>(stile, m, c, P.logS);
+            g = sg0 + it * sgstep;
         } else {
             c = e4 >> LOGN;
             m = e4 & ((1u << LOGN) - 1);
@@ -370,7 +411,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         if constexpr (SRC == Source::Residues && FUSE != Fuse::Combine) {
             // residues: an asynchronous copy straight into shared memory (the inverse strided
             // twiddle, if any, is applied below once the copies have landed)
-            cp_async16(sm + swz(e4), P.data + job * P.job_stride + prime_off + g);
+            cp_async16(sm + swz(e4), P.data + job_offset(P, job) + prime_off + g);
         } else if constexpr (SRC == Source::Limbs) {
             // operand words: whole 16-byte groups copied asynchronously, the ragged end (and the
             // zero padding) written directly; reduced modulo p below once landed
@@ -389,12 +430,13 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
             uint4 x;
             if constexpr (FUSE == Fuse::Combine) {
                 // the merge's products in the transform domain (Montgomery: the 2^-32 is in the CRT scale)
-                const uint32_t* slot0 =
-                    P.data + job * P.job_stride + prime_off + g - (uint64_t)(3 + P.comb_k) * P.comb_slot;
+                const uint64_t mrg = job / 3;
+                const int ck = (int)(job - 3 * mrg);
+                const uint32_t* slot0 = P.data + 6 * mrg * P.comb_slot + prime_off + g;
                 auto at = [&](int o) { return *reinterpret_cast<const uint4*>(slot0 + (uint64_t)o * P.comb_slot); };
-                if (P.comb_k == 2) {
+                if (ck == 2) {
                     uint64_t a, b;
-                    node_range(P.comb_a0, P.comb_b0, P.comb_depth, job, a, b);
+                    node_range(P.comb_a0, P.comb_b0, P.comb_depth, mrg, a, b);
                     const int sgn = merge_r_sign(a, b);
                     const uint4 pl = at(0), rl = at(2), qr = at(4), rr = at(5);
                     uint32_t u, v;
@@ -405,7 +447,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
                     PG_RCOMB(x) PG_RCOMB(y) PG_RCOMB(z) PG_RCOMB(w)
 #undef PG_RCOMB
                 } else {
-                    const uint4 l = at(P.comb_k), r = at(P.comb_k + 3);  // Pl Pr or Ql Qr
+                    const uint4 l = at(ck), r = at(ck + 3);  // Pl Pr or Ql Qr
                     x = make_uint4(mul_mont(l.x, r.x, p, pinv), mul_mont(l.y, r.y, p, pinv), mul_mont(l.z, r.z, p, pinv),
                                    mul_mont(l.w, r.w, p, pinv));
                 }
@@ -416,7 +458,9 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
     if constexpr (SRC == Source::Limbs) {
         cp_async_wait_all();  // this thread's copies; each word of its elements reduced modulo p
         const uint32_t one_p = (uint32_t)(0x100000000ull / p);
-        for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
+#pragma unroll(LAY == Layout::Strided ? E / (4 * NTHREADS) : 1)
+        for (uint32_t it = 0; it < E / (4 * NTHREADS); ++it) {
+        const uint32_t e4 = threadIdx.x * 4 + it * (NTHREADS * 4);
             uint4 w = *reinterpret_cast<uint4*>(sm + swz(e4));
             w = make_uint4(reduce_u32(w.x, p, one_p), reduce_u32(w.y, p, one_p), reduce_u32(w.z, p, one_p),
                            reduce_u32(w.w, p, one_p));
@@ -428,7 +472,9 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         if constexpr (INV && LAY == Layout::Strided) {
             // inverse four-step twiddle before the sub-transform: w_{N'}^-(t * bitrev(m)), on the
             // same elements this thread copied
-            for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
+#pragma unroll
+            for (uint32_t it = 0; it < E / (4 * NTHREADS); ++it) {
+        const uint32_t e4 = threadIdx.x * 4 + it * (NTHREADS * 4);
                 const uint32_t m = e4 >> LOGC, c = e4 & ((1u << LOGC) - 1);
                 uint4 x = *reinterpret_cast<uint4*>(sm + swz(e4));
                 fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
@@ -451,11 +497,12 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         tile_transform<LAY, LOGN, LOGE, NTHREADS, false, 0, NROUND - 1>(sm, stw_f, p);
         constexpr int NG = (1 << LOGE) / 16;
 #pragma unroll 1
-        for (uint32_t g = threadIdx.x; g < NG; g += NTHREADS) {
+        for (uint32_t it = 0; it < NG / NTHREADS; ++it) {
+            const uint32_t g = threadIdx.x + it * NTHREADS;
             const uint32_t blk = g & ((1u << (LOGN - 4)) - 1);
             const uint32_t c = g >> (LOGN - 4);
             const uint32_t m0 = blk * 16;
-            const uint32_t x0 = (c << LOGN) + m0;
+            const uint32_t b0 = swz((c << LOGN) | m0);  // vector q4 at swz_elem(b0, 4 q4, 0)
             const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
             const bool live = R < total_rows;
             uint4 o[4];
@@ -471,7 +518,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
             uint32_t v[16];
 #pragma unroll
             for (int q4 = 0; q4 < 4; ++q4) {
-                const uint4 t = *reinterpret_cast<const uint4*>(sm + swz(x0 + 4 * q4));
+                const uint4 t = *reinterpret_cast<const uint4*>(sm + swz_elem(b0, 4 * q4, 0));
                 v[4 * q4] = t.x;
                 v[4 * q4 + 1] = t.y;
                 v[4 * q4 + 2] = t.z;
@@ -494,7 +541,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
             dit_round<4>(v, 0, 0, stw_i, p);
 #pragma unroll
             for (int q4 = 0; q4 < 4; ++q4)
-                *reinterpret_cast<uint4*>(sm + swz(x0 + 4 * q4)) =
+                *reinterpret_cast<uint4*>(sm + swz_elem(b0, 4 * q4, 0)) =
                     make_uint4(v[4 * q4], v[4 * q4 + 1], v[4 * q4 + 2], v[4 * q4 + 3]);
         }
         __syncthreads();
@@ -502,14 +549,16 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
     }
 
     // ---- store
-    for (uint32_t e4 = threadIdx.x * 4; e4 < E; e4 += NTHREADS * 4) {
+#pragma unroll(LAY == Layout::Strided ? E / (4 * NTHREADS) : 1)
+    for (uint32_t it = 0; it < E / (4 * NTHREADS); ++it) {
+        const uint32_t e4 = threadIdx.x * 4 + it * (NTHREADS * 4);
         uint32_t m, c;
         uint64_t job, g;
         if constexpr (LAY == Layout::Strided) {
             m = e4 >> LOGC;
             c = e4 & ((1u << LOGC) - 1);
             job = sjob;
-            g = gidx<LAY, LOGN, LOGE>(stile, m, c, P.logS);
+            g = sg0 + it * sgstep;
         } else {
             c = e4 >> LOGN;
             m = e4 & ((1u << LOGN) - 1);
@@ -522,7 +571,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE>()) ntt_pa
         if constexpr (!INV && LAY == Layout::Strided) {
             fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
         }
-        *reinterpret_cast<uint4*>(P.out + job * P.job_stride + prime_off + g) = x;
+        *reinterpret_cast<uint4*>(P.out + job_offset(P, job) + prime_off + g) = x;
     }
 }
 

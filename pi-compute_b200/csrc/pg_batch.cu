@@ -13,6 +13,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/pi_b200.h"
@@ -140,13 +141,25 @@ std::string job_msg(size_t i, const char* what) { return "job " + std::to_string
 // Residue words per batch array before a bucket is split into several chunks.
 constexpr uint64_t kBatchChunkWords = 256ull << 20;
 
-static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
-    BatchWork* W = ctx_batch(ctx);
-    if (!W) return fail(ctx, PG_ERR_OOM, "batch state");
-    const DeviceTables& T = ctx_tables(ctx);
-    cudaStream_t st = ctx_stream(ctx);
-    uint64_t* launches = ctx_launches(ctx);
+// A validated batch: items sorted by (transform length, kind), cut into chunks that run as one
+// launch per pass each. prepare_batch sizes every buffer for all chunks and uploads the job tables;
+// enqueue_batch then only enqueues kernels and memsets (no allocation, no host wait), so that it can
+// run inside a stream capture (pg_graph_capture_level).
+struct BatchPlan {
+    struct Chunk {
+        uint64_t k0, k1;  // items [k0, k1)
+        int logL;
+        Kind kind;
+        uint64_t maxw;    // longest output in words
+    };
+    std::vector<Chunk> chunks;
+    uint64_t n = 0;       // items
+    std::vector<std::pair<uint64_t*, size_t>> zero;  // outputs of empty products (bytes)
+};
+
+static pg_status prepare_batch(pg_ctx* ctx, BatchWork* W, const pg_job* jobs, size_t njobs, BatchPlan& bp) {
     const size_t maxl = pg_mul_max_limbs();
+    bp = BatchPlan{};
 
     // Validate, zero the outputs of empty products, bucket the rest.
     std::vector<Item> items;
@@ -173,9 +186,8 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
         if (acc && std::min(J.na, nb) + std::min(nc, nd) > ((size_t)1 << 24))
             return fail(ctx, PG_ERR_TOO_LARGE, job_msg(i, "accumulated products exceed the CRT bound"));
         const bool p1 = J.na && nb, p2 = acc && nc && nd;
-        if (!p1 && !p2) {
-            cudaError_t e = cudaMemsetAsync(J.out, 0, top * 8, st);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "memset");
+        if (!p1 && !p2) {  // an empty product: its output is zeroed when the batch is enqueued
+            bp.zero.push_back({J.out, top * 8});
             continue;
         }
         Item it;
@@ -186,6 +198,8 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
         items.push_back(it);
     }
     if (items.empty()) return PG_OK;
+    bp.n = items.size();
+    cudaStream_t st = ctx_stream(ctx);
     std::stable_sort(items.begin(), items.end(), [](const Item& x, const Item& y) {
         return x.logL != y.logL ? x.logL > y.logL : (int)x.kind < (int)y.kind;
     });
@@ -240,40 +254,72 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(W->d_dst, W->h_dst, n * sizeof(DstEntry), cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "batch table copy");
 
-    // Chunks: consecutive items with the same (logL, kind), bounded by the array budget.
-    uint64_t k0 = 0;
-    while (k0 < n) {
-        const int logL = items[k0].logL;
-        const Kind kind = items[k0].kind;
-        const uint64_t L = 1ull << logL;
-        const uint64_t per = 3 * L;
+    // Chunks: consecutive items with the same (logL, kind), bounded by the array budget; every
+    // buffer sized for the largest chunk before anything is enqueued.
+    uint64_t res_need = 0, sync_need = 0;
+    for (uint64_t k0 = 0; k0 < n;) {
+        BatchPlan::Chunk ch;
+        ch.k0 = k0;
+        ch.logL = items[k0].logL;
+        ch.kind = items[k0].kind;
+        const uint64_t per = 3ull << ch.logL;
         const uint64_t fit = std::max<uint64_t>(1, kBatchChunkWords / per);
         uint64_t k1 = k0;
-        uint64_t maxw = 0;
-        while (k1 < n && k1 - k0 < fit && items[k1].logL == logL && items[k1].kind == kind) {
-            maxw = std::max(maxw, items[k1].nwords);
+        ch.maxw = 0;
+        while (k1 < n && k1 - k0 < fit && items[k1].logL == ch.logL && items[k1].kind == ch.kind) {
+            ch.maxw = std::max(ch.maxw, items[k1].nwords);
             ++k1;
         }
+        ch.k1 = k1;
         const uint64_t m = k1 - k0;
-        if (m * per > W->res_cap) {
-            const uint64_t want = std::max(m * per, W->res_cap + W->res_cap / 2);
-            for (auto*& r : W->res) {
-                if (r) cudaFree(r);
-                r = nullptr;
-            }
-            W->res_cap = 0;
-            for (auto*& r : W->res) {
-                e = pg::dev_malloc((void**)&r, want * 4);
-                if (e != cudaSuccess) {
-                    for (auto*& q : W->res) {
-                        if (q) cudaFree(q);
-                        q = nullptr;
-                    }
-                    return cuda_fail(ctx, e, "batch residues");
-                }
-            }
-            W->res_cap = want;
+        const uint64_t bpj = (ch.maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+        res_need = std::max(res_need, m * per);
+        sync_need = std::max(sync_need, m + m * bpj);
+        bp.chunks.push_back(ch);
+        k0 = k1;
+    }
+    if (res_need > W->res_cap) {
+        const uint64_t want = std::max(res_need, W->res_cap + W->res_cap / 2);
+        for (auto*& r : W->res) {
+            if (r) cudaFree(r);
+            r = nullptr;
         }
+        W->res_cap = 0;
+        for (auto*& r : W->res) {
+            e = pg::dev_malloc((void**)&r, want * 4);
+            if (e != cudaSuccess) {
+                for (auto*& q : W->res) {
+                    if (q) cudaFree(q);
+                    q = nullptr;
+                }
+                return cuda_fail(ctx, e, "batch residues");
+            }
+        }
+        W->res_cap = want;
+    }
+    e = grow_dev(&W->sync, W->sync_cap, sync_need);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch sync words");
+    return PG_OK;
+}
+
+static pg_status enqueue_batch(pg_ctx* ctx, BatchWork* W, const BatchPlan& bp, uint64_t* launches) {
+    const DeviceTables& T = ctx_tables(ctx);
+    cudaStream_t st = ctx_stream(ctx);
+    const uint64_t n = bp.n;
+    cudaError_t e = cudaSuccess;
+    for (const auto& z : bp.zero)
+        if ((e = cudaMemsetAsync(z.first, 0, z.second, st)) != cudaSuccess) return cuda_fail(ctx, e, "memset");
+    if (n == 0) return PG_OK;
+    e = cudaMemsetAsync(W->errw, 0, 4, st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "batch error word");
+    for (const BatchPlan::Chunk& ch : bp.chunks) {
+        const uint64_t k0 = ch.k0;
+        const int logL = ch.logL;
+        const Kind kind = ch.kind;
+        const uint64_t L = 1ull << logL;
+        const uint64_t per = 3 * L;
+        const uint64_t m = ch.k1 - ch.k0;
+        const uint64_t maxw = ch.maxw;
         const Plan plan = T.plan(logL);
         const int last = plan.npass - 1;
         auto base = [&](uint32_t* data, int slot) {
@@ -335,8 +381,7 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
         if (e != cudaSuccess) return cuda_fail(ctx, e, "batch passes");
         // CRT + carry over the chunk.
         const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
-        e = grow_dev(&W->sync, W->sync_cap, m + m * bpj);
-        if (e == cudaSuccess) e = cudaMemsetAsync(W->sync, 0, (m + m * bpj) * 4, st);
+        e = cudaMemsetAsync(W->sync, 0, (m + m * bpj) * 4, st);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "batch sync words");
         CrtParams c{};
         c.res = prod;
@@ -352,11 +397,15 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
         e = launch_crt(c, m * bpj, st, maxw);
         if (e != cudaSuccess) return cuda_fail(ctx, e, "batch CRT");
         ++*launches;
-        k0 = k1;
     }
-    // Wait, then read and clear the error word.
+    return PG_OK;
+}
+
+// Wait for the enqueued batch, then read and clear the error word.
+static pg_status finish_batch(pg_ctx* ctx, BatchWork* W) {
+    cudaStream_t st = ctx_stream(ctx);
     uint32_t err = 0;
-    e = cudaMemcpyAsync(&err, W->errw, 4, cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaMemcpyAsync(&err, W->errw, 4, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "batch");
     if (err) {
@@ -366,6 +415,17 @@ static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
         return fail(ctx, PG_ERR_BAD_ARG, "a job's result is negative (acc = -1 with a*b < c*d)");
     }
     return PG_OK;
+}
+
+static pg_status run_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
+    BatchWork* W = ctx_batch(ctx);
+    if (!W) return fail(ctx, PG_ERR_OOM, "batch state");
+    BatchPlan bp;
+    pg_status s = prepare_batch(ctx, W, jobs, njobs, bp);
+    if (s != PG_OK) return s;
+    s = enqueue_batch(ctx, W, bp, ctx_launches(ctx));
+    if (s != PG_OK || bp.n == 0) return s;
+    return finish_batch(ctx, W);
 }
 
 }  // namespace pg
@@ -379,6 +439,96 @@ pg_status pg_mul_batch(pg_ctx* ctx, const pg_job* jobs, size_t njobs) {
     cudaError_t e = cudaSetDevice(pg::ctx_device(ctx));
     if (e != cudaSuccess) return pg::cuda_fail(ctx, e, "cudaSetDevice");
     return pg::run_batch(ctx, jobs, njobs);
+}
+
+}  // extern "C"
+
+// A captured level: its own buffers (so that later batches on the context, which may regrow the
+// context's buffers, never move memory the graph points at) and the instantiated graph.
+struct pg_graph {
+    pg_ctx* ctx = nullptr;
+    pg::BatchWork* W = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t launches = 0;  // kernels per replay
+    uint64_t njobs = 0;     // products with work (empty products only zero their outputs)
+};
+
+extern "C" {
+
+pg_status pg_graph_capture_level(pg_ctx* ctx, const pg_job* jobs, size_t njobs, pg_graph** out) {
+    if (!ctx || !out || (njobs && !jobs)) return PG_ERR_BAD_ARG;
+    *out = nullptr;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaError_t e = cudaSetDevice(pg::ctx_device(ctx));
+    if (e != cudaSuccess) return pg::cuda_fail(ctx, e, "cudaSetDevice");
+    pg_graph* g = new (std::nothrow) pg_graph;
+    if (!g) return PG_ERR_OOM;
+    g->ctx = ctx;
+    g->W = pg::batch_state_new();
+    if (!g->W) {
+        delete g;
+        return PG_ERR_OOM;
+    }
+    auto drop = [&](pg_status s) {
+        pg::batch_state_delete(g->W);
+        delete g;
+        return s;
+    };
+    // Validation, buffer sizing and the job tables' upload happen before the capture; the
+    // capture records only kernels and memsets.
+    pg::BatchPlan bp;
+    pg_status s = pg::prepare_batch(ctx, g->W, jobs, njobs, bp);
+    if (s != PG_OK) return drop(s);
+    cudaStream_t st = pg::ctx_stream(ctx);
+    e = cudaStreamSynchronize(st);  // the tables are in place before the graph is first replayed
+    if (e != cudaSuccess) return drop(pg::cuda_fail(ctx, e, "stream"));
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return drop(pg::cuda_fail(ctx, e, "begin capture"));
+    uint64_t counted = 0;
+    s = pg::enqueue_batch(ctx, g->W, bp, &counted);
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamEndCapture(st, &graph);
+    if (s != PG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        return drop(s);
+    }
+    if (e != cudaSuccess) return drop(pg::cuda_fail(ctx, e, "end capture"));
+    e = cudaGraphInstantiate(&g->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        g->exec = nullptr;
+        return drop(pg::cuda_fail(ctx, e, "graph instantiate"));
+    }
+    g->launches = counted;
+    g->njobs = bp.n;
+    *out = g;
+    return PG_OK;
+}
+
+pg_status pg_graph_launch(pg_graph* g) {
+    if (!g || !g->exec) return PG_ERR_BAD_ARG;
+    pg_ctx* ctx = g->ctx;
+    std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    cudaError_t e = cudaSetDevice(pg::ctx_device(ctx));
+    if (e != cudaSuccess) return pg::cuda_fail(ctx, e, "cudaSetDevice");
+    e = cudaGraphLaunch(g->exec, pg::ctx_stream(ctx));
+    if (e != cudaSuccess) return pg::cuda_fail(ctx, e, "graph launch");
+    *pg::ctx_launches(ctx) += g->launches;
+    if (g->njobs == 0) return cudaStreamSynchronize(pg::ctx_stream(ctx)) == cudaSuccess ? PG_OK : PG_ERR_DEVICE;
+    return pg::finish_batch(ctx, g->W);
+}
+
+void pg_graph_destroy(pg_graph* g) {
+    if (!g) return;
+    {
+        std::lock_guard<std::mutex> lock(pg::ctx_mutex(g->ctx));
+        cudaSetDevice(pg::ctx_device(g->ctx));
+        cudaStreamSynchronize(pg::ctx_stream(g->ctx));
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        pg::batch_state_delete(g->W);
+    }
+    delete g;
 }
 
 pg_status pg_buf_alloc(pg_ctx* ctx, size_t cap, pg_buf** out) {

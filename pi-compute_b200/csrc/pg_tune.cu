@@ -1,6 +1,6 @@
 // Autotuner of the pass split (pg_tune, pg_tune_save, pg_tune_load).
 //
-// For each transform length 2^logL the product can run as one contiguous pass (logL <= 13)
+// For each transform length 2^logL the product can run as one contiguous pass (logL <= 14)
 // or as 2 or 3 passes whose lengths multiply to 2^logL (plan_valid lists the constraints).
 // pg_tune times every valid split on the device with a balanced product of that length,
 // checks that it reproduces the built-in plan's product word for word, and keeps the fastest.
@@ -31,7 +31,7 @@ namespace {
 // Every valid split of 2^logL points.
 std::vector<Plan> candidates(int logL) {
     std::vector<Plan> out;
-    if (logL <= kTileLog) {
+    if (logL <= kMaxContigLog) {
         const int n[1] = {logL};
         Plan p = plan_from(logL, 1, n);
         if (plan_valid(p)) out.push_back(p);

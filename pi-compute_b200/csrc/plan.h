@@ -5,9 +5,18 @@
 
 namespace pg {
 
-constexpr int kTileLog = 13;        // E = 2^13 residues per CTA tile (32 KB of shared memory)
+constexpr int kTileLog = 13;        // E = 2^13 residues per CTA tile (32 KB of shared memory) ...
+constexpr int kTileLogBig = 14;     // ... or 2^14 (64 KB) for the longest sub-transforms
 constexpr int kMinLogL = 6;         // smallest transform (64 points)
-constexpr int kMaxStridedLog = 10;  // strided passes keep >= 8 adjacent columns per tile
+constexpr int kMaxStridedLog = 12;  // strided passes keep >= 4 adjacent columns per tile
+constexpr int kMaxContigLog = 14;   // contiguous passes hold whole sub-transforms of up to 2^14 points
+
+// Tile of a pass: 2^13 residues, or 2^14 for strided sub-transforms of 2^11 and 2^12 points (8 and 4
+// columns of 16 and 32 bytes, coalesced with the neighbouring tile in L2) and contiguous ones of 2^14.
+// The large tiles make 2^24..2^26-point transforms two passes instead of three.
+constexpr int tile_log(bool strided, int logN) {
+    return strided ? (logN <= 10 ? kTileLog : kTileLogBig) : (logN <= kTileLog ? kTileLog : kTileLogBig);
+}
 
 struct Plan {
     int logL = 0;
@@ -16,7 +25,8 @@ struct Plan {
     int logS[3] = {0, 0, 0};   // element stride of each pass
 };
 
-// Pass split for L = 2^logL: one contiguous pass up to 2^13, two passes up to 2^23, three to 2^26.
+// Pass split for L = 2^logL: one contiguous pass up to 2^13, two passes above (a contiguous last
+// pass of 2^13 points up to 2^23, of 2^14 points from 2^24 to 2^26).
 inline Plan make_plan(int logL) {
     Plan p;
     p.logL = logL;
@@ -27,16 +37,14 @@ inline Plan make_plan(int logL) {
         p.npass = 2;
         p.logN[0] = logL / 2;
         p.logN[1] = logL - logL / 2;
-    } else if (logL <= kTileLog + kMaxStridedLog) {
+    } else if (logL <= kTileLog + 10) {
         p.npass = 2;
         p.logN[0] = logL - kTileLog;
         p.logN[1] = kTileLog;
     } else {
-        p.npass = 3;
-        int rest = logL - kTileLog;
-        p.logN[0] = rest / 2;
-        p.logN[1] = rest - rest / 2;
-        p.logN[2] = kTileLog;
+        p.npass = 2;
+        p.logN[0] = logL - kMaxContigLog;
+        p.logN[1] = kMaxContigLog;
     }
     int s = logL;
     for (int i = 0; i < p.npass; ++i) {
@@ -46,8 +54,8 @@ inline Plan make_plan(int logL) {
     return p;
 }
 
-// Whether a pass split can run: one contiguous last pass of 2^6..2^13 points, strided passes of
-// 2^5..2^10 points whose tiles (2^(13 - N) columns) fit in their stride, every strided pass's
+// Whether a pass split can run: one contiguous last pass of 2^6..2^14 points, strided passes of
+// 2^5..2^12 points whose tiles (2^(tile_log - N) columns) fit in their stride, every strided pass's
 // four-step block at least 2^14 points (the row power tables' range), lengths summing to logL.
 inline bool plan_valid(const Plan& p) {
     if (p.npass < 1 || p.npass > 3) return false;
@@ -55,13 +63,13 @@ inline bool plan_valid(const Plan& p) {
     for (int i = 0; i < p.npass; ++i) sum += p.logN[i];
     if (sum != p.logL) return false;
     const int last = p.npass - 1;
-    if (p.logN[last] < kMinLogL || p.logN[last] > kTileLog) return false;
+    if (p.logN[last] < kMinLogL || p.logN[last] > kMaxContigLog) return false;
     int s = p.logL;
     for (int i = 0; i < last; ++i) {
         s -= p.logN[i];  // stride of pass i
         if (p.logN[i] < 5 || p.logN[i] > kMaxStridedLog) return false;
-        if (s < kTileLog - p.logN[i]) return false;     // C = 2^(13 - N) columns <= S
-        if (p.logN[i] + s < 14) return false;           // four-step block >= 2^14
+        if (s < tile_log(true, p.logN[i]) - p.logN[i]) return false;  // C columns <= S
+        if (p.logN[i] + s < 14) return false;                          // four-step block >= 2^14
     }
     return true;
 }

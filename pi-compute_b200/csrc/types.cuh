@@ -16,7 +16,8 @@ __host__ __device__ inline int __builtin_clz_portable(uint32_t x) {
 #endif
 }
 
-constexpr int kStageLog = 14;  // stage twiddles come from w_{2^14}: sub-transforms up to 2^13 points
+constexpr int kStageLog = 14;  // stage twiddles come from w_{2^14}: sub-transforms up to 2^14 points
+constexpr int kStageEnt = 1 << 14;  // entries per stage table (entry h + x for h <= 2^13)
 constexpr int kFsLog = 13;     // four-step twiddles: w_{2^26}^e = lo[e & 8191] * hi[e >> 13]
 
 // Exponent of w_{2^14} stored at stage-table entry i = h + x (h = 2^k <= i < 2h): w_{2h}^x.
@@ -27,12 +28,14 @@ __host__ __device__ inline uint32_t stage_exponent(uint32_t i) {
 }
 
 constexpr int kRowLogMin = 14;  // row tables exist for four-step blocks of 2^14 .. 2^26 points
-constexpr int kRowNMin = 5, kRowNMax = 10;  // and strided sub-transforms of 2^5 .. 2^10 points
+constexpr int kRowNMin = 5, kRowNMax = 10;  // and strided sub-transforms of 2^5 .. 2^10 points (2^13 tiles)
+constexpr int kRowNBigMin = 11, kRowNBigMax = 12;  // or of 2^11 .. 2^12 points (2^14 tiles)
 constexpr int kRowTables = (kMaxLogL - kRowLogMin + 1) * (kRowNMax - kRowNMin + 1);  // per (dir, prime)
+constexpr int kRowTablesBig = (kMaxLogL - kRowLogMin + 1) * (kRowNBigMax - kRowNBigMin + 1);
 
 struct TwiddleTables {
     // (w, w') Shoup pairs, [dir][prime]; dir 0 = forward (w), 1 = inverse (w^-1).
-    const uint2* stage[2][kNumPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), 2^13 entries
+    const uint2* stage[2][kNumPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), kStageEnt entries
     const uint2* fs_lo[2][kNumPrimes];  // w_{2^26}^j,           j < 2^13
     const uint2* fs_hi[2][kNumPrimes];  // w_{2^26}^(2^13 * i),  i < 2^13
     // Four-step factors of strided tiles: for a block of N' = 2^n points split into sub-transforms
@@ -40,18 +43,27 @@ struct TwiddleTables {
     // (((n - kRowLogMin) * 6 + l - kRowNMin) * 2 + dir) * kNumPrimes + prime holds
     // w_{N'}^(c * bitrev_l(m)) at entry m * C + c (row-major, so a tile row reads consecutively).
     const uint2* row;
-    // 0: the layout above for every (n, l); 1: only (14, 7) then (15, 7) (the fixed-size tables
+    // The same for sub-transforms of 2^11 and 2^12 points in tiles of 2^14 (C = 2^(14 - l) columns,
+    // 2^14 entries): table (((n - kRowLogMin) * 2 + l - kRowNBigMin) * 2 + dir) * kNumPrimes + prime.
+    const uint2* row_big;
+    // 0: the layouts above for every (n, l); 1: only (14, 7) then (15, 7) (the fixed-size tables
     // of pg_mul_noalloc), [n][dir][prime].
     int row_layout;
 };
 
-// Prime-0 four-step factor table of a strided pass (prime j at + j * 2^13), or null.
+// Prime-0 four-step factor table of a strided pass (prime j at + j * 2^(tile log)), or null.
 inline const uint2* row_table(const TwiddleTables& T, int logNp, int logN, int dir) {
     if (T.row_layout == 1) {
         if (logN != 7 || logNp < 14 || logNp > 15) return nullptr;
         return T.row + ((size_t)((logNp - 14) * 2 + dir) * kNumPrimes) * (1u << kFsLog);
     }
-    if (logNp < kRowLogMin || logNp > kMaxLogL || logN < kRowNMin || logN > kRowNMax) return nullptr;
+    if (logNp < kRowLogMin || logNp > kMaxLogL) return nullptr;
+    if (logN >= kRowNBigMin && logN <= kRowNBigMax) {
+        if (!T.row_big) return nullptr;
+        const int t = ((logNp - kRowLogMin) * (kRowNBigMax - kRowNBigMin + 1) + (logN - kRowNBigMin)) * 2 + dir;
+        return T.row_big + ((size_t)t * kNumPrimes) * (1u << 14);
+    }
+    if (logN < kRowNMin || logN > kRowNMax) return nullptr;
     const int t = ((logNp - kRowLogMin) * (kRowNMax - kRowNMin + 1) + (logN - kRowNMin)) * 2 + dir;
     return T.row + ((size_t)t * kNumPrimes) * (1u << kFsLog);
 }
@@ -91,6 +103,10 @@ struct MergeSrc {
     const uint32_t* len;
 };
 
+// Operand slot a merge's output k (0 P^ = Pl Pr, 1 Q^ = Ql Qr, 2 R^ = Qr Rl +- Pl Rr) is written
+// over: Pr, Ql and Rr, each read only by the output that overwrites it.
+__host__ __device__ constexpr int comb_out_slot(int k) { return k == 0 ? 3 : (k == 1 ? 1 : 5); }
+
 struct PassParams {
     uint32_t* data;          // residues of job 0: prime i at data + i*L; job j at data + j*job_stride
     const uint32_t* other;   // Fuse::MulInverse: fully transformed other operand (same layout)
@@ -110,9 +126,12 @@ struct PassParams {
     MergeSrc ms;
     const SrcEntry* src;
     const uint2* rowB;       // strided passes: four-step factor table of prime 0 (set by launch_pass)
-    // Fuse::Combine: output k (0 P^, 1 Q^, 2 R^) of merge `job`, written over operand slot 3 + k;
-    // operand o (Pl Ql Rl Pr Qr Rr) of that merge lies (o - 3 - k) * comb_slot words from it
-    int comb_k;
+    // comb3 = 1 (the splitting's Fuse::Combine pass and the inverse passes after it): job j of the
+    // launch is output k = j % 3 (0 P^, 1 Q^, 2 R^) of merge m = j / 3. Merge m's operands o (Pl Ql
+    // Rl Pr Qr Rr) are at data + (6 m + o) * comb_slot, and output k is written over operand slot
+    // comb_out_slot(k), which no other output of the merge reads, so all three outputs of every
+    // merge run in one launch.
+    int comb3;
     uint64_t comb_slot;
     uint64_t comb_a0, comb_b0;  // the splitting's range and this level's depth (R's sign per merge)
     int comb_depth;
@@ -146,7 +165,7 @@ struct CrtParams {
     // out + i * out_stride, its length (if dlen) at dlen[i]; every job has `nwords` words.
     uint64_t out_stride;
     // merge batch: job = 3 * merge + {P, Q, R}; residues of merge m, output k (0..2) at
-    // res + (6m + 3 + k) * res_stride; the words go to dst[k] + m * dcap[k] (limbs), the
+    // res + (6m + comb_out_slot(k)) * res_stride; the words go to dst[k] + m * dcap[k] (limbs), the
     // length to dlen[3m + k]; node ranges of the level come from [a0, b0) and depth.
     int merge;
     uint64_t res_stride;

@@ -99,3 +99,72 @@ def test_batch_errors(eng):
     # the context stays usable after the error
     a, b = rnd(300, 5), rnd(200, 6)
     assert eng.mul_batch([(a, b)]) == [gmp(a, b)]
+
+
+def test_captured_level_replays_over_new_operands(eng):
+    # One level of products (mul, square, a*b + c*d, a*b - c*d, an empty product) captured once
+    # (pg_graph_capture_level), replayed twice over new operand contents in the same buffers, with
+    # an unrelated batch on the context in between; every replay equals the oracle.
+    import ctypes
+
+    lib = eng.lib
+    shapes = [(700, 300), (2048, None), (500, 400, 450, 420, 1), (900, 800, 600, 500, -1), (0, 64)]
+    bufs, jobs, outs = [], [], []
+
+    def operand(n, seed, big=False):
+        x = pkg.random_operand(n, seed)
+        if big and n:
+            x[-1] |= np.uint64(1 << 63)
+        return x
+
+    for i, sh in enumerate(shapes):
+        na, nb = sh[0], sh[1]
+        acc = sh[4] if len(sh) > 2 else 0
+        nc, nd = (sh[2], sh[3]) if acc else (0, 0)
+        ba = eng.buffer(operand(na, 10 + i)) if na else eng.buffer(np.zeros(2, dtype=np.uint64))
+        bb = eng.buffer(operand(nb, 20 + i)) if nb else None
+        bc = eng.buffer(operand(nc, 30 + i)) if acc else None
+        bd = eng.buffer(operand(nd, 40 + i)) if acc else None
+        top = max(na + (nb if nb is not None else na), nc + nd) + (1 if acc > 0 else 0)
+        bo = pkg.DeviceBuffer(eng, max(top, 1), None)
+        bufs.append((ba, bb, bc, bd, bo, top, na, nb, nc, nd, acc))
+        jobs.append(pkg.PgJob(ba.ptr, na, bb.ptr if bb else None, nb or 0, bc.ptr if bc else None, nc,
+                              bd.ptr if bd else None, nd, acc, bo.ptr, bo.cap))
+    arr = (pkg.PgJob * len(jobs))(*jobs)
+    g = ctypes.c_void_p()
+    assert lib.pg_graph_capture_level(eng.ctx, arr, len(jobs), ctypes.byref(g)) == pkg.PG_OK
+    try:
+        for rep in range(2):
+            exp = []
+            for i, (ba, bb, bc, bd, bo, top, na, nb, nc, nd, acc) in enumerate(bufs):
+                # new contents of the same lengths (for acc = -1, a*b stays larger than c*d)
+                seed = 1000 * (rep + 1) + i
+                A = operand(na, seed, big=True)
+                if na:
+                    assert lib.pg_buf_upload(eng.ctx, ba.h, A.ctypes.data_as(pkg._u64p), na) == 0
+                a = pkg.limbs_to_int(A)
+                b = a
+                if nb:
+                    B = operand(nb, seed + 1, big=True)
+                    assert lib.pg_buf_upload(eng.ctx, bb.h, B.ctypes.data_as(pkg._u64p), nb) == 0
+                    b = pkg.limbs_to_int(B)
+                v = gmp(a, b) if na else 0
+                if acc:
+                    C, D = operand(nc, seed + 2), operand(nd, seed + 3)
+                    assert lib.pg_buf_upload(eng.ctx, bc.h, C.ctypes.data_as(pkg._u64p), nc) == 0
+                    assert lib.pg_buf_upload(eng.ctx, bd.h, D.ctypes.data_as(pkg._u64p), nd) == 0
+                    v += acc * gmp(pkg.limbs_to_int(C), pkg.limbs_to_int(D))
+                exp.append(v)
+            # an unrelated batch between replays
+            x, y = rnd(3000, 5 + rep), rnd(2000, 6 + rep)
+            assert eng.mul_batch([(x, y)]) == [gmp(x, y)]
+            assert lib.pg_graph_launch(g) == pkg.PG_OK
+            for (ba, bb, bc, bd, bo, top, *_), v in zip(bufs, exp):
+                bo.set_len(top)
+                assert pkg.limbs_to_int(bo.download()) == v
+    finally:
+        lib.pg_graph_destroy(g)
+        for t in bufs:
+            for x in t[:5]:
+                if x is not None:
+                    x.free()
