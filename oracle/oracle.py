@@ -170,3 +170,51 @@ def ref_pi(digits: int, threads: int = 1) -> str:
 def ref_mul(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     """Product through the reference's own GmpMultiplier::multiply (compiled from its sources)."""
     return _mul(ref().ref_gmp_mul, a, b)
+
+
+# ------------------------------------------------------------------ the reference with the drop-in
+LIBPIREF_B200 = os.path.join(HERE, "_ref", "libpiref_b200.so")
+_rb = None
+
+
+def refb() -> ctypes.CDLL:
+    """oracle/_ref/libpiref_b200.so: the reference's own BinarySplitting and PiEngine, compiled
+    unchanged, with this build's pi::B200Multiplier behind their Multiplier& (needs a GPU to run)."""
+    global _rb
+    if _rb is None:
+        r = ctypes.CDLL(LIBPIREF_B200)
+        r.refb_bs.argtypes = [ctypes.c_ulong, ctypes.c_ulong, ctypes.c_uint, ctypes.c_size_t, ctypes.c_int,
+                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_ulonglong)]
+        r.refb_bs.restype = ctypes.c_int
+        r.refb_pi.argtypes = [ctypes.c_ulong, ctypes.c_uint, ctypes.c_size_t, ctypes.c_int,
+                              ctypes.POINTER(ctypes.c_ulonglong)]
+        r.refb_pi.restype = ctypes.c_void_p
+        r.refb_free.argtypes = [ctypes.c_void_p]
+        _rb = r
+    return _rb
+
+
+def refb_bs(a: int, b: int, threshold: int, threads: int = 1, device: int = 0):
+    """(P, Q, R, products on the B200) from the reference's BinarySplitting::compute over B200Multiplier."""
+    r = refb()
+    ps = [ctypes.c_void_p() for _ in range(3)]
+    calls = ctypes.c_ulonglong(0)
+    if r.refb_bs(a, b, threads, threshold, device, *(ctypes.byref(p) for p in ps), ctypes.byref(calls)) != 0:
+        raise RuntimeError("refb_bs failed")
+    out = []
+    for p in ps:
+        out.append(int(ctypes.cast(p, ctypes.c_char_p).value.decode(), 16))
+        r.refb_free(p)
+    return out[0], out[1], out[2], calls.value
+
+
+def refb_pi(digits: int, threshold: int, threads: int = 1, device: int = 0):
+    """("3." + digits, products on the B200) from the reference's PiEngine over B200Multiplier."""
+    r = refb()
+    calls = ctypes.c_ulonglong(0)
+    p = r.refb_pi(digits, threads, threshold, device, ctypes.byref(calls))
+    if not p:
+        raise RuntimeError("refb_pi failed")
+    s = ctypes.cast(p, ctypes.c_char_p).value.decode()
+    r.refb_free(p)
+    return s, calls.value

@@ -81,8 +81,11 @@ def build_host() -> str:
     flags = ["-O3", "-std=c++17", "-fPIC", "-pthread", "-Wall", "-I", HOST, "-I", INCLUDE, "-I", cuda_inc]
     rpath = ["-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.dirname(GMP_SO)]
     if _newer(LIBPIB200, lib_srcs + hdr + [LIBPIGPU]):
-        _run([CXX, *flags, "-shared", "-o", LIBPIB200, *lib_srcs, LIBPIGPU, GMP_SO, "-L", cuda_lib, "-lcudart",
-              *rpath])
+        # -Bsymbolic: the library's own classes (pi::BinarySplitting, pi::PiEngine, ...) always bind to
+        # their definitions here, even in a process that also loads another library with classes of the
+        # same names (the test shim that runs the reference's own sources with B200Multiplier).
+        _run([CXX, *flags, "-shared", "-Wl,-Bsymbolic", "-o", LIBPIB200, *lib_srcs, LIBPIGPU, GMP_SO, "-L", cuda_lib,
+              "-lcudart", *rpath])
     main = os.path.join(HOST, "main.cpp")
     if os.path.exists(main) and _newer(PI_B200, [main, LIBPIB200] + hdr):
         _run([CXX, *flags, "-o", PI_B200, main, LIBPIB200, LIBPIGPU, GMP_SO, "-L", cuda_lib, "-lcudart", *rpath])

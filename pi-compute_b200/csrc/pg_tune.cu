@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -145,6 +146,9 @@ pg_status pg_tune(pg_ctx* ctx, int lo, int hi, double* best_us) {
             if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ev0, ev1);
             if (e != cudaSuccess) break;
             const double us = 1e3 * ms / reps;
+            if (std::getenv("PG_TUNE_VERBOSE"))
+                std::fprintf(stderr, "[pg_tune] logL %d split %d %d %d (%d passes): %.1f us\n", logL, p.logN[0],
+                             p.npass > 1 ? p.logN[1] : 0, p.npass > 2 ? p.logN[2] : 0, p.npass, us);
             if (us < best) {
                 best = us;
                 best_plan = p;
