@@ -120,6 +120,214 @@ __device__ __forceinline__ CrtJob crt_job(const CrtParams& P, uint64_t job) {
     return J;
 }
 
+// Carry resolution of one block: each thread holds the signed sums W[0..NW) of NW consecutive output
+// words (thread order = word order; the block is number `bid` of its job, j0 = this thread's first
+// word); the carries between words lie in {-1, 0, 1, 2}. Per-thread carry transfer functions are
+// composed by a warp scan, a block scan and the decoupled look-back across blocks; o receives the
+// exact words and top the index of this thread's highest non-zero word below nwords (-1: none).
+template <int NW, int NT = kCrtThreads>
+__device__ __forceinline__ void carry_resolve(const int64_t (&W)[NW], uint32_t (&o)[NW], int& top, uint32_t bid,
+                                              uint64_t j0, uint64_t nwords, volatile uint32_t* st, const CrtParams& P,
+                                              uint32_t (&s_wagg)[NT / 32], uint32_t& s_carry_in) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t f;
+    {
+        int64_t acc = 0;
+        bool ones_hi = true, zero_hi = true;
+        uint32_t low0 = 0;
+#pragma unroll
+        for (int u = 0; u < NW; ++u) {
+            acc += W[u];
+            uint32_t o = (uint32_t)acc;
+            if (u == 0) {
+                low0 = o;
+            } else {
+                ones_hi &= (o == 0xffffffffu);
+                zero_hi &= (o == 0u);
+            }
+            acc >>= 32;  // arithmetic: floor division by 2^32
+        }
+        const int c0 = (int)acc;
+        const int fm1 = c0 - ((zero_hi && low0 == 0u) ? 1 : 0);
+        const int f1 = c0 + ((ones_hi && low0 == 0xffffffffu) ? 1 : 0);
+        const int f2 = c0 + ((ones_hi && low0 >= 0xfffffffeu) ? 1 : 0);
+        f = (uint32_t)(fm1 + 1) | ((uint32_t)(c0 + 1) << 2) | ((uint32_t)(f1 + 1) << 4) | ((uint32_t)(f2 + 1) << 6);
+    }
+
+    // Warp inclusive scan of transfer functions (lane order = word order).
+    uint32_t incl = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = fcompose(incl, o);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = kFIdentity;
+    if (lane == 31) s_wagg[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        // Exclusive prefix over the block's warps, block aggregate in lane NWARP - 1.
+        constexpr int NWARP = NT / 32;
+        uint32_t wf = (lane < NWARP) ? s_wagg[lane] : kFIdentity;
+        uint32_t wincl = wf;
+#pragma unroll
+        for (int off = 1; off < NWARP; off <<= 1) {
+            uint32_t o = __shfl_up_sync(0xffffffffu, wincl, off);
+            if (lane >= off) wincl = fcompose(wincl, o);
+        }
+        uint32_t wexcl = __shfl_up_sync(0xffffffffu, wincl, 1);
+        if (lane == 0) wexcl = kFIdentity;
+        const uint32_t blk = __shfl_sync(0xffffffffu, wincl, NWARP - 1);
+        __syncwarp();
+        if (lane < NWARP) s_wagg[lane] = wexcl;
+
+        // Decoupled look-back, one window of 32 predecessors per step (lane l reads block
+        // base - l). The window's functions compose into one; the nearest block that already
+        // knows its carry out ends the walk. Carries are stored as u = carry + 1.
+        uint32_t u_in = 1;
+        const bool publish = bid + 1 != P.withhold1;  // false only under the test hook
+        const uint32_t spin_limit = P.spin_limit ? P.spin_limit : kSpinLimit;
+        if (bid == 0) {
+            if (lane == 0 && publish) st[0] = kStIncl | (fapply(blk, 1) << 8);
+        } else {
+            if (lane == 0 && publish) {
+                __threadfence();
+                st[bid] = kStAgg | (blk << 8);
+            }
+            uint32_t look = kFIdentity;
+            int64_t base = (int64_t)bid - 1;
+            uint32_t spins = 0;
+            while (true) {
+                const int64_t jb = base - lane;
+                const uint32_t v = (jb >= 0) ? st[jb] : (uint32_t)(kStIncl | (1u << 8));  // before block 0: carry 0
+                const uint32_t sv = v & 0xffu;
+                const unsigned incl_mask = __ballot_sync(0xffffffffu, sv == kStIncl);
+                const unsigned none_mask = __ballot_sync(0xffffffffu, sv == kStNone);
+                const int first = incl_mask ? (__ffs(incl_mask) - 1) : 32;
+                const unsigned upto = (first >= 31) ? 0xffffffffu : ((2u << first) - 1u);
+                if (none_mask & upto) {
+                    if (++spins > spin_limit) {
+                        if (lane == 0) atomicExch(P.error, 1u);
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                __threadfence();
+                const uint32_t pay = (v >> 8) & 0xffu;
+                uint32_t g = (lane < first) ? pay : (lane == first ? fconst(pay) : kFIdentity);
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    uint32_t o = __shfl_down_sync(0xffffffffu, g, off);
+                    if (lane + off < 32) g = fcompose(g, o);
+                }
+                g = __shfl_sync(0xffffffffu, g, 0);
+                look = fcompose(look, g);
+                if (first < 32) {
+                    u_in = fapply(look, 1);
+                    break;
+                }
+                base -= 32;
+            }
+            if (lane == 0 && publish) {
+                __threadfence();
+                st[bid] = kStIncl | (fapply(blk, u_in) << 8);
+            }
+        }
+        if (lane == 0) {
+            s_carry_in = u_in;
+            if ((uint64_t)(bid + 1) * NT * NW >= nwords && fapply(blk, u_in) != 1)
+                atomicExch(P.error, 2u);  // carry out of the top word: the result does not fit
+        }
+    }
+    __syncthreads();
+    const int c = (int)fapply(excl, fapply(s_wagg[warp], s_carry_in)) - 1;
+
+    // Final words.
+    top = -1;
+    {
+        int64_t acc = c;
+#pragma unroll
+        for (int u = 0; u < NW; ++u) {
+            acc += W[u];
+            o[u] = (uint32_t)acc;
+            if (o[u] != 0 && j0 + u < nwords) top = u;
+            acc >>= 32;
+        }
+    }
+}
+
+// Carry transfer function of NW consecutive signed word sums: f packed as above, entry u = carry-in
+// + 1 -> carry-out + 1 (carries in {-1, 0, 1, 2}).
+template <int NW>
+__device__ __forceinline__ uint32_t words_transfer(const int64_t (&W)[NW]) {
+    int64_t acc = 0;
+    bool ones_hi = true, zero_hi = true;
+    uint32_t low0 = 0;
+#pragma unroll
+    for (int u = 0; u < NW; ++u) {
+        acc += W[u];
+        const uint32_t o = (uint32_t)acc;
+        if (u == 0) {
+            low0 = o;
+        } else {
+            ones_hi &= (o == 0xffffffffu);
+            zero_hi &= (o == 0u);
+        }
+        acc >>= 32;
+    }
+    const int c0 = (int)acc;
+    const int fm1 = c0 - ((zero_hi && low0 == 0u) ? 1 : 0);
+    const int f1 = c0 + ((ones_hi && low0 == 0xffffffffu) ? 1 : 0);
+    const int f2 = c0 + ((ones_hi && low0 >= 0xfffffffeu) ? 1 : 0);
+    return (uint32_t)(fm1 + 1) | ((uint32_t)(c0 + 1) << 2) | ((uint32_t)(f1 + 1) << 4) | ((uint32_t)(f2 + 1) << 6);
+}
+
+// Carry resolution inside one block only, with carry-in 0 at the block's first word: o receives
+// the words, the return value (valid in every thread) is the block's transfer function. The
+// blocks' carries are then joined by crt_fix_kernel (a scan over the block functions and a
+// correction of each block's first words), so no block waits for another.
+template <int NW, int NT>
+__device__ __forceinline__ uint32_t carry_local(const int64_t (&W)[NW], uint32_t (&o)[NW], uint32_t (&s_wagg)[NT / 32],
+                                                uint32_t& s_blk) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NWARP = NT / 32;
+    const uint32_t f = words_transfer<NW>(W);
+    uint32_t incl = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = fcompose(incl, x);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = kFIdentity;
+    if (lane == 31) s_wagg[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t wincl = (lane < NWARP) ? s_wagg[lane] : kFIdentity;
+#pragma unroll
+        for (int off = 1; off < NWARP; off <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, wincl, off);
+            if (lane >= off) wincl = fcompose(wincl, x);
+        }
+        uint32_t wexcl = __shfl_up_sync(0xffffffffu, wincl, 1);
+        if (lane == 0) wexcl = kFIdentity;
+        const uint32_t blk = __shfl_sync(0xffffffffu, wincl, NWARP - 1);
+        __syncwarp();
+        if (lane < NWARP) s_wagg[lane] = wexcl;
+        if (lane == 0) s_blk = blk;
+    }
+    __syncthreads();
+    int64_t acc = (int)fapply(excl, fapply(s_wagg[warp], 1u)) - 1;
+#pragma unroll
+    for (int u = 0; u < NW; ++u) {
+        acc += W[u];
+        o[u] = (uint32_t)acc;
+        acc >>= 32;
+    }
+    return s_blk;
+}
+
 __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) {
     __shared__ uint32_t s_tail[kCrtThreads / 32][3];
     __shared__ uint32_t s_wagg[kCrtThreads / 32];
@@ -205,132 +413,9 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
         w += (int64_t)(int32_t)((u >= 2) ? a2[u - 2] : (u == 1 ? pw2a : pw2b));
         W[u] = w;
     }
-    uint32_t f;
-    {
-        int64_t acc = 0;
-        bool ones_hi = true, zero_hi = true;
-        uint32_t low0 = 0;
-#pragma unroll
-        for (int u = 0; u < kCrtWords; ++u) {
-            acc += W[u];
-            uint32_t o = (uint32_t)acc;
-            if (u == 0) {
-                low0 = o;
-            } else {
-                ones_hi &= (o == 0xffffffffu);
-                zero_hi &= (o == 0u);
-            }
-            acc >>= 32;  // arithmetic: floor division by 2^32
-        }
-        const int c0 = (int)acc;
-        const int fm1 = c0 - ((zero_hi && low0 == 0u) ? 1 : 0);
-        const int f1 = c0 + ((ones_hi && low0 == 0xffffffffu) ? 1 : 0);
-        const int f2 = c0 + ((ones_hi && low0 >= 0xfffffffeu) ? 1 : 0);
-        f = (uint32_t)(fm1 + 1) | ((uint32_t)(c0 + 1) << 2) | ((uint32_t)(f1 + 1) << 4) | ((uint32_t)(f2 + 1) << 6);
-    }
-
-    // Warp inclusive scan of transfer functions (lane order = word order).
-    uint32_t incl = f;
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        uint32_t o = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl = fcompose(incl, o);
-    }
-    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lane == 0) excl = kFIdentity;
-    if (lane == 31) s_wagg[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        // Exclusive prefix over the block's warps (lanes 0..7), block aggregate in lane 7.
-        constexpr int NW = kCrtThreads / 32;
-        uint32_t wf = (lane < NW) ? s_wagg[lane] : kFIdentity;
-        uint32_t wincl = wf;
-#pragma unroll
-        for (int off = 1; off < NW; off <<= 1) {
-            uint32_t o = __shfl_up_sync(0xffffffffu, wincl, off);
-            if (lane >= off) wincl = fcompose(wincl, o);
-        }
-        uint32_t wexcl = __shfl_up_sync(0xffffffffu, wincl, 1);
-        if (lane == 0) wexcl = kFIdentity;
-        const uint32_t blk = __shfl_sync(0xffffffffu, wincl, NW - 1);
-        __syncwarp();
-        if (lane < NW) s_wagg[lane] = wexcl;
-
-        // Decoupled look-back, one window of 32 predecessors per step (lane l reads block
-        // base - l). The window's functions compose into one; the nearest block that already
-        // knows its carry out ends the walk. Carries are stored as u = carry + 1.
-        uint32_t u_in = 1;
-        const bool publish = bid + 1 != P.withhold1;  // false only under the test hook
-        const uint32_t spin_limit = P.spin_limit ? P.spin_limit : kSpinLimit;
-        if (bid == 0) {
-            if (lane == 0 && publish) st[0] = kStIncl | (fapply(blk, 1) << 8);
-        } else {
-            if (lane == 0 && publish) {
-                __threadfence();
-                st[bid] = kStAgg | (blk << 8);
-            }
-            uint32_t look = kFIdentity;
-            int64_t base = (int64_t)bid - 1;
-            uint32_t spins = 0;
-            while (true) {
-                const int64_t jb = base - lane;
-                const uint32_t v = (jb >= 0) ? st[jb] : (uint32_t)(kStIncl | (1u << 8));  // before block 0: carry 0
-                const uint32_t sv = v & 0xffu;
-                const unsigned incl_mask = __ballot_sync(0xffffffffu, sv == kStIncl);
-                const unsigned none_mask = __ballot_sync(0xffffffffu, sv == kStNone);
-                const int first = incl_mask ? (__ffs(incl_mask) - 1) : 32;
-                const unsigned upto = (first >= 31) ? 0xffffffffu : ((2u << first) - 1u);
-                if (none_mask & upto) {
-                    if (++spins > spin_limit) {
-                        if (lane == 0) atomicExch(P.error, 1u);
-                        break;
-                    }
-                    __nanosleep(64);
-                    continue;
-                }
-                __threadfence();
-                const uint32_t pay = (v >> 8) & 0xffu;
-                uint32_t g = (lane < first) ? pay : (lane == first ? fconst(pay) : kFIdentity);
-#pragma unroll
-                for (int off = 1; off < 32; off <<= 1) {
-                    uint32_t o = __shfl_down_sync(0xffffffffu, g, off);
-                    if (lane + off < 32) g = fcompose(g, o);
-                }
-                g = __shfl_sync(0xffffffffu, g, 0);
-                look = fcompose(look, g);
-                if (first < 32) {
-                    u_in = fapply(look, 1);
-                    break;
-                }
-                base -= 32;
-            }
-            if (lane == 0 && publish) {
-                __threadfence();
-                st[bid] = kStIncl | (fapply(blk, u_in) << 8);
-            }
-        }
-        if (lane == 0) {
-            s_carry_in = u_in;
-            if ((uint64_t)(bid + 1) * kCrtThreads * kCrtWords >= J.nwords && fapply(blk, u_in) != 1)
-                atomicExch(P.error, 2u);  // carry out of the top word: the result does not fit
-        }
-    }
-    __syncthreads();
-    const int c = (int)fapply(excl, fapply(s_wagg[warp], s_carry_in)) - 1;
-
-    // Final words.
     uint32_t o[kCrtWords];
     int top = -1;
-    {
-        int64_t acc = c;
-#pragma unroll
-        for (int u = 0; u < kCrtWords; ++u) {
-            acc += W[u];
-            o[u] = (uint32_t)acc;
-            if (o[u] != 0 && j0 + u < J.nwords) top = u;
-            acc >>= 32;
-        }
-    }
+    carry_resolve<kCrtWords>(W, o, top, bid, j0, J.nwords, st, P, s_wagg, s_carry_in);
     if (j0 + kCrtWords <= J.nwords) {
 #pragma unroll
         for (int u = 0; u < kCrtWords; u += 4)
@@ -347,6 +432,200 @@ __global__ void __launch_bounds__(kCrtThreads, 4) crt_carry_kernel(CrtParams P) 
         for (int off = 16; off > 0; off >>= 1) lim = max(lim, __shfl_xor_sync(0xffffffffu, lim, off));
         if (lane == 0 && lim) atomicMax(J.len, lim);
     }
+}
+
+// ---- The wide configuration: 64-bit coefficients over five primes (modarith.cuh).
+// Coefficient i is rebuilt by Garner's method as x = y0 + y1 q0 + y2 q0 q1 + y3 q0 q1 q2 +
+// y4 q0 q1 q2 q3 (y_k < q_k), with y_k = r_k c_k - sum_{m<k} y_m k_mk (mod q_k): fifteen Shoup
+// products, the inverse transform's 1/L and the pointwise product's 2^-32 folded into c_k. x < 2^154
+// sits in five 32-bit words at bit 64 i, so output word 2i receives x_i[0] + x_{i-1}[2] + x_{i-2}[4]
+// and word 2i+1 receives x_i[1] + x_{i-1}[3]: at most three words, carries in {0, 1, 2}, resolved by
+// the same scan as above.
+struct CrtWideConsts {
+    uint32_t c[kWidePrimes], cp[kWidePrimes];            // c_k and Shoup companions (mod q_k)
+    uint32_t k[kWidePrimes][kWidePrimes], kp[kWidePrimes][kWidePrimes];  // k_mk = P_m / P_k mod q_k, m < k
+    uint32_t Pw[kWidePrimes][kWidePrimes - 1];           // words of P_m = q0 ... q_{m-1}
+};
+
+struct X5 {
+    uint32_t w[5];
+};
+
+__device__ __forceinline__ X5 crt5(const uint32_t (&r)[kWidePrimes], const CrtWideConsts& K) {
+    uint32_t y[kWidePrimes];
+#pragma unroll
+    for (int kk = 0; kk < kWidePrimes; ++kk) {
+        const uint32_t q = prime_of(kWidePrimes, kk);
+        uint32_t acc = mul_shoup(r[kk], K.c[kk], K.cp[kk], q);
+#pragma unroll
+        for (int m = 0; m < kk; ++m) acc = sub_mod(acc, mul_shoup(y[m], K.k[m][kk], K.kp[m][kk], q), q);
+        y[kk] = acc;
+    }
+    uint64_t col[5] = {y[0], 0, 0, 0, 0};
+#pragma unroll
+    for (int m = 1; m < kWidePrimes; ++m)
+#pragma unroll
+        for (int w = 0; w < m; ++w) {
+            const uint64_t pr = (uint64_t)y[m] * K.Pw[m][w];
+            col[w] += (uint32_t)pr;
+            col[w + 1] += pr >> 32;
+        }
+    X5 x;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+        col[w + 1] += col[w] >> 32;
+        x.w[w] = (uint32_t)col[w];
+    }
+    x.w[4] = (uint32_t)col[4];
+    return x;
+}
+
+constexpr int kWideCoefs = 4;                  // coefficients per thread
+constexpr int kWideWords = 2 * kWideCoefs;     // output words per thread
+
+// One product in the wide configuration: residues of prime k at res + k * L (natural order),
+// output words to out (nwords), blocks of kWideThreads * kWideWords words, each block's words with
+// carry-in 0 and its carry transfer function in fblk[block]; crt_fix_kernel then joins the blocks.
+constexpr int kWideThreads = 512;
+__global__ void __launch_bounds__(kWideThreads, 2) crt_wide_kernel(CrtParams P, CrtWideConsts K) {
+    __shared__ uint32_t s_tail[kWideThreads / 32][4];
+    __shared__ uint32_t s_wagg[kWideThreads / 32];
+    __shared__ uint32_t s_blk;
+    const uint32_t bid = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t i0 = ((uint64_t)bid * kWideThreads + threadIdx.x) * kWideCoefs;  // first coefficient
+    const uint64_t j0 = 2 * i0;                                                     // first word
+    auto coef = [&](uint64_t i) {
+        X5 x = {{0, 0, 0, 0, 0}};
+        if (i < P.L) {
+            uint32_t r[kWidePrimes];
+#pragma unroll
+            for (int kk = 0; kk < kWidePrimes; ++kk) r[kk] = P.res[(uint64_t)kk * P.L + i];
+            x = crt5(r, K);
+        }
+        return x;
+    };
+    X5 x[kWideCoefs];
+    if (i0 + kWideCoefs <= P.L) {
+        uint4 v[kWidePrimes];
+#pragma unroll
+        for (int kk = 0; kk < kWidePrimes; ++kk) v[kk] = *reinterpret_cast<const uint4*>(P.res + (uint64_t)kk * P.L + i0);
+#pragma unroll
+        for (int u = 0; u < kWideCoefs; ++u) {
+            uint32_t r[kWidePrimes];
+#pragma unroll
+            for (int kk = 0; kk < kWidePrimes; ++kk) r[kk] = u == 0 ? v[kk].x : u == 1 ? v[kk].y : u == 2 ? v[kk].z : v[kk].w;
+            x[u] = crt5(r, K);
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kWideCoefs; ++u) x[u] = coef(i0 + u);
+    }
+    // Words 2..4 of the coefficient just below i0 and word 4 of the one below that.
+    uint32_t b2 = __shfl_up_sync(0xffffffffu, x[kWideCoefs - 1].w[2], 1);
+    uint32_t b3 = __shfl_up_sync(0xffffffffu, x[kWideCoefs - 1].w[3], 1);
+    uint32_t b4 = __shfl_up_sync(0xffffffffu, x[kWideCoefs - 1].w[4], 1);
+    uint32_t bb4 = __shfl_up_sync(0xffffffffu, x[kWideCoefs - 2].w[4], 1);
+    if (lane == 31) {
+        s_tail[warp][0] = x[kWideCoefs - 1].w[2];
+        s_tail[warp][1] = x[kWideCoefs - 1].w[3];
+        s_tail[warp][2] = x[kWideCoefs - 1].w[4];
+        s_tail[warp][3] = x[kWideCoefs - 2].w[4];
+    }
+    __syncthreads();
+    if (lane == 0) {
+        if (warp > 0) {
+            b2 = s_tail[warp - 1][0];
+            b3 = s_tail[warp - 1][1];
+            b4 = s_tail[warp - 1][2];
+            bb4 = s_tail[warp - 1][3];
+        } else if (i0 >= 1) {
+            // first thread of the block: rebuild the two coefficients below its range
+            const X5 m1 = coef(i0 - 1);
+            const X5 m2 = i0 >= 2 ? coef(i0 - 2) : X5{{0, 0, 0, 0, 0}};
+            b2 = m1.w[2];
+            b3 = m1.w[3];
+            b4 = m1.w[4];
+            bb4 = m2.w[4];
+        } else {
+            b2 = b3 = b4 = bb4 = 0;
+        }
+    }
+    int64_t W[kWideWords];
+#pragma unroll
+    for (int u = 0; u < kWideCoefs; ++u) {
+        // word 2 (i0 + u): x_i[0] + x_{i-1}[2] + x_{i-2}[4]; word 2 (i0 + u) + 1: x_i[1] + x_{i-1}[3]
+        const uint32_t p2 = u >= 1 ? x[u - 1].w[2] : b2;
+        const uint32_t p3 = u >= 1 ? x[u - 1].w[3] : b3;
+        const uint32_t p4 = u >= 2 ? x[u - 2].w[4] : (u == 1 ? b4 : bb4);
+        W[2 * u] = (int64_t)x[u].w[0] + p2 + p4;
+        W[2 * u + 1] = (int64_t)x[u].w[1] + p3;
+    }
+    uint32_t o[kWideWords];
+    const uint32_t fb = carry_local<kWideWords, kWideThreads>(W, o, s_wagg, s_blk);
+    if (threadIdx.x == 0) P.status[bid] = fb;
+    if (j0 + kWideWords <= P.nwords) {
+#pragma unroll
+        for (int u = 0; u < kWideWords; u += 4)
+            *reinterpret_cast<uint4*>(P.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
+    } else {
+#pragma unroll
+        for (int u = 0; u < kWideWords; ++u)
+            if (j0 + u < P.nwords) P.out[j0 + u] = o[u];
+    }
+}
+
+// Joins the blocks of crt_wide_kernel: one block of kFixThreads threads scans the nb block transfer
+// functions (fblk, in word order), and adds each block's carry-in to its first words (the carry runs
+// on only while words overflow, and stops at the block's end, past which the next block's carry-in
+// accounts for it). A carry out of the top word sets *error = 2 (the result does not fit).
+constexpr int kFixThreads = 1024;
+__global__ void __launch_bounds__(kFixThreads) crt_fix_kernel(const uint32_t* fblk, uint64_t nb, uint64_t block_words,
+                                                            uint32_t* out, uint64_t nwords, uint32_t* error) {
+    __shared__ uint32_t s_w[kFixThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t per = (nb + kFixThreads - 1) / kFixThreads;  // consecutive blocks per thread
+    const uint64_t b0 = (uint64_t)threadIdx.x * per;
+    uint32_t tf = kFIdentity;  // this thread's blocks composed
+    for (uint64_t i = 0; i < per; ++i)
+        if (b0 + i < nb) tf = fcompose(fblk[b0 + i], tf);
+    uint32_t incl = tf;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = fcompose(incl, x);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = kFIdentity;
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = s_w[lane];
+        uint32_t wi = w;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, wi, off);
+            if (lane >= off) wi = fcompose(wi, x);
+        }
+        uint32_t we = __shfl_up_sync(0xffffffffu, wi, 1);
+        if (lane == 0) we = kFIdentity;
+        __syncwarp();
+        s_w[lane] = we;
+    }
+    __syncthreads();
+    uint32_t u = fapply(excl, fapply(s_w[warp], 1u));  // carry-in + 1 of this thread's first block
+    for (uint64_t i = 0; i < per && b0 + i < nb; ++i) {
+        const uint64_t b = b0 + i;
+        const uint64_t end = min((b + 1) * block_words, nwords);
+        int64_t c = (int)u - 1;
+        for (uint64_t j = b * block_words; c != 0 && j < end; ++j) {
+            const int64_t t = (int64_t)out[j] + c;
+            out[j] = (uint32_t)t;
+            c = t >> 32;  // floor: -1, 0 or 1 after the first word
+        }
+        u = fapply(fblk[b], u);
+    }
+    if (b0 < nb && b0 + per >= nb && u != 1) atomicExch(error, 2u);  // the last block's carry out
 }
 
 // Short jobs (at most 32 * kCrtWords output words): one warp per job, no look-back. The same

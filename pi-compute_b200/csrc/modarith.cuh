@@ -29,17 +29,40 @@ namespace pg {
 constexpr int kNumPrimes = 3;
 constexpr int kMaxLogL = 26;
 
+// The wide configuration: 64-bit coefficients (one per limb, no repacking) over five primes,
+//   q0 = 2113929217 = 63 * 2^25 + 1   generator 5
+//   q1 = 2013265921 = 15 * 2^27 + 1   generator 31
+//   q2 = 1811939329 = 27 * 2^26 + 1   generator 13
+//   q3 = 1711276033 = 51 * 2^25 + 1   generator 29
+//   q4 = 1107296257 = 33 * 2^25 + 1   generator 10
+// all < 2^31, each with a primitive 2^25-th root of unity; q0 q1 q2 q3 q4 ~ 2^153.36. A product of
+// na x nb limbs has na + nb - 1 coefficients (half as many as with 32-bit coefficients) and its
+// largest coefficient min(na, nb) (2^64 - 1)^2 stays below the modulus for min(na, nb) < 2^25.35,
+// i.e. for every product of up to 2^25 limbs. Five transforms of L points against three of 2L:
+// 5/6 of the residue work per product bit.
+constexpr int kWidePrimes = 5;
+constexpr int kWideMaxLogL = 25;
+constexpr int kMaxPrimes = 5;
+
+// Primes and generators of a configuration with NP primes (3: 32-bit coefficients, 5: wide).
+__host__ __device__ constexpr uint32_t prime_of(int np, int j) {
+    return np == 5 ? (j == 0 ? 2113929217u : j == 1 ? 2013265921u : j == 2 ? 1811939329u : j == 3 ? 1711276033u
+                                                                                                   : 1107296257u)
+                   : (j == 0 ? 2013265921u : (j == 1 ? 1811939329u : 469762049u));
+}
+__host__ __device__ constexpr uint32_t generator_of(int np, int j) {
+    return np == 5 ? (j == 0 ? 5u : j == 1 ? 31u : j == 2 ? 13u : j == 3 ? 29u : 10u) : (j == 0 ? 31u : (j == 1 ? 13u : 3u));
+}
+// log2 of the longest transform (the 2-power order of the common roots of unity).
+__host__ __device__ constexpr int root_log_of(int np) { return np == 5 ? kWideMaxLogL : kMaxLogL; }
+
 struct PrimeConst {
     uint32_t p;
     uint32_t pinv;   // p^-1 mod 2^32 (Montgomery)
 };
 
-__host__ __device__ constexpr uint32_t kPrime(int j) {
-    return j == 0 ? 2013265921u : (j == 1 ? 1811939329u : 469762049u);
-}
-__host__ __device__ constexpr uint32_t kGenerator(int j) {
-    return j == 0 ? 31u : (j == 1 ? 13u : 3u);
-}
+__host__ __device__ constexpr uint32_t kPrime(int j) { return prime_of(3, j); }
+__host__ __device__ constexpr uint32_t kGenerator(int j) { return generator_of(3, j); }
 
 // p^-1 mod 2^32 by Newton iteration (x <- x * (2 - p*x)), exact after 5 steps from x = p.
 __host__ __device__ constexpr uint32_t inv_mod_2_32(uint32_t p) {
@@ -80,6 +103,7 @@ __device__ __forceinline__ uint32_t mul_shoup_lazy(uint32_t x, uint32_t w, uint3
 
 // floor((2^64 - 1) / p), used to form Shoup companions on the device without a division.
 __host__ __device__ constexpr uint64_t kRecip64(int j) { return ~0ull / kPrime(j); }
+__host__ __device__ constexpr uint64_t recip64_of(int np, int j) { return ~0ull / prime_of(np, j); }
 
 // Shoup companion floor(w * 2^32 / p) of w < p. With R = floor(2^64 / p) = 2^64/p - d
 // (0 <= d < 1), floor(w * R / 2^32) undershoots floor(w * 2^32 / p) by at most one because

@@ -8,7 +8,7 @@
 
 #include "crt_carry.cuh"
 #include "ntt_engine.cuh"
-#include "ntt_pass.cuh"
+#include "pass_launch.cuh"
 
 namespace pg {
 
@@ -26,24 +26,28 @@ uint32_t inv_mod(uint32_t a, uint32_t p) { return pow_mod(a, p - 2, p); }
 uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
 
 // ---------------------------------------------------------------- tables
-// Layout of the single table allocation, in uint2 entries:
+// One table allocation per configuration (NP = 3 primes with roots w_{2^26}, NP = 5 with w_{2^25}),
+// in uint2 entries:
 //   [dir][prime] stage  (2^14 each): entry h + x = w_{2h}^x for h = 2^k, x < h (entry 0 unused)
-//   [dir][prime] fs_lo  (2^13 each): w_{2^26}^j
-//   [dir][prime] fs_hi  (2^13 each): w_{2^26}^(2^13 j)
+//   [dir][prime] fs_lo  (2^13 each): w_{2^root}^j
+//   [dir][prime] fs_hi  (2^13 each): w_{2^root}^(2^13 j)
 //   [n][l][dir][prime] row (2^13 each): w_{2^n}^(c bitrev_l(m)) at m * 2^(13-l) + c, for four-step
-//                       blocks of 2^n points (n = 14..26) and strided sub-transforms of 2^l points
+//                       blocks of 2^n points (n = 14..root) and strided sub-transforms of 2^l points
 //                       (l = 5..10, tiles of 2^13)
 //   [n][l][dir][prime] row_big (2^14 each): the same for l = 11, 12 in tiles of 2^14 (m * 2^(14-l) + c)
-// The host computes the stage and fs tables (1.5 MB); a kernel derives every row table from fs_lo and
-// fs_hi on the device (w_{2^26}^e = lo[e mod 2^13] * hi[e / 2^13]), so a context's 50 MB of tables
-// cost no host arithmetic and no upload.
+// The host computes the stage and fs tables (2.5 MB); a kernel derives every row table from fs_lo and
+// fs_hi on the device (w_{2^root}^e = lo[e mod 2^13] * hi[e / 2^13]), so a context's tables cost no
+// host arithmetic and no upload beyond those.
 namespace {
 constexpr size_t kFsEnt = 1u << kFsLog;
-constexpr size_t kSmallTables = (size_t)2 * kNumPrimes * (kStageEnt + 2 * kFsEnt);  // entries
-constexpr size_t kRowEnt = (size_t)kRowTables * 2 * kNumPrimes * kFsEnt;
-constexpr size_t kRowBigEnt = (size_t)kRowTablesBig * 2 * kNumPrimes * (1u << 14);
+constexpr size_t small_entries(int np) { return (size_t)2 * np * (kStageEnt + 2 * kFsEnt); }
+constexpr size_t row_entries(int np) { return (size_t)kRowTables * 2 * np * kFsEnt; }
+constexpr size_t row_big_entries(int np) { return (size_t)kRowTablesBig * 2 * np * (1u << 14); }
 
+template <int NP>
 __global__ void fill_row_tables_kernel(uint2* row, uint2* row_big, TwiddleTables tw) {
+    constexpr uint64_t kRowEnt = row_entries(NP), kRowBigEnt = row_big_entries(NP);
+    constexpr int root = root_log_of(NP);
     const uint64_t total = kRowEnt + kRowBigEnt;
     for (uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
          idx += (uint64_t)gridDim.x * blockDim.x) {
@@ -52,40 +56,40 @@ __global__ void fill_row_tables_kernel(uint2* row, uint2* row_big, TwiddleTables
         const int logE = big ? 14 : 13;
         const uint32_t i = (uint32_t)(k & ((1u << logE) - 1));  // entry in its table
         const uint64_t t = k >> logE;                            // ((n, l) * 2 + dir) * primes + prime
-        const int j = (int)(t % kNumPrimes);
-        const int dir = (int)((t / kNumPrimes) & 1);
-        const uint64_t nl = t / (2 * kNumPrimes);
+        const int j = (int)(t % NP);
+        const int dir = (int)((t / NP) & 1);
+        const uint64_t nl = t / (2 * NP);
         const int nls = big ? (kRowNBigMax - kRowNBigMin + 1) : (kRowNMax - kRowNMin + 1);
         const int n = kRowLogMin + (int)(nl / nls);
+        if (n > root) continue;  // blocks longer than the configuration's transforms: never used
         const int l = (big ? kRowNBigMin : kRowNMin) + (int)(nl % nls);
         const uint32_t m = i >> (logE - l), c = i & ((1u << (logE - l)) - 1);
         const uint32_t kr = __brev(m) >> (32 - l);  // bitrev_l(m)
-        const uint32_t e = (c * kr) << (kMaxLogL - n);  // c * kr < 2^logE <= 2^n: e < 2^26
-        const uint32_t p = kPrime(j);
+        const uint32_t e = (c * kr) << (root - n);  // c * kr < 2^logE <= 2^n: e < 2^root
+        const uint32_t p = prime_of(NP, j);
         const uint2 a = tw.fs_lo[dir][j][e & (kFsEnt - 1)];
         const uint2 b = tw.fs_hi[dir][j][e >> kFsLog];
         const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
-        (big ? row_big : row)[k] = make_uint2(w, shoup_companion_dev(w, p, kRecip64(j)));
+        (big ? row_big : row)[k] = make_uint2(w, shoup_companion_dev(w, p, recip64_of(NP, j)));
     }
 }
-}  // namespace
 
-static cudaError_t allow_big_tiles();
-
-cudaError_t DeviceTables::build(int device) {
-    (void)device;
-    std::vector<uint2> h(kSmallTables);
-    auto stage_at = [&](int dir, int j) { return h.data() + (size_t)(dir * kNumPrimes + j) * kStageEnt; };
+// Builds the tables of the configuration with NP primes into one allocation (*base).
+template <int NP>
+cudaError_t build_tables(uint2*& base, TwiddleTables& tw) {
+    constexpr int root = root_log_of(NP);
+    std::vector<uint2> h(small_entries(NP));
+    auto stage_at = [&](int dir, int j) { return h.data() + (size_t)(dir * NP + j) * kStageEnt; };
     auto fs_at = [&](int which, int dir, int j) {
-        return h.data() + (size_t)2 * kNumPrimes * kStageEnt + ((size_t)(which * 2 + dir) * kNumPrimes + j) * kFsEnt;
+        return h.data() + (size_t)2 * NP * kStageEnt + ((size_t)(which * 2 + dir) * NP + j) * kFsEnt;
     };
     for (int dir = 0; dir < 2; ++dir)
-        for (int j = 0; j < kNumPrimes; ++j) {
-            const uint32_t p = kPrime(j);
-            uint32_t w26 = pow_mod(kGenerator(j), (uint64_t)(p - 1) >> kMaxLogL, p);  // primitive 2^26-th root
-            if (dir == 1) w26 = inv_mod(w26, p);
-            const uint32_t w14 = pow_mod(w26, 1ull << (kMaxLogL - kStageLog), p);
-            const uint32_t w26hi = pow_mod(w26, 1ull << kFsLog, p);
+        for (int j = 0; j < NP; ++j) {
+            const uint32_t p = prime_of(NP, j);
+            uint32_t wr = pow_mod(generator_of(NP, j), (uint64_t)(p - 1) >> root, p);  // primitive 2^root-th root
+            if (dir == 1) wr = inv_mod(wr, p);
+            const uint32_t w14 = pow_mod(wr, 1ull << (root - kStageLog), p);
+            const uint32_t wrhi = pow_mod(wr, 1ull << kFsLog, p);
             uint2* st = stage_at(dir, j);
             uint2* lo = fs_at(0, dir, j);
             uint2* hi = fs_at(1, dir, j);
@@ -103,36 +107,51 @@ cudaError_t DeviceTables::build(int device) {
             for (size_t i = 0; i < kFsEnt; ++i) {
                 lo[i] = make_uint2((uint32_t)b, shoup_companion((uint32_t)b, p));
                 hi[i] = make_uint2((uint32_t)c, shoup_companion((uint32_t)c, p));
-                b = b * w26 % p;
-                c = c * w26hi % p;
+                b = b * wr % p;
+                c = c * wrhi % p;
             }
         }
-    cudaError_t e = pg::dev_malloc(&base, (kSmallTables + kRowEnt + kRowBigEnt) * sizeof(uint2));
+    cudaError_t e = pg::dev_malloc(&base, (small_entries(NP) + row_entries(NP) + row_big_entries(NP)) * sizeof(uint2));
     if (e != cudaSuccess) return e;
     e = cudaMemcpy(base, h.data(), h.size() * sizeof(uint2), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return e;
+    tw = TwiddleTables{};
+    tw.nprimes = NP;
+    tw.root_log = root;
     for (int dir = 0; dir < 2; ++dir)
-        for (int j = 0; j < kNumPrimes; ++j) {
-            tw.stage[dir][j] = base + (size_t)(dir * kNumPrimes + j) * kStageEnt;
-            tw.fs_lo[dir][j] = base + (size_t)2 * kNumPrimes * kStageEnt + ((size_t)(0 * 2 + dir) * kNumPrimes + j) * kFsEnt;
-            tw.fs_hi[dir][j] = base + (size_t)2 * kNumPrimes * kStageEnt + ((size_t)(1 * 2 + dir) * kNumPrimes + j) * kFsEnt;
+        for (int j = 0; j < NP; ++j) {
+            tw.stage[dir][j] = base + (size_t)(dir * NP + j) * kStageEnt;
+            tw.fs_lo[dir][j] = base + (size_t)2 * NP * kStageEnt + ((size_t)(0 * 2 + dir) * NP + j) * kFsEnt;
+            tw.fs_hi[dir][j] = base + (size_t)2 * NP * kStageEnt + ((size_t)(1 * 2 + dir) * NP + j) * kFsEnt;
         }
-    uint2* row = base + kSmallTables;
-    uint2* row_big = row + kRowEnt;
+    uint2* row = base + small_entries(NP);
+    uint2* row_big = row + row_entries(NP);
     tw.row = row;
     tw.row_big = row_big;
     tw.row_layout = 0;
-    e = allow_big_tiles();
-    if (e != cudaSuccess) return e;
-    fill_row_tables_kernel<<<148 * 8, 256>>>(row, row_big, tw);
-    e = cudaGetLastError();
+    fill_row_tables_kernel<NP><<<148 * 8, 256>>>(row, row_big, tw);
+    return cudaGetLastError();
+}
+}  // namespace
+
+static cudaError_t allow_big_tiles();
+
+cudaError_t DeviceTables::build(int device) {
+    (void)device;
+    cudaError_t e = allow_big_tiles();
+    if (e == cudaSuccess) e = build_tables<kNumPrimes>(base, tw);
+    if (e == cudaSuccess) e = build_tables<kWidePrimes>(base_wide, tw_wide);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) wide = true;
     return e;
 }
 
 void DeviceTables::release() {
     if (base) cudaFree(base);
     base = nullptr;
+    if (base_wide) cudaFree(base_wide);
+    base_wide = nullptr;
+    wide = false;
 }
 
 // ---------------------------------------------------------------- workspace
@@ -191,131 +210,16 @@ void Workspace::release() {
 }
 
 // ---------------------------------------------------------------- pass dispatch
-// Dynamic shared memory of a pass: the tile, plus the four-step row factors of a strided tile.
-template <Layout LAY, int LOGN>
-constexpr size_t pass_smem() {
-    return ((size_t)4 << tile_log(LAY == Layout::Strided, LOGN)) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
-}
-
-template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
-static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cudaStream_t st) {
-    constexpr int LOGE = tile_log(LAY == Layout::Strided, LOGN);
-    constexpr int NT = pass_threads(LOGE);
-    uint64_t tiles;
-    if constexpr (LAY == Layout::Strided) {
-        tiles = (uint64_t)prm.njobs << (prm.logL - LOGE);
-    } else {
-        const uint64_t rows = (uint64_t)prm.njobs << (prm.logL - LOGN);
-        const uint64_t per = 1ull << (LOGE - LOGN);
-        tiles = (rows + per - 1) / per;
-    }
-    auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, NT, INV, SRC, FUSE>;
-    constexpr size_t smem = pass_smem<LAY, LOGN>();
-    dim3 grid((unsigned)tiles, kNumPrimes);
-    kern<<<grid, NT, smem, st>>>(prm, tw);
-    return cudaGetLastError();
-}
-
-// Kernels whose tiles need more than the default 48 KB of dynamic shared memory opt in on the
-// current device; done for every such kernel when a context's tables are built, so that no
-// attribute is set in the middle of a stream capture.
-template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE>
-static cudaError_t allow_smem() {
-    constexpr int LOGE = tile_log(LAY == Layout::Strided, LOGN);
-    constexpr size_t smem = pass_smem<LAY, LOGN>();
-    if constexpr (smem <= 48 * 1024) return cudaSuccess;
-    return cudaFuncSetAttribute(ntt_pass_kernel<LAY, LOGN, LOGE, pass_threads(LOGE), INV, SRC, FUSE>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
-
-template <int N>
-static cudaError_t allow_smem_contig() {
-    cudaError_t e = allow_smem<Layout::Contig, N, true, Source::Residues, Fuse::Combine>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, true, Source::Residues, Fuse::None>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Limbs, Fuse::None>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Limbs, Fuse::MulInverse>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Limbs, Fuse::SqrInverse>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Residues, Fuse::None>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Residues, Fuse::MulInverse>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Contig, N, false, Source::Residues, Fuse::SqrInverse>();
-    return e;
-}
-
-template <int N>
-static cudaError_t allow_smem_strided() {
-    cudaError_t e = allow_smem<Layout::Strided, N, true, Source::Residues, Fuse::None>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Strided, N, false, Source::Limbs, Fuse::None>();
-    if (e == cudaSuccess) e = allow_smem<Layout::Strided, N, false, Source::Residues, Fuse::None>();
-    return e;
+cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm,
+                        const TwiddleTables& tw, cudaStream_t st) {
+    if (tw.nprimes == kWidePrimes) return launch_pass_wide(plan, pass, inverse, src, fuse, prm, tw, st);
+    return launch_pass_np<kNumPrimes>(plan, pass, inverse, src, fuse, prm, tw, st);
 }
 
 static cudaError_t allow_big_tiles() {
-    cudaError_t e = allow_smem_contig<14>();
-    if (e == cudaSuccess) e = allow_smem_strided<11>();
-    if (e == cudaSuccess) e = allow_smem_strided<12>();
+    cudaError_t e = allow_big_tiles_np<kNumPrimes>();
+    if (e == cudaSuccess) e = allow_big_tiles_wide();
     return e;
-}
-
-#define PG_CONTIG_CASE(N)                                                                                    \
-    case N:                                                                                                  \
-        if (inverse && fuse == Fuse::Combine)                                                                \
-            return run_pass<Layout::Contig, N, true, Source::Residues, Fuse::Combine>(prm, tw, st);          \
-        if (inverse) return run_pass<Layout::Contig, N, true, Source::Residues, Fuse::None>(prm, tw, st);   \
-        if (src == Source::Limbs) {                                                                          \
-            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::None>(prm, tw, st); \
-            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::MulInverse>(prm, tw, st); \
-            return run_pass<Layout::Contig, N, false, Source::Limbs, Fuse::SqrInverse>(prm, tw, st);        \
-        } else {                                                                                             \
-            if (fuse == Fuse::None) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::None>(prm, tw, st); \
-            if (fuse == Fuse::MulInverse) return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::MulInverse>(prm, tw, st); \
-            return run_pass<Layout::Contig, N, false, Source::Residues, Fuse::SqrInverse>(prm, tw, st);     \
-        }
-
-#define PG_STRIDED_CASE(N)                                                                                   \
-    case N:                                                                                                  \
-        if (inverse) return run_pass<Layout::Strided, N, true, Source::Residues, Fuse::None>(prm, tw, st);  \
-        if (src == Source::Limbs) return run_pass<Layout::Strided, N, false, Source::Limbs, Fuse::None>(prm, tw, st); \
-        return run_pass<Layout::Strided, N, false, Source::Residues, Fuse::None>(prm, tw, st);
-
-cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fuse fuse, const PassParams& prm0,
-                        const TwiddleTables& tw, cudaStream_t st) {
-    const int logN = plan.logN[pass];
-    const bool contig = (pass == plan.npass - 1);
-    PassParams prm = prm0;
-    if (!contig) {
-        prm.rowB = row_table(tw, plan.logN[pass] + plan.logS[pass], logN, inverse ? 1 : 0);
-        if (!prm.rowB) return cudaErrorInvalidValue;  // no four-step table for this split
-    }
-    if (contig) {
-        if (inverse && (src != Source::Residues || (fuse != Fuse::None && fuse != Fuse::Combine)))
-            return cudaErrorInvalidValue;
-        switch (logN) {
-            PG_CONTIG_CASE(6)
-            PG_CONTIG_CASE(7)
-            PG_CONTIG_CASE(8)
-            PG_CONTIG_CASE(9)
-            PG_CONTIG_CASE(10)
-            PG_CONTIG_CASE(11)
-            PG_CONTIG_CASE(12)
-            PG_CONTIG_CASE(13)
-            PG_CONTIG_CASE(14)
-            default:
-                return cudaErrorInvalidValue;
-        }
-    } else {
-        switch (logN) {
-            PG_STRIDED_CASE(5)
-            PG_STRIDED_CASE(6)
-            PG_STRIDED_CASE(7)
-            PG_STRIDED_CASE(8)
-            PG_STRIDED_CASE(9)
-            PG_STRIDED_CASE(10)
-            PG_STRIDED_CASE(11)
-            PG_STRIDED_CASE(12)
-            default:
-                return cudaErrorInvalidValue;
-        }
-    }
 }
 
 // Test hooks of the look-back wait, read on every launch so that a test can set and clear them
@@ -382,16 +286,72 @@ CrtConsts make_crt_consts(int logL) {
 }
 
 // ---------------------------------------------------------------- one product
+// Garner constants of the wide configuration for transforms of 2^logL points (see crt5).
+static CrtWideConsts make_crt_wide_consts(int logL) {
+    CrtWideConsts K{};
+    uint32_t q[kWidePrimes];
+    for (int i = 0; i < kWidePrimes; ++i) q[i] = prime_of(kWidePrimes, i);
+    // P_m = q_0 ... q_{m-1} as 32-bit words, and P_m mod q_k
+    uint32_t Pw[kWidePrimes][kWidePrimes] = {};
+    Pw[0][0] = 1;
+    for (int m = 1; m < kWidePrimes; ++m) {
+        uint64_t carry = 0;
+        for (int w = 0; w < kWidePrimes; ++w) {
+            const uint64_t t = (uint64_t)Pw[m - 1][w] * q[m - 1] + carry;
+            Pw[m][w] = (uint32_t)t;
+            carry = t >> 32;
+        }
+    }
+    auto pmod = [&](int m, uint32_t p) {  // P_m mod p, Horner over the words
+        uint64_t r = 0;
+        for (int w = kWidePrimes - 1; w >= 0; --w) r = ((r << 32) + Pw[m][w]) % p;
+        return (uint32_t)r;
+    };
+    for (int kk = 0; kk < kWidePrimes; ++kk) {
+        const uint32_t p = q[kk];
+        const uint64_t linv = inv_mod(pow_mod(2, (uint64_t)logL, p), p);
+        const uint64_t scale = linv * pow_mod(2, 32, p) % p;  // 1/L and the 2^-32 of the pointwise product
+        const uint64_t pkinv = inv_mod(pmod(kk, p), p);
+        K.c[kk] = (uint32_t)(scale * pkinv % p);
+        K.cp[kk] = shoup_companion(K.c[kk], p);
+        for (int m = 0; m < kk; ++m) {
+            K.k[m][kk] = (uint32_t)((uint64_t)pmod(m, p) * pkinv % p);
+            K.kp[m][kk] = shoup_companion(K.k[m][kk], p);
+        }
+    }
+    for (int m = 0; m < kWidePrimes; ++m)
+        for (int w = 0; w < kWidePrimes - 1; ++w) K.Pw[m][w] = Pw[m][w];
+    return K;
+}
+
+// Wide CRT: every block independently (words with carry-in 0, block transfer functions into
+// c.status), then one block joins the blocks' carries.
+static cudaError_t launch_crt_wide(const CrtParams& c, uint64_t blocks, int logL, cudaStream_t st) {
+    crt_wide_kernel<<<(unsigned)blocks, kWideThreads, 0, st>>>(c, make_crt_wide_consts(logL));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    crt_fix_kernel<<<1, kFixThreads, 0, st>>>(c.status, blocks, (uint64_t)kWideThreads * kWideWords, c.out, c.nwords,
+                                             c.error);
+    return cudaGetLastError();
+}
+
+// The product's launch sequence in one configuration: 32-bit coefficients over three primes, or
+// (wide) 64-bit coefficients over five primes with the tables T.tw_wide.
 static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
                                 const uint64_t* d_b, size_t nb, int logL, uint64_t nwords, uint64_t* d_out,
-                                cudaStream_t st, uint64_t* launches) {
+                                cudaStream_t st, uint64_t* launches, bool wide = false) {
     const bool square = (d_b == nullptr);
     if (square) nb = na;
-    const Plan plan = T.plan(logL);
+    const int np = wide ? kWidePrimes : kNumPrimes;
+    const TwiddleTables& tw = wide ? T.tw_wide : T.tw;
+    const Source limbs = wide ? Source::Limbs64 : Source::Limbs;
+    const uint64_t coef_per_limb = wide ? 1 : 2;
+    const Plan plan = wide ? T.plan_wide(logL) : T.plan(logL);
     const uint64_t L = 1ull << logL;
-    cudaError_t e = W.ensure_res(3 * L);
+    cudaError_t e = W.ensure_res(np * L);
     if (e != cudaSuccess) return e;
-    const uint64_t crt_blocks = (nwords + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+    const uint64_t block_words = wide ? (uint64_t)kWideThreads * kWideWords : (uint64_t)kCrtThreads * kCrtWords;
+    const uint64_t crt_blocks = (nwords + block_words - 1) / block_words;
     e = W.ensure_sync(crt_blocks);
     if (e != cudaSuccess) return e;
 
@@ -400,13 +360,13 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
         p.data = data;
         p.out = data;
         p.other = nullptr;
-        p.other_stride = 3 * L;
+        p.other_stride = np * L;
         p.words_stride = 0;
         p.words = reinterpret_cast<const uint32_t*>(limbs);
         p.ncoef = ncoef;
         p.L = L;
         p.logL = logL;
-        p.job_stride = 3 * L;
+        p.job_stride = np * L;
         p.njobs = 1;
         p.merge = 0;
         return p;
@@ -416,32 +376,32 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
     const int last = plan.npass - 1;
     // Operand a: full forward transform (all but the last pass when squaring).
     {
-        PassParams p = base(W.a_res, d_a, 2ull * na);
+        PassParams p = base(W.a_res, d_a, coef_per_limb * na);
         const int upto = square ? last : plan.npass;
         for (int i = 0; i < upto; ++i) {
             set_pass(p, i);
             Fuse f = Fuse::None;
-            e = launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, f, p, T.tw, st);
+            e = launch_pass(plan, i, false, i == 0 ? limbs : Source::Residues, f, p, tw, st);
             if (e != cudaSuccess) return e;
         }
         if (square) {
             set_pass(p, last);
-            e = launch_pass(plan, last, false, last == 0 ? Source::Limbs : Source::Residues, Fuse::SqrInverse, p,
-                            T.tw, st);
+            e = launch_pass(plan, last, false, last == 0 ? limbs : Source::Residues, Fuse::SqrInverse, p,
+                            tw, st);
             if (e != cudaSuccess) return e;
         }
     }
     uint32_t* prod = W.a_res;
     if (!square) {
-        PassParams p = base(W.b_res, d_b, 2ull * nb);
+        PassParams p = base(W.b_res, d_b, coef_per_limb * nb);
         for (int i = 0; i < last; ++i) {
             set_pass(p, i);
-            e = launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, Fuse::None, p, T.tw, st);
+            e = launch_pass(plan, i, false, i == 0 ? limbs : Source::Residues, Fuse::None, p, tw, st);
             if (e != cudaSuccess) return e;
         }
         set_pass(p, last);
         p.other = W.a_res;
-        e = launch_pass(plan, last, false, last == 0 ? Source::Limbs : Source::Residues, Fuse::MulInverse, p, T.tw,
+        e = launch_pass(plan, last, false, last == 0 ? limbs : Source::Residues, Fuse::MulInverse, p, tw,
                         st);
         if (e != cudaSuccess) return e;
         prod = W.b_res;
@@ -451,7 +411,7 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
         PassParams p = base(prod, nullptr, 0);
         for (int i = last - 1; i >= 0; --i) {
             set_pass(p, i);
-            e = launch_pass(plan, i, true, Source::Residues, Fuse::None, p, T.tw, st);
+            e = launch_pass(plan, i, true, Source::Residues, Fuse::None, p, tw, st);
             if (e != cudaSuccess) return e;
         }
     }
@@ -468,17 +428,45 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
     c.error = W.sync;
     c.blocks_per_job = crt_blocks;
     c.merge = 0;
-    c.k = make_crt_consts(logL);
-    e = launch_crt(c, crt_blocks, st, nwords);
+    if (wide) {
+        e = launch_crt_wide(c, crt_blocks, logL, st);
+    } else {
+        c.k = make_crt_consts(logL);
+        e = launch_crt(c, crt_blocks, st, nwords);
+    }
     if (e != cudaSuccess) return e;
-    if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + 1;
+    if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + (wide ? 2 : 1);
     return cudaGetLastError();
+}
+
+// The smallest na + nb (limbs) that runs in the wide configuration: the context's value, or the
+// environment's PG_WIDE_MIN_LIMBS (read on every call, so that tests can move the boundary).
+static uint64_t wide_min_limbs(const DeviceTables& T) {
+    if (const char* e = std::getenv("PG_WIDE_MIN_LIMBS")) return std::strtoull(e, nullptr, 10);
+    return T.wide_min_limbs;
+}
+
+cudaError_t enqueue_product_config(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                                   const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st, bool wide) {
+    const size_t mb = d_b ? nb : na;
+    if (wide) {
+        if (!T.wide || product_logL_wide(na, mb) > kWideMaxLogL) return cudaErrorInvalidValue;
+        return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL_wide(na, mb), 2ull * (na + mb), d_out, st, nullptr,
+                            true);
+    }
+    return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL(na, mb), 2ull * (na + mb), d_out, st, nullptr);
 }
 
 cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
                             const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
                             uint64_t* launches) {
     const size_t mb = d_b ? nb : na;
+    // Configuration from the proven bound: the wide one holds every product of up to 2^25 limbs
+    // (min(na, nb) (2^64 - 1)^2 < q0 ... q4 for min(na, nb) < 2^25.35) in half the transform length.
+    const uint64_t wmin = T.wide ? wide_min_limbs(T) : 0;
+    if (wmin && na + mb >= wmin && product_logL_wide(na, mb) <= kWideMaxLogL)
+        return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL_wide(na, mb), 2ull * (na + mb), d_out, st, launches,
+                            true);
     return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL(na, mb), 2ull * (na + mb), d_out, st, launches);
 }
 

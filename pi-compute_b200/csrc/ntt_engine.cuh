@@ -48,11 +48,16 @@ cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st, uin
 void set_pass(PassParams& p, const Plan& plan, int i);
 
 struct DeviceTables {
-    uint2* base = nullptr;  // one allocation holding every table
+    uint2* base = nullptr;  // one allocation holding every table of the 32-bit configuration
     TwiddleTables tw{};
+    uint2* base_wide = nullptr;  // and of the wide one (64-bit coefficients, five primes)
+    TwiddleTables tw_wide{};
+    bool wide = false;           // tw_wide is built (contexts made by pg_create)
     // Pass splits chosen by the autotuner (pg_tune / pg_tune_load): tuned[logL] = {npass,
     // logN[0..2]}, npass == 0 meaning the built-in make_plan split.
     int8_t tuned[kMaxLogL + 1][4] = {};
+    // The same for the wide configuration's transforms (2^6 .. 2^25 points).
+    int8_t tuned_wide[kMaxLogL + 1][4] = {};
     Plan plan(int logL) const {
         if (logL >= 0 && logL <= kMaxLogL && tuned[logL][0] > 0) {
             const int n[3] = {tuned[logL][1], tuned[logL][2], tuned[logL][3]};
@@ -60,6 +65,16 @@ struct DeviceTables {
         }
         return make_plan(logL);
     }
+    Plan plan_wide(int logL) const {
+        if (logL >= 0 && logL <= kWideMaxLogL && tuned_wide[logL][0] > 0) {
+            const int n[3] = {tuned_wide[logL][1], tuned_wide[logL][2], tuned_wide[logL][3]};
+            return plan_from(logL, tuned_wide[logL][0], n);
+        }
+        return make_plan(logL);
+    }
+    // Products of at least this many limbs (na + nb) run in the wide configuration when its tables
+    // are built (PG_WIDE_MIN_LIMBS overrides it; 0 keeps every product in the 32-bit one).
+    uint64_t wide_min_limbs = 1ull << 13;
     cudaError_t build(int device);
     void release();
 };
@@ -87,6 +102,11 @@ struct Workspace {
 cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
                             const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
                             uint64_t* launches = nullptr);
+
+// The same product in a forced configuration (wide: 64-bit coefficients over five primes), for the
+// autotuner; cudaErrorInvalidValue when the wide tables are absent or the product is too long for them.
+cudaError_t enqueue_product_config(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                                   const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st, bool wide);
 
 // Enqueue the wrapped product for a caller-chosen transform length L = 2^logL (2 na <= L and
 // 2 nb <= L words; b == nullptr means square): out[0 .. L/2 + 1) receives sum_{i<L} c_i 2^(32 i)

@@ -328,14 +328,14 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
 // The pass kernel. grid = (tiles over all jobs, primes). Tile contents move with 16-byte
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
-template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE>
+template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE, int NP = kNumPrimes>
 __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
     extern __shared__ uint32_t sm[];
     constexpr int LOGC = LOGE - LOGN;
     constexpr uint32_t E = 1u << LOGE;
     static_assert(E % (4 * NTHREADS) == 0, "tile copies: whole 16-byte chunks per thread");
-    const int j = blockIdx.y;
-    const uint32_t p = kPrime(j);
+    const int j = blockIdx.y;  // prime index (NP primes: grid.y)
+    const uint32_t p = prime_of(NP, j);
     const int dir = INV ? 1 : 0;
     const uint32_t pinv = inv_mod_2_32(p);
     const uint64_t prime_off = (uint64_t)j * P.L;
@@ -357,12 +357,12 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
     if constexpr (LAY == Layout::Strided) {
         rowB = P.rowB + ((size_t)j << LOGE);  // one table per prime, an entry per tile element
         const uint32_t t0 = tcol<LAY, LOGN, LOGE>(stile, 0, P.logS);
-        const int sh = kMaxLogL - P.logNp;
+        const int sh = root_log_of(NP) - P.logNp;
         const uint2* lo = T.fs_lo[dir][j];
         const uint2* hi = T.fs_hi[dir][j];
-        const uint64_t R = kRecip64(j);
+        const uint64_t R = recip64_of(NP, j);
         for (uint32_t i = threadIdx.x; i < (1u << LOGN); i += NTHREADS) {
-            const uint32_t E0 = (t0 * bitrev_n(i, LOGN)) << sh;  // t0 * k < N', exponent of w_{2^26}
+            const uint32_t E0 = (t0 * bitrev_n(i, LOGN)) << sh;  // t0 * k < N', exponent of w_{2^root_log}
             const uint2 a = __ldg(lo + (E0 & ((1u << kFsLog) - 1)));
             const uint2 b = __ldg(hi + (E0 >> kFsLog));
             const uint32_t w = mul_shoup(a.x, b.x, b.y, p);
@@ -384,7 +384,14 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
     // A strided tile belongs to one job: its source words are looked up once, not per element.
     const uint32_t* swords = nullptr;
     uint64_t sncoef = 0;
-    if constexpr (SRC == Source::Limbs && LAY == Layout::Strided) job_source(P, sjob, swords, sncoef);
+    if constexpr (SRC != Source::Residues && LAY == Layout::Strided) job_source(P, sjob, swords, sncoef);
+    // 64-bit coefficients: x = hi 2^32 + lo = hi * (2^32 mod p) + lo (mod p)
+    uint32_t one_p64 = 0, r32 = 0, r32p = 0;
+    if constexpr (SRC == Source::Limbs64) {
+        one_p64 = (uint32_t)(0x100000000ull / p);
+        r32 = 0u - one_p64 * p;  // 2^32 - p floor(2^32 / p) < p
+        r32p = shoup_companion_dev(r32, p, recip64_of(NP, j));
+    }
 
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
 #pragma unroll(LAY == Layout::Strided ? E / (4 * NTHREADS) : 1)
@@ -412,6 +419,31 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
             // residues: an asynchronous copy straight into shared memory (the inverse strided
             // twiddle, if any, is applied below once the copies have landed)
             cp_async16(sm + swz(e4), P.data + job_offset(P, job) + prime_off + g);
+        } else if constexpr (SRC == Source::Limbs64) {
+            // four 64-bit coefficients (32 bytes of limbs) reduced modulo p in registers; past the
+            // operand's end (ncoef limbs), zeros
+            const uint32_t* words = swords;
+            uint64_t ncoef = sncoef;
+            if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
+            uint32_t w[8];
+            if (g + 4 <= ncoef) {
+                const uint4 v0 = __ldg(reinterpret_cast<const uint4*>(words + 2 * g));
+                const uint4 v1 = __ldg(reinterpret_cast<const uint4*>(words + 2 * g + 4));
+                w[0] = v0.x; w[1] = v0.y; w[2] = v0.z; w[3] = v0.w;
+                w[4] = v1.x; w[5] = v1.y; w[6] = v1.z; w[7] = v1.w;
+            } else {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const bool in = g + u < ncoef;
+                    w[2 * u] = in ? __ldg(words + 2 * (g + u)) : 0u;
+                    w[2 * u + 1] = in ? __ldg(words + 2 * (g + u) + 1) : 0u;
+                }
+            }
+            uint32_t r[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                r[u] = add_mod(reduce_u32(w[2 * u], p, one_p64), mul_shoup(w[2 * u + 1], r32, r32p, p), p);
+            *reinterpret_cast<uint4*>(sm + swz(e4)) = make_uint4(r[0], r[1], r[2], r[3]);
         } else if constexpr (SRC == Source::Limbs) {
             // operand words: whole 16-byte groups copied asynchronously, the ragged end (and the
             // zero padding) written directly; reduced modulo p below once landed

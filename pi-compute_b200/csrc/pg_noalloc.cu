@@ -129,6 +129,8 @@ pg_status setup_device(int dev, cudaStream_t st) {
         }
     d.tw.row = tables + (size_t)3 * 2 * pg::kNumPrimes * kTableEnt;
     d.tw.row_layout = 1;
+    d.tw.nprimes = pg::kNumPrimes;
+    d.tw.root_log = pg::kMaxLogL;
     d.scratch = scratch;
     d.ready = true;
     return PG_OK;

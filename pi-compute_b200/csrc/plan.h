@@ -101,6 +101,13 @@ inline int product_logL(size_t na, size_t nb) {
     return l < kMinLogL ? kMinLogL : l;
 }
 
+// Transform length for an na x nb limb product with 64-bit coefficients (the wide configuration):
+// na + nb - 1 coefficients.
+inline int product_logL_wide(size_t na, size_t nb) {
+    int l = ceil_log2((uint64_t)(na + nb) - 1);
+    return l < kMinLogL ? kMinLogL : l;
+}
+
 uint32_t pow_mod(uint32_t b, uint64_t e, uint32_t p);
 uint32_t inv_mod(uint32_t a, uint32_t p);
 uint32_t shoup_companion(uint32_t w, uint32_t p);

@@ -34,17 +34,20 @@ constexpr int kRowTables = (kMaxLogL - kRowLogMin + 1) * (kRowNMax - kRowNMin + 
 constexpr int kRowTablesBig = (kMaxLogL - kRowLogMin + 1) * (kRowNBigMax - kRowNBigMin + 1);
 
 struct TwiddleTables {
-    // (w, w') Shoup pairs, [dir][prime]; dir 0 = forward (w), 1 = inverse (w^-1).
-    const uint2* stage[2][kNumPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), kStageEnt entries
-    const uint2* fs_lo[2][kNumPrimes];  // w_{2^26}^j,           j < 2^13
-    const uint2* fs_hi[2][kNumPrimes];  // w_{2^26}^(2^13 * i),  i < 2^13
+    // (w, w') Shoup pairs, [dir][prime]; dir 0 = forward (w), 1 = inverse (w^-1). The tables of one
+    // configuration: nprimes primes (3, or 5 for the wide one) with roots w_{2^root_log} (26 or 25).
+    int nprimes;
+    int root_log;
+    const uint2* stage[2][kMaxPrimes];  // entry h + x = w_{2h}^x (h = 2^k, x < h), kStageEnt entries
+    const uint2* fs_lo[2][kMaxPrimes];  // w_{2^root_log}^j,           j < 2^13
+    const uint2* fs_hi[2][kMaxPrimes];  // w_{2^root_log}^(2^13 * i),  i < 2^13
     // Four-step factors of strided tiles: for a block of N' = 2^n points split into sub-transforms
     // of N = 2^l points (tile of C = 2^(13 - l) columns), table
-    // (((n - kRowLogMin) * 6 + l - kRowNMin) * 2 + dir) * kNumPrimes + prime holds
+    // (((n - kRowLogMin) * 6 + l - kRowNMin) * 2 + dir) * nprimes + prime holds
     // w_{N'}^(c * bitrev_l(m)) at entry m * C + c (row-major, so a tile row reads consecutively).
     const uint2* row;
     // The same for sub-transforms of 2^11 and 2^12 points in tiles of 2^14 (C = 2^(14 - l) columns,
-    // 2^14 entries): table (((n - kRowLogMin) * 2 + l - kRowNBigMin) * 2 + dir) * kNumPrimes + prime.
+    // 2^14 entries): table (((n - kRowLogMin) * 2 + l - kRowNBigMin) * 2 + dir) * nprimes + prime.
     const uint2* row_big;
     // 0: the layouts above for every (n, l); 1: only (14, 7) then (15, 7) (the fixed-size tables
     // of pg_mul_noalloc), [n][dir][prime].
@@ -57,19 +60,21 @@ inline const uint2* row_table(const TwiddleTables& T, int logNp, int logN, int d
         if (logN != 7 || logNp < 14 || logNp > 15) return nullptr;
         return T.row + ((size_t)((logNp - 14) * 2 + dir) * kNumPrimes) * (1u << kFsLog);
     }
-    if (logNp < kRowLogMin || logNp > kMaxLogL) return nullptr;
+    if (logNp < kRowLogMin || logNp > T.root_log) return nullptr;
     if (logN >= kRowNBigMin && logN <= kRowNBigMax) {
         if (!T.row_big) return nullptr;
         const int t = ((logNp - kRowLogMin) * (kRowNBigMax - kRowNBigMin + 1) + (logN - kRowNBigMin)) * 2 + dir;
-        return T.row_big + ((size_t)t * kNumPrimes) * (1u << 14);
+        return T.row_big + ((size_t)t * T.nprimes) * (1u << 14);
     }
     if (logN < kRowNMin || logN > kRowNMax) return nullptr;
     const int t = ((logNp - kRowLogMin) * (kRowNMax - kRowNMin + 1) + (logN - kRowNMin)) * 2 + dir;
-    return T.row + ((size_t)t * kNumPrimes) * (1u << kFsLog);
+    return T.row + ((size_t)t * T.nprimes) * (1u << kFsLog);
 }
 
 enum class Layout : int { Strided = 0, Contig = 1 };
-enum class Source : int { Residues = 0, Limbs = 1 };
+// Residues: a previous pass's output. Limbs: operand limbs as 32-bit coefficients (two per limb).
+// Limbs64: operand limbs as 64-bit coefficients (the wide configuration), one per element.
+enum class Source : int { Residues = 0, Limbs = 1, Limbs64 = 2 };
 // Combine (inverse contiguous pass of a binary-splitting level only): the tile is formed on load
 // from the merge's forward-transformed operands, P^ = Pl Pr, Q^ = Ql Qr or R^ = Qr Rl +- Pl Rr.
 enum class Fuse : int { None = 0, MulInverse = 1, SqrInverse = 2, Combine = 3 };
