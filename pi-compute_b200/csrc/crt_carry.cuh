@@ -575,20 +575,28 @@ __global__ void __launch_bounds__(kWideThreads, 2) crt_wide_kernel(CrtParams P, 
     }
 }
 
-// Joins the blocks of crt_wide_kernel: one block of kFixThreads threads scans the nb block transfer
-// functions (fblk, in word order), and adds each block's carry-in to its first words (the carry runs
-// on only while words overflow, and stops at the block's end, past which the next block's carry-in
-// accounts for it). A carry out of the top word sets *error = 2 (the result does not fit).
+// Joins the blocks of crt_wide_kernel in two launches.
+// crt_scan_kernel: one block of kFixThreads threads stages the nb block transfer functions (fblk, in
+// word order) in shared memory, scans them and overwrites fblk[b] with block b's carry-in + 1. A
+// carry out of the top word sets *error = 2 (the result does not fit).
+// crt_apply_kernel: one warp per block adds its carry-in to the block's words, 128 words per step
+// (a warp scan of the words' carry transfer functions), and stops as soon as the carry does or at
+// the block's end, past which the next block's carry-in accounts for it. A carry that runs through
+// a long stretch of all-ones (or, borrowing, all-zero) words therefore costs one step per 128 words
+// on one warp, not a serial walk word by word.
 constexpr int kFixThreads = 1024;
-__global__ void __launch_bounds__(kFixThreads) crt_fix_kernel(const uint32_t* fblk, uint64_t nb, uint64_t block_words,
-                                                            uint32_t* out, uint64_t nwords, uint32_t* error) {
+constexpr uint64_t kFixMaxBlocks = 16384;  // shared-memory staging: 64 KB
+__global__ void __launch_bounds__(kFixThreads) crt_scan_kernel(uint32_t* fblk, uint64_t nb, uint32_t* error) {
+    extern __shared__ uint32_t s_f[];
     __shared__ uint32_t s_w[kFixThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint64_t i = threadIdx.x; i < nb; i += kFixThreads) s_f[i] = fblk[i];
+    __syncthreads();
     const uint64_t per = (nb + kFixThreads - 1) / kFixThreads;  // consecutive blocks per thread
     const uint64_t b0 = (uint64_t)threadIdx.x * per;
     uint32_t tf = kFIdentity;  // this thread's blocks composed
     for (uint64_t i = 0; i < per; ++i)
-        if (b0 + i < nb) tf = fcompose(fblk[b0 + i], tf);
+        if (b0 + i < nb) tf = fcompose(s_f[b0 + i], tf);
     uint32_t incl = tf;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
@@ -600,8 +608,7 @@ __global__ void __launch_bounds__(kFixThreads) crt_fix_kernel(const uint32_t* fb
     if (lane == 31) s_w[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        uint32_t w = s_w[lane];
-        uint32_t wi = w;
+        uint32_t wi = s_w[lane];
 #pragma unroll
         for (int off = 1; off < 32; off <<= 1) {
             const uint32_t x = __shfl_up_sync(0xffffffffu, wi, off);
@@ -615,17 +622,64 @@ __global__ void __launch_bounds__(kFixThreads) crt_fix_kernel(const uint32_t* fb
     __syncthreads();
     uint32_t u = fapply(excl, fapply(s_w[warp], 1u));  // carry-in + 1 of this thread's first block
     for (uint64_t i = 0; i < per && b0 + i < nb; ++i) {
-        const uint64_t b = b0 + i;
-        const uint64_t end = min((b + 1) * block_words, nwords);
-        int64_t c = (int)u - 1;
-        for (uint64_t j = b * block_words; c != 0 && j < end; ++j) {
-            const int64_t t = (int64_t)out[j] + c;
-            out[j] = (uint32_t)t;
-            c = t >> 32;  // floor: -1, 0 or 1 after the first word
-        }
-        u = fapply(fblk[b], u);
+        fblk[b0 + i] = u;
+        u = fapply(s_f[b0 + i], u);
     }
     if (b0 < nb && b0 + per >= nb && u != 1) atomicExch(error, 2u);  // the last block's carry out
+}
+
+constexpr int kApplyWarps = 8;
+__global__ void __launch_bounds__(32 * kApplyWarps) crt_apply_kernel(const uint32_t* cin, uint64_t nb,
+                                                                  uint64_t block_words, uint32_t* out,
+                                                                  uint64_t nwords) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t b = (uint64_t)blockIdx.x * kApplyWarps + (threadIdx.x >> 5);
+    if (b >= nb) return;
+    uint32_t u = cin[b];  // carry + 1 entering the block's first word
+    if (u == 1) return;
+    const uint64_t end = min((b + 1) * block_words, nwords);
+    for (uint64_t j0 = b * block_words; j0 < end && u != 1; j0 += 128) {
+        const uint64_t j = j0 + 4 * (uint64_t)lane;
+        int64_t W[4];
+        const bool whole = j + 4 <= end;
+        if (whole) {
+            const uint4 v = *reinterpret_cast<const uint4*>(out + j);
+            W[0] = v.x; W[1] = v.y; W[2] = v.z; W[3] = v.w;
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) W[q] = j + q < end ? out[j + q] : 0;
+        }
+        // words past the end transfer carries unchanged: identity
+        const uint32_t f = j < end ? words_transfer<4>(W) : kFIdentity;
+        uint32_t incl = f;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
+            if (lane >= off) incl = fcompose(incl, x);
+        }
+        uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+        if (lane == 0) excl = kFIdentity;
+        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+        const uint32_t my = fapply(excl, u);  // carry + 1 entering this lane's first word
+        if (my != 1 && j < end) {
+            int64_t acc = (int)my - 1;
+            uint32_t o[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                acc += W[q];
+                o[q] = (uint32_t)acc;
+                acc >>= 32;
+            }
+            if (whole) {
+                *reinterpret_cast<uint4*>(out + j) = make_uint4(o[0], o[1], o[2], o[3]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    if (j + q < end) out[j + q] = o[q];
+            }
+        }
+        u = fapply(total, u);
+    }
 }
 
 // Short jobs (at most 32 * kCrtWords output words): one warp per job, no look-back. The same

@@ -219,6 +219,9 @@ cudaError_t launch_pass(const Plan& plan, int pass, bool inverse, Source src, Fu
 static cudaError_t allow_big_tiles() {
     cudaError_t e = allow_big_tiles_np<kNumPrimes>();
     if (e == cudaSuccess) e = allow_big_tiles_wide();
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(crt_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(kFixMaxBlocks * sizeof(uint32_t)));
     return e;
 }
 
@@ -330,8 +333,12 @@ static cudaError_t launch_crt_wide(const CrtParams& c, uint64_t blocks, int logL
     crt_wide_kernel<<<(unsigned)blocks, kWideThreads, 0, st>>>(c, make_crt_wide_consts(logL));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    crt_fix_kernel<<<1, kFixThreads, 0, st>>>(c.status, blocks, (uint64_t)kWideThreads * kWideWords, c.out, c.nwords,
-                                             c.error);
+    if (blocks > kFixMaxBlocks) return cudaErrorInvalidValue;
+    crt_scan_kernel<<<1, kFixThreads, blocks * sizeof(uint32_t), st>>>(c.status, blocks, c.error);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    crt_apply_kernel<<<(unsigned)((blocks + kApplyWarps - 1) / kApplyWarps), 32 * kApplyWarps, 0, st>>>(
+        c.status, blocks, (uint64_t)kWideThreads * kWideWords, c.out, c.nwords);
     return cudaGetLastError();
 }
 
@@ -435,7 +442,7 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
         e = launch_crt(c, crt_blocks, st, nwords);
     }
     if (e != cudaSuccess) return e;
-    if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + (wide ? 2 : 1);
+    if (launches) *launches += (square ? plan.npass : 2 * plan.npass) + (plan.npass - 1) + (wide ? 3 : 1);
     return cudaGetLastError();
 }
 

@@ -497,22 +497,27 @@ void final_formula(DevArith& A, DevNum& pi_int, const DevNum& Q, const DevNum& R
         mul_trunc(S);
         mul_trunc(Z);
         mul_trunc(F);
-        if (e >= -160) throw DevError(PG_ERR_INTERNAL, "final formula: not enough fraction bits");
+        if (e >= 0) throw DevError(PG_ERR_INTERNAL, "final formula: no fraction bits");
         const size_t fb = (size_t)(-e);
         // Z and S are within 2 units of their exact values (>= 2^(k-1)), the truncations of Qt,
-        // Rt and the three products within 1 unit each: relative error < 16 * 2^-(k-1), and
-        // pi 10^d < 2^(P - guard), so the absolute error is below 2^-(guard + 59); the floor is
-        // certain unless the fraction is within 2^-100 of an integer (guard >= 128).
-        // fr = X mod 2^fb; top = fr >> (fb - 100) (100 bits), low = fr mod 2^(fb-100).
-        Num fr(A), top(A), low(A);
+        // Rt and the three products within 1 unit each: the relative error is below
+        // 16 * 2^-(k-1) = 2^(5-k). With V = X / 2^fb < 2^ib the absolute error is below
+        // 2^-eb, eb = k - 5 - ib (for pi 10^d < 2^(P - guard): eb >= guard + 59). The floor is
+        // certain when the computed fraction lies at least 2^-tw, tw = eb - 2, from an integer;
+        // each larger guard narrows that window, so a value closer to an integer than one
+        // guard resolves is settled by the next.
+        const size_t xb = A.bits(X);
+        const size_t ib = xb > fb ? xb - fb : 0;
+        if (k < ib + 5 + 64 + 2 || k - 5 - ib - 2 > fb)
+            throw DevError(PG_ERR_INTERNAL, "final formula: not enough fraction bits");
+        const size_t tw = k - 5 - ib - 2;
+        // fr = X mod 2^fb: below <=> fr < 2^(fb-tw); above <=> 2^fb - fr < 2^(fb-tw)
+        Num fr(A), c(A);
         A.tdiv_r_2exp(fr, X, fb);
-        A.tdiv_q_2exp(top, fr, fb - 100);
-        A.tdiv_r_2exp(low, fr, fb - 100);
-        const u128 tv = download_u128(A, top);
-        const u128 all_ones = ((u128)1 << 100) - 1;
-        const bool below = tv == 0;                          // fr < 2^(fb-100)
-        A.exact(low);  // a zero low part has sign 0 only with its exact length
-        const bool above = tv == all_ones && low.v.sign != 0;  // fr > 2^fb - 2^(fb-100)
+        const bool below = A.bits(fr) <= fb - tw;
+        A.set_pow2(c, fb);
+        A.sub(c, c, fr);
+        const bool above = A.bits(c) <= fb - tw;
         if (!below && !above) {
             A.tdiv_q_2exp(pi_int, X, fb);
             return;

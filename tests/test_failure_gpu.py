@@ -44,14 +44,18 @@ def _with_env(env, fn):
 
 
 def test_lookback_wait_runs_out_and_context_recovers(eng):
-    # 2^15 x 2^15 limbs: 2^17 output words, 32 carry blocks; block 2 never publishes its carry
+    # 2^15 x 2^15 limbs in the 32-bit configuration (the one whose CRT carries look back):
+    # 2^17 output words, 32 carry blocks; block 2 never publishes its carry
     a = pkg.random_operand(1 << 15, 11)
     b = pkg.random_operand(1 << 15, 12)
+    narrow = {"PG_WIDE_MIN_LIMBS": "0"}
     with pytest.raises(pkg.PgError) as err:
-        _with_env({"PG_TEST_CRT_SPIN_LIMIT": "2000", "PG_TEST_CRT_WITHHOLD": "2"}, lambda: eng.mul_limbs(a, b))
+        _with_env(dict(narrow, PG_TEST_CRT_SPIN_LIMIT="2000", PG_TEST_CRT_WITHHOLD="2"), lambda: eng.mul_limbs(a, b))
     assert err.value.status == pkg.PG_ERR_TIMEOUT
     assert "look-back" in eng.last_error()
-    assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b))
+    exp = oracle.mul_gmp(a, b)
+    assert np.array_equal(_with_env(narrow, lambda: eng.mul_limbs(a, b)), exp)
+    assert np.array_equal(eng.mul_limbs(a, b), exp)
 
 
 def test_device_allocation_failure_is_oom_and_context_recovers(eng):

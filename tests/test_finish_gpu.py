@@ -101,6 +101,53 @@ def test_pi_finish_from_oracle_series(eng):
     assert eng.pi_finish(q, r, 1000) == ref
 
 
+def _near_integer_root(m: int, digits: int, above_bits: int, below: bool, seed: int):
+    """Q, R whose final-formula value V = 426880 sqrt(10005) Q 10^d / R lies within about
+    2^-above_bits of the integer m: just above it (floor m) or, with below=True, just under it
+    (floor m - 1). R = floor(S / m) (or + 1) with S = 426880 sqrt(10005) Q 10^d makes
+    V - m = m frac(S / m) / R, so R's size sets how close V comes. Returns Q, R, floor(V) and
+    the distance of V from m in bits (checked with exact integers)."""
+    rng = np.random.default_rng(seed)
+    rbits = m.bit_length() + above_bits
+    qbits = rbits - (426880 * 100).bit_length() + 1
+    q = int.from_bytes(rng.bytes((qbits + 7) // 8), "little") >> (8 * ((qbits + 7) // 8) - qbits)
+    q |= 1 << (qbits - 1)
+    base = 426880 * q * 10**digits
+    r = math.isqrt(10005 * base * base) // m + (1 if below else 0)
+    G = rbits + 64
+    v_fix = math.isqrt(10005 * (base << G) ** 2) // r  # floor(V 2^G)
+    fl = v_fix >> G
+    dist = abs(v_fix - (m << G))  # |V - m| 2^G, to within one unit
+    return q, r, fl, G - dist.bit_length()
+
+
+@pytest.mark.parametrize("case", ["above", "below"])
+def test_pi_finish_near_an_integer(eng, case):
+    """Values within 2^-300 of an integer are closer than the first guard's error window: the
+    formula must rerun with a larger guard and still return the exact floor (m, or m - 1 from
+    just below), never a rounded one."""
+    ref = open(os.path.join(GOLDEN, "pi_1000.txt")).read().strip()
+    m = int(ref.replace(".", ""))
+    q, r, fl, dbits = _near_integer_root(m, 1000, 300, case == "below", seed=7)
+    assert 280 <= dbits <= 330  # the construction really lands near m
+    want = m if case == "above" else m - 1
+    assert fl == want
+    s = str(want)
+    assert eng.pi_finish(q, r, 1000) == s[0] + "." + s[1:]
+
+
+def test_pi_finish_too_close_to_an_integer_fails_loudly(eng):
+    """A value within 2^-1600 of an integer is beyond every guard the formula tries: it must
+    report PG_ERR_INTERNAL rather than guess the floor."""
+    ref = open(os.path.join(GOLDEN, "pi_1000.txt")).read().strip()
+    m = int(ref.replace(".", ""))
+    q, r, fl, dbits = _near_integer_root(m, 1000, 1600, False, seed=8)
+    assert fl == m and dbits >= 1500
+    with pytest.raises(pkg.PgError) as ei:
+        eng.pi_finish(q, r, 1000)
+    assert ei.value.status == pkg.PG_ERR_INTERNAL
+
+
 @pytest.mark.parametrize("digits", [1, 10, 100, 999, 1000, 1001, 20_000])
 def test_pg_pi_prefixes(eng, digits):
     ref = open(os.path.join(GOLDEN, "pi_1000.txt")).read().strip()
