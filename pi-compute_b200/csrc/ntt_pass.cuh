@@ -325,6 +325,14 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
     }
 }
 
+// What a contiguous tile's load needs of each of its rows, looked up once per row rather than per
+// 16-byte chunk: the source limbs (first forward pass) or, for the splitting's combining pass, the
+// sign of R's second product (ncoef = 1 for +, 0 for -).
+struct RowSrc {
+    const uint32_t* words;
+    uint64_t ncoef;
+};
+
 // The pass kernel. grid = (tiles over all jobs, primes). Tile contents move with 16-byte
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
@@ -349,6 +357,31 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
     }
     const uint64_t total_rows = (uint64_t)P.njobs << (P.logL - LOGN);
     const int logRows = P.logL - LOGN;
+
+    // Contiguous tiles: the per-row sources, after the tile in shared memory.
+    static_assert(FUSE != Fuse::Combine || LAY == Layout::Contig, "the combining pass is contiguous");
+    constexpr bool kRowSrc = LAY == Layout::Contig && (SRC != Source::Residues || FUSE == Fuse::Combine);
+    RowSrc* rsrc = reinterpret_cast<RowSrc*>(sm + E);
+    if constexpr (kRowSrc) {
+        for (uint32_t c = threadIdx.x; c < (1u << LOGC); c += NTHREADS) {
+            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            RowSrc r{nullptr, 0};
+            if (R < total_rows) {
+                const uint64_t job = R >> logRows;
+                if constexpr (SRC != Source::Residues) job_source(P, job, r.words, r.ncoef);
+                if constexpr (FUSE == Fuse::Combine) {
+                    const uint64_t mrg = job / 3;
+                    if (job - 3 * mrg == 2) {
+                        uint64_t a, b;
+                        node_range(P.comb_a0, P.comb_b0, P.comb_depth, mrg, a, b);
+                        r.ncoef = merge_r_sign(a, b) > 0 ? 1 : 0;
+                    }
+                }
+            }
+            rsrc[c] = r;
+        }
+        __syncthreads();
+    }
 
     // Strided tiles: four-step row factors A[m] = w_{N'}^{t0 bitrev(m)} of this tile's first
     // column t0, after the tile in shared memory; B is the row power table of N'.
@@ -424,7 +457,10 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
             // operand's end (ncoef limbs), zeros
             const uint32_t* words = swords;
             uint64_t ncoef = sncoef;
-            if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
+            if constexpr (LAY == Layout::Contig) {
+                words = rsrc[c].words;
+                ncoef = rsrc[c].ncoef;
+            }
             uint32_t w[8];
             if (g + 4 <= ncoef) {
                 const uint4 v0 = __ldg(reinterpret_cast<const uint4*>(words + 2 * g));
@@ -449,7 +485,10 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
             // zero padding) written directly; reduced modulo p below once landed
             const uint32_t* words = swords;
             uint64_t ncoef = sncoef;
-            if constexpr (LAY == Layout::Contig) job_source(P, job, words, ncoef);
+            if constexpr (LAY == Layout::Contig) {
+                words = rsrc[c].words;
+                ncoef = rsrc[c].ncoef;
+            }
             if (g + 4 <= ncoef) {
                 cp_async16(sm + swz(e4), words + g);
             } else {
@@ -467,9 +506,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
                 const uint32_t* slot0 = P.data + 6 * mrg * P.comb_slot + prime_off + g;
                 auto at = [&](int o) { return *reinterpret_cast<const uint4*>(slot0 + (uint64_t)o * P.comb_slot); };
                 if (ck == 2) {
-                    uint64_t a, b;
-                    node_range(P.comb_a0, P.comb_b0, P.comb_depth, mrg, a, b);
-                    const int sgn = merge_r_sign(a, b);
+                    const int sgn = rsrc[c].ncoef ? 1 : -1;
                     const uint4 pl = at(0), rl = at(2), qr = at(4), rr = at(5);
                     uint32_t u, v;
 #define PG_RCOMB(f)                                         \

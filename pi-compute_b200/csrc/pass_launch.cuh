@@ -9,10 +9,12 @@
 
 namespace pg {
 
-// Dynamic shared memory of a pass: the tile, plus the four-step row factors of a strided tile.
+// Dynamic shared memory of a pass: the tile, plus the four-step row factors of a strided tile or
+// the per-row sources of a contiguous one (RowSrc, 16 bytes a row).
 template <Layout LAY, int LOGN>
 constexpr size_t pass_smem() {
-    return ((size_t)4 << tile_log(LAY == Layout::Strided, LOGN)) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : 0);
+    constexpr int LOGE = tile_log(LAY == Layout::Strided, LOGN);
+    return ((size_t)4 << LOGE) + (LAY == Layout::Strided ? ((size_t)8 << LOGN) : ((size_t)16 << (LOGE - LOGN)));
 }
 
 template <Layout LAY, int LOGN, bool INV, Source SRC, Fuse FUSE, int NP>
