@@ -339,6 +339,7 @@ struct DepthPlan {
     uint32_t cap[3];  // limbs
     int kind;         // 0 pair, 1 warp schoolbook, 2 ntt
     int logL;         // ntt
+    bool wide;        // ntt in the wide configuration (64-bit coefficients, five primes)
 };
 
 constexpr uint32_t kWarpMaxC = 64;
@@ -365,6 +366,7 @@ struct DeviceBS {
     uint64_t moves = 0;           // buffer reallocations so far
     cudaGraphExec_t gexec = nullptr;  // captured for [g_a0, g_b0); destroyed when a buffer moves
     uint64_t g_a0 = ~0ull, g_b0 = 0;
+    uint64_t g_wmin = 0;              // the wide configuration's crossover the graph was planned with
     LevelView groot{};
     uint64_t glaunches = 0;
 
@@ -402,7 +404,8 @@ struct DeviceBS {
     // later call on the same range, with no buffer moved since, replays the graph alone.
     cudaError_t run_graph(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
         if (trace_on()) return run(a0, b0, root, err);  // tracing waits between depths
-        if (gexec && g_a0 == a0 && g_b0 == b0) {  // no buffer moved since the capture
+        const uint64_t wmin = T->wide ? wide_min_limbs(*T) : 0;
+        if (gexec && g_a0 == a0 && g_b0 == b0 && g_wmin == wmin) {  // no buffer moved since the capture
             root = groot;
             if (launches) *launches += glaunches;
             return cudaGraphLaunch(gexec, st);
@@ -444,6 +447,7 @@ struct DeviceBS {
         groot = root;
         g_a0 = a0;
         g_b0 = b0;
+        g_wmin = wmin;
         glaunches = counted;
         if (launches) *launches += counted;
         return cudaGraphLaunch(gexec, st);
@@ -570,6 +574,19 @@ struct DeviceBS {
                     err = "binary-splitting merge exceeds the proven CRT bound";
                     return {};
                 }
+                // The wide configuration (the crossover of single products, applied to the level's
+                // longest product) when its bound holds: R^'s two convolutions of 64-bit
+                // coefficients, (min(capQ, capR) + min(capP, capR)) (2^64 - 1)^2 < q0 ... q4 / 2.
+                const uint64_t convl = conv / 2;
+                const double wbound = (double)(std::min(C.cap[1], C.cap[2]) + std::min(C.cap[0], C.cap[2])) *
+                                      3.402823669209385e38;  // (2^64 - 1)^2 rounded up
+                const double whalf =
+                    2113929217.0 * 2013265921.0 * 1811939329.0 * 1711276033.0 * 1107296257.0 / 2.0 * (1.0 - 1e-12);
+                P.wide = false;
+                if (use_wide(*T, convl - convl / 2, convl / 2) && wbound < whalf) {
+                    P.wide = true;
+                    P.logL = std::max(ceil_log2(convl), kMinLogL);
+                }
             }
         }
         return dp;
@@ -577,14 +594,17 @@ struct DeviceBS {
 
     cudaError_t launch_ntt_level(const DepthPlan& P, const DepthPlan& C, const LevelView& in, const LevelView& out,
                                  uint64_t a0, uint64_t b0, int depth) {
-        const Plan plan = T->plan(P.logL);
+        const Plan plan = P.wide ? T->plan_wide(P.logL) : T->plan(P.logL);
+        const TwiddleTables& tw = P.wide ? T->tw_wide : T->tw;
+        const Source limbs = P.wide ? Source::Limbs64 : Source::Limbs;
         const uint64_t L = 1ull << P.logL;
         const uint64_t M = P.nodes;
-        const uint64_t stride = 3 * L;
+        const uint64_t stride = (P.wide ? kWidePrimes : kNumPrimes) * L;
         cudaError_t e = grow((void**)&res, res_cap, 6 * M * stride * 4);
         if (e != cudaSuccess) return e;
         // forward transforms of all 6M operands
         PassParams p{};
+        p.error = errw;
         p.data = res;
         p.out = res;
         p.L = L;
@@ -599,7 +619,7 @@ struct DeviceBS {
         p.ms.len = in.len;
         for (int i = 0; i < plan.npass; ++i) {
             set_pass(p, plan, i);
-            e = launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, Fuse::None, p, T->tw, st);
+            e = launch_pass(plan, i, false, i == 0 ? limbs : Source::Residues, Fuse::None, p, tw, st);
             if (e != cudaSuccess) return e;
             if (launches) ++*launches;
         }
@@ -610,6 +630,7 @@ struct DeviceBS {
         // separate pointwise kernel and no pass over the products).
         {
             PassParams q{};
+            q.error = errw;
             q.data = res;
             q.out = res;
             q.L = L;
@@ -625,15 +646,34 @@ struct DeviceBS {
             for (int i = plan.npass - 1; i >= 0; --i) {
                 set_pass(q, plan, i);
                 e = launch_pass(plan, i, true, Source::Residues, i == plan.npass - 1 ? Fuse::Combine : Fuse::None, q,
-                                T->tw, st);
+                                tw, st);
                 if (e != cudaSuccess) return e;
                 if (launches) ++*launches;
             }
         }
         // CRT + carry for all 3M outputs
         uint64_t maxw = 2ull * std::max({out.cap[0], out.cap[1], out.cap[2]});
-        const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
         const uint64_t jobs = 3 * M;
+        if (P.wide) {
+            const uint64_t bpj = (maxw + crt_wide_block_words() - 1) / crt_wide_block_words();
+            CrtParams c{};
+            c.L = L;
+            c.error = errw;
+            c.status = sync;
+            c.merge = 1;
+            c.res = res;
+            c.res_stride = stride;
+            for (int k = 0; k < 3; ++k) {
+                c.dst[k] = out.X[k];
+                c.dcap[k] = out.cap[k];
+            }
+            c.dlen = out.len;
+            c.a0 = a0;
+            c.b0 = b0;
+            c.depth = depth;
+            return launch_crt_wide(c, jobs, bpj, P.logL, st, launches);
+        }
+        const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
         e = grow((void**)&sync, sync_cap, (jobs + jobs * bpj) * 4);
         if (e != cudaSuccess) return e;
         e = cudaMemsetAsync(sync, 0, (jobs + jobs * bpj) * 4, st);
@@ -699,9 +739,10 @@ struct DeviceBS {
                 len_need[s] = std::max<uint64_t>(len_need[s], P.nodes * 3 * 4);
                 if (P.kind == 2) {
                     const uint64_t L = 1ull << P.logL, M = P.nodes;
-                    res_need = std::max<uint64_t>(res_need, 6 * M * 3 * L * 4);
+                    res_need = std::max<uint64_t>(res_need, 6 * M * (P.wide ? kWidePrimes : kNumPrimes) * L * 4);
                     const uint64_t maxw = 2ull * std::max({P.cap[0], P.cap[1], P.cap[2]});
-                    const uint64_t bpj = (maxw + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+                    const uint64_t bw = P.wide ? crt_wide_block_words() : (uint64_t)kCrtThreads * kCrtWords;
+                    const uint64_t bpj = (maxw + bw - 1) / bw;
                     sync_need = std::max<uint64_t>(sync_need, (3 * M + 3 * M * bpj) * 4);
                 }
             }
@@ -786,7 +827,7 @@ struct DeviceBS {
                 cudaStreamSynchronize(st);
                 std::fprintf(stderr, "[pg_bs] depth %2d: %8llu merges, caps %u/%u/%u limbs, %s L=2^%d: %.3f ms\n", d,
                              (unsigned long long)P.nodes, P.cap[0], P.cap[1], P.cap[2],
-                             P.kind == 1 ? "warp" : "ntt ", P.logL,
+                             P.kind == 1 ? "warp" : (P.wide ? "wide" : "ntt "), P.logL,
                              std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl0).count());
             }
             slot = oslot;
@@ -855,8 +896,10 @@ pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView
         return PG_ERR_DEVICE;
     }
     if (herr) {
-        ctx_set_error(ctx, herr == 1 ? "carry look-back wait ran out of iterations" : "carry out of the top word");
-        return herr == 1 ? PG_ERR_TIMEOUT : PG_ERR_INTERNAL;
+        const bool tmo = herr == 1 || (herr & 4);
+        ctx_set_error(ctx, herr == 1 ? "carry look-back wait ran out of iterations"
+                                     : (herr & 4) ? "tile load wait ran out of iterations" : "carry out of the top word");
+        return tmo ? PG_ERR_TIMEOUT : PG_ERR_INTERNAL;
     }
     return PG_OK;
 }

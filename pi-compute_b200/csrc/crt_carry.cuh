@@ -236,7 +236,7 @@ __device__ __forceinline__ void carry_resolve(const int64_t (&W)[NW], uint32_t (
         }
         if (lane == 0) {
             s_carry_in = u_in;
-            if ((uint64_t)(bid + 1) * NT * NW >= nwords && fapply(blk, u_in) != 1)
+            if ((uint64_t)(bid + 1) * NT * NW >= nwords && fapply(blk, u_in) != 1 && !P.top_ok)
                 atomicExch(P.error, 2u);  // carry out of the top word: the result does not fit
         }
     }
@@ -445,13 +445,17 @@ struct CrtWideConsts {
     uint32_t c[kWidePrimes], cp[kWidePrimes];            // c_k and Shoup companions (mod q_k)
     uint32_t k[kWidePrimes][kWidePrimes], kp[kWidePrimes][kWidePrimes];  // k_mk = P_m / P_k mod q_k, m < k
     uint32_t Pw[kWidePrimes][kWidePrimes - 1];           // words of P_m = q0 ... q_{m-1}
+    uint32_t h[kWidePrimes];                             // Garner digits of floor(P_5 / 2)
+    uint32_t Pi[kWidePrimes];                            // words of P_5 = q0 ... q4
 };
 
 struct X5 {
     uint32_t w[5];
 };
 
-__device__ __forceinline__ X5 crt5(const uint32_t (&r)[kWidePrimes], const CrtWideConsts& K) {
+// Coefficient x from its five residues; centred: x - P_5 when x > P_5 / 2 (a signed combination of
+// products), as a 160-bit two's-complement number (the top word then reads as a negative int32).
+__device__ __forceinline__ X5 crt5(const uint32_t (&r)[kWidePrimes], const CrtWideConsts& K, bool centred) {
     uint32_t y[kWidePrimes];
 #pragma unroll
     for (int kk = 0; kk < kWidePrimes; ++kk) {
@@ -477,31 +481,58 @@ __device__ __forceinline__ X5 crt5(const uint32_t (&r)[kWidePrimes], const CrtWi
         x.w[w] = (uint32_t)col[w];
     }
     x.w[4] = (uint32_t)col[4];
+    if (centred) {
+        // x > P/2 <=> its Garner digits (y4 .. y0) exceed those of floor(P/2), lexicographically
+        int cmp = 0;
+#pragma unroll
+        for (int kk = kWidePrimes - 1; kk >= 0; --kk)
+            if (cmp == 0) cmp = y[kk] > K.h[kk] ? 1 : (y[kk] < K.h[kk] ? -1 : 0);
+        if (cmp > 0) {
+            int64_t br = 0;
+#pragma unroll
+            for (int w = 0; w < 5; ++w) {
+                const int64_t t = (int64_t)x.w[w] - K.Pi[w] + br;
+                x.w[w] = (uint32_t)t;
+                br = t >> 32;
+            }
+        }
+    }
     return x;
 }
 
 constexpr int kWideCoefs = 4;                  // coefficients per thread
 constexpr int kWideWords = 2 * kWideCoefs;     // output words per thread
 
-// One product in the wide configuration: residues of prime k at res + k * L (natural order),
-// output words to out (nwords), blocks of kWideThreads * kWideWords words, each block's words with
-// carry-in 0 and its carry transfer function in fblk[block]; crt_fix_kernel then joins the blocks.
+// Products in the wide configuration, any batch form of CrtParams (crt_job): blocks_per_job blocks
+// of kWideThreads * kWideWords words per job (grid = jobs * blocks_per_job). Each block computes its
+// words with carry-in 0 and stores its carry transfer function in status[block];
+// crt_scan_kernel / crt_scan_warp_kernel and crt_apply_kernel then join the blocks of each job.
+//
+// status[block] = f | (t << 8): f the block's carry transfer function (8 bits), t - 1 the index
+// within the block of its highest non-zero word with carry-in 0 (t = 0: none), which bounds where a
+// job's final length can lie (crt_len_kernel).
 constexpr int kWideThreads = 512;
 __global__ void __launch_bounds__(kWideThreads, 2) crt_wide_kernel(CrtParams P, CrtWideConsts K) {
     __shared__ uint32_t s_tail[kWideThreads / 32][4];
     __shared__ uint32_t s_wagg[kWideThreads / 32];
     __shared__ uint32_t s_blk;
-    const uint32_t bid = blockIdx.x;
+    __shared__ uint32_t s_top;
+    if (threadIdx.x == 0) s_top = 0;
+    const uint64_t bid = blockIdx.x;
+    const uint64_t job = bid / P.blocks_per_job;
+    const uint64_t blk = bid - job * P.blocks_per_job;
+    const CrtJob J = crt_job(P, job);
+    const bool cen = J.centred;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t i0 = ((uint64_t)bid * kWideThreads + threadIdx.x) * kWideCoefs;  // first coefficient
-    const uint64_t j0 = 2 * i0;                                                     // first word
+    const uint64_t i0 = (blk * kWideThreads + threadIdx.x) * kWideCoefs;  // first coefficient
+    const uint64_t j0 = 2 * i0;                                           // first word
     auto coef = [&](uint64_t i) {
         X5 x = {{0, 0, 0, 0, 0}};
         if (i < P.L) {
             uint32_t r[kWidePrimes];
 #pragma unroll
-            for (int kk = 0; kk < kWidePrimes; ++kk) r[kk] = P.res[(uint64_t)kk * P.L + i];
-            x = crt5(r, K);
+            for (int kk = 0; kk < kWidePrimes; ++kk) r[kk] = J.res[(uint64_t)kk * P.L + i];
+            x = crt5(r, K, cen);
         }
         return x;
     };
@@ -509,13 +540,13 @@ __global__ void __launch_bounds__(kWideThreads, 2) crt_wide_kernel(CrtParams P, 
     if (i0 + kWideCoefs <= P.L) {
         uint4 v[kWidePrimes];
 #pragma unroll
-        for (int kk = 0; kk < kWidePrimes; ++kk) v[kk] = *reinterpret_cast<const uint4*>(P.res + (uint64_t)kk * P.L + i0);
+        for (int kk = 0; kk < kWidePrimes; ++kk) v[kk] = *reinterpret_cast<const uint4*>(J.res + (uint64_t)kk * P.L + i0);
 #pragma unroll
         for (int u = 0; u < kWideCoefs; ++u) {
             uint32_t r[kWidePrimes];
 #pragma unroll
             for (int kk = 0; kk < kWidePrimes; ++kk) r[kk] = u == 0 ? v[kk].x : u == 1 ? v[kk].y : u == 2 ? v[kk].z : v[kk].w;
-            x[u] = crt5(r, K);
+            x[u] = crt5(r, K, cen);
         }
     } else {
 #pragma unroll
@@ -555,42 +586,54 @@ __global__ void __launch_bounds__(kWideThreads, 2) crt_wide_kernel(CrtParams P, 
 #pragma unroll
     for (int u = 0; u < kWideCoefs; ++u) {
         // word 2 (i0 + u): x_i[0] + x_{i-1}[2] + x_{i-2}[4]; word 2 (i0 + u) + 1: x_i[1] + x_{i-1}[3]
+        // (the top word x[4] is signed: below 2^26 for a plain coefficient, negative for a lifted one)
         const uint32_t p2 = u >= 1 ? x[u - 1].w[2] : b2;
         const uint32_t p3 = u >= 1 ? x[u - 1].w[3] : b3;
         const uint32_t p4 = u >= 2 ? x[u - 2].w[4] : (u == 1 ? b4 : bb4);
-        W[2 * u] = (int64_t)x[u].w[0] + p2 + p4;
+        W[2 * u] = (int64_t)x[u].w[0] + p2 + (int32_t)p4;
         W[2 * u + 1] = (int64_t)x[u].w[1] + p3;
     }
     uint32_t o[kWideWords];
     const uint32_t fb = carry_local<kWideWords, kWideThreads>(W, o, s_wagg, s_blk);
-    if (threadIdx.x == 0) P.status[bid] = fb;
-    if (j0 + kWideWords <= P.nwords) {
+    uint32_t t = 0;  // 1 + index within the block of this thread's highest non-zero word
+#pragma unroll
+    for (int u = 0; u < kWideWords; ++u)
+        if (o[u] != 0 && j0 + u < J.nwords) t = threadIdx.x * kWideWords + u + 1;
+    t = __reduce_max_sync(0xffffffffu, t);
+    if (lane == 0 && t) atomicMax(&s_top, t);
+    __syncthreads();
+    if (threadIdx.x == 0) P.status[bid] = fb | (s_top << 8);
+    if (j0 + kWideWords <= J.nwords) {
 #pragma unroll
         for (int u = 0; u < kWideWords; u += 4)
-            *reinterpret_cast<uint4*>(P.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
+            *reinterpret_cast<uint4*>(J.out + j0 + u) = make_uint4(o[u], o[u + 1], o[u + 2], o[u + 3]);
     } else {
 #pragma unroll
         for (int u = 0; u < kWideWords; ++u)
-            if (j0 + u < P.nwords) P.out[j0 + u] = o[u];
+            if (j0 + u < J.nwords) J.out[j0 + u] = o[u];
     }
 }
 
-// Joins the blocks of crt_wide_kernel in two launches.
-// crt_scan_kernel: one block of kFixThreads threads stages the nb block transfer functions (fblk, in
-// word order) in shared memory, scans them and overwrites fblk[b] with block b's carry-in + 1. A
-// carry out of the top word sets *error = 2 (the result does not fit).
+// Joins the blocks of crt_wide_kernel per job in two launches.
+// crt_scan_kernel (one block of kFixThreads threads per job) / crt_scan_warp_kernel (one warp per
+// job, for at most 64 blocks a job): scan the job's block transfer functions (fblk + job * bpj, in
+// word order) and overwrite each with its block's carry-in + 1. A carry out of the job's top word
+// sets *error = 2 (the result does not fit) unless top_ok (a wrapped product, whose top is dropped).
 // crt_apply_kernel: one warp per block adds its carry-in to the block's words, 128 words per step
 // (a warp scan of the words' carry transfer functions), and stops as soon as the carry does or at
 // the block's end, past which the next block's carry-in accounts for it. A carry that runs through
 // a long stretch of all-ones (or, borrowing, all-zero) words therefore costs one step per 128 words
 // on one warp, not a serial walk word by word.
 constexpr int kFixThreads = 1024;
-constexpr uint64_t kFixMaxBlocks = 16384;  // shared-memory staging: 64 KB
-__global__ void __launch_bounds__(kFixThreads) crt_scan_kernel(uint32_t* fblk, uint64_t nb, uint32_t* error) {
+constexpr uint64_t kFixMaxBlocks = 16384;  // shared-memory staging of one job: 64 KB
+constexpr uint64_t kScanWarpMax = 64;      // blocks per job up to which a warp scans a job
+__global__ void __launch_bounds__(kFixThreads) crt_scan_kernel(uint32_t* fblk, uint64_t nb, uint32_t* error,
+                                                             int top_ok) {
     extern __shared__ uint32_t s_f[];
     __shared__ uint32_t s_w[kFixThreads / 32];
+    fblk += (uint64_t)blockIdx.x * nb;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (uint64_t i = threadIdx.x; i < nb; i += kFixThreads) s_f[i] = fblk[i];
+    for (uint64_t i = threadIdx.x; i < nb; i += kFixThreads) s_f[i] = fblk[i] & 0xffu;
     __syncthreads();
     const uint64_t per = (nb + kFixThreads - 1) / kFixThreads;  // consecutive blocks per thread
     const uint64_t b0 = (uint64_t)threadIdx.x * per;
@@ -622,22 +665,61 @@ __global__ void __launch_bounds__(kFixThreads) crt_scan_kernel(uint32_t* fblk, u
     __syncthreads();
     uint32_t u = fapply(excl, fapply(s_w[warp], 1u));  // carry-in + 1 of this thread's first block
     for (uint64_t i = 0; i < per && b0 + i < nb; ++i) {
-        fblk[b0 + i] = u;
+        fblk[b0 + i] = (fblk[b0 + i] & ~0xffu) | u;
         u = fapply(s_f[b0 + i], u);
     }
-    if (b0 < nb && b0 + per >= nb && u != 1) atomicExch(error, 2u);  // the last block's carry out
+    if (!top_ok && b0 < nb && b0 + per >= nb && u != 1) atomicExch(error, 2u);  // the last block's carry out
+}
+
+__global__ void __launch_bounds__(256) crt_scan_warp_kernel(uint32_t* fblk, uint64_t nb, uint64_t njobs,
+                                                          uint32_t* error, int top_ok) {
+    const uint64_t job = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (job >= njobs) return;
+    fblk += job * nb;
+    const uint64_t per = (nb + 31) / 32;  // at most 2
+    const uint64_t b0 = (uint64_t)lane * per;
+    uint32_t f[2] = {kFIdentity, kFIdentity}, hi[2] = {0, 0};
+    uint32_t tf = kFIdentity;
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+        if (i < (int)per && b0 + i < nb) {
+            const uint32_t st = fblk[b0 + i];
+            f[i] = st & 0xffu;
+            hi[i] = st & ~0xffu;
+            tf = fcompose(f[i], tf);
+        }
+    uint32_t incl = tf;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = fcompose(incl, x);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = kFIdentity;
+    uint32_t u = fapply(excl, 1u);
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+        if (i < (int)per && b0 + i < nb) {
+            fblk[b0 + i] = hi[i] | u;
+            u = fapply(f[i], u);
+        }
+    if (!top_ok && b0 < nb && b0 + per >= nb && u != 1) atomicExch(error, 2u);
 }
 
 constexpr int kApplyWarps = 8;
-__global__ void __launch_bounds__(32 * kApplyWarps) crt_apply_kernel(const uint32_t* cin, uint64_t nb,
-                                                                  uint64_t block_words, uint32_t* out,
-                                                                  uint64_t nwords) {
+__global__ void __launch_bounds__(32 * kApplyWarps) crt_apply_kernel(CrtParams P, uint64_t nblocks,
+                                                                  uint64_t block_words) {
     const int lane = threadIdx.x & 31;
-    const uint64_t b = (uint64_t)blockIdx.x * kApplyWarps + (threadIdx.x >> 5);
-    if (b >= nb) return;
-    uint32_t u = cin[b];  // carry + 1 entering the block's first word
+    const uint64_t wb = (uint64_t)blockIdx.x * kApplyWarps + (threadIdx.x >> 5);  // block over all jobs
+    if (wb >= nblocks) return;
+    uint32_t u = P.status[wb] & 0xffu;  // carry + 1 entering the block's first word
     if (u == 1) return;
-    const uint64_t end = min((b + 1) * block_words, nwords);
+    const uint64_t job = wb / P.blocks_per_job;
+    const uint64_t b = wb - job * P.blocks_per_job;
+    const CrtJob J = crt_job(P, job);
+    uint32_t* out = J.out;
+    const uint64_t end = min((b + 1) * block_words, J.nwords);
     for (uint64_t j0 = b * block_words; j0 < end && u != 1; j0 += 128) {
         const uint64_t j = j0 + 4 * (uint64_t)lane;
         int64_t W[4];
@@ -680,6 +762,50 @@ __global__ void __launch_bounds__(32 * kApplyWarps) crt_apply_kernel(const uint3
         }
         u = fapply(total, u);
     }
+}
+
+// Lengths in limbs of the jobs' final words (jobs with a length slot), one warp per job. The job's
+// highest non-zero word lies in its highest block b with a non-zero word at carry-in 0 or a non-zero
+// carry-in: a carry-in adds at most one word above the block's own top (the words above it are zero,
+// so a carry stops there), and a block whose final words were all zero would pass a carry to the
+// block above. So the warp finds b from the status words (scanning down 32 blocks a step), then
+// scans b's final words down from just above its own top.
+__global__ void __launch_bounds__(256) crt_len_kernel(CrtParams P, uint64_t njobs, uint64_t block_words) {
+    const uint64_t job = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (job >= njobs) return;
+    const CrtJob J = crt_job(P, job);
+    if (!J.len) return;
+    const uint32_t* st = P.status + job * P.blocks_per_job;
+    const uint64_t nb = min(P.blocks_per_job, (J.nwords + block_words - 1) / block_words);
+    uint64_t b = ~0ull;
+    uint32_t sb = 0;
+    for (uint64_t top = nb; top > 0; top = top > 32 ? top - 32 : 0) {
+        const uint64_t i = top - 1 - lane;
+        const uint32_t v = top > (uint64_t)lane ? st[i] : 0x1u;  // carry-in 0, no words
+        const uint32_t m = __ballot_sync(0xffffffffu, (v >> 8) != 0 || (v & 0xffu) != 1);
+        if (m) {
+            const int l = __ffs(m) - 1;
+            b = top - 1 - (uint64_t)l;
+            sb = __shfl_sync(0xffffffffu, v, l);
+            break;
+        }
+    }
+    uint32_t len = 0;
+    if (b != ~0ull) {
+        const uint64_t start = b * block_words;
+        const uint64_t end = min(min(start + (uint64_t)(sb >> 8) + 1, (b + 1) * block_words), J.nwords);
+        for (uint64_t top = end; top > start; top = top - start > 32 ? top - 32 : start) {
+            const uint64_t i = top - 1 - lane;
+            const bool nz = top - start > (uint64_t)lane && J.out[i] != 0;
+            const uint32_t m = __ballot_sync(0xffffffffu, nz);
+            if (m) {
+                len = (uint32_t)((top - 1 - (uint64_t)(__ffs(m) - 1)) / 2 + 1);
+                break;
+            }
+        }
+    }
+    if (lane == 0) *J.len = len;
 }
 
 // Short jobs (at most 32 * kCrtWords output words): one warp per job, no look-back. The same
@@ -782,7 +908,7 @@ __global__ void __launch_bounds__(256) crt_warp_kernel(CrtParams P, uint64_t njo
             if (j0 + u < J.nwords) J.out[j0 + u] = o[u];
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    const bool bad = __any_sync(0xffffffffu, spill) || fapply(total, 1u) != 1u;
+    const bool bad = !P.top_ok && (__any_sync(0xffffffffu, spill) || fapply(total, 1u) != 1u);
     if (lane == 0 && bad) atomicExch(P.error, 2u);  // the result does not fit its words
     if (J.len) {
         uint32_t lim = top >= 0 ? (uint32_t)((j0 + top) / 2 + 1) : 0u;

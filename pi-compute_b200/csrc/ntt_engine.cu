@@ -324,22 +324,66 @@ static CrtWideConsts make_crt_wide_consts(int logL) {
     }
     for (int m = 0; m < kWidePrimes; ++m)
         for (int w = 0; w < kWidePrimes - 1; ++w) K.Pw[m][w] = Pw[m][w];
+    // P_5 = P_4 q_4 (five words), floor(P_5 / 2) and its Garner digits (remainders of successive
+    // divisions by q_0 .. q_4)
+    uint32_t P5[kWidePrimes] = {};
+    {
+        uint64_t carry = 0;
+        for (int w = 0; w < kWidePrimes; ++w) {
+            const uint64_t t = (uint64_t)Pw[kWidePrimes - 1][w] * q[kWidePrimes - 1] + carry;
+            P5[w] = (uint32_t)t;
+            carry = t >> 32;
+        }
+    }
+    uint32_t half[kWidePrimes];
+    for (int w = 0; w < kWidePrimes; ++w)
+        half[w] = (P5[w] >> 1) | (w + 1 < kWidePrimes ? (P5[w + 1] << 31) : 0u);
+    for (int kk = 0; kk < kWidePrimes; ++kk) {
+        uint64_t r = 0;
+        for (int w = kWidePrimes - 1; w >= 0; --w) {
+            const uint64_t cur = (r << 32) | half[w];
+            half[w] = (uint32_t)(cur / q[kk]);
+            r = cur % q[kk];
+        }
+        K.h[kk] = (uint32_t)r;
+    }
+    for (int w = 0; w < kWidePrimes; ++w) K.Pi[w] = P5[w];
     return K;
 }
 
+uint64_t crt_wide_block_words() { return (uint64_t)kWideThreads * kWideWords; }
+
 // Wide CRT: every block independently (words with carry-in 0, block transfer functions into
-// c.status), then one block joins the blocks' carries.
-static cudaError_t launch_crt_wide(const CrtParams& c, uint64_t blocks, int logL, cudaStream_t st) {
+// c.status), then a scan per job and the carries applied.
+cudaError_t launch_crt_wide(CrtParams c, uint64_t jobs, uint64_t bpj, int logL, cudaStream_t st, uint64_t* launches) {
+    const bool top_ok = c.top_ok != 0;
+    if (!jobs || !bpj) return cudaSuccess;
+    if (bpj > kFixMaxBlocks) return cudaErrorInvalidValue;
+    c.blocks_per_job = bpj;
+    const uint64_t blocks = jobs * bpj;
     crt_wide_kernel<<<(unsigned)blocks, kWideThreads, 0, st>>>(c, make_crt_wide_consts(logL));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (blocks > kFixMaxBlocks) return cudaErrorInvalidValue;
-    crt_scan_kernel<<<1, kFixThreads, blocks * sizeof(uint32_t), st>>>(c.status, blocks, c.error);
+    if (bpj <= kScanWarpMax)
+        crt_scan_warp_kernel<<<(unsigned)((jobs * 32 + 255) / 256), 256, 0, st>>>(c.status, bpj, jobs, c.error,
+                                                                                 top_ok ? 1 : 0);
+    else
+        crt_scan_kernel<<<(unsigned)jobs, kFixThreads, bpj * sizeof(uint32_t), st>>>(c.status, bpj, c.error,
+                                                                                    top_ok ? 1 : 0);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     crt_apply_kernel<<<(unsigned)((blocks + kApplyWarps - 1) / kApplyWarps), 32 * kApplyWarps, 0, st>>>(
-        c.status, blocks, (uint64_t)kWideThreads * kWideWords, c.out, c.nwords);
-    return cudaGetLastError();
+        c, blocks, crt_wide_block_words());
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    uint64_t n = 3;
+    if (c.merge == 1 || (c.merge == 0 && c.dlen)) {
+        crt_len_kernel<<<(unsigned)((jobs * 32 + 255) / 256), 256, 0, st>>>(c, jobs, crt_wide_block_words());
+        e = cudaGetLastError();
+        ++n;
+    }
+    if (launches) *launches += n;
+    return e;
 }
 
 // The product's launch sequence in one configuration: 32-bit coefficients over three primes, or
@@ -376,6 +420,7 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
         p.job_stride = np * L;
         p.njobs = 1;
         p.merge = 0;
+        p.error = W.sync;  // the product's error word (also the CRT's)
         return p;
     };
     auto set_pass = [&](PassParams& p, int i) { pg::set_pass(p, plan, i); };
@@ -436,7 +481,7 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
     c.blocks_per_job = crt_blocks;
     c.merge = 0;
     if (wide) {
-        e = launch_crt_wide(c, crt_blocks, logL, st);
+        e = launch_crt_wide(c, 1, crt_blocks, logL, st);
     } else {
         c.k = make_crt_consts(logL);
         e = launch_crt(c, crt_blocks, st, nwords);
@@ -448,9 +493,14 @@ static cudaError_t enqueue_impl(const DeviceTables& T, Workspace& W, const uint6
 
 // The smallest na + nb (limbs) that runs in the wide configuration: the context's value, or the
 // environment's PG_WIDE_MIN_LIMBS (read on every call, so that tests can move the boundary).
-static uint64_t wide_min_limbs(const DeviceTables& T) {
+uint64_t wide_min_limbs(const DeviceTables& T) {
     if (const char* e = std::getenv("PG_WIDE_MIN_LIMBS")) return std::strtoull(e, nullptr, 10);
     return T.wide_min_limbs;
+}
+
+bool use_wide(const DeviceTables& T, uint64_t na, uint64_t nb) {
+    const uint64_t wmin = T.wide ? wide_min_limbs(T) : 0;
+    return wmin && na + nb >= wmin && product_logL_wide(na, nb) <= kWideMaxLogL;
 }
 
 cudaError_t enqueue_product_config(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,

@@ -44,6 +44,21 @@ CrtConsts make_crt_consts(int logL);
 // the longest job's word count: jobs of at most 32 * 16 words run one warp each.
 cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st, uint64_t max_words = 0);
 
+// Launch the wide configuration's CRT + carry over `jobs` jobs of blocks_per_job blocks each (any
+// batch form of CrtParams; c.status needs jobs * blocks_per_job words, c.blocks_per_job is set
+// here): the blocks, the per-job scan of their carries, the carry application and, for jobs with a
+// length slot, the lengths (c.top_ok: a carry out of the top word is dropped instead of reported).
+// *launches (if given) counts the kernels.
+cudaError_t launch_crt_wide(CrtParams c, uint64_t jobs, uint64_t blocks_per_job, int logL, cudaStream_t st,
+                            uint64_t* launches = nullptr);
+// Whether a product of na x nb limbs runs in the wide configuration (the context's crossover, or
+// PG_WIDE_MIN_LIMBS; 0 = never).
+struct DeviceTables;
+bool use_wide(const DeviceTables& T, uint64_t na, uint64_t nb);
+uint64_t wide_min_limbs(const DeviceTables& T);
+// Output words per block of the wide CRT.
+uint64_t crt_wide_block_words();
+
 // Stride and four-step block size of pass i.
 void set_pass(PassParams& p, const Plan& plan, int i);
 

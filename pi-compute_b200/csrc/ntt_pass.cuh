@@ -26,6 +26,7 @@
 
 #include "modarith.cuh"
 #include "series.cuh"
+#include "tma.cuh"
 #include "types.cuh"
 
 namespace pg {
@@ -163,7 +164,11 @@ __device__ __forceinline__ uint32_t swz_elem(uint32_t b0, uint32_t q, int qb) {
 // Run the radix rounds of one sub-transform direction over the whole tile.
 // Stages are processed from half size N/2 down to 1 (DIF) or 1 up to N/2 (DIT).
 // Rounds [RR0, RR1) of the schedule run (in the direction's order); the default is all of them.
-template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, int RR0 = 0, int RR1 = 64>
+// TIN: the tile arrived by TMA (layout tma_swz); the first round run reads that layout and writes
+// the passes' own. Every warp's groups of that round cover whole 128-byte lines that no other warp
+// (or other group of the same warp) touches, so the warp only has to finish its reads before it
+// writes (__syncwarp).
+template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, int RR0 = 0, int RR1 = 64, bool TIN = false>
 __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, uint32_t p) {
     constexpr int LOGC = LOGE - LOGN;
     // Radix schedule: the remainder (LOGN % 4 stages) is the top round (largest stride), then
@@ -175,6 +180,7 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
 #pragma unroll
     for (int rr = 0; rr < NROUND; ++rr) {
         if (rr < RR0 || rr >= RR1) continue;
+        const bool tin = TIN && rr == RR0;
         // DIF: the first rounds take the highest stages. DIT: reversed order.
         const int r = INV ? (NROUND - 1 - rr) : rr;
         const bool is_rem = (REM != 0) && (r == 0);
@@ -210,7 +216,22 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                 uint32_t v[R];
                 // A contiguous tile's stride-1 round reads 16 consecutive words: 4 vectors.
                 const bool vec = (LAY == Layout::Contig) && logs == 0;
-                if (vec) {
+                if (tin) {
+                    const uint32_t bt = tma_swz(x0);
+                    if (vec) {
+#pragma unroll
+                        for (int q4 = 0; q4 < R / 4; ++q4) {
+                            const uint4 t = *reinterpret_cast<const uint4*>(sm + tma_elem(bt, 4 * q4, 0));
+                            v[4 * q4] = t.x;
+                            v[4 * q4 + 1] = t.y;
+                            v[4 * q4 + 2] = t.z;
+                            v[4 * q4 + 3] = t.w;
+                        }
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < R; ++q) v[q] = sm[tma_elem(bt, q, qb)];
+                    }
+                } else if (vec) {
 #pragma unroll
                     for (int q4 = 0; q4 < R / 4; ++q4) {
                         const uint4 t = *reinterpret_cast<const uint4*>(sm + swz_elem(b0, 4 * q4, 0));
@@ -227,6 +248,7 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                     dit_round<4>(v, tp, logs, stw, p);
                 else
                     dif_round<4>(v, tp, logs, stw, p);
+                if (tin) __syncwarp();
                 if (vec) {
 #pragma unroll
                     for (int q4 = 0; q4 < R / 4; ++q4)
@@ -260,12 +282,19 @@ __device__ __forceinline__ void tile_transform(uint32_t* sm, const uint2* stw, u
                 constexpr int qb = (LAY == Layout::Strided) ? LOGSR + LOGC : LOGSR;
                 const uint32_t b0 = swz(x0);
                 uint32_t v[R];
+                if (tin) {
+                    const uint32_t bt = tma_swz(x0);
 #pragma unroll
-                for (int q = 0; q < R; ++q) v[q] = sm[swz_elem(b0, q, qb)];
+                    for (int q = 0; q < R; ++q) v[q] = sm[tma_elem(bt, q, qb)];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < R; ++q) v[q] = sm[swz_elem(b0, q, qb)];
+                }
                 if (INV)
                     dit_round<LRX>(v, tp, LOGSR, stw, p);
                 else
                     dif_round<LRX>(v, tp, LOGSR, stw, p);
+                if (tin) __syncwarp();
 #pragma unroll
                 for (int q = 0; q < R; ++q) sm[swz_elem(b0, q, qb)] = v[q];
             }
@@ -307,7 +336,9 @@ __device__ __forceinline__ uint64_t job_offset(const PassParams& P, uint64_t job
     return job * P.job_stride;
 }
 
-// Source limbs of job `job` (first forward pass).
+// Source limbs of job `job` (first forward pass); ncoef counts the source's coefficients (two
+// per limb for 32-bit ones, one for 64-bit ones).
+template <Source SRC>
 __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, const uint32_t*& words,
                                            uint64_t& ncoef) {
     if (P.merge == 2) {
@@ -318,7 +349,7 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
         const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
         const int which = (int)(o % 3);
         words = reinterpret_cast<const uint32_t*>(P.ms.X[which] + child * P.ms.cap[which]);
-        ncoef = 2ull * P.ms.len[3 * child + which];
+        ncoef = (SRC == Source::Limbs64 ? 1ull : 2ull) * P.ms.len[3 * child + which];
     } else {
         words = P.words + job * P.words_stride;
         ncoef = P.ncoef;
@@ -336,9 +367,19 @@ struct RowSrc {
 // The pass kernel. grid = (tiles over all jobs, primes). Tile contents move with 16-byte
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
-template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE, int NP = kNumPrimes>
-__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) ntt_pass_kernel(PassParams P, TwiddleTables T) {
-    extern __shared__ uint32_t sm[];
+//
+// TMA: the tile (residues, uniform job layout) is loaded by the TMA unit from `tmap` (built by the
+// launcher: contiguous tiles as [job][prime][line][32 words], strided ones as
+// [job * NP + prime][block][row][column chunk][32 words]) into the 128-byte-swizzled layout, and the
+// first radix round (or, for an inverse strided tile, the four-step twiddle loop) rewrites it in the
+// passes' own layout. Without TMA the tile is copied by cp.async (tmap unused).
+template <Layout LAY, int LOGN, int LOGE, int NTHREADS, bool INV, Source SRC, Fuse FUSE, int NP = kNumPrimes,
+          bool TMA = false>
+__global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
+    ntt_pass_kernel(PassParams P, TwiddleTables T, const __grid_constant__ CUtensorMap tmap) {
+    extern __shared__ __align__(1024) uint32_t sm[];
+    static_assert(!TMA || (SRC == Source::Residues && FUSE != Fuse::Combine), "TMA tiles hold residues");
+    static_assert(!TMA || LAY == Layout::Contig || LOGE - LOGN >= 5, "TMA strided tiles: rows of >= 32 words");
     constexpr int LOGC = LOGE - LOGN;
     constexpr uint32_t E = 1u << LOGE;
     static_assert(E % (4 * NTHREADS) == 0, "tile copies: whole 16-byte chunks per thread");
@@ -368,7 +409,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
             RowSrc r{nullptr, 0};
             if (R < total_rows) {
                 const uint64_t job = R >> logRows;
-                if constexpr (SRC != Source::Residues) job_source(P, job, r.words, r.ncoef);
+                if constexpr (SRC != Source::Residues) job_source<SRC>(P, job, r.words, r.ncoef);
                 if constexpr (FUSE == Fuse::Combine) {
                     const uint64_t mrg = job / 3;
                     if (job - 3 * mrg == 2) {
@@ -417,7 +458,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
     // A strided tile belongs to one job: its source words are looked up once, not per element.
     const uint32_t* swords = nullptr;
     uint64_t sncoef = 0;
-    if constexpr (SRC != Source::Residues && LAY == Layout::Strided) job_source(P, sjob, swords, sncoef);
+    if constexpr (SRC != Source::Residues && LAY == Layout::Strided) job_source<SRC>(P, sjob, swords, sncoef);
     // 64-bit coefficients: x = hi 2^32 + lo = hi * (2^32 mod p) + lo (mod p)
     uint32_t one_p64 = 0, r32 = 0, r32p = 0;
     if constexpr (SRC == Source::Limbs64) {
@@ -427,6 +468,62 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
     }
 
     // ---- load (4 consecutive elements along the contiguous dimension per thread step)
+    if constexpr (TMA) {
+        // the barrier sits after the tile and its row data (pass_smem's 16 extra bytes)
+        uint64_t* bar = reinterpret_cast<uint64_t*>(
+            reinterpret_cast<char*>(sm) + ((size_t)4 << LOGE) +
+            (LAY == Layout::Strided ? ((size_t)8 << LOGN) : ((size_t)16 << (LOGE - LOGN))));
+        if (threadIdx.x == 0) {
+            mbar_init(bar, 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(bar, 4u << LOGE);
+            if constexpr (LAY == Layout::Contig) {
+                const uint64_t first = (uint64_t)blockIdx.x << LOGE;  // over all jobs' arrays
+                const int job = (int)(first >> P.logL);
+                if (P.logL >= LOGE) {
+                    // boxes of 256 lines (32 KB)
+                    const int line = (int)((first & (P.L - 1)) >> 5);
+#pragma unroll
+                    for (int k = 0; k < ((1 << LOGE) >> 13); ++k)
+                        tma_load_4d(sm + (k << 13), &tmap, bar, 0, line + 256 * k, j, job);
+                } else {
+                    tma_load_4d(sm, &tmap, bar, 0, 0, j, job);  // one box of E / L whole arrays
+                }
+            } else {
+                const int logTpb = P.logS - LOGC;
+                const int blk = (int)(stile >> logTpb);
+                const int cc0 = (int)((stile & ((1ull << logTpb) - 1)) << LOGC) >> 5;
+                const int jp = (int)(sjob * NP + (uint64_t)j);
+                constexpr int kRows = LOGN > 8 ? 256 : (1 << LOGN);
+#pragma unroll
+                for (int k = 0; k < (1 << LOGN) / kRows; ++k)
+                    tma_load_5d(sm + ((k * kRows) << LOGC), &tmap, bar, 0, cc0, k * kRows, blk, jp);
+            }
+        }
+        uint32_t polls = 0;
+        while (!mbar_try_wait(bar, 0)) {
+            if (++polls >= kTmaSpinLimit) {
+                if (P.error) atomicOr(P.error, kErrTmaWait);
+                break;
+            }
+        }
+        if constexpr (INV && LAY == Layout::Strided) {
+            // inverse four-step twiddle, reading the TMA layout and writing the passes' own: each
+            // step's chunks fill whole lines of this warp (8 lanes a line)
+#pragma unroll
+            for (uint32_t it = 0; it < E / (4 * NTHREADS); ++it) {
+                const uint32_t e4 = threadIdx.x * 4 + it * (NTHREADS * 4);
+                const uint32_t m = e4 >> LOGC, c = e4 & ((1u << LOGC) - 1);
+                uint4 x = *reinterpret_cast<uint4*>(sm + tma_swz(e4));
+                fourstep_twiddle4(x, c, m, LOGC, smA[m], rowB, p);
+                __syncwarp();
+                *reinterpret_cast<uint4*>(sm + swz(e4)) = x;
+            }
+        }
+    } else {
 #pragma unroll(LAY == Layout::Strided ? E / (4 * NTHREADS) : 1)
     for (uint32_t it = 0; it < E / (4 * NTHREADS); ++it) {
         const uint32_t e4 = threadIdx.x * 4 + it * (NTHREADS * 4);
@@ -551,10 +648,13 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
             }
         }
     }
+    }  // cp.async load
     __syncthreads();
+    // the first round reads a TMA tile's layout (an inverse strided tile was rewritten above)
+    constexpr bool kTin = TMA && !(INV && LAY == Layout::Strided);
 
     if constexpr (FUSE == Fuse::None || FUSE == Fuse::Combine) {
-        tile_transform<LAY, LOGN, LOGE, NTHREADS, INV>(sm, T.stage[dir][j], p);
+        tile_transform<LAY, LOGN, LOGE, NTHREADS, INV, 0, 64, kTin>(sm, T.stage[dir][j], p);
     } else {
         // Forward rounds but the last; then, per 16-word group, the last forward round (stride 1),
         // the pointwise product and the first inverse round (stride 1, the same 16 words) in
@@ -563,7 +663,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>()) 
         constexpr int NROUND = LOGN / 4 + ((LOGN % 4) ? 1 : 0);
         const uint2* stw_f = T.stage[0][j];
         const uint2* stw_i = T.stage[1][j];
-        tile_transform<LAY, LOGN, LOGE, NTHREADS, false, 0, NROUND - 1>(sm, stw_f, p);
+        tile_transform<LAY, LOGN, LOGE, NTHREADS, false, 0, NROUND - 1, kTin>(sm, stw_f, p);
         constexpr int NG = (1 << LOGE) / 16;
 #pragma unroll 1
         for (uint32_t it = 0; it < NG / NTHREADS; ++it) {

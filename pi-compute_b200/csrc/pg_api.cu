@@ -91,6 +91,7 @@ pg_status check_device_error(pg_ctx* c) {
         cudaMemsetAsync(c->ws.sync, 0, 4, c->stream);
         cudaStreamSynchronize(c->stream);
         if (err == 1) return fail(c, PG_ERR_TIMEOUT, "carry look-back wait ran out of iterations");
+        if (err & 4) return fail(c, PG_ERR_TIMEOUT, "tile load wait ran out of iterations");
         return fail(c, PG_ERR_INTERNAL, "carry out of the most significant word");
     }
     return PG_OK;

@@ -333,6 +333,7 @@ static pg_status enqueue_batch(pg_ctx* ctx, BatchWork* W, const BatchPlan& bp, u
             p.njobs = (uint32_t)m;
             p.merge = 2;
             p.src = W->d_src + (uint64_t)slot * n + k0;
+            p.error = W->errw;
             return p;
         };
         auto forward = [&](uint32_t* data, int slot, Fuse fuse_last, const uint32_t* other) -> cudaError_t {
@@ -412,6 +413,7 @@ static pg_status finish_batch(pg_ctx* ctx, BatchWork* W) {
         cudaMemsetAsync(W->errw, 0, 4, st);
         cudaStreamSynchronize(st);
         if (err == 1) return fail(ctx, PG_ERR_TIMEOUT, "carry look-back wait ran out of iterations");
+        if (err & 4) return fail(ctx, PG_ERR_TIMEOUT, "tile load wait ran out of iterations");
         return fail(ctx, PG_ERR_BAD_ARG, "a job's result is negative (acc = -1 with a*b < c*d)");
     }
     return PG_OK;

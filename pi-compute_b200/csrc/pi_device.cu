@@ -90,19 +90,35 @@ struct SharedProduct {
         cap = want;
     }
 
+    // out[j] = a[j] * b for njobs operands a[j] (a + j sa, na limbs each) and one shared b: b is
+    // transformed once; the jobs run in chunks of the residue budget, in the configuration the
+    // product's size selects (use_wide). With cyc = 2^c limbs (na, nb <= cyc) the product is
+    // cyclic instead: out[j] receives cyc limbs, a[j] b modulo 2^(64 cyc) - 1 up to the carries
+    // near its bottom and top (a middle product: the wrapped-around part lands in the low limbs,
+    // and the carry out of the top is dropped).
     void run(const DeviceTables& T, cudaStream_t st, uint64_t* launches, const uint64_t* a, uint64_t sa, uint64_t na,
-             uint64_t njobs, const uint64_t* b, uint64_t nb, uint64_t* out, uint64_t so) {
+             uint64_t njobs, const uint64_t* b, uint64_t nb, uint64_t* out, uint64_t so, uint64_t cyc = 0) {
         if (!njobs) return;
-        if (product_logL(na, nb) > split_logL()) throw DevError(PG_ERR_TOO_LARGE, "batched product too long");
+        // a cyclic product's length is its own: the wide configuration holds it up to 2^25 limbs
+        const uint64_t wmin = T.wide ? wide_min_limbs(T) : 0;
+        const bool wide = cyc ? (wmin && na + nb >= wmin && ceil_log2(cyc) <= kWideMaxLogL) : use_wide(T, na, nb);
+        if (cyc && (na > cyc || nb > cyc || (cyc & (cyc - 1))))
+            throw DevError(PG_ERR_INTERNAL, "cyclic product operands longer than its length");
+        if (!wide && (cyc ? ceil_log2(2 * cyc) : product_logL(na, nb)) > split_logL())
+            throw DevError(PG_ERR_TOO_LARGE, "batched product too long");
         if ((sa | so) & 1) throw DevError(PG_ERR_INTERNAL, "batched product strides must be even");
         if (!errw) {
             if (pg::dev_malloc((void**)&errw, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "error word");
             cudaMemsetAsync(errw, 0, 4, st);
         }
-        const int logL = product_logL(na, nb);
-        const Plan plan = T.plan(logL);
+        const int logL = cyc ? std::max(ceil_log2(wide ? cyc : 2 * cyc), kMinLogL)
+                             : (wide ? product_logL_wide(na, nb) : product_logL(na, nb));
+        const Plan plan = wide ? T.plan_wide(logL) : T.plan(logL);
+        const TwiddleTables& tw = wide ? T.tw_wide : T.tw;
+        const Source limbs = wide ? Source::Limbs64 : Source::Limbs;
+        const uint64_t per_limb = wide ? 1 : 2;  // transform coefficients per limb
         const int last = plan.npass - 1;
-        const uint64_t L = 1ull << logL, per = 3 * L;
+        const uint64_t L = 1ull << logL, per = (wide ? kWidePrimes : kNumPrimes) * L;
         auto check = [](cudaError_t e) {
             if (e != cudaSuccess) {
                 cudaGetLastError();
@@ -116,7 +132,8 @@ struct SharedProduct {
             p.data = bres;
             p.out = bres;
             p.words = reinterpret_cast<const uint32_t*>(b);
-            p.ncoef = 2 * nb;
+            p.ncoef = per_limb * nb;
+            p.error = errw;
             p.L = L;
             p.logL = logL;
             p.job_stride = per;
@@ -124,14 +141,15 @@ struct SharedProduct {
             p.njobs = 1;
             for (int i = 0; i < plan.npass; ++i) {
                 set_pass(p, plan, i);
-                check(launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues, Fuse::None, p, T.tw, st));
+                check(launch_pass(plan, i, false, i == 0 ? limbs : Source::Residues, Fuse::None, p, tw, st));
                 ++*launches;
             }
         }
         const uint64_t budget = 256ull << 20;  // residue words per chunk of jobs
         const uint64_t m_max = std::max<uint64_t>(1, budget / per);
-        const uint64_t nwords = 2 * (na + nb);
-        const uint64_t bpj = (nwords + kCrtThreads * kCrtWords - 1) / (kCrtThreads * kCrtWords);
+        const uint64_t nwords = cyc ? 2 * cyc : 2 * (na + nb);
+        const uint64_t block_words = wide ? crt_wide_block_words() : (uint64_t)kCrtThreads * kCrtWords;
+        const uint64_t bpj = (nwords + block_words - 1) / block_words;
         for (uint64_t j0 = 0; j0 < njobs; j0 += m_max) {
             const uint64_t m = std::min(m_max, njobs - j0);
             grow(&res, res_cap, m * per, st);
@@ -140,7 +158,8 @@ struct SharedProduct {
             p.out = res;
             p.words = reinterpret_cast<const uint32_t*>(a + j0 * sa);
             p.words_stride = 2 * sa;
-            p.ncoef = 2 * na;
+            p.ncoef = per_limb * na;
+            p.error = errw;
             p.L = L;
             p.logL = logL;
             p.job_stride = per;
@@ -149,17 +168,15 @@ struct SharedProduct {
             p.njobs = (uint32_t)m;
             for (int i = 0; i < plan.npass; ++i) {
                 set_pass(p, plan, i);
-                check(launch_pass(plan, i, false, i == 0 ? Source::Limbs : Source::Residues,
-                                  i == last ? Fuse::MulInverse : Fuse::None, p, T.tw, st));
+                check(launch_pass(plan, i, false, i == 0 ? limbs : Source::Residues,
+                                  i == last ? Fuse::MulInverse : Fuse::None, p, tw, st));
                 ++*launches;
             }
             for (int i = last - 1; i >= 0; --i) {
                 set_pass(p, plan, i);
-                check(launch_pass(plan, i, true, Source::Residues, Fuse::None, p, T.tw, st));
+                check(launch_pass(plan, i, true, Source::Residues, Fuse::None, p, tw, st));
                 ++*launches;
             }
-            grow(&sync, sync_cap, m + m * bpj, st);
-            check(cudaMemsetAsync(sync, 0, (m + m * bpj) * 4, st));
             CrtParams c{};
             c.res = res;
             c.res_stride = per;
@@ -167,14 +184,23 @@ struct SharedProduct {
             c.nwords = nwords;
             c.out = reinterpret_cast<uint32_t*>(out + j0 * so);
             c.out_stride = 2 * so;
-            c.ticket = sync;
-            c.status = sync + m;
             c.error = errw;
-            c.blocks_per_job = bpj;
-            c.k = make_crt_consts(logL);
             c.merge = 0;
-            check(launch_crt(c, m * bpj, st, nwords));
-            ++*launches;
+            c.top_ok = cyc ? 1 : 0;
+            if (wide) {
+                grow(&sync, sync_cap, m * bpj, st);
+                c.status = sync;
+                check(launch_crt_wide(c, m, bpj, logL, st, launches));
+            } else {
+                grow(&sync, sync_cap, m + m * bpj, st);
+                check(cudaMemsetAsync(sync, 0, (m + m * bpj) * 4, st));
+                c.ticket = sync;
+                c.status = sync + m;
+                c.blocks_per_job = bpj;
+                c.k = make_crt_consts(logL);
+                check(launch_crt(c, m * bpj, st, nwords));
+                ++*launches;
+            }
         }
     }
 
@@ -739,6 +765,295 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
                      std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tw0).count());
 }
 
+// ------------------------------------------------------------------ pi's digits by a scaled remainder tree
+// The n = digits + 1 decimal digits of floor(pi 10^digits) are the first n digits of y = pi / 10
+// in (0, 1). Digit positions count from the most significant (position 0 is the "3"), padded on
+// the low side to 2^J. A node of the tree covers positions [s, s + m) and holds the fraction
+// v = frac(y 10^s), whose first m digits are the node's; its children are (s, m/2) holding v itself
+// and (s + m/2, m/2) holding frac(v 10^(m/2)). Each node keeps v to w limbs (v ~= V / 2^(64 w)):
+// the high child takes V's top limbs, the low child the top limbs of the low w limbs of
+// V * 10^(m/2), a middle product that one cyclic transform of about w limbs gives (the part that
+// wraps around lands below the limbs taken). So the conversion is one batched product per level
+// (all nodes share 10^(m/2)) and no division; 1024-digit leaves are written by one warp each
+// multiplying its fraction by 10^19. Precision: a leaf keeps 1024 log2(10) + 128 bits, and a node
+// w(lo) + ceil((m/2) log2(10) / 64) + 1 limbs, so the error of 10^(m/2) v (a few units of V's last
+// limb, times 10^(m/2)) stays below one unit of the low child's last limb at every level. A leaf
+// whose remaining fraction ends within 2^-128 of 0 or 1 cannot be trusted (the digits next to it
+// may carry); it raises a flag and the caller converts exactly instead (expected about once in
+// 2^120 leaves).
+constexpr int kSrtLeafLog = 10;
+constexpr int kSrtGuardBits = 128;
+constexpr double kLog2Ten = 3.3219280948873623;
+
+// Children of a level: child j (parent i = j / 2) takes limbs [off, off + wc) of the parent's fraction
+// (even j) or of its cyclic product with 10^(m/2) (odd j). Blocks of 256 threads copy 2048 limbs each.
+__global__ void srt_children_kernel(const uint64_t* Y, uint64_t wy, const uint64_t* prod, uint64_t wp, uint64_t off,
+                                    uint64_t* out, uint64_t wc, uint64_t nchild, uint64_t segs) {
+    const uint64_t j = blockIdx.x / segs, seg = blockIdx.x - j * segs;
+    if (j >= nchild) return;
+    const uint64_t i = j >> 1;
+    const uint4* src = reinterpret_cast<const uint4*>(((j & 1) ? prod + i * wp : Y + i * wy) + off);
+    uint4* dst = reinterpret_cast<uint4*>(out + j * wc);
+    const uint64_t pairs = wc / 2;
+    for (uint64_t q = seg * 1024 + threadIdx.x; q < min(pairs, (seg + 1) * 1024); q += blockDim.x) dst[q] = src[q];
+}
+
+// One warp per leaf: the fraction V / 2^(64 wl) (wl <= 64 limbs, two per lane) is multiplied by 10^19
+// fifty-three times and by 10^17 once; each product's integer part is the next 19 (17) digits. A
+// product's limb sums carry between lanes by a warp-wide carry-lookahead (generate / propagate
+// ballots). Digits at positions >= n are not written. flag |= 1 when the remaining fraction lies within
+// 2^-128 of 0 or 1.
+constexpr int kSrtChunks = 54;
+__global__ void __launch_bounds__(128) srt_leaves_kernel(const uint64_t* Y, uint64_t wl, uint64_t nleaves,
+                                                         uint64_t n, char* out, uint32_t* flag) {
+    __shared__ uint64_t s_chunk[4][kSrtChunks];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t leaf = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (leaf >= nleaves) return;  // whole warps
+    const int nl = (int)(wl / 2);  // lanes holding limbs
+    const uint64_t* y = Y + leaf * wl;
+    uint64_t f0 = lane < nl ? y[2 * lane] : 0, f1 = lane < nl ? y[2 * lane + 1] : 0;
+    for (int step = 0; step < kSrtChunks; ++step) {
+        const uint64_t M = step < kSrtChunks - 1 ? 10000000000000000000ull : 100000000000000000ull;
+        const uint64_t lo0 = f0 * M, hi0 = __umul64hi(f0, M);
+        const uint64_t lo1 = f1 * M, hi1 = __umul64hi(f1, M);
+        uint64_t hp = __shfl_up_sync(0xffffffffu, hi1, 1);
+        if (lane == 0) hp = 0;
+        const uint64_t s0 = lo0 + hp;
+        const uint32_t c0 = s0 < lo0;
+        const uint64_t s1 = lo1 + hi0;
+        const uint32_t c1 = s1 < lo1;
+        const uint64_t s1b = s1 + c0;
+        const uint32_t g = c1 | (c0 & (s1b == 0));
+        const uint32_t pr = (s0 == ~0ull) & (s1b == ~0ull);
+        const uint32_t G = __ballot_sync(0xffffffffu, g), P = __ballot_sync(0xffffffffu, pr);
+        const uint32_t a = G | P;
+        const uint32_t cm = (a + G) ^ a ^ G;  // bit l: carry into lane l
+        const uint32_t cin = (cm >> lane) & 1u;
+        const uint64_t r0 = s0 + cin;
+        const uint32_t cr0 = cin & (r0 == 0);
+        f0 = r0;
+        f1 = s1b + cr0;
+        // the integer part: the top limb's high word plus the carry out of the top lane
+        if (lane == nl - 1) s_chunk[warp][step] = hi1 + ((cm >> nl) & 1u);
+    }
+    if (lane == nl - 1 && ((f1 == 0 && f0 == 0) || (f1 == ~0ull && f0 == ~0ull))) atomicOr(flag, 1u);
+    __syncwarp();
+    const uint64_t base = leaf << kSrtLeafLog;
+    for (int c = lane; c < kSrtChunks; c += 32) {
+        uint64_t v = s_chunk[warp][c];
+        const int nd = c < kSrtChunks - 1 ? 19 : 17;
+        const uint64_t p0 = base + 19ull * c;
+        for (int d = nd - 1; d >= 0; --d) {
+            const uint64_t q = v / 10;
+            if (p0 + d < n) out[p0 + d] = (char)('0' + (v - q * 10));
+            v = q;
+        }
+    }
+}
+
+// Limbs per node at each level (t = 0 .. J - kSrtLeafLog, the last the leaves) and live nodes, for n
+// digit positions padded to 2^J.
+struct SrtPlan {
+    int J = 0;
+    uint64_t n = 0;
+    std::vector<uint64_t> w, live;
+};
+
+uint64_t srt_peel_limbs(uint64_t m) {  // limbs 10^(m/2) can span: ceil((m/2) log2(10) / 64)
+    return (uint64_t)std::ceil((double)(m / 2) * kLog2Ten / 64.0) + 1;
+}
+
+// w of the node (s, m): its kept digits min(m, n - s) and its live children decide it.
+uint64_t srt_node_limbs(uint64_t s, uint64_t m, uint64_t n, uint64_t wleaf) {
+    if (m <= (1ull << kSrtLeafLog)) return wleaf;
+    const uint64_t wh = srt_node_limbs(s, m / 2, n, wleaf);
+    if (s + m / 2 >= n) return wh;
+    const uint64_t wl = srt_node_limbs(s + m / 2, m / 2, n, wleaf);
+    uint64_t w = std::max(wh, wl + srt_peel_limbs(m) + 1);
+    return (w + 1) & ~1ull;  // even: 16-byte aligned nodes
+}
+
+SrtPlan srt_plan(uint64_t n) {
+    SrtPlan P;
+    P.n = n;
+    P.J = kSrtLeafLog;
+    while ((1ull << P.J) < n) ++P.J;
+    const uint64_t wleaf = ((uint64_t)std::ceil(((1ull << kSrtLeafLog) * kLog2Ten + kSrtGuardBits) / 64.0) + 1) & ~1ull;
+    for (int t = 0; t <= P.J - kSrtLeafLog; ++t) {
+        const uint64_t m = 1ull << (P.J - t);
+        // the first node of a level is full, or (at the top) the only live one: it needs the most
+        P.w.push_back(srt_node_limbs(0, m, n, wleaf));
+        P.live.push_back((n + m - 1) / m);
+    }
+    return P;
+}
+
+// y = pi / 10 to w limbs, V ~= y 2^(64 w) within a few units, from the series root Q, R: the final
+// formula's truncated reciprocal, square root and products, 42688 sqrt(10005) Q / R.
+void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R, uint64_t w) {
+    if (Q.sign <= 0 || R.sign <= 0) throw DevError(PG_ERR_BAD_ARG, "final formula needs Q, R > 0");
+    const size_t k = 64 * w + 64;  // relative error 2^(5 - k): below 2^-59 of V's last unit
+    const size_t bQ = A.bits(Q), bR = A.bits(R);
+    Num Qt(A), Rt(A), Z(A), S(A), t(A);
+    const long long eQ = (long long)bQ - (long long)k;
+    const long long eR = (long long)bR - (long long)k;
+    if (eQ >= 0) A.tdiv_q_2exp(Qt, Q, (size_t)eQ); else A.shl(Qt, Q, (size_t)-eQ);
+    if (eR >= 0) A.tdiv_q_2exp(Rt, R, (size_t)eR); else A.shl(Rt, R, (size_t)-eR);
+    {
+        Timer tm("reciprocal of R");
+        recip_floor(A, Z, Rt, false);
+    }
+    {
+        Timer tm("sqrt(10005)");
+        sqrt_scaled(A, S, 10005, k, false);
+    }
+    Timer tm("two truncated products");
+    A.mul_ui(V, Qt, 42688);
+    long long e = eQ - eR - 3 * (long long)k;  // pi / 10 = V 2^e (before the truncations below)
+    auto mul_trunc = [&](const DevNum& y) {
+        A.mul(t, V, y);
+        const long long over = (long long)A.bits(t) - (long long)k;
+        if (over > 0) {
+            A.tdiv_q_2exp(V, t, (size_t)over);
+            e += over;
+        } else {
+            A.copy(V, t);
+        }
+    };
+    mul_trunc(S);
+    mul_trunc(Z);
+    const long long sh = e + 64 * (long long)w;  // V 2^e = (V 2^sh) / 2^(64 w)
+    if (sh >= 0) A.shl(V, V, (size_t)sh); else A.fdiv_q_2exp(V, V, (size_t)-sh);
+}
+
+// Whether every level of the tree fits one transform of the batched product.
+bool srt_fits(const SrtPlan& P) {
+    for (size_t t = 0; t + 1 < P.w.size(); ++t)
+        if (ceil_log2(2 * P.w[t] + 64) > kWideMaxLogL + 1) return false;
+    return true;
+}
+
+// out[0 .. n) = the first n digits of V / 2^(64 w[0]) (V: the root's fraction). Returns false if a
+// leaf's digits could not be trusted (the caller then converts exactly).
+bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, char* out) {
+    cudaStream_t st = A.stream();
+    const int levels = (int)P.w.size() - 1;  // product levels; P.w[levels] is the leaves'
+    const uint64_t n = P.n;
+    if (n > sp.digits_cap) {
+        A.sync();
+        if (sp.digits) cudaFree(sp.digits);
+        sp.digits = nullptr;
+        sp.digits_cap = 0;
+        if (pg::dev_malloc((void**)&sp.digits, n) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
+        sp.digits_cap = n;
+    }
+    // powers 10^(2^j), j = kSrtLeafLog .. J - 1
+    std::vector<Num*> pw;
+    struct Owner {
+        std::vector<Num*>& a;
+        ~Owner() {
+            for (auto* p : a) delete p;
+        }
+    } own{pw};
+    {
+        Timer tm("power tree");
+        Num p(A);
+        A.set_ui(p, 10);
+        for (int j = 0; j < P.J; ++j) {
+            if (j >= kSrtLeafLog) {
+                pw.push_back(new Num(A));
+                A.exact(p);
+                A.copy(*pw.back(), p);
+            }
+            if (j + 1 < P.J) A.sqr(p, p);
+        }
+    }
+    // level t peels 10^(2^(J - t - 1)), t < levels = J - kSrtLeafLog
+    auto power = [&](int t) -> DevNum& { return pw[(size_t)(P.J - t - 1 - kSrtLeafLog)]->v; };
+    Timer tm("tree levels and leaves");
+    Num lv0(A), lv1(A), prod(A);
+    DevNum* cur = &lv0.v;
+    DevNum* nxt = &lv1.v;
+    A.reserve(*cur, P.w[0]);
+    // the root: V's w[0] limbs (V < 2^(64 w[0]); shorter V is padded with zeros)
+    A.exact(V);
+    if (V.n > P.w[0]) throw DevError(PG_ERR_INTERNAL, "pi digits: root fraction longer than its precision");
+    cudaMemsetAsync(cur->d, 0, P.w[0] * 8, st);
+    if (V.n) cudaMemcpyAsync(cur->d, V.d, V.n * 8, cudaMemcpyDeviceToDevice, st);
+    for (int t = 0; t < levels; ++t) {
+        const uint64_t m = 1ull << (P.J - t), wt = P.w[t], wc = P.w[t + 1];
+        const uint64_t kids = P.live[t + 1];
+        const uint64_t klo = n > m / 2 ? (n - m / 2 + m - 1) / m : 0;  // parents with a live low child
+        const DevNum& T = power(t);
+        uint64_t cyc = 1;
+        while (cyc < std::max(wt, T.n + wc + 8)) cyc <<= 1;
+        if (klo) {
+            A.reserve(prod, klo * cyc);
+            sp.run(A.tables(), st, A.launches(), cur->d, wt, wt, klo, T.d, T.n, prod.v.d, cyc, cyc);
+        }
+        A.reserve(*nxt, kids * wc);
+        const uint64_t segs = (wc / 2 + 1023) / 1024;
+        srt_children_kernel<<<(unsigned)(kids * segs), 256, 0, st>>>(cur->d, wt, prod.v.d, cyc, wt - wc, nxt->d, wc,
+                                                                    kids, segs);
+        ++*A.launches();
+        std::swap(cur, nxt);
+    }
+    uint32_t* flag = sp.flags;
+    if (!flag || sp.flags_cap < 1) {
+        A.sync();
+        if (sp.flags) cudaFree(sp.flags);
+        sp.flags = nullptr;
+        sp.flags_cap = 0;
+        if (pg::dev_malloc((void**)&sp.flags, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
+        sp.flags_cap = 1;
+        flag = sp.flags;
+    }
+    cudaMemsetAsync(flag, 0, 4, st);
+    const uint64_t leaves = P.live[levels];
+    srt_leaves_kernel<<<(unsigned)((leaves * 32 + 127) / 128), 128, 0, st>>>(cur->d, P.w[levels], leaves, n, sp.digits,
+                                                                           flag);
+    ++*A.launches();
+    if (sp.error(st)) throw DevError(PG_ERR_INTERNAL, "pi digits: product check failed");
+    uint32_t hf = 0;
+    cudaMemcpyAsync(&hf, flag, 4, cudaMemcpyDeviceToHost, st);
+    A.sync();
+    if (hf) return false;
+    if (cudaMemcpyAsync(out, sp.digits, n, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        throw DevError(PG_ERR_DEVICE, "digit copy");
+    A.sync();
+    return true;
+}
+
+// "3." and `digits` digits of pi into out from the series root Q, R: the scaled remainder tree when
+// every level fits one transform and no leaf is in doubt, otherwise the exact final formula and
+// divide-and-conquer conversion.
+void pi_digits(DevArith& A, SharedProduct& sp, const DevNum& Q, const DevNum& R, size_t digits, char* out,
+               double* t_final) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const SrtPlan P = srt_plan(digits + 1);
+    const bool tree = srt_fits(P) && !std::getenv("PG_EXACT_CONVERSION");
+    char* body = out + 1;  // the integer's digits: "3" then the fraction digits
+    if (tree) {
+        Num V(A);
+        pi_tenth_fraction(A, V, Q, R, P.w[0]);
+        A.sync();
+        if (t_final) *t_final = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (srt_digits(A, sp, P, V, body)) {
+            out[0] = body[0];
+            out[1] = '.';
+            return;
+        }
+    }
+    Num X(A);
+    final_formula(A, X, Q, R, digits);
+    A.sync();
+    if (t_final && !tree) *t_final = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    to_decimal(A, sp, X, digits + 1, body);
+    out[0] = body[0];
+    out[1] = '.';
+}
+
 // ------------------------------------------------------------------ checkpoints
 // Writes one integer held in HBM in the checkpoint format (ckpt_io.h): the header, then its
 // bytes streamed through the pinned staging buffers.
@@ -1104,14 +1419,10 @@ pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t
     return pg::guarded(ctx, [&] {
         pg::FinishState& fs = *pg::ctx_finish(ctx);
         pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
-        pg::Num Q(A), R(A), X(A);
+        pg::Num Q(A), R(A);
         A.upload(Q, q, nq, 1);
         A.upload(R, r, nr, 1);
-        pg::final_formula(A, X, Q, R, digits);
-        // floor(pi 10^digits) has digits + 1 decimal digits: "3" then the fraction
-        pg::to_decimal(A, fs.sp, X, digits + 1, out + 1);
-        out[0] = out[1];
-        out[1] = '.';
+        pg::pi_digits(A, fs.sp, Q, R, digits, out, nullptr);
     });
 }
 
@@ -1138,7 +1449,7 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
         pg::FinishState& fs = *pg::ctx_finish(ctx);
         pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
         // Q, R of the root (both positive for a = 0)
-        pg::Num Q(A), R(A), X(A);
+        pg::Num Q(A), R(A);
         if (big) {
             pg::Node x(A);
             pg_ckpt_report rep{};
@@ -1160,12 +1471,7 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
             R.v.sign = hl[2] ? 1 : 0;
             Q.v.slack = R.v.slack = 0;
         }
-        pg::final_formula(A, X, Q, R, digits);
-        t_final = secs(t1);
-        char* body = out + 1;  // the integer's digits: "3" then the fraction digits
-        pg::to_decimal(A, fs.sp, X, digits + 1, body);
-        out[0] = body[0];
-        out[1] = '.';
+        pg::pi_digits(A, fs.sp, Q, R, digits, out, &t_final);
     });
     if (seconds) {
         seconds[0] = t_bs;

@@ -140,6 +140,7 @@ struct PassParams {
     uint64_t comb_slot;
     uint64_t comb_a0, comb_b0;  // the splitting's range and this level's depth (R's sign per merge)
     int comb_depth;
+    uint32_t* error;         // optional: bounded waits that give up OR a flag into it (TMA tile loads)
 };
 
 struct CrtConsts {
@@ -186,6 +187,9 @@ struct CrtParams {
     // launch_crt fills both from the environment (PG_TEST_CRT_SPIN_LIMIT, PG_TEST_CRT_WITHHOLD).
     uint32_t spin_limit;
     uint32_t withhold1;
+    // 1: a carry out of a job's top word is dropped instead of reported (a wrapped product, whose
+    // words past the transform length are not wanted).
+    int top_ok;
 };
 
 constexpr int kCrtThreads = 256;

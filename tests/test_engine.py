@@ -158,6 +158,36 @@ def test_batched_bs_matches_oracle(lib, a, b):
     assert bs(lib, a, b, BATCHED) == oracle.bs(a, b), (a, b)
 
 
+@pytest.fixture(params=["1", "0"], ids=["wide", "narrow"])
+def bs_config(request):
+    """Every transform level of the splitting in the wide configuration (64-bit coefficients over
+    five primes, PG_WIDE_MIN_LIMBS=1) or none of them (0); read whenever a range is planned."""
+    old = os.environ.get("PG_WIDE_MIN_LIMBS")
+    os.environ["PG_WIDE_MIN_LIMBS"] = request.param
+    yield request.param
+    if old is None:
+        os.environ.pop("PG_WIDE_MIN_LIMBS", None)
+    else:
+        os.environ["PG_WIDE_MIN_LIMBS"] = old
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("a,b", [(0, 79), (100, 357), (0, 1000), (1000, 9000), (0, 4097), (12345, 31000),
+                                 (0, 70000)])
+def test_batched_bs_both_configurations(lib, bs_config, a, b):
+    # merges whose R^ subtracts (centred CRT lift) and adds both occur at every level
+    assert bs(lib, a, b, BATCHED) == oracle.bs(a, b), (a, b, bs_config)
+
+
+@pytest.mark.gpu
+def test_batched_bs_golden_hash_1m_terms_both_configurations(lib, bs_config):
+    g = json.load(open(os.path.join(GOLDEN, "bs_golden.json")))
+    for key, hs in g["hash_ranges"].items():
+        a, b = map(int, key.split(","))
+        vals = bs(lib, a, b, BATCHED)
+        assert [hashlib.sha256(hex(v).encode()).hexdigest() for v in vals] == hs, (key, bs_config)
+
+
 @pytest.mark.gpu
 def test_batched_bs_golden_hash_1m_terms(lib):
     g = json.load(open(os.path.join(GOLDEN, "bs_golden.json")))

@@ -82,6 +82,16 @@ def test_to_decimal_matches_str(eng, nd):
     assert eng.to_decimal(x, nd) == str(x).zfill(nd)
 
 
+@pytest.mark.parametrize("wmin", ["1", "0"], ids=["wide", "narrow"])
+@pytest.mark.parametrize("nd", [300_007, 2_000_000])
+def test_to_decimal_both_configurations(eng, wmin, nd, monkeypatch):
+    # the conversion's batched products (one shared power per level) in either configuration
+    monkeypatch.setenv("PG_WIDE_MIN_LIMBS", wmin)
+    x = rnd_bits(max(1, int(nd * 3.3219280948873623) - 2), nd + 1) % (10 ** nd)
+    x = x - x % 10**40 + (10**40 - 1)  # a run of nines at the bottom: long carries
+    assert eng.to_decimal(x, nd) == str(x).zfill(nd)
+
+
 def test_to_decimal_edges(eng):
     assert eng.to_decimal(0, 5) == "00000"
     assert eng.to_decimal(7, 300) == "0" * 299 + "7"
@@ -157,6 +167,20 @@ def test_pg_pi_prefixes(eng, digits):
         assert got == ref[: digits + 2]
     else:
         assert got[:1002] == ref
+
+
+@pytest.mark.parametrize("digits", [1022, 1023, 1024, 2047, 2048, 2049, 4095, 70_001, 1_048_575, 1_048_577])
+def test_pg_pi_tree_conversion_matches_exact_conversion(eng, digits, monkeypatch):
+    """The digits come from the scaled remainder tree (a fraction of pi / 10 split by batched
+    middle products, no division); with PG_EXACT_CONVERSION set they come from the exact final
+    formula and divide-and-conquer conversion instead. Both must agree everywhere, at leaf and level
+    boundaries of the tree included."""
+    ref = open(os.path.join(GOLDEN, "pi_1000.txt")).read().strip()
+    tree = eng.pi(digits)
+    monkeypatch.setenv("PG_EXACT_CONVERSION", "1")
+    exact = eng.pi(digits)
+    assert tree == exact
+    assert tree.decode()[:min(digits, 1000) + 2] == ref[:min(digits, 1000) + 2]
 
 
 def test_pg_pi_repeated_and_interleaved_runs(eng):
