@@ -75,6 +75,55 @@ __device__ __forceinline__ void sb_addsub(uint64_t* x, int n, const uint64_t* y,
     }
 }
 
+// Carry resolution of n <= 32 * K limbs across a warp: limb i's value before carries is v(i), a
+// signed 128-bit number in (-2^65, 3 * 2^64); the carries between limbs lie in {-1, 0, 1, 2}. Each
+// lane takes K consecutive limbs, tabulates its carry transfer function (carry in -> carry out, four
+// two-bit entries of carry + 1), and a warp scan of the functions gives every lane its carry in.
+// Writes dst[0 .. n) and returns the length without leading zero limbs (in every lane).
+template <int K, class V>
+__device__ __forceinline__ int warp_resolve(V v, int n, uint64_t* dst) {
+    typedef __int128 i128;
+    const int lane = threadIdx.x & 31;
+    const int c0 = lane * K;
+    i128 val[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) val[i] = c0 + i < n ? v(c0 + i) : 0;
+    auto apply = [](uint32_t f, uint32_t u) { return (f >> (2 * u)) & 3u; };
+    auto compose = [&](uint32_t g, uint32_t f) {  // g after f
+        return apply(g, apply(f, 0)) | (apply(g, apply(f, 1)) << 2) | (apply(g, apply(f, 2)) << 4) |
+               (apply(g, apply(f, 3)) << 6);
+    };
+    uint32_t f = 0;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        long long c = u - 1;
+#pragma unroll
+        for (int i = 0; i < K; ++i) c = (long long)((val[i] + c) >> 64);
+        const long long uo = c + 1 < 0 ? 0 : (c + 1 > 3 ? 3 : c + 1);  // out of range only off the real path
+        f |= (uint32_t)uo << (2 * u);
+    }
+    uint32_t incl = f;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
+        if (lane >= off) incl = compose(incl, x);
+    }
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) excl = 0u | (1u << 2) | (2u << 4) | (3u << 6);
+    long long c = (long long)apply(excl, 1u) - 1;
+    int top = -1;
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        if (c0 + i < n) {
+            const i128 t = val[i] + c;
+            dst[c0 + i] = (uint64_t)t;
+            if ((uint64_t)t) top = c0 + i;
+            c = (long long)(t >> 64);
+        }
+    }
+    return __reduce_max_sync(0xffffffffu, top) + 1;
+}
+
 // Leaf magnitudes of term k (binary_splitting.cpp:137-159): |P| = (6k-5)(2k-1)(6k-1),
 // Q = k^3 * 640320^3/24, |R| = |P| * (13591409 + 545140134 k); k = 0: 1, 1, 13591409.
 __device__ void leaf_values(uint64_t k, uint64_t P[2], int& nP, uint64_t Q[3], int& nQ, uint64_t R[3], int& nR) {
@@ -216,7 +265,8 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
     node_range(a0, b0, depth, m, a, b);
     const int sgn = merge_r_sign(a, b);
 
-    // product helper: column sums then lane-0 carry pass into dst (nx + ny limbs)
+    // product helper: column sums, then the warp's carry resolution into dst (nx + ny limbs)
+    constexpr int KR = (2 * MAXC + 1 + 31) / 32;
     auto product = [&](int ox, int oy, uint64_t* dst) -> int {
         const int nx = n[ox], ny = n[oy];
         const uint64_t* x = s_op[warp][ox];
@@ -239,25 +289,20 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
             s_col[warp][2][c] = hi;
         }
         __syncwarp();
-        int len = 0;
-        if (lane == 0) {
-            u128 carry = 0;  // < 2^129 never happens: column sums < MAXC * 2^128 << 2^192
-            uint64_t carry_hi = 0;
-            for (int c = 0; c < nx + ny; ++c) {
-                uint64_t lo = c < ncol ? s_col[warp][0][c] : 0;
-                uint64_t mid = c < ncol ? s_col[warp][1][c] : 0;
-                uint64_t hi = c < ncol ? s_col[warp][2][c] : 0;
-                const u128 t0 = (u128)lo + (uint64_t)carry;
-                dst[c] = (uint64_t)t0;
-                const u128 t1 = (u128)mid + (uint64_t)(carry >> 64) + (uint64_t)(t0 >> 64);
-                const uint64_t nh = hi + carry_hi + (uint64_t)(t1 >> 64);
-                carry = ((u128)nh << 64) | (uint64_t)t1;
-                carry_hi = 0;
-            }
-            len = sb_len(dst, nx + ny);
-        }
+        // limb c = lo_c + mid_{c-1} + hi_{c-2} (each < 2^64; column sums < MAXC 2^128, so hi < MAXC)
+        const uint64_t* cl = s_col[warp][0];
+        const uint64_t* cm = s_col[warp][1];
+        const uint64_t* ch = s_col[warp][2];
+        const int len = warp_resolve<KR>(
+            [&](int c) {
+                __int128 t = c < ncol ? cl[c] : 0;
+                if (c >= 1 && c - 1 < ncol) t += cm[c - 1];
+                if (c >= 2 && c - 2 < ncol) t += ch[c - 2];
+                return t;
+            },
+            nx + ny, dst);
         __syncwarp();
-        return __shfl_sync(0xffffffffu, len, 0);
+        return len;
     };
 
     // P = Pl * Pr
@@ -280,17 +325,21 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
     {
         const int lx = product(4, 2, s_res[warp][0]);
         const int ly = product(0, 5, s_res[warp][1]);
-        // |R| < 2 max(|Qr Rl|, |Pl Rr|): max(lx, ly) + 1 limbs
+        // |R| < 2 max(|Qr Rl|, |Pl Rr|): max(lx, ly) + 1 limbs; limb i = x_i + sgn y_i before carries
         const int nr = (lx > ly ? lx : ly) + 1;
-        if (lane == 0) {
-            uint64_t* x = s_res[warp][0];
-            for (int t = lx; t < nr; ++t) x[t] = 0;
-            sb_addsub(x, nr, s_res[warp][1], ly, sgn);
-        }
+        const uint64_t* x = s_res[warp][0];
+        const uint64_t* y = s_res[warp][1];
+        uint64_t* r = s_res[warp][0];  // in place over x: every lane reads its limbs before any writes
+        const int lr = warp_resolve<KR>(
+            [&](int i) {
+                const __int128 xi = i < lx ? x[i] : 0, yi = i < ly ? y[i] : 0;
+                return sgn > 0 ? xi + yi : xi - yi;
+            },
+            nr, r);
         __syncwarp();
         uint64_t* dst = out.X[2] + m * out.cap[2];
         for (int t = lane; t < (int)out.cap[2]; t += 32) dst[t] = t < nr ? s_res[warp][0][t] : 0;
-        if (lane == 0) out.len[3 * m + 2] = sb_len(s_res[warp][0], nr < (int)out.cap[2] ? nr : out.cap[2]);
+        if (lane == 0) out.len[3 * m + 2] = lr < (int)out.cap[2] ? lr : out.cap[2];
         __syncwarp();
     }
 }

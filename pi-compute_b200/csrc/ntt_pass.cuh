@@ -364,7 +364,7 @@ struct RowSrc {
     uint64_t ncoef;
 };
 
-// The pass kernel. grid = (tiles over all jobs, primes). Tile contents move with 16-byte
+// The pass kernel. grid = tiles over all jobs x primes (1-D, tile-major). Tile contents move with 16-byte
 // vector accesses along the contiguous dimension. Job j's residues are the array at
 // data + j * job_stride (prime i at + i * L).
 //
@@ -383,7 +383,10 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
     constexpr int LOGC = LOGE - LOGN;
     constexpr uint32_t E = 1u << LOGE;
     static_assert(E % (4 * NTHREADS) == 0, "tile copies: whole 16-byte chunks per thread");
-    const int j = blockIdx.y;  // prime index (NP primes: grid.y)
+    // 1-D grid, the NP primes of a tile adjacent: CTAs that read the same operand limbs (first pass)
+    // run together, so the limbs come from L2 for all but the first prime
+    const uint32_t tile = blockIdx.x / NP;
+    const int j = (int)(blockIdx.x - tile * NP);  // prime index
     const uint32_t p = prime_of(NP, j);
     const int dir = INV ? 1 : 0;
     const uint32_t pinv = inv_mod_2_32(p);
@@ -393,8 +396,8 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
     uint64_t sjob = 0, stile = 0;
     if constexpr (LAY == Layout::Strided) {
         const int logTpj = P.logL - LOGE;
-        sjob = (uint64_t)blockIdx.x >> logTpj;
-        stile = (uint64_t)blockIdx.x & ((1ull << logTpj) - 1);
+        sjob = (uint64_t)tile >> logTpj;
+        stile = (uint64_t)tile & ((1ull << logTpj) - 1);
     }
     const uint64_t total_rows = (uint64_t)P.njobs << (P.logL - LOGN);
     const int logRows = P.logL - LOGN;
@@ -405,7 +408,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
     RowSrc* rsrc = reinterpret_cast<RowSrc*>(sm + E);
     if constexpr (kRowSrc) {
         for (uint32_t c = threadIdx.x; c < (1u << LOGC); c += NTHREADS) {
-            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            const uint64_t R = ((uint64_t)tile << LOGC) + c;
             RowSrc r{nullptr, 0};
             if (R < total_rows) {
                 const uint64_t job = R >> logRows;
@@ -481,7 +484,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
         if (threadIdx.x == 0) {
             mbar_arrive_expect_tx(bar, 4u << LOGE);
             if constexpr (LAY == Layout::Contig) {
-                const uint64_t first = (uint64_t)blockIdx.x << LOGE;  // over all jobs' arrays
+                const uint64_t first = (uint64_t)tile << LOGE;  // over all jobs' arrays
                 const int job = (int)(first >> P.logL);
                 if (P.logL >= LOGE) {
                     // boxes of 256 lines (32 KB)
@@ -537,7 +540,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
         } else {
             c = e4 >> LOGN;
             m = e4 & ((1u << LOGN) - 1);
-            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            const uint64_t R = ((uint64_t)tile << LOGC) + c;
             if (R >= total_rows) {
                 *reinterpret_cast<uint4*>(sm + swz(e4)) = make_uint4(0, 0, 0, 0);
                 continue;
@@ -672,7 +675,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
             const uint32_t c = g >> (LOGN - 4);
             const uint32_t m0 = blk * 16;
             const uint32_t b0 = swz((c << LOGN) | m0);  // vector q4 at swz_elem(b0, 4 q4, 0)
-            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            const uint64_t R = ((uint64_t)tile << LOGC) + c;
             const bool live = R < total_rows;
             uint4 o[4];
             if constexpr (FUSE == Fuse::MulInverse) {
@@ -731,7 +734,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
         } else {
             c = e4 >> LOGN;
             m = e4 & ((1u << LOGN) - 1);
-            const uint64_t R = ((uint64_t)blockIdx.x << LOGC) + c;
+            const uint64_t R = ((uint64_t)tile << LOGC) + c;
             if (R >= total_rows) continue;
             job = R >> logRows;
             g = gidx<LAY, LOGN, LOGE>(R & ((1ull << logRows) - 1), m, c, 0);

@@ -108,8 +108,8 @@ static cudaError_t run_pass(const PassParams& prm, const TwiddleTables& tw, cuda
     }
     auto kern = ntt_pass_kernel<LAY, LOGN, LOGE, NT, INV, SRC, FUSE, NP, TMA>;
     constexpr size_t smem = pass_smem<LAY, LOGN, TMA>();
-    dim3 grid((unsigned)tiles, NP);
-    kern<<<grid, NT, smem, st>>>(prm, tw, tmap);
+    if (tiles * NP > 0x7fffffffull) return cudaErrorInvalidValue;
+    kern<<<(unsigned)(tiles * NP), NT, smem, st>>>(prm, tw, tmap);
     return cudaGetLastError();
 }
 

@@ -24,7 +24,11 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <exception>
+#include <functional>
+#include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <dirent.h>
@@ -236,11 +240,20 @@ struct CkptStaging {
 };
 
 // Per-context state of the device finish, kept across calls: the arithmetic pool, the
-// batched-product buffers and the checkpoint staging.
+// batched-product buffers and the checkpoint staging; and a second stream with its own product
+// workspace and pool, on which a helper thread computes what does not depend on the series
+// (sqrt(10005), powers of ten) while the splitting and the reciprocal run.
 struct FinishState {
     DevPool pool;
     SharedProduct sp;
     CkptStaging stage;
+    DevPool pool2;
+    Workspace ws2;
+    cudaStream_t st2 = nullptr;
+    ~FinishState() {
+        ws2.release();
+        if (st2) cudaStreamDestroy(st2);
+    }
 };
 FinishState* finish_state_new() { return new FinishState; }
 void finish_state_delete(FinishState* f) { delete f; }
@@ -354,11 +367,16 @@ void recip_floor(DevArith& A, DevNum& Z, const DevNum& R, bool exact = true) {
     const size_t h = k / 2 + 32;
     Num Rh(A), Zh(A), Z0(A), T(A), E(A), D(A);
     A.tdiv_q_2exp(Rh, R, k - h);
-    recip_floor(A, Zh, Rh);
+    // The half-precision reciprocal without its exact correction: within c <= 2 units of
+    // 2^(2h)/Rh (the bound this step keeps, below), which saves a product and its host waits at
+    // every level of the recursion.
+    recip_floor(A, Zh, Rh, false);
     A.shl(Z0, Zh, k - h);
     // E = 2^(2k) - R Z0. With R = 2^(k-h) (Rh + f), 0 <= f < 1, and Rh >= 2^(h-1):
-    // |2^(2k)/R - Z0| <= 2^(k-h+2), so |E| < 2^(2k-h+2): E follows from R Z0 modulo
-    // 2^(32 L) - 1 for a transform about 3/4 the length of the full product's.
+    // |2^(2k)/R - Z0| <= (c + 4) 2^(k-h), so |E| < (c + 4) 2^(2k-h) < 2^(2k-h+3): E follows from
+    // R Z0 modulo 2^(32 L) - 1 for a transform about 3/4 the length of the full product's. The
+    // Newton step leaves (c + 4)^2 2^(k-2h+1) < 2^-57 of error, plus the truncations below (under
+    // 2 units), so this level's result is within 2 units as well.
     const int lw = wrap_logL(2 * k - h + 3, R.n, Z0.v.n);
     if (lw) {
         A.mul_wrap(T, R, Z0, lw);
@@ -891,9 +909,14 @@ SrtPlan srt_plan(uint64_t n) {
 
 // y = pi / 10 to w limbs, V ~= y 2^(64 w) within a few units, from the series root Q, R: the final
 // formula's truncated reciprocal, square root and products, 42688 sqrt(10005) Q / R.
-void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R, uint64_t w) {
+size_t pi_tenth_bits(uint64_t w) { return 64 * w + 64; }
+
+// sqrt_pre (optional): called after the reciprocal, returns sqrt(10005) 2^k computed elsewhere (a
+// helper's, waited for there) or nullptr to compute it here.
+void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R, uint64_t w,
+                       const std::function<const DevNum*()>& sqrt_pre = nullptr) {
     if (Q.sign <= 0 || R.sign <= 0) throw DevError(PG_ERR_BAD_ARG, "final formula needs Q, R > 0");
-    const size_t k = 64 * w + 64;  // relative error 2^(5 - k): below 2^-59 of V's last unit
+    const size_t k = pi_tenth_bits(w);  // relative error 2^(5 - k): below 2^-59 of V's last unit
     const size_t bQ = A.bits(Q), bR = A.bits(R);
     Num Qt(A), Rt(A), Z(A), S(A), t(A);
     const long long eQ = (long long)bQ - (long long)k;
@@ -904,10 +927,12 @@ void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R,
         Timer tm("reciprocal of R");
         recip_floor(A, Z, Rt, false);
     }
-    {
+    const DevNum* S_pre = sqrt_pre ? sqrt_pre() : nullptr;
+    if (!S_pre) {
         Timer tm("sqrt(10005)");
         sqrt_scaled(A, S, 10005, k, false);
     }
+    const DevNum& Sv = S_pre ? *S_pre : S.v;
     Timer tm("two truncated products");
     A.mul_ui(V, Qt, 42688);
     long long e = eQ - eR - 3 * (long long)k;  // pi / 10 = V 2^e (before the truncations below)
@@ -921,7 +946,7 @@ void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R,
             A.copy(V, t);
         }
     };
-    mul_trunc(S);
+    mul_trunc(Sv);
     mul_trunc(Z);
     const long long sh = e + 64 * (long long)w;  // V 2^e = (V 2^sh) / 2^(64 w)
     if (sh >= 0) A.shl(V, V, (size_t)sh); else A.fdiv_q_2exp(V, V, (size_t)-sh);
@@ -936,7 +961,23 @@ bool srt_fits(const SrtPlan& P) {
 
 // out[0 .. n) = the first n digits of V / 2^(64 w[0]) (V: the root's fraction). Returns false if a
 // leaf's digits could not be trusted (the caller then converts exactly).
-bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, char* out) {
+// powers 10^(2^j), j = kSrtLeafLog .. J - 1, into pw (owned by the caller, made on A)
+void srt_powers(DevArith& A, int J, std::vector<Num*>& pw) {
+    Timer tm("power tree");
+    Num p(A);
+    A.set_ui(p, 10);
+    for (int j = 0; j < J; ++j) {
+        if (j >= kSrtLeafLog) {
+            pw.push_back(new Num(A));
+            A.exact(p);
+            A.copy(*pw.back(), p);
+        }
+        if (j + 1 < J) A.sqr(p, p);
+    }
+}
+
+bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, char* out,
+                const std::vector<Num*>* pw_pre = nullptr) {
     cudaStream_t st = A.stream();
     const int levels = (int)P.w.size() - 1;  // product levels; P.w[levels] is the leaves'
     const uint64_t n = P.n;
@@ -948,27 +989,16 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
         if (pg::dev_malloc((void**)&sp.digits, n) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
         sp.digits_cap = n;
     }
-    // powers 10^(2^j), j = kSrtLeafLog .. J - 1
-    std::vector<Num*> pw;
+    // powers 10^(2^j), j = kSrtLeafLog .. J - 1 (given, or made here)
+    std::vector<Num*> own_pw;
     struct Owner {
         std::vector<Num*>& a;
         ~Owner() {
             for (auto* p : a) delete p;
         }
-    } own{pw};
-    {
-        Timer tm("power tree");
-        Num p(A);
-        A.set_ui(p, 10);
-        for (int j = 0; j < P.J; ++j) {
-            if (j >= kSrtLeafLog) {
-                pw.push_back(new Num(A));
-                A.exact(p);
-                A.copy(*pw.back(), p);
-            }
-            if (j + 1 < P.J) A.sqr(p, p);
-        }
-    }
+    } own{own_pw};
+    if (!pw_pre) srt_powers(A, P.J, own_pw);
+    const std::vector<Num*>& pw = pw_pre ? *pw_pre : own_pw;
     // level t peels 10^(2^(J - t - 1)), t < levels = J - kSrtLeafLog
     auto power = [&](int t) -> DevNum& { return pw[(size_t)(P.J - t - 1 - kSrtLeafLog)]->v; };
     Timer tm("tree levels and leaves");
@@ -1025,21 +1055,89 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
     return true;
 }
 
+// Whether pi's digits for `digits` take the scaled remainder tree (every level in one transform;
+// PG_EXACT_CONVERSION unset).
+bool pi_tree_path(size_t digits) { return srt_fits(srt_plan(digits + 1)) && !std::getenv("PG_EXACT_CONVERSION"); }
+
+// sqrt(10005) 2^k and the tree's powers of ten, computed by a helper host thread on the finish
+// state's second stream (lowest priority, its own product workspace and pool) while the caller's
+// stream runs the splitting and the reciprocal; join() waits for it and rethrows its error.
+struct PiHelper {
+    FinishState& fs;
+    const DeviceTables& T;
+    int device;
+    uint64_t* ctx_launches;  // the helper's kernels are added here when it is done
+    uint64_t launches = 0;
+    std::unique_ptr<DevArith> A;
+    std::unique_ptr<Num> S;
+    std::vector<Num*> pw;
+    std::exception_ptr err;
+    std::thread th;
+    PiHelper(FinishState& f, const DeviceTables& t, int dev, uint64_t* cl) : fs(f), T(t), device(dev), ctx_launches(cl) {}
+    void start(size_t digits) {
+        if (!fs.st2) {
+            int lo = 0, hi = 0;
+            cudaDeviceGetStreamPriorityRange(&lo, &hi);
+            if (cudaStreamCreateWithPriority(&fs.st2, cudaStreamNonBlocking, lo) != cudaSuccess) {
+                cudaGetLastError();
+                fs.st2 = nullptr;
+                throw DevError(PG_ERR_DEVICE, "helper stream");
+            }
+        }
+        const SrtPlan P = srt_plan(digits + 1);
+        const size_t k = pi_tenth_bits(P.w[0]);
+        const int J = P.J;
+        A.reset(new DevArith(T, fs.ws2, fs.st2, &launches, fs.pool2));
+        th = std::thread([this, k, J] {
+            try {
+                cudaSetDevice(device);
+                S.reset(new Num(*A));
+                {
+                    Timer tm("sqrt(10005), helper stream");
+                    sqrt_scaled(*A, S->v, 10005, k, false);
+                }
+                srt_powers(*A, J, pw);
+                A->sync();
+            } catch (...) {
+                err = std::current_exception();
+            }
+        });
+    }
+    void join() {
+        if (th.joinable()) th.join();
+        if (err) std::rethrow_exception(err);
+    }
+    ~PiHelper() {
+        if (th.joinable()) th.join();
+        for (auto* p : pw) delete p;
+        S.reset();
+        A.reset();
+        if (ctx_launches) *ctx_launches += launches;
+    }
+};
+
 // "3." and `digits` digits of pi into out from the series root Q, R: the scaled remainder tree when
 // every level fits one transform and no leaf is in doubt, otherwise the exact final formula and
-// divide-and-conquer conversion.
+// divide-and-conquer conversion. helper (optional, started for these digits) supplies sqrt(10005)
+// and the powers of ten.
 void pi_digits(DevArith& A, SharedProduct& sp, const DevNum& Q, const DevNum& R, size_t digits, char* out,
-               double* t_final) {
+               double* t_final, PiHelper* helper = nullptr) {
     const auto t0 = std::chrono::steady_clock::now();
     const SrtPlan P = srt_plan(digits + 1);
     const bool tree = srt_fits(P) && !std::getenv("PG_EXACT_CONVERSION");
     char* body = out + 1;  // the integer's digits: "3" then the fraction digits
     if (tree) {
         Num V(A);
-        pi_tenth_fraction(A, V, Q, R, P.w[0]);
+        std::function<const DevNum*()> pre;
+        if (helper)  // the reciprocal runs on this stream first, while the helper finishes
+            pre = [helper]() -> const DevNum* {
+                helper->join();
+                return &helper->S->v;
+            };
+        pi_tenth_fraction(A, V, Q, R, P.w[0], pre);
         A.sync();
         if (t_final) *t_final = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        if (srt_digits(A, sp, P, V, body)) {
+        if (srt_digits(A, sp, P, V, body, helper ? &helper->pw : nullptr)) {
             out[0] = body[0];
             out[1] = '.';
             return;
@@ -1419,10 +1517,15 @@ pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t
     return pg::guarded(ctx, [&] {
         pg::FinishState& fs = *pg::ctx_finish(ctx);
         pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        std::unique_ptr<pg::PiHelper> helper;
+        if (pg::pi_tree_path(digits)) {
+            helper.reset(new pg::PiHelper(fs, pg::ctx_tables(ctx), pg::ctx_device(ctx), pg::ctx_launches(ctx)));
+            helper->start(digits);
+        }
         pg::Num Q(A), R(A);
         A.upload(Q, q, nq, 1);
         A.upload(R, r, nr, 1);
-        pg::pi_digits(A, fs.sp, Q, R, digits, out, nullptr);
+        pg::pi_digits(A, fs.sp, Q, R, digits, out, nullptr, helper.get());
     });
 }
 
@@ -1437,6 +1540,17 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
     // terms as the reference's PiEngine: terms_needed(digits + 100) (pi_engine.cpp:214-220,
     // binary_splitting.cpp terms_needed); each term adds log10(151931373056000) ~= 14.18 digits
     const unsigned long terms = (unsigned long)std::ceil((double)(digits + 100) / 14.1816474627) + 1;
+    // sqrt(10005) and the powers of ten on the helper stream, alongside the splitting
+    std::unique_ptr<pg::PiHelper> helper;
+    if (pg::pi_tree_path(digits)) {
+        try {
+            helper.reset(new pg::PiHelper(*pg::ctx_finish(ctx), pg::ctx_tables(ctx), pg::ctx_device(ctx),
+                                          pg::ctx_launches(ctx)));
+            helper->start(digits);
+        } catch (...) {
+            helper.reset();  // no helper: pi_digits computes both itself
+        }
+    }
     pg::LevelView root;
     uint32_t hl[3];
     pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl);
@@ -1471,7 +1585,7 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
             R.v.sign = hl[2] ? 1 : 0;
             Q.v.slack = R.v.slack = 0;
         }
-        pg::pi_digits(A, fs.sp, Q, R, digits, out, &t_final);
+        pg::pi_digits(A, fs.sp, Q, R, digits, out, &t_final, helper.get());
     });
     if (seconds) {
         seconds[0] = t_bs;
