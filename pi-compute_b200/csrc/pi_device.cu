@@ -1060,8 +1060,8 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
 bool pi_tree_path(size_t digits) { return srt_fits(srt_plan(digits + 1)) && !std::getenv("PG_EXACT_CONVERSION"); }
 
 // sqrt(10005) 2^k and the tree's powers of ten, computed by a helper host thread on the finish
-// state's second stream (lowest priority, its own product workspace and pool) while the caller's
-// stream runs the splitting and the reciprocal; join() waits for it and rethrows its error.
+// state's second stream (its own product workspace and pool) while the caller's stream runs the
+// splitting and the reciprocal; join() waits for it and rethrows its error.
 struct PiHelper {
     FinishState& fs;
     const DeviceTables& T;
@@ -1078,7 +1078,10 @@ struct PiHelper {
         if (!fs.st2) {
             int lo = 0, hi = 0;
             cudaDeviceGetStreamPriorityRange(&lo, &hi);
-            if (cudaStreamCreateWithPriority(&fs.st2, cudaStreamNonBlocking, lo) != cudaSuccess) {
+            // PG_HELPER_PRIORITY=1: the lowest priority (measured no better than the default)
+            const char* pe = std::getenv("PG_HELPER_PRIORITY");
+            const int prio = (pe && std::atoi(pe) == 1) ? lo : 0;
+            if (cudaStreamCreateWithPriority(&fs.st2, cudaStreamNonBlocking, prio) != cudaSuccess) {
                 cudaGetLastError();
                 fs.st2 = nullptr;
                 throw DevError(PG_ERR_DEVICE, "helper stream");
