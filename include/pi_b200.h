@@ -95,8 +95,9 @@ uint64_t pg_launch_count(const pg_ctx* ctx);
 
 /* Level-batched, device-resident Chudnovsky binary splitting of the term range [a, b):
  * P(a,b), Q(a,b), R(a,b) as magnitudes in HOST buffers of `cap` limbs each (P may be NULL
- * when it is not needed, as for the root of a pi computation), their lengths in len[3] and
- * signs in sign[3]. Same series, leaves and split point as the reference's BinarySplitting
+ * when it is not needed, as for the root of a pi computation: then P is not computed at all,
+ * nor the P of the rightmost node of any depth, and len[0] = sign[0] = 0), their lengths in
+ * len[3] and signs in sign[3]. Same series, leaves and split point as the reference's BinarySplitting
  * (src/engine/binary_splitting.cpp:137-159, 161-293, 295-348), so the values are identical;
  * every depth of the tree runs as a few launches over all of its merges, with operands kept
  * in device memory from the leaves to the root. Replaces BinarySplitting::compute

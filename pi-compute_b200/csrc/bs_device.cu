@@ -416,6 +416,7 @@ struct DeviceBS {
     cudaGraphExec_t gexec = nullptr;  // captured for [g_a0, g_b0); destroyed when a buffer moves
     uint64_t g_a0 = ~0ull, g_b0 = 0;
     uint64_t g_wmin = 0;              // the wide configuration's crossover the graph was planned with
+    bool g_skip = false;              // the graph leaves out the rightmost nodes' P
     LevelView groot{};
     uint64_t glaunches = 0;
 
@@ -451,10 +452,10 @@ struct DeviceBS {
     // run() through a CUDA graph: the range is planned and every buffer sized first (host work
     // and allocations, outside any capture), then its launch sequence is captured and replayed; a
     // later call on the same range, with no buffer moved since, replays the graph alone.
-    cudaError_t run_graph(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
-        if (trace_on()) return run(a0, b0, root, err);  // tracing waits between depths
+    cudaError_t run_graph(uint64_t a0, uint64_t b0, LevelView& root, std::string& err, bool skipP) {
+        if (trace_on()) return run(a0, b0, root, err, skipP);  // tracing waits between depths
         const uint64_t wmin = T->wide ? wide_min_limbs(*T) : 0;
-        if (gexec && g_a0 == a0 && g_b0 == b0 && g_wmin == wmin) {  // no buffer moved since the capture
+        if (gexec && g_a0 == a0 && g_b0 == b0 && g_wmin == wmin && g_skip == skipP) {  // no buffer moved since
             root = groot;
             if (launches) *launches += glaunches;
             return cudaGraphLaunch(gexec, st);
@@ -475,28 +476,29 @@ struct DeviceBS {
         if (e != cudaSuccess) {
             launches = saved;
             cudaGetLastError();
-            return enqueue(a0, b0, dp, D, root);  // run directly instead
+            return enqueue(a0, b0, dp, D, root, skipP);  // run directly instead
         }
         const uint64_t m0 = moves;
-        cudaError_t er = enqueue(a0, b0, dp, D, root);
+        cudaError_t er = enqueue(a0, b0, dp, D, root, skipP);
         e = cudaStreamEndCapture(st, &g);
         launches = saved;
         if (er != cudaSuccess || e != cudaSuccess || moves != m0) {
             if (g) cudaGraphDestroy(g);
             cudaGetLastError();
-            return enqueue(a0, b0, dp, D, root);
+            return enqueue(a0, b0, dp, D, root, skipP);
         }
         e = cudaGraphInstantiate(&gexec, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) {
             gexec = nullptr;
             cudaGetLastError();
-            return enqueue(a0, b0, dp, D, root);
+            return enqueue(a0, b0, dp, D, root, skipP);
         }
         groot = root;
         g_a0 = a0;
         g_b0 = b0;
         g_wmin = wmin;
+        g_skip = skipP;
         glaunches = counted;
         if (launches) *launches += counted;
         return cudaGraphLaunch(gexec, st);
@@ -641,8 +643,10 @@ struct DeviceBS {
         return dp;
     }
 
+    // skipP: the level's last merge needs no P (nor its right child's P): its Pr slot and P^ output,
+    // the last of the batch's operands and outputs, are left out.
     cudaError_t launch_ntt_level(const DepthPlan& P, const DepthPlan& C, const LevelView& in, const LevelView& out,
-                                 uint64_t a0, uint64_t b0, int depth) {
+                                 uint64_t a0, uint64_t b0, int depth, bool skipP) {
         const Plan plan = P.wide ? T->plan_wide(P.logL) : T->plan(P.logL);
         const TwiddleTables& tw = P.wide ? T->tw_wide : T->tw;
         const Source limbs = P.wide ? Source::Limbs64 : Source::Limbs;
@@ -659,7 +663,7 @@ struct DeviceBS {
         p.L = L;
         p.logL = P.logL;
         p.job_stride = stride;
-        p.njobs = (uint32_t)(6 * M);
+        p.njobs = (uint32_t)(6 * M - (skipP ? 1 : 0));
         p.merge = 1;
         for (int k = 0; k < 3; ++k) {
             p.ms.X[k] = in.X[k];
@@ -674,7 +678,7 @@ struct DeviceBS {
         }
         // inverse transforms of the 3M outputs, one launch per pass over all of them: output k of
         // merge m (P^ = Pl Pr, Q^ = Ql Qr, R^ = Qr Rl +- Pl Rr) is formed on load by the first
-        // (contiguous) inverse pass and written over operand slot comb_out_slot(k) (Pr, Ql, Rr),
+        // (contiguous) inverse pass and written over operand slot comb_out_slot(k) (Ql, Rr, Pr),
         // which no other output reads, so the three outputs need no order among themselves (no
         // separate pointwise kernel and no pass over the products).
         {
@@ -685,7 +689,7 @@ struct DeviceBS {
             q.L = L;
             q.logL = P.logL;
             q.job_stride = 0;
-            q.njobs = (uint32_t)(3 * M);
+            q.njobs = (uint32_t)(3 * M - (skipP ? 1 : 0));
             q.merge = 0;
             q.comb3 = 1;
             q.comb_slot = stride;
@@ -702,7 +706,7 @@ struct DeviceBS {
         }
         // CRT + carry for all 3M outputs
         uint64_t maxw = 2ull * std::max({out.cap[0], out.cap[1], out.cap[2]});
-        const uint64_t jobs = 3 * M;
+        const uint64_t jobs = 3 * M - (skipP ? 1 : 0);
         if (P.wide) {
             const uint64_t bpj = (maxw + crt_wide_block_words() - 1) / crt_wide_block_words();
             CrtParams c{};
@@ -809,7 +813,7 @@ struct DeviceBS {
 
     // Enqueues the splitting of [a0, b0) planned and sized by prepare(): kernels and memsets only
     // (no allocation, no host wait), so it may run inside a stream capture.
-    cudaError_t enqueue(uint64_t a0, uint64_t b0, std::vector<DepthPlan>& dp, int D, LevelView& root) {
+    cudaError_t enqueue(uint64_t a0, uint64_t b0, std::vector<DepthPlan>& dp, int D, LevelView& root, bool skipP) {
         const bool tr = trace_on();
         cudaError_t e = cudaMemsetAsync(errw, 0, 4, st);
         if (e != cudaSuccess) return e;
@@ -869,7 +873,7 @@ struct DeviceBS {
                 e = cudaGetLastError();
                 if (launches) ++*launches;
             } else {
-                e = launch_ntt_level(P, C, in, out, a0, b0, d);
+                e = launch_ntt_level(P, C, in, out, a0, b0, d, skipP);
             }
             if (e != cudaSuccess) return e;
             if (tr) {
@@ -885,12 +889,12 @@ struct DeviceBS {
         return cudaSuccess;
     }
 
-    cudaError_t run(uint64_t a0, uint64_t b0, LevelView& root, std::string& err) {
+    cudaError_t run(uint64_t a0, uint64_t b0, LevelView& root, std::string& err, bool skipP) {
         std::vector<DepthPlan> dp;
         int D = 0;
         cudaError_t e = prepare(a0, b0, dp, D, err);
         if (e != cudaSuccess) return e;
-        return enqueue(a0, b0, dp, D, root);
+        return enqueue(a0, b0, dp, D, root, skipP);
     }
 };
 
@@ -918,14 +922,14 @@ namespace pg {
 // Runs the level-batched splitting of [a, b) with the context lock held by the caller. On
 // PG_OK the root's P, Q, R stay in the context's level buffers (root.X[k], hl[k] limbs) until
 // the next splitting on this context.
-pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3]) {
+pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3], bool need_P) {
     cudaSetDevice(ctx_device(ctx));
     DeviceBS& bs = *ctx_bs(ctx);  // buffers persist in the context across calls
     bs.T = &ctx_tables(ctx);
     bs.st = ctx_stream(ctx);
     bs.launches = ctx_launches(ctx);
     std::string err;
-    cudaError_t e = bs.run_graph(a, b, root, err);
+    cudaError_t e = bs.run_graph(a, b, root, err, !need_P);
     if (!err.empty()) {
         ctx_set_error(ctx, err);
         return PG_ERR_TOO_LARGE;
@@ -940,6 +944,7 @@ pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView
     e = cudaMemcpyAsync(hl, root.len, 12, cudaMemcpyDeviceToHost, bs.st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&herr, bs.errw, 4, cudaMemcpyDeviceToHost, bs.st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(bs.st);
+    if (!need_P) hl[0] = 0;  // not computed
     if (e != cudaSuccess) {
         ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
         return PG_ERR_DEVICE;
@@ -960,7 +965,7 @@ extern "C" pg_status pg_bs(pg_ctx* ctx, unsigned long a, unsigned long b, uint64
     std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
     pg::LevelView root;
     uint32_t hl[3];
-    pg_status s = pg::bs_run_locked(ctx, a, b, root, hl);
+    pg_status s = pg::bs_run_locked(ctx, a, b, root, hl, P != nullptr);
     if (s == PG_ERR_TOO_LARGE && b - a > 1) {  // subtrees merged with block products
         pg::ctx_set_error(ctx, "");
         return pg::bs_split_to_host(ctx, a, b, P, Q, R, cap, len, sign);

@@ -106,8 +106,9 @@ __device__ __forceinline__ CrtJob crt_job(const CrtParams& P, uint64_t job) {
         return J;
     }
     const uint64_t m = job / 3;
-    const int which = (int)(job % 3);
-    J.res = P.res + (6 * m + comb_out_slot(which)) * P.res_stride;
+    const int k = (int)(job - 3 * m);  // output: 0 Q^, 1 R^, 2 P^
+    const int which = merge_out_value(k);
+    J.res = P.res + (6 * m + comb_out_slot(k)) * P.res_stride;
     J.out = reinterpret_cast<uint32_t*>(P.dst[which] + m * P.dcap[which]);
     J.nwords = 2ull * P.dcap[which];
     J.len = P.dlen + 3 * m + which;

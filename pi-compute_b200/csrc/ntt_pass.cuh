@@ -345,9 +345,10 @@ __device__ __forceinline__ void job_source(const PassParams& P, uint64_t job, co
         words = P.src[job].words;
         ncoef = P.src[job].ncoef;
     } else if (P.merge == 1) {
-        const uint64_t m = job / 6, o = job % 6;
-        const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
-        const int which = (int)(o % 3);
+        const uint64_t m = job / 6;
+        const int o = (int)(job - 6 * m);
+        const uint64_t child = 2 * m + merge_slot_child(o);
+        const int which = merge_slot_value(o);
         words = reinterpret_cast<const uint32_t*>(P.ms.X[which] + child * P.ms.cap[which]);
         ncoef = (SRC == Source::Limbs64 ? 1ull : 2ull) * P.ms.len[3 * child + which];
     } else {
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
                 if constexpr (SRC != Source::Residues) job_source<SRC>(P, job, r.words, r.ncoef);
                 if constexpr (FUSE == Fuse::Combine) {
                     const uint64_t mrg = job / 3;
-                    if (job - 3 * mrg == 2) {
+                    if (job - 3 * mrg == 1) {  // R^
                         uint64_t a, b;
                         node_range(P.comb_a0, P.comb_b0, P.comb_depth, mrg, a, b);
                         r.ncoef = merge_r_sign(a, b) > 0 ? 1 : 0;
@@ -605,9 +606,9 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
                 const int ck = (int)(job - 3 * mrg);
                 const uint32_t* slot0 = P.data + 6 * mrg * P.comb_slot + prime_off + g;
                 auto at = [&](int o) { return *reinterpret_cast<const uint4*>(slot0 + (uint64_t)o * P.comb_slot); };
-                if (ck == 2) {
+                if (ck == 1) {  // R^ = Qr Rl +- Pl Rr
                     const int sgn = rsrc[c].ncoef ? 1 : -1;
-                    const uint4 pl = at(0), rl = at(2), qr = at(4), rr = at(5);
+                    const uint4 pl = at(0), rl = at(2), qr = at(3), rr = at(4);
                     uint32_t u, v;
 #define PG_RCOMB(f)                                         \
     u = mul_mont(qr.f, rl.f, p, pinv);                      \
@@ -616,7 +617,7 @@ __global__ void __launch_bounds__(NTHREADS, pass_min_blocks<LAY, FUSE, LOGE>())
                     PG_RCOMB(x) PG_RCOMB(y) PG_RCOMB(z) PG_RCOMB(w)
 #undef PG_RCOMB
                 } else {
-                    const uint4 l = at(ck), r = at(ck + 3);  // Pl Pr or Ql Qr
+                    const uint4 l = ck == 0 ? at(1) : at(0), r = ck == 0 ? at(3) : at(5);  // Ql Qr or Pl Pr
                     x = make_uint4(mul_mont(l.x, r.x, p, pinv), mul_mont(l.y, r.y, p, pinv), mul_mont(l.z, r.z, p, pinv),
                                    mul_mont(l.w, r.w, p, pinv));
                 }

@@ -40,6 +40,7 @@
 #include "../../include/pi_b200.h"
 #include "ckpt_io.h"
 #include "devnum.h"
+#include "host_div.h"
 
 namespace pg {
 
@@ -50,7 +51,8 @@ std::mutex& ctx_mutex(pg_ctx* c);
 uint64_t* ctx_launches(pg_ctx* c);
 void ctx_set_error(pg_ctx* c, const std::string& msg);
 int ctx_device(pg_ctx* c);
-pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3]);
+pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3],
+                        bool need_P = true);
 bool trace_on();
 
 // ------------------------------------------------------------------ batched shared-operand product
@@ -351,9 +353,20 @@ void residue_diff(DevArith& A, DevNum& e, size_t p, const DevNum& xm, int logL) 
 // then |Z - 2^(2k)/R| < 2. The ideal Newton update Z0 + Z0 E / 2^(2k) has error eps^2 / z* with
 // eps = z* - Z0, |eps| <= 2^(k-h+2) and z* = 2^(2k)/R > 2^k, i.e. below 2^(k - 2h + 4) = 2^-60;
 // dropping E's low bits costs < 1/2 and the floor < 1 (the lower levels stay exact).
+// Reciprocals of up to this many bits are divided on the host (exact): the Newton levels below it
+// (k -> k/2 + 32 down to 64 bits, a dozen of them) would cost more in launches and host waits.
+constexpr size_t kHostRecipBits = 4096;
+
 void recip_floor(DevArith& A, DevNum& Z, const DevNum& R, bool exact = true) {
     const size_t k = A.bits(R);
     if (k == 0 || R.sign < 0) throw DevError(PG_ERR_BAD_ARG, "recip_floor: R must be positive");
+    if (k > 64 && k <= kHostRecipBits) {
+        std::vector<uint64_t> r((k + 63) / 64);
+        A.download(R, r.data());
+        const std::vector<uint64_t> z = host_pow2_div(2 * k, r);
+        A.upload(Z, z.data(), z.size(), 1);
+        return;
+    }
     if (k <= 64) {
         const uint64_t r = (uint64_t)download_u128(A, R);
         u128 z;
@@ -911,47 +924,6 @@ SrtPlan srt_plan(uint64_t n) {
 // formula's truncated reciprocal, square root and products, 42688 sqrt(10005) Q / R.
 size_t pi_tenth_bits(uint64_t w) { return 64 * w + 64; }
 
-// sqrt_pre (optional): called after the reciprocal, returns sqrt(10005) 2^k computed elsewhere (a
-// helper's, waited for there) or nullptr to compute it here.
-void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R, uint64_t w,
-                       const std::function<const DevNum*()>& sqrt_pre = nullptr) {
-    if (Q.sign <= 0 || R.sign <= 0) throw DevError(PG_ERR_BAD_ARG, "final formula needs Q, R > 0");
-    const size_t k = pi_tenth_bits(w);  // relative error 2^(5 - k): below 2^-59 of V's last unit
-    const size_t bQ = A.bits(Q), bR = A.bits(R);
-    Num Qt(A), Rt(A), Z(A), S(A), t(A);
-    const long long eQ = (long long)bQ - (long long)k;
-    const long long eR = (long long)bR - (long long)k;
-    if (eQ >= 0) A.tdiv_q_2exp(Qt, Q, (size_t)eQ); else A.shl(Qt, Q, (size_t)-eQ);
-    if (eR >= 0) A.tdiv_q_2exp(Rt, R, (size_t)eR); else A.shl(Rt, R, (size_t)-eR);
-    {
-        Timer tm("reciprocal of R");
-        recip_floor(A, Z, Rt, false);
-    }
-    const DevNum* S_pre = sqrt_pre ? sqrt_pre() : nullptr;
-    if (!S_pre) {
-        Timer tm("sqrt(10005)");
-        sqrt_scaled(A, S, 10005, k, false);
-    }
-    const DevNum& Sv = S_pre ? *S_pre : S.v;
-    Timer tm("two truncated products");
-    A.mul_ui(V, Qt, 42688);
-    long long e = eQ - eR - 3 * (long long)k;  // pi / 10 = V 2^e (before the truncations below)
-    auto mul_trunc = [&](const DevNum& y) {
-        A.mul(t, V, y);
-        const long long over = (long long)A.bits(t) - (long long)k;
-        if (over > 0) {
-            A.tdiv_q_2exp(V, t, (size_t)over);
-            e += over;
-        } else {
-            A.copy(V, t);
-        }
-    };
-    mul_trunc(Sv);
-    mul_trunc(Z);
-    const long long sh = e + 64 * (long long)w;  // V 2^e = (V 2^sh) / 2^(64 w)
-    if (sh >= 0) A.shl(V, V, (size_t)sh); else A.fdiv_q_2exp(V, V, (size_t)-sh);
-}
-
 // Whether every level of the tree fits one transform of the batched product.
 bool srt_fits(const SrtPlan& P) {
     for (size_t t = 0; t + 1 < P.w.size(); ++t)
@@ -1106,18 +1078,114 @@ struct PiHelper {
             }
         });
     }
+    // Second task, once the first is done: X1 = 42688 Qt sqrt(10005) 2^k truncated to k bits (over1:
+    // the bits dropped), on the helper stream after `ev` (recorded once Qt is on the caller's
+    // stream), while the caller computes the reciprocal of R.
+    std::unique_ptr<Num> X1;
+    long long over1 = 0;
+    void start_first_product(const DevNum* Qt, cudaEvent_t ev, size_t k) {
+        std::thread prev = std::move(th);
+        th = std::thread([this, Qt, ev, k, prev = std::move(prev)]() mutable {
+            if (prev.joinable()) prev.join();
+            if (err) return;
+            try {
+                cudaSetDevice(device);
+                if (cudaStreamWaitEvent(fs.st2, ev, 0) != cudaSuccess) throw DevError(PG_ERR_DEVICE, "helper stream wait");
+                Timer tm("42688 Q sqrt(10005), helper stream");
+                X1.reset(new Num(*A));
+                Num t(*A);
+                A->mul_ui(*X1, *Qt, 42688);
+                A->mul(t, *X1, S->v);
+                const long long over = (long long)A->bits(t) - (long long)k;
+                if (over > 0) {
+                    A->tdiv_q_2exp(*X1, t, (size_t)over);
+                    over1 = over;
+                } else {
+                    A->copy(*X1, t);
+                    over1 = 0;
+                }
+                A->sync();
+            } catch (...) {
+                err = std::current_exception();
+            }
+        });
+    }
     void join() {
         if (th.joinable()) th.join();
         if (err) std::rethrow_exception(err);
     }
     ~PiHelper() {
         if (th.joinable()) th.join();
+        X1.reset();
         for (auto* p : pw) delete p;
         S.reset();
         A.reset();
         if (ctx_launches) *ctx_launches += launches;
     }
 };
+
+// y = pi / 10 to w limbs, V ~= y 2^(64 w) within a few units, from the series root Q, R: the final
+// formula's truncated reciprocal, square root and products, 42688 sqrt(10005) Q / R. With a helper,
+// sqrt(10005) comes from it and so does the first product, 42688 Q sqrt(10005), computed on its
+// stream while this one computes the reciprocal of R.
+void pi_tenth_fraction(DevArith& A, DevNum& V, const DevNum& Q, const DevNum& R, uint64_t w, PiHelper* helper) {
+    if (Q.sign <= 0 || R.sign <= 0) throw DevError(PG_ERR_BAD_ARG, "final formula needs Q, R > 0");
+    const size_t k = pi_tenth_bits(w);  // relative error 2^(5 - k): below 2^-59 of V's last unit
+    const size_t bQ = A.bits(Q), bR = A.bits(R);
+    Num Qt(A), Rt(A), Z(A), S(A), t(A);
+    const long long eQ = (long long)bQ - (long long)k;
+    const long long eR = (long long)bR - (long long)k;
+    if (eQ >= 0) A.tdiv_q_2exp(Qt, Q, (size_t)eQ); else A.shl(Qt, Q, (size_t)-eQ);
+    cudaEvent_t ev = nullptr;
+    if (helper) {
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(ev, A.stream()) != cudaSuccess) {
+            cudaGetLastError();
+            if (ev) cudaEventDestroy(ev);
+            throw DevError(PG_ERR_DEVICE, "final formula: event");
+        }
+        helper->start_first_product(&Qt.v, ev, k);
+    }
+    struct EventGuard {
+        cudaEvent_t e;
+        ~EventGuard() {
+            if (e) cudaEventDestroy(e);
+        }
+    } eg{ev};
+    if (eR >= 0) A.tdiv_q_2exp(Rt, R, (size_t)eR); else A.shl(Rt, R, (size_t)-eR);
+    {
+        Timer tm("reciprocal of R");
+        recip_floor(A, Z, Rt, false);
+    }
+    long long e = eQ - eR - 3 * (long long)k;  // pi / 10 = V 2^e (before the truncations below)
+    auto mul_trunc = [&](const DevNum& x, const DevNum& y) {
+        A.mul(t, x, y);
+        const long long over = (long long)A.bits(t) - (long long)k;
+        if (over > 0) {
+            A.tdiv_q_2exp(V, t, (size_t)over);
+            e += over;
+        } else {
+            A.copy(V, t);
+        }
+    };
+    if (helper) {
+        helper->join();  // X1 = 42688 Qt S, truncated
+        e += helper->over1;
+        Timer tm("truncated product by the reciprocal");
+        mul_trunc(helper->X1->v, Z);
+    } else {
+        {
+            Timer tm("sqrt(10005)");
+            sqrt_scaled(A, S, 10005, k, false);
+        }
+        Timer tm("two truncated products");
+        A.mul_ui(V, Qt, 42688);
+        mul_trunc(V, S);
+        mul_trunc(V, Z);
+    }
+    const long long sh = e + 64 * (long long)w;  // V 2^e = (V 2^sh) / 2^(64 w)
+    if (sh >= 0) A.shl(V, V, (size_t)sh); else A.fdiv_q_2exp(V, V, (size_t)-sh);
+}
 
 // "3." and `digits` digits of pi into out from the series root Q, R: the scaled remainder tree when
 // every level fits one transform and no leaf is in doubt, otherwise the exact final formula and
@@ -1131,13 +1199,7 @@ void pi_digits(DevArith& A, SharedProduct& sp, const DevNum& Q, const DevNum& R,
     char* body = out + 1;  // the integer's digits: "3" then the fraction digits
     if (tree) {
         Num V(A);
-        std::function<const DevNum*()> pre;
-        if (helper)  // the reciprocal runs on this stream first, while the helper finishes
-            pre = [helper]() -> const DevNum* {
-                helper->join();
-                return &helper->S->v;
-            };
-        pi_tenth_fraction(A, V, Q, R, P.w[0], pre);
+        pi_tenth_fraction(A, V, Q, R, P.w[0], helper);
         A.sync();
         if (t_final) *t_final = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         if (srt_digits(A, sp, P, V, body, helper ? &helper->pw : nullptr)) {
@@ -1556,7 +1618,7 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
     }
     pg::LevelView root;
     uint32_t hl[3];
-    pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl);
+    pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl, false);  // the root's P is not used
     const bool big = (s == PG_ERR_TOO_LARGE);  // split into subtrees below, merged on the device
     if (s != PG_OK && !big) return s;
     if (big) pg::ctx_set_error(ctx, "");

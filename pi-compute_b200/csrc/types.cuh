@@ -108,9 +108,17 @@ struct MergeSrc {
     const uint32_t* len;
 };
 
-// Operand slot a merge's output k (0 P^ = Pl Pr, 1 Q^ = Ql Qr, 2 R^ = Qr Rl +- Pl Rr) is written
-// over: Pr, Ql and Rr, each read only by the output that overwrites it.
-__host__ __device__ constexpr int comb_out_slot(int k) { return k == 0 ? 3 : (k == 1 ? 1 : 5); }
+// A merge's six operand slots in a transform batch, in the order Pl Ql Rl Qr Rr Pr, and its three
+// outputs in the order Q^ = Ql Qr, R^ = Qr Rl +- Pl Rr, P^ = Pl Pr: the P's last, so that a batch
+// whose last merge needs no P (the rightmost node of every depth when the root's P is not wanted)
+// just ends one slot and one output early.
+// Slot o holds the value (0 P, 1 Q, 2 R) of the left (child 0) or right (child 1) child:
+__host__ __device__ constexpr int merge_slot_child(int o) { return o >= 3 ? 1 : 0; }
+__host__ __device__ constexpr int merge_slot_value(int o) { return o < 3 ? o : (o == 3 ? 1 : (o == 4 ? 2 : 0)); }
+// Output k holds the value (0 P, 1 Q, 2 R):
+__host__ __device__ constexpr int merge_out_value(int k) { return k == 0 ? 1 : (k == 1 ? 2 : 0); }
+// Output k is written over the operand slot that only it reads: Q^ over Ql, R^ over Rr, P^ over Pr.
+__host__ __device__ constexpr int comb_out_slot(int k) { return k == 0 ? 1 : (k == 1 ? 4 : 5); }
 
 struct PassParams {
     uint32_t* data;          // residues of job 0: prime i at data + i*L; job j at data + j*job_stride
@@ -132,8 +140,8 @@ struct PassParams {
     const SrcEntry* src;
     const uint2* rowB;       // strided passes: four-step factor table of prime 0 (set by launch_pass)
     // comb3 = 1 (the splitting's Fuse::Combine pass and the inverse passes after it): job j of the
-    // launch is output k = j % 3 (0 P^, 1 Q^, 2 R^) of merge m = j / 3. Merge m's operands o (Pl Ql
-    // Rl Pr Qr Rr) are at data + (6 m + o) * comb_slot, and output k is written over operand slot
+    // launch is output k = j % 3 (0 Q^, 1 R^, 2 P^) of merge m = j / 3. Merge m's operands o (Pl Ql
+    // Rl Qr Rr Pr) are at data + (6 m + o) * comb_slot, and output k is written over operand slot
     // comb_out_slot(k), which no other output of the merge reads, so all three outputs of every
     // merge run in one launch.
     int comb3;
@@ -170,9 +178,9 @@ struct CrtParams {
     // plain batch (merge == 0): job i's residues at res + i * res_stride, its words at
     // out + i * out_stride, its length (if dlen) at dlen[i]; every job has `nwords` words.
     uint64_t out_stride;
-    // merge batch: job = 3 * merge + {P, Q, R}; residues of merge m, output k (0..2) at
-    // res + (6m + comb_out_slot(k)) * res_stride; the words go to dst[k] + m * dcap[k] (limbs), the
-    // length to dlen[3m + k]; node ranges of the level come from [a0, b0) and depth.
+    // merge batch: job = 3 * merge + k, output k (0 Q^, 1 R^, 2 P^) of value v = merge_out_value(k);
+    // its residues at res + (6m + comb_out_slot(k)) * res_stride; the words go to dst[v] + m * dcap[v]
+    // (limbs), the length to dlen[3m + v]; node ranges of the level come from [a0, b0) and depth.
     int merge;
     uint64_t res_stride;
     uint64_t* dst[3];
