@@ -272,18 +272,27 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
         const uint64_t* x = s_op[warp][ox];
         const uint64_t* y = s_op[warp][oy];
         const int ncol = nx + ny - 1;
+        // two interleaved partial sums per column (even and odd i): independent carry chains
+        auto acc = [](uint64_t& lo, uint64_t& mid, uint64_t& hi, u128 t) {
+            const u128 s = (u128)lo + (uint64_t)t;
+            lo = (uint64_t)s;
+            const u128 s2 = (u128)mid + (uint64_t)(t >> 64) + (uint64_t)(s >> 64);
+            mid = (uint64_t)s2;
+            hi += (uint64_t)(s2 >> 64);
+        };
         for (int c = lane; c < ncol; c += 32) {
-            uint64_t lo = 0, mid = 0, hi = 0;
+            uint64_t lo = 0, mid = 0, hi = 0, lo2 = 0, mid2 = 0, hi2 = 0;
             const int i0 = c - ny + 1 > 0 ? c - ny + 1 : 0;
             const int i1 = c < nx - 1 ? c : nx - 1;
-            for (int i = i0; i <= i1; ++i) {
-                const u128 t = (u128)x[i] * y[c - i];
-                const u128 s = (u128)lo + (uint64_t)t;
-                lo = (uint64_t)s;
-                const u128 s2 = (u128)mid + (uint64_t)(t >> 64) + (uint64_t)(s >> 64);
-                mid = (uint64_t)s2;
-                hi += (uint64_t)(s2 >> 64);
+            int i = i0;
+            for (; i + 1 <= i1; i += 2) {
+                acc(lo, mid, hi, (u128)x[i] * y[c - i]);
+                acc(lo2, mid2, hi2, (u128)x[i + 1] * y[c - i - 1]);
             }
+            if (i <= i1) acc(lo, mid, hi, (u128)x[i] * y[c - i]);
+            acc(lo, mid, hi, lo2);
+            acc(lo, mid, hi, (u128)mid2 << 64);
+            hi += hi2;
             s_col[warp][0][c] = lo;
             s_col[warp][1][c] = mid;
             s_col[warp][2][c] = hi;
