@@ -73,3 +73,19 @@ def test_device_allocation_failure_is_oom_and_context_recovers(eng):
     assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b))
     assert eng.lib.pg_buf_alloc(eng.ctx, 1 << 20, ctypes.byref(buf)) == pkg.PG_OK and buf.value
     eng.lib.pg_buf_free(eng.ctx, buf)
+
+
+def test_pi_allocation_failure_is_oom_and_context_recovers():
+    """A fresh context computing pi with every device allocation failing: the splitting and the
+    helper thread (sqrt(10005) and the powers of ten on the second stream) both fail; the call must
+    report PG_ERR_OOM after the helper has finished, and the same context must then compute the
+    digits."""
+    e = pkg.Engine(0)
+    try:
+        with pytest.raises(pkg.PgError) as err:
+            _with_env({"PG_TEST_FAIL_DEVICE_ALLOC": "1"}, lambda: e.pi(200_000))
+        assert err.value.status == pkg.PG_ERR_OOM
+        ref = open(os.path.join(os.path.dirname(__file__), "golden", "pi_1000.txt")).read().strip()
+        assert e.pi(200_000).decode()[:1002] == ref
+    finally:
+        e.close()
