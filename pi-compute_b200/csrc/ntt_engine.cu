@@ -7,6 +7,7 @@
 #include <vector>
 
 #include "crt_carry.cuh"
+#include "radix3.cuh"
 #include "ntt_engine.cuh"
 #include "pass_launch.cuh"
 
@@ -40,7 +41,9 @@ uint32_t shoup_companion(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)
 // host arithmetic and no upload beyond those.
 namespace {
 constexpr size_t kFsEnt = 1u << kFsLog;
-constexpr size_t small_entries(int np) { return (size_t)2 * np * (kStageEnt + 2 * kFsEnt); }
+// the wide configuration's radix-3 tables: [lo, hi][dir][prime], 2^13 entries each
+constexpr size_t t3_entries(int np) { return np == kWidePrimes ? (size_t)2 * 2 * np * kFsEnt : 0; }
+constexpr size_t small_entries(int np) { return (size_t)2 * np * (kStageEnt + 2 * kFsEnt) + t3_entries(np); }
 constexpr size_t row_entries(int np) { return (size_t)kRowTables * 2 * np * kFsEnt; }
 constexpr size_t row_big_entries(int np) { return (size_t)kRowTablesBig * 2 * np * (1u << 14); }
 
@@ -110,6 +113,21 @@ cudaError_t build_tables(uint2*& base, TwiddleTables& tw) {
                 b = b * wr % p;
                 c = c * wrhi % p;
             }
+            if (t3_entries(NP)) {
+                // W of order 3 * 2^root (3 and 2^root both divide p - 1 for every wide prime)
+                uint32_t W = pow_mod(generator_of(NP, j), (uint64_t)(p - 1) / (3ull << root), p);
+                if (dir == 1) W = inv_mod(W, p);
+                const uint32_t Whi = pow_mod(W, 1ull << kFsLog, p);
+                uint2* l3 = h.data() + (size_t)2 * NP * (kStageEnt + 2 * kFsEnt) + ((size_t)(0 * 2 + dir) * NP + j) * kFsEnt;
+                uint2* h3 = h.data() + (size_t)2 * NP * (kStageEnt + 2 * kFsEnt) + ((size_t)(1 * 2 + dir) * NP + j) * kFsEnt;
+                uint64_t x = 1, y = 1;
+                for (size_t i = 0; i < kFsEnt; ++i) {
+                    l3[i] = make_uint2((uint32_t)x, shoup_companion((uint32_t)x, p));
+                    h3[i] = make_uint2((uint32_t)y, shoup_companion((uint32_t)y, p));
+                    x = x * W % p;
+                    y = y * Whi % p;
+                }
+            }
         }
     cudaError_t e = pg::dev_malloc(&base, (small_entries(NP) + row_entries(NP) + row_big_entries(NP)) * sizeof(uint2));
     if (e != cudaSuccess) return e;
@@ -124,6 +142,22 @@ cudaError_t build_tables(uint2*& base, TwiddleTables& tw) {
             tw.fs_lo[dir][j] = base + (size_t)2 * NP * kStageEnt + ((size_t)(0 * 2 + dir) * NP + j) * kFsEnt;
             tw.fs_hi[dir][j] = base + (size_t)2 * NP * kStageEnt + ((size_t)(1 * 2 + dir) * NP + j) * kFsEnt;
         }
+    if (t3_entries(NP)) {
+        for (int dir = 0; dir < 2; ++dir)
+            for (int j = 0; j < NP; ++j) {
+                const uint32_t p = prime_of(NP, j);
+                tw.t3_lo[dir][j] = base + (size_t)2 * NP * (kStageEnt + 2 * kFsEnt) + ((size_t)(0 * 2 + dir) * NP + j) * kFsEnt;
+                tw.t3_hi[dir][j] = base + (size_t)2 * NP * (kStageEnt + 2 * kFsEnt) + ((size_t)(1 * 2 + dir) * NP + j) * kFsEnt;
+                // w3 = W^(2^root) of order 3 (the inverse direction's is its inverse)
+                uint32_t W = pow_mod(generator_of(NP, j), (uint64_t)(p - 1) / (3ull << root), p);
+                if (dir == 1) W = inv_mod(W, p);
+                const uint64_t w3 = pow_mod(W, 1ull << root, p), w3sq = w3 * w3 % p;
+                const uint64_t half = (p + 1) / 2;
+                const uint32_t cc = (uint32_t)((w3 + p - w3sq) % p * half % p);
+                tw.t3_c[dir][j] = make_uint2(cc, shoup_companion(cc, p));
+                if (dir == 0) tw.t3_h[j] = make_uint2((uint32_t)half, shoup_companion((uint32_t)half, p));
+            }
+    }
     uint2* row = base + small_entries(NP);
     uint2* row_big = row + row_entries(NP);
     tw.row = row;
@@ -290,7 +324,8 @@ CrtConsts make_crt_consts(int logL) {
 
 // ---------------------------------------------------------------- one product
 // Garner constants of the wide configuration for transforms of 2^logL points (see crt5).
-static CrtWideConsts make_crt_wide_consts(int logL) {
+// three: the transform has 3 * 2^logL points (its 1/L includes 1/3).
+static CrtWideConsts make_crt_wide_consts(int logL, bool three = false) {
     CrtWideConsts K{};
     uint32_t q[kWidePrimes];
     for (int i = 0; i < kWidePrimes; ++i) q[i] = prime_of(kWidePrimes, i);
@@ -312,7 +347,7 @@ static CrtWideConsts make_crt_wide_consts(int logL) {
     };
     for (int kk = 0; kk < kWidePrimes; ++kk) {
         const uint32_t p = q[kk];
-        const uint64_t linv = inv_mod(pow_mod(2, (uint64_t)logL, p), p);
+        const uint64_t linv = inv_mod((uint32_t)((uint64_t)pow_mod(2, (uint64_t)logL, p) * (three ? 3 : 1) % p), p);
         const uint64_t scale = linv * pow_mod(2, 32, p) % p;  // 1/L and the 2^-32 of the pointwise product
         const uint64_t pkinv = inv_mod(pmod(kk, p), p);
         K.c[kk] = (uint32_t)(scale * pkinv % p);
@@ -355,13 +390,14 @@ uint64_t crt_wide_block_words() { return (uint64_t)kWideThreads * kWideWords; }
 
 // Wide CRT: every block independently (words with carry-in 0, block transfer functions into
 // c.status), then a scan per job and the carries applied.
-cudaError_t launch_crt_wide(CrtParams c, uint64_t jobs, uint64_t bpj, int logL, cudaStream_t st, uint64_t* launches) {
+cudaError_t launch_crt_wide(CrtParams c, uint64_t jobs, uint64_t bpj, int logL, cudaStream_t st, uint64_t* launches,
+                            bool three) {
     const bool top_ok = c.top_ok != 0;
     if (!jobs || !bpj) return cudaSuccess;
     if (bpj > kFixMaxBlocks) return cudaErrorInvalidValue;
     c.blocks_per_job = bpj;
     const uint64_t blocks = jobs * bpj;
-    crt_wide_kernel<<<(unsigned)blocks, kWideThreads, 0, st>>>(c, make_crt_wide_consts(logL));
+    crt_wide_kernel<<<(unsigned)blocks, kWideThreads, 0, st>>>(c, make_crt_wide_consts(logL, three));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (bpj <= kScanWarpMax)
@@ -503,6 +539,123 @@ bool use_wide(const DeviceTables& T, uint64_t na, uint64_t nb) {
     return wmin && na + nb >= wmin && product_logL_wide(na, nb) <= kWideMaxLogL;
 }
 
+// A wide product as a transform of L = 3 * 2^m points: a radix-3 step from the limbs into three rows
+// of 2^m points (rows as jobs: [row][prime][2^m]), the 2^m-point passes of the tuned wide plan over the
+// three rows (the pointwise product fused into b's last forward pass as usual), their inverse, the
+// inverse radix-3 step into [prime][3 * 2^m] and the CRT with 1/L = 1/(3 * 2^m). Transforms of this
+// length use roots of order 3 * 2^25, which every wide prime has.
+static cudaError_t enqueue_impl3(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
+                                 const uint64_t* d_b, size_t nb, int logM, uint64_t nwords, uint64_t* d_out,
+                                 cudaStream_t st, uint64_t* launches) {
+    const bool square = (d_b == nullptr);
+    if (square) nb = na;
+    constexpr int np = kWidePrimes;
+    const TwiddleTables& tw = T.tw_wide;
+    if (!tw.t3_lo[0][0] || logM < kMinLogL || logM > kWideMaxLogL - 1) return cudaErrorInvalidValue;
+    const Plan plan = T.plan_wide(logM);
+    const uint64_t M = 1ull << logM, L3 = 3 * M, rows_stride = (uint64_t)np * M;
+    cudaError_t e = W.ensure_res(np * L3);
+    if (e != cudaSuccess) return e;
+    const uint64_t block_words = (uint64_t)kWideThreads * kWideWords;
+    const uint64_t crt_blocks = (nwords + block_words - 1) / block_words;
+    e = W.ensure_sync(crt_blocks);
+    if (e != cudaSuccess) return e;
+    const unsigned r3_grid = (unsigned)(((M / 4 + kR3Threads - 1) / kR3Threads) * np);
+    auto rows = [&](uint32_t* data) {
+        PassParams p{};
+        p.data = data;
+        p.out = data;
+        p.L = M;
+        p.logL = logM;
+        p.job_stride = rows_stride;
+        p.other_stride = rows_stride;
+        p.njobs = 3;
+        p.merge = 0;
+        p.error = W.sync;
+        return p;
+    };
+    const int last = plan.npass - 1;
+    uint64_t n = 0;
+    // a: radix-3 step from the limbs, then the 2^m-point forward passes (the last fused with the
+    // squaring when b is a)
+    radix3_fwd_kernel<np><<<r3_grid, kR3Threads, 0, st>>>(reinterpret_cast<const uint32_t*>(d_a), na, W.a_res, M, logM,
+                                                         rows_stride, tw);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    ++n;
+    {
+        PassParams p = rows(W.a_res);
+        for (int i = 0; i < plan.npass; ++i) {
+            set_pass(p, plan, i);
+            const Fuse f = (square && i == last) ? Fuse::SqrInverse : Fuse::None;
+            if ((e = launch_pass(plan, i, false, Source::Residues, f, p, tw, st)) != cudaSuccess) return e;
+            ++n;
+        }
+    }
+    uint32_t* prod = W.a_res;
+    if (!square) {
+        radix3_fwd_kernel<np><<<r3_grid, kR3Threads, 0, st>>>(reinterpret_cast<const uint32_t*>(d_b), nb, W.b_res, M,
+                                                             logM, rows_stride, tw);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        ++n;
+        PassParams p = rows(W.b_res);
+        for (int i = 0; i < plan.npass; ++i) {
+            set_pass(p, plan, i);
+            if (i == last) p.other = W.a_res;
+            const Fuse f = i == last ? Fuse::MulInverse : Fuse::None;
+            if ((e = launch_pass(plan, i, false, Source::Residues, f, p, tw, st)) != cudaSuccess) return e;
+            ++n;
+        }
+        prod = W.b_res;
+    }
+    {
+        PassParams p = rows(prod);
+        for (int i = last - 1; i >= 0; --i) {
+            set_pass(p, plan, i);
+            if ((e = launch_pass(plan, i, true, Source::Residues, Fuse::None, p, tw, st)) != cudaSuccess) return e;
+            ++n;
+        }
+    }
+    // inverse radix-3 step into the other buffer ([prime][3M], natural order), then the CRT
+    uint32_t* coef = (prod == W.a_res) ? W.b_res : W.a_res;
+    radix3_inv_kernel<np><<<r3_grid, kR3Threads, 0, st>>>(prod, coef, M, logM, rows_stride, tw);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    ++n;
+    e = cudaMemsetAsync(W.sync + 1, 0, (crt_blocks + 1) * 4, st);
+    if (e != cudaSuccess) return e;
+    CrtParams c{};
+    c.res = coef;
+    c.L = L3;
+    c.nwords = nwords;
+    c.out = reinterpret_cast<uint32_t*>(d_out);
+    c.ticket = W.sync + 1;
+    c.status = W.sync + 2;
+    c.error = W.sync;
+    c.merge = 0;
+    e = launch_crt_wide(c, 1, crt_blocks, logM, st, &n, true);
+    if (launches) *launches += n;
+    return e;
+}
+
+// Whether a wide product of n = na + nb - 1 coefficients takes a 3 * 2^m-point transform: when that
+// length (3/4 of the next power of two) holds it, for m >= kR3MinLog (PG_RADIX3=0: never). Measured
+// on a B200 (the multiply sweep): 2-7% faster from m = 20 on, slower below (at m = 17-19 the two
+// radix-3 steps, which cost about one transform pass each, outweigh the quarter of the points saved).
+constexpr int kR3MinLog = 20;
+// PG_RADIX3=k (k >= kMinLogL) moves the threshold to m >= k (tests use it to reach the path at small
+// sizes).
+static int radix3_logM(uint64_t ncoef) {
+    int mmin = kR3MinLog;
+    if (const char* e = std::getenv("PG_RADIX3")) {
+        const long v = std::strtol(e, nullptr, 10);
+        if (v == 0) return -1;
+        if (v >= kMinLogL) mmin = (int)v;
+    }
+    const int l2 = ceil_log2(ncoef);
+    const int m = l2 - 2;
+    if (m < mmin || m > kWideMaxLogL - 1) return -1;
+    return (3ull << m) >= ncoef ? m : -1;
+}
+
 cudaError_t enqueue_product_config(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
                                    const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st, bool wide) {
     const size_t mb = d_b ? nb : na;
@@ -521,9 +674,12 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
     // Configuration from the proven bound: the wide one holds every product of up to 2^25 limbs
     // (min(na, nb) (2^64 - 1)^2 < q0 ... q4 for min(na, nb) < 2^25.35) in half the transform length.
     const uint64_t wmin = T.wide ? wide_min_limbs(T) : 0;
-    if (wmin && na + mb >= wmin && product_logL_wide(na, mb) <= kWideMaxLogL)
+    if (wmin && na + mb >= wmin && product_logL_wide(na, mb) <= kWideMaxLogL) {
+        const int m3 = radix3_logM((uint64_t)(na + mb) - 1);
+        if (m3 >= 0) return enqueue_impl3(T, W, d_a, na, d_b, nb, m3, 2ull * (na + mb), d_out, st, launches);
         return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL_wide(na, mb), 2ull * (na + mb), d_out, st, launches,
                             true);
+    }
     return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL(na, mb), 2ull * (na + mb), d_out, st, launches);
 }
 

@@ -50,7 +50,7 @@ cudaError_t launch_crt(const CrtParams& c, uint64_t blocks, cudaStream_t st, uin
 // length slot, the lengths (c.top_ok: a carry out of the top word is dropped instead of reported).
 // *launches (if given) counts the kernels.
 cudaError_t launch_crt_wide(CrtParams c, uint64_t jobs, uint64_t blocks_per_job, int logL, cudaStream_t st,
-                            uint64_t* launches = nullptr);
+                            uint64_t* launches = nullptr, bool three = false);
 // Whether a product of na x nb limbs runs in the wide configuration (the context's crossover, or
 // PG_WIDE_MIN_LIMBS; 0 = never).
 struct DeviceTables;

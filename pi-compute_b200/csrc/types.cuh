@@ -52,6 +52,14 @@ struct TwiddleTables {
     // 0: the layouts above for every (n, l); 1: only (14, 7) then (15, 7) (the fixed-size tables
     // of pg_mul_noalloc), [n][dir][prime].
     int row_layout;
+    // Transforms of 3 * 2^m points (the wide configuration; null otherwise): W a root of order
+    // 3 * 2^25, t3_lo[dir][prime][j] = W^(+-j) and t3_hi[dir][prime][i] = W^(+-2^13 i) (2^13 entries
+    // each); the radix-3 butterfly's constants as Shoup pairs: t3_c[dir] = (w3 - w3^2) / 2 with
+    // w3 = W^(+-2^25), and t3_h = 1/2.
+    const uint2* t3_lo[2][kMaxPrimes];
+    const uint2* t3_hi[2][kMaxPrimes];
+    uint2 t3_c[2][kMaxPrimes];
+    uint2 t3_h[kMaxPrimes];
 };
 
 // Prime-0 four-step factor table of a strided pass (prime j at + j * 2^(tile log)), or null.

@@ -71,3 +71,27 @@ def test_every_wide_length_boundary(eng, config):
             nb = max(1, tot - na)
             a, b = pkg.random_operand(na, l * 10 + s + 5), pkg.random_operand(nb, l * 10 + s + 6)
             assert np.array_equal(eng.mul_limbs(a, b), oracle.mul_gmp(a, b)), (na, nb)
+
+
+R3_SIZES = [(6000, 6000), (4097, 8000), (3 << 14, 3 << 14), (100000, 90000), (150000, 3000), (1 << 17, 1 << 16),
+            (3 << 19, (3 << 19) - 5)]
+
+
+@pytest.mark.parametrize("na,nb", R3_SIZES)
+def test_three_times_power_of_two_lengths(eng, na, nb, monkeypatch):
+    """Wide products whose na + nb - 1 coefficients fit 3 * 2^m points (3/4 of the next power of
+    two) run a radix-3 step plus 2^m-point passes (the transform's roots have order 3 * 2^25);
+    PG_RADIX3=0 sends the same product through the power-of-two length. Both bit-exact against
+    the oracle, squares and all-ones operands (the largest coefficients) included."""
+    monkeypatch.setenv("PG_WIDE_MIN_LIMBS", "1")
+    monkeypatch.setenv("PG_RADIX3", "12")  # from 3 * 2^12 points (the default starts at 3 * 2^20)
+    a = pkg.random_operand(na, 29 * na + nb)
+    b = pkg.random_operand(nb, 31 * nb + na)
+    exp = oracle.mul_gmp(a, b)
+    assert np.array_equal(eng.mul_limbs(a, b), exp)
+    monkeypatch.setenv("PG_RADIX3", "0")
+    assert np.array_equal(eng.mul_limbs(a, b), exp)
+    monkeypatch.setenv("PG_RADIX3", "12")
+    assert np.array_equal(eng.sqr_limbs(a), oracle.mul_gmp(a, a))
+    ones = np.full(na, np.uint64(0xFFFFFFFFFFFFFFFF))
+    assert np.array_equal(eng.mul_limbs(ones, b), oracle.mul_gmp(ones, b))
