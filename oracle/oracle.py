@@ -179,7 +179,7 @@ _rb = None
 
 def refb() -> ctypes.CDLL:
     """oracle/_ref/libpiref_b200.so: the reference's own BinarySplitting and PiEngine, compiled
-    unchanged, with this build's pi::B200Multiplier behind their Multiplier& (needs a GPU to run)."""
+    unchanged, with the library's pi::B200Multiplier behind their Multiplier& (needs a GPU to run)."""
     global _rb
     if _rb is None:
         r = ctypes.CDLL(LIBPIREF_B200)

@@ -4,7 +4,7 @@
 //
 // The drop-in check: the reference's UNCHANGED BinarySplitting (src/engine/binary_splitting.cpp:
 // 161-293, 295-394, 605-644) and PiEngine (src/engine/pi_engine.cpp:207-603), driven through its
-// own `pi::Multiplier&` seam (src/engine/binary_splitting.h:39, pi_engine.h:34) by this build's
+// own `pi::Multiplier&` seam (src/engine/binary_splitting.h:39, pi_engine.h:34) by the library's
 // pi::B200Multiplier, exactly as the reference's main.cpp:128-176 hands them its GPU multipliers.
 //   refb_bs   P/Q/R of [a, b) as hex strings
 //   refb_pi   "3." + digits of pi
@@ -12,7 +12,7 @@
 // mpz_mul, the reference's should_use_gpu rule) and report how many products the B200 computed.
 //
 // This translation unit sees the reference's pi::Multiplier declaration; the multiplier object
-// comes from ref_dropin_factory.cpp, which sees this build's identical declaration (the two headers
+// comes from ref_dropin_factory.cpp, which sees the library's identical declaration (the two headers
 // cannot meet in one translation unit).
 #include <cstdint>
 #include <cstdlib>

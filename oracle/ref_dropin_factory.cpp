@@ -1,5 +1,5 @@
-// ORACLE -- test infrastructure only (see ref_dropin.cpp). Makes this build's pi::B200Multiplier
-// for the reference's BinarySplitting / PiEngine; this translation unit sees this build's
+// ORACLE -- test infrastructure only (see ref_dropin.cpp). Makes the library's pi::B200Multiplier
+// for the reference's BinarySplitting / PiEngine; this translation unit sees the library's
 // pi::Multiplier declaration, which is the reference's (src/arithmetic/multiplier.h:16-41)
 // member for member, so the object is used through the reference's declaration unchanged.
 #include <cstddef>
