@@ -350,20 +350,20 @@ def run_b200(args):
         if not args.no_e2e:
             # five fresh processes (CUDA start-up dominates and varies from run to run): the median
             runs, sha, parts = [], None, []
-            env = dict(os.environ, PI_B200_TRACE="1")
+            env = {k: v for k, v in os.environ.items() if k != "PI_B200_TRACE"}  # the untraced path
             with tempfile.TemporaryDirectory() as td:
                 out = os.path.join(td, "pi.txt")
                 for _ in range(5):
                     t0 = time.perf_counter()
                     flags = ["--batched"] if mode == PIB_MODE_BATCHED else ["--gpu", "--gpu-threshold", str(args.threshold)]
                     cp = subprocess.run([pkg.PI_B200_BIN, *flags, "--digits", str(D), "--threads", str(threads),
-                                         "--device", str(local), "--output", out], check=True, env=env,
+                                         "--device", str(local), "--output", out, "--verbose"], check=True, env=env,
                                         stdout=subprocess.PIPE, text=True)
                     wall = time.perf_counter() - t0
                     runs.append(wall)
                     got_sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
                     sha = got_sha if sha in (None, got_sha) else "differs between runs"
-                    # "Process: main X ms, device context Y ms, compute Z ms, file W ms" (the CLI's trace)
+                    # "Process: main X ms, device context Y ms, compute Z ms, file W ms" (--verbose)
                     for line in cp.stdout.splitlines():
                         if line.strip().startswith("Process:"):
                             ms = [float(t.split()[-2]) for t in line.split(":", 1)[1].split(",")]
@@ -376,8 +376,8 @@ def run_b200(args):
                 breakdown = {"process_start_and_exit": round(float(med[0]), 3),
                              "device_context_and_tables": round(float(med[1]), 3),
                              "compute": round(float(med[2]), 3), "file_write": round(float(med[3]), 3),
-                             "how": "median over the runs of the CLI's own trace (PI_B200_TRACE); process start and "
-                                    "exit = wall clock minus the traced parts"}
+                             "how": "median over the runs of the CLI's own timing (--verbose); process start and "
+                                    "exit = wall clock minus the timed parts"}
             e2e = {"value": round(D / e2e_s, 1), "unit": "digits/s", "h2d_bytes_per_step": 0,
                    "d2h_bytes_per_step": D + 2, "seconds": round(e2e_s, 3),
                    "runs_s": [round(x, 3) for x in runs],

@@ -391,13 +391,18 @@ unsigned grid_for(uint64_t work, unsigned per = 256) {
 
 // ------------------------------------------------------------------ DevArith
 void DevPool::trim() {
-    for (auto& p : all_) cudaFree(p.first);
+    for (auto& p : all_) dev_free(p.first);
     all_.clear();
+    for (void* a : arenas_) dev_free(a);
+    arenas_.clear();
+    carved_.clear();
+    arena_next_ = nullptr;
+    arena_left_ = 0;
     free_.clear();
-    if (scratch_) cudaFree(scratch_);
-    if (flags_) cudaFree(flags_);
-    if (seg_) cudaFree(seg_);
-    if (host_word_) cudaFreeHost(host_word_);
+    if (scratch_) dev_free(scratch_);
+    if (flags_) dev_free(flags_);
+    if (seg_) dev_free(seg_);
+    if (host_word_) pinned_free(host_word_);
     scratch_ = nullptr;
     flags_ = nullptr;
     seg_ = nullptr;
@@ -405,11 +410,41 @@ void DevPool::trim() {
     scratch_cap_ = flags_cap_ = seg_cap_ = 0;
 }
 
+bool DevPool::reserve_arena(size_t bytes) {
+    if (arena_left_ >= bytes) return true;
+    void* a = nullptr;
+    if (pg::dev_malloc(&a, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    arenas_.push_back(a);
+    arena_next_ = static_cast<char*>(a);
+    arena_left_ = bytes;
+    return true;
+}
+
+uint64_t* DevPool::carve(size_t bytes) {
+    const size_t step = (bytes + 511) & ~(size_t)511;
+    if (!arena_next_ || step > arena_left_) return nullptr;
+    uint64_t* p = reinterpret_cast<uint64_t*>(arena_next_);
+    arena_next_ += step;
+    arena_left_ -= step;
+    carved_.push_back({p, bytes / 8});
+    return p;
+}
+
+size_t DevPool::held_bytes() const {
+    size_t b = 0;
+    for (const auto& x : all_) b += x.second * 8;
+    for (const auto& x : carved_) b += x.second * 8;
+    return b;
+}
+
 DevArith::DevArith(const DeviceTables& T, Workspace& W, cudaStream_t st, uint64_t* launches, DevPool& pool)
     : T_(T), W_(W), st_(st), launches_(launches), P_(pool), pool_(pool.free_), all_(pool.all_),
       scratch_(pool.scratch_), scratch_cap_(pool.scratch_cap_), flags_(pool.flags_), flags_cap_(pool.flags_cap_),
       seg_(pool.seg_), seg_cap_(pool.seg_cap_), host_word_(pool.host_word_) {
-    if (!host_word_ && cudaMallocHost((void**)&host_word_, 64) != cudaSuccess) throw DevError(4, "pinned word");
+    if (!host_word_ && pinned_malloc(&host_word_, 64) != cudaSuccess) throw DevError(4, "pinned word");
 }
 
 DevArith::~DevArith() { cudaStreamSynchronize(st_); }
@@ -431,7 +466,7 @@ void DevArith::reserve(DevNum& x, size_t limbs) {
     if (it != pool_.end()) {
         x.d = it->second;
         pool_.erase(it);
-    } else {
+    } else if (!(x.d = P_.carve(cap * 8))) {
         check(pg::dev_malloc((void**)&x.d, cap * 8), "DevArith allocation");
         all_.push_back({x.d, cap});
     }
@@ -450,11 +485,11 @@ uint64_t* DevArith::scratch(size_t limbs) {
     if (limbs > scratch_cap_) {
         if (scratch_) {
             cudaStreamSynchronize(st_);
-            cudaFree(scratch_);
+            dev_free(scratch_);
         }
+        const size_t cap = std::max(limbs, scratch_cap_ * 3 / 2);
         scratch_ = nullptr;
         scratch_cap_ = 0;
-        const size_t cap = std::max(limbs, scratch_cap_ * 3 / 2);
         check(pg::dev_malloc((void**)&scratch_, cap * 8), "DevArith scratch");
         scratch_cap_ = cap;
     }
@@ -465,10 +500,11 @@ uint32_t* DevArith::flags(size_t n) {
     if (n > flags_cap_) {
         if (flags_) {
             cudaStreamSynchronize(st_);
-            cudaFree(flags_);
+            dev_free(flags_);
         }
+        const size_t cap = std::max<size_t>({n, 1024, flags_cap_ + flags_cap_ / 2});
         flags_ = nullptr;
-        const size_t cap = std::max<size_t>(n, 1024);
+        flags_cap_ = 0;
         check(pg::dev_malloc((void**)&flags_, cap * 8), "DevArith flags");
         flags_cap_ = cap;
     }
@@ -497,10 +533,11 @@ void DevArith::run_add(const AddArgs& a0, int form) {
     if (a.njobs * nseg > seg_cap_) {
         if (seg_) {
             cudaStreamSynchronize(st_);
-            cudaFree(seg_);
+            dev_free(seg_);
         }
+        const size_t cap = std::max<size_t>({a.njobs * nseg, 4096, seg_cap_ + seg_cap_ / 2});
         seg_ = nullptr;
-        const size_t cap = std::max<size_t>(a.njobs * nseg, 4096);
+        seg_cap_ = 0;
         check(pg::dev_malloc((void**)&seg_, cap * 4), "DevArith segments");
         seg_cap_ = cap;
     }

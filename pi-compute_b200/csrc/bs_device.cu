@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <functional>
 #include <string>
 #include <thread>
 #include <vector>
@@ -436,12 +437,12 @@ struct DeviceBS {
     void release() {
         for (int s = 0; s < 2; ++s) {
             for (int k = 0; k < 3; ++k)
-                if (lev[s][k]) cudaFree(lev[s][k]), lev[s][k] = nullptr, lev_cap[s][k] = 0;
-            if (lev_len[s]) cudaFree(lev_len[s]), lev_len[s] = nullptr, lev_len_cap[s] = 0;
+                if (lev[s][k]) dev_free(lev[s][k]), lev[s][k] = nullptr, lev_cap[s][k] = 0;
+            if (lev_len[s]) dev_free(lev_len[s]), lev_len[s] = nullptr, lev_len_cap[s] = 0;
         }
-        if (res) cudaFree(res), res = nullptr, res_cap = 0;
-        if (sync) cudaFree(sync), sync = nullptr, sync_cap = 0;
-        if (errw) cudaFree(errw), errw = nullptr, errw_cap = 0;
+        if (res) dev_free(res), res = nullptr, res_cap = 0;
+        if (sync) dev_free(sync), sync = nullptr, sync_cap = 0;
+        if (errw) dev_free(errw), errw = nullptr, errw_cap = 0;
     }
     cudaError_t grow(void** p, uint64_t& cap, uint64_t need) {
         if (need <= cap) return cudaSuccess;
@@ -450,7 +451,7 @@ struct DeviceBS {
             cudaGraphExecDestroy(gexec);
             gexec = nullptr;
         }
-        if (*p) cudaFree(*p);
+        if (*p) dev_free(*p);
         *p = nullptr;
         cap = 0;
         cudaError_t e = pg::dev_malloc(p, need);
@@ -930,8 +931,11 @@ void bs_state_delete(DeviceBS* b) { delete b; }
 namespace pg {
 // Runs the level-batched splitting of [a, b) with the context lock held by the caller. On
 // PG_OK the root's P, Q, R stay in the context's level buffers (root.X[k], hl[k] limbs) until
-// the next splitting on this context.
-pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3], bool need_P) {
+// the next splitting on this context. while_running (optional) is called once the splitting is
+// enqueued, before the wait for it: host work (allocations for the next steps) that then
+// overlaps the device's.
+pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3], bool need_P,
+                        const std::function<void()>* while_running = nullptr) {
     cudaSetDevice(ctx_device(ctx));
     DeviceBS& bs = *ctx_bs(ctx);  // buffers persist in the context across calls
     bs.T = &ctx_tables(ctx);
@@ -948,6 +952,7 @@ pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView
         ctx_set_error(ctx, std::string("pg_bs: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? PG_ERR_OOM : PG_ERR_DEVICE;
     }
+    if (while_running && *while_running) (*while_running)();
     uint32_t herr = 0;
     hl[0] = hl[1] = hl[2] = 0;
     e = cudaMemcpyAsync(hl, root.len, 12, cudaMemcpyDeviceToHost, bs.st);

@@ -36,10 +36,16 @@ public:
 
 // Device memory behind DevArith: limb buffers cached by power-of-two size class, scratch and
 // flag words, and a pinned word for small reads. Kept by the context across calls, released
-// with it (or by trim()).
+// with it (or by trim()). A caller that knows how much a computation will hold can reserve an
+// arena first: class buffers are then carved from that one allocation (one cudaMalloc, made
+// while the device is busy with other work, instead of one per size class on the critical path).
 struct DevPool {
     std::multimap<size_t, uint64_t*> free_;   // free buffers by capacity (limbs)
-    std::vector<std::pair<uint64_t*, size_t>> all_;
+    std::vector<std::pair<uint64_t*, size_t>> all_;     // buffers of their own cudaMalloc (limbs)
+    std::vector<std::pair<uint64_t*, size_t>> carved_;  // buffers carved from an arena (limbs)
+    std::vector<void*> arenas_;
+    char* arena_next_ = nullptr;
+    size_t arena_left_ = 0;                   // bytes
     uint64_t* scratch_ = nullptr;
     size_t scratch_cap_ = 0;
     uint32_t* flags_ = nullptr;
@@ -49,6 +55,12 @@ struct DevPool {
     uint64_t* host_word_ = nullptr;           // pinned, 8 words
     ~DevPool() { trim(); }
     void trim();                              // frees everything (no DevNum may be live)
+    // Opens an arena of `bytes` unless the open one has that much room left; false (and nothing
+    // changed) when the allocation fails.
+    bool reserve_arena(size_t bytes);
+    // `bytes` (a multiple of 8) from the open arena, 512-byte aligned; nullptr when it has no room.
+    uint64_t* carve(size_t bytes);
+    size_t held_bytes() const;                // every buffer's capacity, own and carved
 };
 
 class DevArith {

@@ -181,16 +181,16 @@ cudaError_t DeviceTables::build(int device) {
 }
 
 void DeviceTables::release() {
-    if (base) cudaFree(base);
+    if (base) dev_free(base);
     base = nullptr;
-    if (base_wide) cudaFree(base_wide);
+    if (base_wide) dev_free(base_wide);
     base_wide = nullptr;
     wide = false;
 }
 
 // ---------------------------------------------------------------- workspace
 static cudaError_t grow(void** ptr, uint64_t bytes) {
-    if (*ptr) cudaFree(*ptr);
+    if (*ptr) dev_free(*ptr);
     *ptr = nullptr;
     return pg::dev_malloc(ptr, bytes);
 }
@@ -211,9 +211,9 @@ cudaError_t Workspace::ensure_limbs(uint64_t n) {
     if (e == cudaSuccess) e = grow((void**)&in_b, n * 8);
     if (e == cudaSuccess) e = grow((void**)&outl, n * 8);
     if (e == cudaSuccess) {
-        if (pinned) cudaFreeHost(pinned);
+        if (pinned) pinned_free(pinned);
         pinned = nullptr;
-        e = cudaMallocHost((void**)&pinned, 3 * n * 8);
+        e = pinned_malloc(&pinned, 3 * n * 8);
     }
     limb_cap = (e == cudaSuccess) ? n : 0;
     return e;
@@ -232,14 +232,22 @@ cudaError_t Workspace::ensure_sync(uint64_t nblocks) {
     return e;
 }
 
+cudaError_t Workspace::reserve_for(const DeviceTables& T, size_t na, size_t nb) {
+    cudaError_t e = ensure_res(product_res_elems(T, na, nb));
+    const uint64_t nwords = 2ull * (na + nb);
+    const uint64_t bw = std::min<uint64_t>((uint64_t)kWideThreads * kWideWords, (uint64_t)kCrtThreads * kCrtWords);
+    if (e == cudaSuccess) e = ensure_sync((nwords + bw - 1) / bw);
+    return e;
+}
+
 void Workspace::release() {
-    if (a_res) cudaFree(a_res);
-    if (b_res) cudaFree(b_res);
-    if (in_a) cudaFree(in_a);
-    if (in_b) cudaFree(in_b);
-    if (outl) cudaFree(outl);
-    if (sync) cudaFree(sync);
-    if (pinned) cudaFreeHost(pinned);
+    if (a_res) dev_free(a_res);
+    if (b_res) dev_free(b_res);
+    if (in_a) dev_free(in_a);
+    if (in_b) dev_free(in_b);
+    if (outl) dev_free(outl);
+    if (sync) dev_free(sync);
+    if (pinned) pinned_free(pinned);
     *this = Workspace{};
 }
 
@@ -681,6 +689,16 @@ cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t*
                             true);
     }
     return enqueue_impl(T, W, d_a, na, d_b, nb, product_logL(na, mb), 2ull * (na + mb), d_out, st, launches);
+}
+
+uint64_t product_res_elems(const DeviceTables& T, size_t na, size_t nb) {
+    const uint64_t wmin = T.wide ? wide_min_limbs(T) : 0;
+    if (wmin && na + nb >= wmin && product_logL_wide(na, nb) <= kWideMaxLogL) {
+        const int m3 = radix3_logM((uint64_t)(na + nb) - 1);
+        if (m3 >= 0) return (uint64_t)kWidePrimes * 3 * (1ull << m3);
+        return (uint64_t)kWidePrimes << product_logL_wide(na, nb);
+    }
+    return (uint64_t)kNumPrimes << product_logL(na, nb);
 }
 
 cudaError_t enqueue_product_wrap(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,

@@ -109,6 +109,9 @@ struct Workspace {
     cudaError_t ensure_res(uint64_t n);
     cudaError_t ensure_limbs(uint64_t n);
     cudaError_t ensure_sync(uint64_t nblocks);
+    // Residues and carry words for an na x nb product (and every smaller one) in one allocation
+    // each, instead of growing level by level.
+    cudaError_t reserve_for(const DeviceTables& T, size_t na, size_t nb);
     void release();
 };
 
@@ -117,6 +120,10 @@ struct Workspace {
 cudaError_t enqueue_product(const DeviceTables& T, Workspace& W, const uint64_t* d_a, size_t na,
                             const uint64_t* d_b, size_t nb, uint64_t* d_out, cudaStream_t st,
                             uint64_t* launches = nullptr);
+
+// The residue count per operand array (Workspace::ensure_res) that enqueue_product requests for
+// an na x nb product: a caller that knows its largest product can size the workspace once.
+uint64_t product_res_elems(const DeviceTables& T, size_t na, size_t nb);
 
 // The same product in a forced configuration (wide: 64-bit coefficients over five primes), for the
 // autotuner; cudaErrorInvalidValue when the wide tables are absent or the product is too long for them.

@@ -54,13 +54,13 @@ struct BatchWork {
 
     ~BatchWork() {
         for (auto* r : res)
-            if (r) cudaFree(r);
-        if (sync) cudaFree(sync);
-        if (errw) cudaFree(errw);
-        if (d_src) cudaFree(d_src);
-        if (d_dst) cudaFree(d_dst);
-        if (h_src) cudaFreeHost(h_src);
-        if (h_dst) cudaFreeHost(h_dst);
+            if (r) dev_free(r);
+        if (sync) dev_free(sync);
+        if (errw) dev_free(errw);
+        if (d_src) dev_free(d_src);
+        if (d_dst) dev_free(d_dst);
+        if (h_src) pinned_free(h_src);
+        if (h_dst) pinned_free(h_dst);
     }
 };
 
@@ -73,7 +73,7 @@ template <class T>
 cudaError_t grow_dev(T** p, uint64_t& cap, uint64_t n) {
     if (n <= cap) return cudaSuccess;
     n = std::max(n, cap + cap / 2);
-    if (*p) cudaFree(*p);
+    if (*p) dev_free(*p);
     *p = nullptr;
     cap = 0;
     cudaError_t e = pg::dev_malloc((void**)p, n * sizeof(T));
@@ -211,14 +211,14 @@ static pg_status prepare_batch(pg_ctx* ctx, BatchWork* W, const pg_job* jobs, si
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "stream");
     if (4 * n > W->h_cap) {
-        if (W->h_src) cudaFreeHost(W->h_src);
-        if (W->h_dst) cudaFreeHost(W->h_dst);
+        if (W->h_src) pinned_free(W->h_src);
+        if (W->h_dst) pinned_free(W->h_dst);
         W->h_src = nullptr;
         W->h_dst = nullptr;
         W->h_cap = 0;
         const uint64_t cap = std::max<uint64_t>(4 * n, 1024);
-        e = cudaMallocHost((void**)&W->h_src, cap * sizeof(SrcEntry));
-        if (e == cudaSuccess) e = cudaMallocHost((void**)&W->h_dst, cap * sizeof(DstEntry));
+        e = pinned_malloc(&W->h_src, cap * sizeof(SrcEntry));
+        if (e == cudaSuccess) e = pinned_malloc(&W->h_dst, cap * sizeof(DstEntry));
         if (e != cudaSuccess) return cuda_fail(ctx, e, "pinned tables");
         W->h_cap = cap;
     }
@@ -281,7 +281,7 @@ static pg_status prepare_batch(pg_ctx* ctx, BatchWork* W, const pg_job* jobs, si
     if (res_need > W->res_cap) {
         const uint64_t want = std::max(res_need, W->res_cap + W->res_cap / 2);
         for (auto*& r : W->res) {
-            if (r) cudaFree(r);
+            if (r) dev_free(r);
             r = nullptr;
         }
         W->res_cap = 0;
@@ -289,7 +289,7 @@ static pg_status prepare_batch(pg_ctx* ctx, BatchWork* W, const pg_job* jobs, si
             e = pg::dev_malloc((void**)&r, want * 4);
             if (e != cudaSuccess) {
                 for (auto*& q : W->res) {
-                    if (q) cudaFree(q);
+                    if (q) dev_free(q);
                     q = nullptr;
                 }
                 return cuda_fail(ctx, e, "batch residues");
@@ -544,7 +544,7 @@ pg_status pg_buf_alloc(pg_ctx* ctx, size_t cap, pg_buf** out) {
     if (e == cudaSuccess && cap) e = pg::dev_malloc((void**)&b->d, cap * 8);
     if (e == cudaSuccess && cap) e = cudaMemsetAsync(b->d, 0, cap * 8, pg::ctx_stream(ctx));
     if (e != cudaSuccess) {
-        if (b->d) cudaFree(b->d);
+        if (b->d) pg::dev_free(b->d);
         delete b;
         return pg::cuda_fail(ctx, e, "pg_buf_alloc");
     }
@@ -556,7 +556,7 @@ void pg_buf_free(pg_ctx* ctx, pg_buf* b) {
     if (!b) return;
     cudaSetDevice(b->device);
     if (ctx) cudaStreamSynchronize(pg::ctx_stream(ctx));
-    if (b->d) cudaFree(b->d);
+    if (b->d) pg::dev_free(b->d);
     delete b;
 }
 

@@ -189,11 +189,11 @@ pg_status pg_tune(pg_ctx* ctx, int lo, int hi, double* best_us) {
     }
     // the device error word stays as it was: every product here was checked above
     cudaStreamSynchronize(st);
-    if (a) cudaFree(a);
-    if (b) cudaFree(b);
-    if (ref) cudaFree(ref);
-    if (out) cudaFree(out);
-    if (cnt) cudaFree(cnt);
+    if (a) dev_free(a);
+    if (b) dev_free(b);
+    if (ref) dev_free(ref);
+    if (out) dev_free(out);
+    if (cnt) dev_free(cnt);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (e != cudaSuccess) {

@@ -52,7 +52,7 @@ uint64_t* ctx_launches(pg_ctx* c);
 void ctx_set_error(pg_ctx* c, const std::string& msg);
 int ctx_device(pg_ctx* c);
 pg_status bs_run_locked(pg_ctx* ctx, unsigned long a, unsigned long b, LevelView& root, uint32_t hl[3],
-                        bool need_P = true);
+                        bool need_P = true, const std::function<void()>* while_running = nullptr);
 bool trace_on();
 
 // ------------------------------------------------------------------ batched shared-operand product
@@ -73,21 +73,21 @@ struct SharedProduct {
     uint64_t digits_cap = 0;
 
     ~SharedProduct() {
-        if (res) cudaFree(res);
-        if (bres) cudaFree(bres);
-        if (sync) cudaFree(sync);
-        if (errw) cudaFree(errw);
-        if (flags) cudaFree(flags);
-        if (digits) cudaFree(digits);
+        if (res) dev_free(res);
+        if (bres) dev_free(bres);
+        if (sync) dev_free(sync);
+        if (errw) dev_free(errw);
+        if (flags) dev_free(flags);
+        if (digits) dev_free(digits);
     }
 
     static void grow(uint32_t** p, uint64_t& cap, uint64_t words, cudaStream_t st) {
         if (words <= cap) return;
         cudaStreamSynchronize(st);
-        if (*p) cudaFree(*p);
+        const uint64_t want = std::max(words, cap + cap / 2);
+        if (*p) dev_free(*p);
         *p = nullptr;
         cap = 0;
-        const uint64_t want = std::max(words, cap + cap / 2);
         cudaError_t e = pg::dev_malloc((void**)p, want * 4);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -227,13 +227,13 @@ struct CkptStaging {
     cudaEvent_t ev[2] = {nullptr, nullptr};
     ~CkptStaging() {
         for (int i = 0; i < 2; ++i) {
-            if (buf[i]) cudaFreeHost(buf[i]);
+            if (buf[i]) pinned_free(buf[i]);
             if (ev[i]) cudaEventDestroy(ev[i]);
         }
     }
     void ensure() {
         for (int i = 0; i < 2; ++i) {
-            if (!buf[i] && cudaMallocHost((void**)&buf[i], kChunk) != cudaSuccess)
+            if (!buf[i] && pinned_malloc(&buf[i], kChunk) != cudaSuccess)
                 throw DevError(PG_ERR_OOM, "checkpoint staging buffer");
             if (!ev[i] && cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess)
                 throw DevError(PG_ERR_DEVICE, "checkpoint staging event");
@@ -257,6 +257,29 @@ struct FinishState {
         if (st2) cudaStreamDestroy(st2);
     }
 };
+// The trace's high-water marks of the finish's buffers (bytes held at the end of a call).
+void trace_buffers(pg_ctx* ctx, FinishState& fs) {
+    auto pool_bytes = [](const DevPool& p) {
+        size_t b = 0;
+        for (const auto& x : p.all_) b += x.second * 8;
+        return std::make_pair(p.all_.size(), b);
+    };
+    const Workspace& w = ctx_workspace(ctx);
+    const auto p1 = pool_bytes(fs.pool), p2 = pool_bytes(fs.pool2);
+    FreeList& f = free_list();
+    size_t pend = 0;
+    {
+        std::lock_guard<std::mutex> lk(f.mu);
+        pend = f.pending_bytes;
+    }
+    std::fprintf(stderr,
+                 "[pi_device] buffers: workspace %.1f MB residues + %.1f MB limbs, helper workspace %.1f MB residues, "
+                 "shared product %.1f + %.1f MB, pool %zu numbers %.1f MB, helper pool %zu numbers %.1f MB, "
+                 "deferred frees %.1f MB\n",
+                 2e-6 * 4 * w.res_cap, 3e-6 * 8 * w.limb_cap, 2e-6 * 4 * fs.ws2.res_cap, 4e-6 * fs.sp.res_cap,
+                 4e-6 * fs.sp.bres_cap, p1.first, 1e-6 * p1.second, p2.first, 1e-6 * p2.second, 1e-6 * pend);
+}
+
 FinishState* finish_state_new() { return new FinishState; }
 void finish_state_delete(FinishState* f) { delete f; }
 FinishState* ctx_finish(pg_ctx* c);
@@ -276,13 +299,36 @@ struct Num {
     operator DevNum&() { return v; }
 };
 
+// Allocation counters of the process (dev_alloc.h), for the trace.
+struct AllocSnap {
+    uint64_t n, bytes, ns, frees, free_ns, pinned, pinned_ns;
+    static AllocSnap now() {
+        const AllocStats& s = alloc_stats();
+        return {s.allocs.load(), s.alloc_bytes.load(), s.alloc_ns.load(), s.frees.load(), s.free_ns.load(),
+                s.pinned.load(), s.pinned_ns.load()};
+    }
+};
+
+// " (N cudaMalloc, X MB, T ms; ...)" for the allocations made since `a`, or "" when none.
+std::string alloc_delta(const AllocSnap& a) {
+    const AllocSnap b = AllocSnap::now();
+    if (b.n == a.n && b.frees == a.frees && b.pinned == a.pinned) return "";
+    char buf[192];
+    std::snprintf(buf, sizeof buf, " (%llu cudaMalloc, %.1f MB, %.3f ms; %llu cudaFree, %.3f ms; %llu pinned, %.3f ms)",
+                  (unsigned long long)(b.n - a.n), (double)(b.bytes - a.bytes) / 1e6, (double)(b.ns - a.ns) / 1e6,
+                  (unsigned long long)(b.frees - a.frees), (double)(b.free_ns - a.free_ns) / 1e6,
+                  (unsigned long long)(b.pinned - a.pinned), (double)(b.pinned_ns - a.pinned_ns) / 1e6);
+    return buf;
+}
+
 struct Timer {
     const char* what;
     std::chrono::steady_clock::time_point t0;
-    explicit Timer(const char* w) : what(w), t0(std::chrono::steady_clock::now()) {}
+    AllocSnap a0;
+    explicit Timer(const char* w) : what(w), t0(std::chrono::steady_clock::now()), a0(AllocSnap::now()) {}
     double ms() const { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); }
     ~Timer() {
-        if (trace_on()) std::fprintf(stderr, "[pi_device] %s: %.3f ms\n", what, ms());
+        if (trace_on()) std::fprintf(stderr, "[pi_device] %s: %.3f ms%s\n", what, ms(), alloc_delta(a0).c_str());
     }
 };
 
@@ -609,7 +655,7 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
     // device synchronisation each and, now and then, tens of milliseconds
     if (nd > sp.digits_cap) {
         A.sync();
-        if (sp.digits) cudaFree(sp.digits);
+        if (sp.digits) dev_free(sp.digits);
         sp.digits = nullptr;
         sp.digits_cap = 0;
         if (pg::dev_malloc((void**)&sp.digits, nd) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
@@ -719,7 +765,7 @@ void to_decimal(DevArith& A, SharedProduct& sp, const DevNum& x, size_t nd, char
         const uint64_t most = (uint64_t)1 << (J - kLeafLog);
         if (most + 1 > sp.flags_cap) {
             A.sync();
-            if (sp.flags) cudaFree(sp.flags);
+            if (sp.flags) dev_free(sp.flags);
             sp.flags = nullptr;
             sp.flags_cap = 0;
             if (pg::dev_malloc((void**)&sp.flags, (most + 1) * 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
@@ -955,7 +1001,7 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
     const uint64_t n = P.n;
     if (n > sp.digits_cap) {
         A.sync();
-        if (sp.digits) cudaFree(sp.digits);
+        if (sp.digits) dev_free(sp.digits);
         sp.digits = nullptr;
         sp.digits_cap = 0;
         if (pg::dev_malloc((void**)&sp.digits, n) != cudaSuccess) throw DevError(PG_ERR_OOM, "digit buffer");
@@ -1004,7 +1050,7 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
     uint32_t* flag = sp.flags;
     if (!flag || sp.flags_cap < 1) {
         A.sync();
-        if (sp.flags) cudaFree(sp.flags);
+        if (sp.flags) dev_free(sp.flags);
         sp.flags = nullptr;
         sp.flags_cap = 0;
         if (pg::dev_malloc((void**)&sp.flags, 4) != cudaSuccess) throw DevError(PG_ERR_OOM, "flags");
@@ -1030,6 +1076,27 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
 // Whether pi's digits for `digits` take the scaled remainder tree (every level in one transform;
 // PG_EXACT_CONVERSION unset).
 bool pi_tree_path(size_t digits) { return srt_fits(srt_plan(digits + 1)) && !std::getenv("PG_EXACT_CONVERSION"); }
+
+// Buffers of a pi run's finish sized before it starts, so that a fresh process does not grow
+// them step by step (each growth a cudaMalloc on the critical path; a process's first run made
+// some 450 of them): the product workspace for the largest product (two k-bit factors, k the
+// final formula's precision) and an arena of `units` buffers of the k-bit size class for the
+// numbers. The arena is opened only while the pool holds less (a later run finds its buffers
+// cached). Failures are left to the steps themselves, which allocate as before.
+void presize_finish(const DeviceTables& T, Workspace& W, DevPool& pool, size_t digits, size_t units) {
+    const SrtPlan P = srt_plan(digits + 1);
+    const size_t n = (pi_tenth_bits(P.w[0]) + 63) / 64 + 2;
+    if (W.reserve_for(T, n, n) != cudaSuccess) cudaGetLastError();
+    size_t cls = 2;
+    while (cls < n) cls <<= 1;
+    const size_t want = units * cls * 8, held = pool.held_bytes();
+    if (held < want) pool.reserve_arena(want - held);
+}
+
+// Arena sizes in k-bit size classes: what the two finishes hold at the end of a 100M-digit run
+// (the caller's pool 17 classes, the helper's 12).
+constexpr size_t kFinishArenaUnits = 16;
+constexpr size_t kHelperArenaUnits = 12;
 
 // sqrt(10005) 2^k and the tree's powers of ten, computed by a helper host thread on the finish
 // state's second stream (its own product workspace and pool) while the caller's stream runs the
@@ -1063,9 +1130,13 @@ struct PiHelper {
         const size_t k = pi_tenth_bits(P.w[0]);
         const int J = P.J;
         A.reset(new DevArith(T, fs.ws2, fs.st2, &launches, fs.pool2));
-        th = std::thread([this, k, J] {
+        th = std::thread([this, k, J, digits] {
             try {
                 cudaSetDevice(device);
+                {
+                    Timer tm("helper buffers");
+                    presize_finish(T, fs.ws2, fs.pool2, digits, kHelperArenaUnits);
+                }
                 S.reset(new Num(*A));
                 {
                     Timer tm("sqrt(10005), helper stream");
@@ -1578,6 +1649,7 @@ pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t
                        char* out) {
     if (!ctx || !q || !r || !out || nq == 0 || nr == 0) return PG_ERR_BAD_ARG;
     std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    pg::DeferFrees defer;  // no cudaFree (a wait for the idle device) until the call returns
     cudaSetDevice(pg::ctx_device(ctx));
     return pg::guarded(ctx, [&] {
         pg::FinishState& fs = *pg::ctx_finish(ctx);
@@ -1597,6 +1669,7 @@ pg_status pg_pi_finish(pg_ctx* ctx, const uint64_t* q, size_t nq, const uint64_t
 pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
     if (!ctx || !out || digits == 0) return PG_ERR_BAD_ARG;
     std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    pg::DeferFrees defer;  // no cudaFree (a wait for the idle device) until the call returns
     cudaSetDevice(pg::ctx_device(ctx));
     const auto t0 = std::chrono::steady_clock::now();
     auto secs = [](std::chrono::steady_clock::time_point a) {
@@ -1618,7 +1691,17 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
     }
     pg::LevelView root;
     uint32_t hl[3];
-    pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl, false);  // the root's P is not used
+    std::unique_ptr<pg::Timer> tbs(new pg::Timer("binary splitting"));
+    // while the splitting runs: the finish's buffers (tree path)
+    std::function<void()> presize;
+    if (helper)
+        presize = [&] {
+            pg::Timer tm("finish buffers, during the splitting");
+            pg::presize_finish(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_finish(ctx)->pool, digits,
+                               pg::kFinishArenaUnits);
+        };
+    pg_status s = pg::bs_run_locked(ctx, 0, terms, root, hl, false, &presize);  // the root's P is not used
+    tbs.reset();
     const bool big = (s == PG_ERR_TOO_LARGE);  // split into subtrees below, merged on the device
     if (s != PG_OK && !big) return s;
     if (big) pg::ctx_set_error(ctx, "");
@@ -1650,7 +1733,11 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
             R.v.sign = hl[2] ? 1 : 0;
             Q.v.slack = R.v.slack = 0;
         }
-        pg::pi_digits(A, fs.sp, Q, R, digits, out, &t_final, helper.get());
+        {
+            pg::Timer tf("final formula and digits");
+            pg::pi_digits(A, fs.sp, Q, R, digits, out, &t_final, helper.get());
+        }
+        if (pg::trace_on()) pg::trace_buffers(ctx, fs);
     });
     if (seconds) {
         seconds[0] = t_bs;
@@ -1690,6 +1777,7 @@ pg_status pg_pi_checkpointed(pg_ctx* ctx, size_t digits, const char* dir, char* 
                              pg_ckpt_report* report) {
     if (!ctx || !out || !dir || !*dir || digits == 0) return PG_ERR_BAD_ARG;
     std::lock_guard<std::mutex> lock(pg::ctx_mutex(ctx));
+    pg::DeferFrees defer;  // no cudaFree (a wait for the idle device) until the call returns
     cudaSetDevice(pg::ctx_device(ctx));
     const auto t0 = std::chrono::steady_clock::now();
     auto secs = [](std::chrono::steady_clock::time_point t) {

@@ -78,12 +78,14 @@ PiResult PiEngine::compute(const PiConfig& cfg) {
         // The whole computation on the device (pg_pi): splitting, final formula, conversion.
         pg_ctx* ctx = shared_context(cfg.device);
         const uint64_t l0 = pg_launch_count(ctx);
-        std::string s(cfg.digits + 2, '0');
+        std::string s;
+        if (!cfg.digits_out) s.assign(cfg.digits + 2, '0');
+        char* out = cfg.digits_out ? cfg.digits_out : &s[0];
         double sec[4] = {0, 0, 0, 0};
         pg_ckpt_report rep{};
         const bool ckpt = !cfg.checkpoint_dir.empty();
-        const pg_status st = ckpt ? pg_pi_checkpointed(ctx, cfg.digits, cfg.checkpoint_dir.c_str(), &s[0], sec, &rep)
-                                  : pg_pi(ctx, cfg.digits, &s[0], sec);
+        const pg_status st = ckpt ? pg_pi_checkpointed(ctx, cfg.digits, cfg.checkpoint_dir.c_str(), out, sec, &rep)
+                                  : pg_pi(ctx, cfg.digits, out, sec);
         if (st != PG_OK)
             throw std::runtime_error(std::string(ckpt ? "pg_pi_checkpointed: " : "pg_pi: ") + pg_last_error(ctx) +
                                      " (status " + std::to_string(st) + ")");

@@ -32,6 +32,9 @@ struct PiConfig {
     size_t gpu_threshold = 1024;    // Newton finish: min limbs of the smaller operand for the GPU
     bool verbose = false;
     std::string checkpoint_dir;     // batched device mode: resume from / save checkpoint files here
+    // Batched device mode: when set, the digits + 2 output bytes ("3." and the decimals) are written
+    // here (for instance into a mapping of the output file) and PiResult::digits stays empty.
+    char* digits_out = nullptr;
 };
 
 struct PiTimings {
