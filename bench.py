@@ -354,26 +354,38 @@ def run_b200(args):
             with tempfile.TemporaryDirectory() as td:
                 out = os.path.join(td, "pi.txt")
                 for _ in range(5):
+                    w0 = time.time_ns()
                     t0 = time.perf_counter()
                     flags = ["--batched"] if mode == PIB_MODE_BATCHED else ["--gpu", "--gpu-threshold", str(args.threshold)]
                     cp = subprocess.run([pkg.PI_B200_BIN, *flags, "--digits", str(D), "--threads", str(threads),
                                          "--device", str(local), "--output", out, "--verbose"], check=True, env=env,
                                         stdout=subprocess.PIPE, text=True)
                     wall = time.perf_counter() - t0
+                    w1 = time.time_ns()
                     runs.append(wall)
                     got_sha = hashlib.sha256(open(out, "rb").read()).hexdigest()
                     sha = got_sha if sha in (None, got_sha) else "differs between runs"
                     # "Process: main X ms, device context Y ms, compute Z ms, file W ms" (--verbose)
+                    ms, clock = None, None
                     for line in cp.stdout.splitlines():
                         if line.strip().startswith("Process:"):
                             ms = [float(t.split()[-2]) for t in line.split(":", 1)[1].split(",")]
-                            if len(ms) == 4:
-                                parts.append([wall - sum(ms) / 1e3 + ms[0] / 1e3] + [m / 1e3 for m in ms[1:]])
+                        elif line.strip().startswith("Clock:"):
+                            clock = [int(t.split()[-2]) for t in line.split(":", 1)[1].split(",")]
+                    if ms and len(ms) == 4:
+                        # start-up: launch to main (+ argument parsing); exit: the exit stamp to the return of
+                        # subprocess.run (driver tear-down of the context); wall clocks of one host
+                        start = (clock[0] - w0) / 1e9 + ms[0] / 1e3 if clock else None
+                        end = (w1 - clock[1]) / 1e9 if clock else None
+                        parts.append([wall - sum(ms) / 1e3 + ms[0] / 1e3] + [m / 1e3 for m in ms[1:]]
+                                     + ([start, end] if clock else [float("nan"), float("nan")]))
             e2e_s = float(np.median(runs))
             breakdown = None
             if parts:
                 med = np.median(np.array(parts), axis=0)
                 breakdown = {"process_start_and_exit": round(float(med[0]), 3),
+                             "of_which_start": round(float(med[4]), 3) if np.isfinite(med[4]) else None,
+                             "of_which_exit": round(float(med[5]), 3) if np.isfinite(med[5]) else None,
                              "device_context_and_tables": round(float(med[1]), 3),
                              "compute": round(float(med[2]), 3), "file_write": round(float(med[3]), 3),
                              "how": "median over the runs of the CLI's own timing (--verbose); process start and "

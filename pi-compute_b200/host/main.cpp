@@ -75,6 +75,7 @@ static void usage() {
 
 int main(int argc, char** argv) {
     const auto t_main = std::chrono::steady_clock::now();
+    const auto wall_main = std::chrono::system_clock::now();
     // Load every kernel when the CUDA context is created (unless the caller chose otherwise): a run
     // uses most of them, and loading them one by one at first launch costs this one-shot process
     // more (measured on a B200: the twiddle-table build 49 -> 6 ms, the first pi run 10-20 ms less).
@@ -191,6 +192,14 @@ int main(int argc, char** argv) {
         // The output file is closed and checked: leave without tearing the device context down
         // (freeing gigabytes of device buffers one by one takes longer than the driver's own
         // clean-up of an exiting process).
+        if (cfg.verbose || std::getenv("PI_B200_TRACE")) {
+            // wall-clock stamps of main's entry and of the exit, for a caller that splits its own
+            // measurement of the process into start-up, the timed parts and the exit
+            auto ns = [](std::chrono::system_clock::time_point t) {
+                return (long long)std::chrono::duration_cast<std::chrono::nanoseconds>(t.time_since_epoch()).count();
+            };
+            std::printf("  Clock: main %lld ns, exit %lld ns\n", ns(wall_main), ns(std::chrono::system_clock::now()));
+        }
         std::fflush(stdout);
         std::fflush(stderr);
         _exit(0);
