@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "bigint.cuh"
@@ -174,6 +175,116 @@ __global__ void __launch_bounds__(kBigThreads) add_final_kernel(AddArgs A, uint6
     const uint32_t segcin = (A.seg[blockIdx.x] >> 2) & 1u;
     // carry into this warp: segment carry-in through the earlier warps
     uint32_t cw = segcin;
+    for (int w = 0; w < warp; ++w) cw = gp_apply(s_w[w], cw);
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, incl, 1);
+    uint32_t carry = lane == 0 ? cw : gp_apply(prev, cw);
+    uint64_t* z = A.z + job * A.sz;
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        if (base + k < A.n) {
+            const uint64_t r = s[k] + carry;
+            carry = ((gen >> k) & 1u) | (r < s[k] ? 1u : 0u);
+            z[base + k] = r;
+        }
+    }
+}
+
+// Plain sums of long numbers in one launch (njobs x nseg blocks): block b sums segment
+// s = b % nseg of job b / nseg, publishes the segment's (g, p), looks back over the job's earlier
+// segments, 32 at a time across a warp, until one has published its carry out (composing the
+// aggregates passed over), publishes its own carry out and writes its limbs. Status word: bits 0-1 (g, p), bit 2 the
+// carry out, bit 3 (g, p) valid, bit 4 carry out valid, bits 8-31 the call's epoch (words of
+// earlier calls never pass for this one's, so the array needs no reset between calls). Blocks
+// start in index order, so a wait is on a block already running; past kAddSpinLimit polls the
+// block records kErrAddWait and goes on with carry 0 (the result is then wrong and flagged).
+__global__ void __launch_bounds__(kBigThreads) add_onepass_kernel(AddArgs A, uint64_t nseg, uint32_t epoch) {
+    __shared__ uint32_t s_w[kBigThreads / 32];
+    __shared__ uint32_t s_cin;
+    const uint64_t job = blockIdx.x / nseg, seg = blockIdx.x % nseg;
+    if (A.enable && !A.enable[job]) return;
+    const uint64_t base = seg * kBigSeg + (uint64_t)threadIdx.x * kBigLimbs;
+    uint64_t s[kBigLimbs];
+    uint32_t gen = 0, gp = 2;
+#pragma unroll
+    for (int k = 0; k < kBigLimbs; ++k) {
+        s[k] = 0;
+        if (base + k < A.n) {
+            uint64_t u, v;
+            add_fetch<AddForm::Plain>(A, job, base + k, u, v);
+            s[k] = u + v;
+            const uint32_t gk = s[k] < u ? 1u : 0u;
+            gen |= gk << k;
+            gp = gp_compose(gk | ((s[k] == ~0ull ? 1u : 0u) << 1), gp);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t incl = gp_warp_scan(gp, lane);
+    if (lane == 31) s_w[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        // the segment's aggregate, published first: later segments may pass over this one
+        uint32_t agg = 2;
+        for (int w = 0; w < kBigThreads / 32; ++w) agg = gp_compose(s_w[w], agg);
+        volatile uint32_t* stw = A.seg + (blockIdx.x - seg);  // the job's status words
+        const uint32_t tag = epoch << 8;
+        if (lane == 0 && seg > 0) stw[seg] = tag | 8u | agg;
+        // look back 32 segments at a time: lane l reads segment j - l (j the window's nearest);
+        // once every word of the window is valid, the nearest lane holding a carry out ends the
+        // walk, and the window's function is the composition of the aggregates nearer than it
+        // (lane order = from the nearest segment down). Segment -1 stands for the carry in.
+        uint32_t cin = A.cin;
+        if (seg > 0) {
+            uint32_t acc = 2;  // (g, p) of the segments passed over so far (identity)
+            long long j = (long long)seg - 1;
+            uint32_t polls = 0;
+            bool timed_out = false;
+            for (;;) {
+                const long long idx = j - lane;
+                uint32_t w = idx < 0 ? (tag | 16u | (A.cin << 2)) : stw[idx];
+                bool valid = (w >> 8) == epoch && (w & 24u);
+                while (!__all_sync(0xffffffffu, valid)) {
+                    if (++polls > kAddSpinLimit) {
+                        timed_out = true;
+                        break;
+                    }
+                    if (!valid) {
+                        w = stw[idx];
+                        valid = (w >> 8) == epoch && (w & 24u);
+                    }
+                }
+                if (timed_out) break;
+                const unsigned inc = __ballot_sync(0xffffffffu, (w & 16u) != 0);
+                const int first = inc ? __ffs(inc) - 1 : 32;  // nearest segment with a carry out
+                // lane function: the aggregate before `first`, the carry out at `first` (a constant:
+                // g = carry, p = 0), identity beyond
+                uint32_t x = lane < first ? (w & 3u) : (lane == first ? ((w >> 2) & 1u) : 2u);
+#pragma unroll
+                for (int off = 1; off < 32; off <<= 1) {
+                    const uint32_t y = __shfl_down_sync(0xffffffffu, x, off);
+                    if (lane + off < 32) x = gp_compose(x, y);
+                }
+                x = __shfl_sync(0xffffffffu, x, 0);
+                acc = gp_compose(acc, x);
+                if (inc) {
+                    cin = acc & 1u;  // p = 0 past a carry out: g is the carry
+                    break;
+                }
+                j -= 32;
+            }
+            if (timed_out) {
+                if (lane == 0 && A.err) atomicOr(A.err, kErrAddWait);
+                cin = 0;
+            }
+        }
+        if (lane == 0) {
+            const uint32_t cout = gp_apply(agg, cin);
+            stw[seg] = tag | 16u | 8u | (cout << 2) | agg;
+            if (seg == nseg - 1 && A.carry_out) A.carry_out[job] = cout;
+            s_cin = cin;
+        }
+    }
+    __syncthreads();
+    uint32_t cw = s_cin;
     for (int w = 0; w < warp; ++w) cw = gp_apply(s_w[w], cw);
     const uint32_t prev = __shfl_up_sync(0xffffffffu, incl, 1);
     uint32_t carry = lane == 0 ? cw : gp_apply(prev, cw);
@@ -515,6 +626,16 @@ void DevArith::sync() {
     check(cudaStreamSynchronize(st_), "DevArith");
 }
 
+// Plain long sums in one launch (add_onepass_kernel) unless PG_ADD_ONEPASS=0 (three launches, no
+// wait between blocks).
+static bool add_onepass() {
+    static const bool on = [] {
+        const char* e = std::getenv("PG_ADD_ONEPASS");
+        return !(e && e[0] == '0' && e[1] == 0);
+    }();
+    return on;
+}
+
 void DevArith::run_add(const AddArgs& a0, int form) {
     AddArgs a = a0;
     if (a.n == 0) return;
@@ -539,10 +660,24 @@ void DevArith::run_add(const AddArgs& a0, int form) {
         seg_ = nullptr;
         seg_cap_ = 0;
         check(pg::dev_malloc((void**)&seg_, cap * 4), "DevArith segments");
+        // no stale epoch may match a later call's (one-pass status words)
+        check(cudaMemsetAsync(seg_, 0, cap * 4, st_), "DevArith segments");
         seg_cap_ = cap;
     }
     a.seg = seg_;
     const unsigned blocks = (unsigned)(a.njobs * nseg);
+    if (form == 0 && add_onepass()) {
+        if (!W_.sync) check(W_.ensure_sync(1), "error word");
+        a.err = W_.sync;
+        if (++P_.add_epoch_ > 0xffffffu) {  // the epoch field wraps: clear the words, start again
+            check(cudaMemsetAsync(seg_, 0, seg_cap_ * 4, st_), "DevArith segments");
+            P_.add_epoch_ = 1;
+        }
+        add_onepass_kernel<<<blocks, kBigThreads, 0, st_>>>(a, nseg, P_.add_epoch_);
+        check(cudaGetLastError(), "add");
+        ++*launches_;
+        return;
+    }
     if (form == 0)
         add_seg_kernel<AddForm::Plain><<<blocks, kBigThreads, 0, st_>>>(a, nseg);
     else

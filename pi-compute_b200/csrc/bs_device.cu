@@ -76,16 +76,18 @@ __device__ __forceinline__ void sb_addsub(uint64_t* x, int n, const uint64_t* y,
     }
 }
 
-// Carry resolution of n <= 32 * K limbs across a warp: limb i's value before carries is v(i), a
-// signed 128-bit number in (-2^65, 3 * 2^64); the carries between limbs lie in {-1, 0, 1, 2}. Each
-// lane takes K consecutive limbs, tabulates its carry transfer function (carry in -> carry out, four
-// two-bit entries of carry + 1), and a warp scan of the functions gives every lane its carry in.
-// Writes dst[0 .. n) and returns the length without leading zero limbs (in every lane).
-template <int K, class V>
-__device__ __forceinline__ int warp_resolve(V v, int n, uint64_t* dst) {
+// Carry resolution of n <= G * K limbs across a group of G lanes (G a power of two <= 32; the
+// groups tile the warp and every lane of the warp calls this together): limb i's value before
+// carries is v(i), a signed 128-bit number in (-2^65, 3 * 2^64); the carries between limbs lie in
+// {-1, 0, 1, 2}. Each lane takes K consecutive limbs, tabulates its carry transfer function (carry
+// in -> carry out, four two-bit entries of carry + 1), and a scan of the functions over the group
+// gives every lane its carry in. Writes dst[0 .. n) and returns the length without leading zero
+// limbs (in every lane of the group). Every lane reads its v(i) before any lane writes dst.
+template <int K, int G, class V>
+__device__ __forceinline__ int group_resolve(V v, int n, uint64_t* dst) {
     typedef __int128 i128;
-    const int lane = threadIdx.x & 31;
-    const int c0 = lane * K;
+    const int gl = threadIdx.x & (G - 1);
+    const int c0 = gl * K;
     i128 val[K];
 #pragma unroll
     for (int i = 0; i < K; ++i) val[i] = c0 + i < n ? v(c0 + i) : 0;
@@ -105,12 +107,12 @@ __device__ __forceinline__ int warp_resolve(V v, int n, uint64_t* dst) {
     }
     uint32_t incl = f;
 #pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl = compose(incl, x);
+    for (int off = 1; off < G; off <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, incl, off, G);
+        if (gl >= off) incl = compose(incl, x);
     }
-    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1);
-    if (lane == 0) excl = 0u | (1u << 2) | (2u << 4) | (3u << 6);
+    uint32_t excl = __shfl_up_sync(0xffffffffu, incl, 1, G);
+    if (gl == 0) excl = 0u | (1u << 2) | (2u << 4) | (3u << 6);
     long long c = (long long)apply(excl, 1u) - 1;
     int top = -1;
 #pragma unroll
@@ -122,7 +124,9 @@ __device__ __forceinline__ int warp_resolve(V v, int n, uint64_t* dst) {
             c = (long long)(t >> 64);
         }
     }
-    return __reduce_max_sync(0xffffffffu, top) + 1;
+#pragma unroll
+    for (int off = G / 2; off > 0; off >>= 1) top = max(top, __shfl_xor_sync(0xffffffffu, top, off, G));
+    return top + 1;
 }
 
 // Leaf magnitudes of term k (binary_splitting.cpp:137-159): |P| = (6k-5)(2k-1)(6k-1),
@@ -240,40 +244,46 @@ __global__ void __launch_bounds__(128) bs_thread_merge_kernel(LevelView in, Leve
     emit(2, r0, nr);
 }
 
-// One warp per merge with operands of at most MAXC limbs (shared memory schoolbook).
-// Column sums are computed in parallel by the lanes; lane 0 propagates carries.
-template <int MAXC>
-__global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelView out, uint64_t merges,
-                                                            uint64_t a0, uint64_t b0, int depth) {
-    constexpr int W = 4;  // warps per block
-    __shared__ uint64_t s_op[W][6][MAXC];
-    __shared__ uint64_t s_col[W][3][2 * MAXC];  // 192-bit column sums: lo, mid, hi
-    __shared__ uint64_t s_res[W][2][2 * MAXC + 1];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t m = (uint64_t)blockIdx.x * W + warp;
-    if (m >= merges) return;
+// A group of G lanes per merge with operands of at most MAXC limbs (shared-memory schoolbook),
+// 128 / G merges per block: the lanes of a group take the product's columns in turn, each column
+// summed in two independent 192-bit chains, and resolve the carries together (group_resolve).
+// Groups sized to the operands keep every lane busy from the bottom depths (millions of merges of
+// a few limbs) up to 64-limb children, with no per-thread arrays in local memory. Every lane of a
+// warp runs every step (the shuffles need them all): a group past the last merge computes zeros
+// and stores nothing.
+template <int MAXC, int G>
+__global__ void __launch_bounds__(128) bs_group_merge_kernel(LevelView in, LevelView out, uint64_t merges,
+                                                             uint64_t a0, uint64_t b0, int depth) {
+    constexpr int NG = 128 / G;  // merges per block
+    __shared__ uint64_t s_op[NG][6][MAXC];
+    __shared__ uint64_t s_col[NG][3][2 * MAXC];  // 192-bit column sums: lo, mid, hi
+    __shared__ uint64_t s_res[NG][2][2 * MAXC + 1];
+    const int g = threadIdx.x / G, gl = threadIdx.x & (G - 1);
+    const uint64_t m = (uint64_t)blockIdx.x * NG + g;
+    const bool live = m < merges;
+    if (!__any_sync(0xffffffffu, live)) return;  // whole warps past the end
     // load Pl Ql Rl Pr Qr Rr
     int n[6];
     for (int o = 0; o < 6; ++o) {
         const uint64_t child = 2 * m + (o >= 3 ? 1 : 0);
         const int k = o % 3;
-        n[o] = (int)in.len[3 * child + k];
+        n[o] = live ? (int)in.len[3 * child + k] : 0;
         const uint64_t* src = in.X[k] + child * in.cap[k];
-        for (int t = lane; t < MAXC; t += 32) s_op[warp][o][t] = t < n[o] ? src[t] : 0;
+        for (int t = gl; t < MAXC; t += G) s_op[g][o][t] = t < n[o] ? src[t] : 0;
     }
     __syncwarp();
-    uint64_t a, b;
-    node_range(a0, b0, depth, m, a, b);
-    const int sgn = merge_r_sign(a, b);
+    uint64_t a = 0, b = 0;
+    if (live) node_range(a0, b0, depth, m, a, b);
+    const int sgn = live ? merge_r_sign(a, b) : 1;
 
-    // product helper: column sums, then the warp's carry resolution into dst (nx + ny limbs)
-    constexpr int KR = (2 * MAXC + 1 + 31) / 32;
+    // product helper: column sums, then the group's carry resolution into dst (nx + ny limbs);
+    // an empty operand gives 0
+    constexpr int KR = (2 * MAXC + 1 + G - 1) / G;
     auto product = [&](int ox, int oy, uint64_t* dst) -> int {
         const int nx = n[ox], ny = n[oy];
-        const uint64_t* x = s_op[warp][ox];
-        const uint64_t* y = s_op[warp][oy];
+        const uint64_t* x = s_op[g][ox];
+        const uint64_t* y = s_op[g][oy];
         const int ncol = nx + ny - 1;
-        // two interleaved partial sums per column (even and odd i): independent carry chains
         auto acc = [](uint64_t& lo, uint64_t& mid, uint64_t& hi, u128 t) {
             const u128 s = (u128)lo + (uint64_t)t;
             lo = (uint64_t)s;
@@ -281,7 +291,7 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
             mid = (uint64_t)s2;
             hi += (uint64_t)(s2 >> 64);
         };
-        for (int c = lane; c < ncol; c += 32) {
+        for (int c = gl; c < ncol; c += G) {
             uint64_t lo = 0, mid = 0, hi = 0, lo2 = 0, mid2 = 0, hi2 = 0;
             const int i0 = c - ny + 1 > 0 ? c - ny + 1 : 0;
             const int i1 = c < nx - 1 ? c : nx - 1;
@@ -294,16 +304,16 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
             acc(lo, mid, hi, lo2);
             acc(lo, mid, hi, (u128)mid2 << 64);
             hi += hi2;
-            s_col[warp][0][c] = lo;
-            s_col[warp][1][c] = mid;
-            s_col[warp][2][c] = hi;
+            s_col[g][0][c] = lo;
+            s_col[g][1][c] = mid;
+            s_col[g][2][c] = hi;
         }
         __syncwarp();
         // limb c = lo_c + mid_{c-1} + hi_{c-2} (each < 2^64; column sums < MAXC 2^128, so hi < MAXC)
-        const uint64_t* cl = s_col[warp][0];
-        const uint64_t* cm = s_col[warp][1];
-        const uint64_t* ch = s_col[warp][2];
-        const int len = warp_resolve<KR>(
+        const uint64_t* cl = s_col[g][0];
+        const uint64_t* cm = s_col[g][1];
+        const uint64_t* ch = s_col[g][2];
+        const int len = group_resolve<KR, G>(
             [&](int c) {
                 __int128 t = c < ncol ? cl[c] : 0;
                 if (c >= 1 && c - 1 < ncol) t += cm[c - 1];
@@ -314,43 +324,42 @@ __global__ void __launch_bounds__(128) bs_warp_merge_kernel(LevelView in, LevelV
         __syncwarp();
         return len;
     };
+    auto store = [&](int k, const uint64_t* v, int l, int lenv) {
+        if (live) {
+            uint64_t* dst = out.X[k] + m * out.cap[k];
+            for (int t = gl; t < (int)out.cap[k]; t += G) dst[t] = t < l ? v[t] : 0;
+            if (gl == 0) out.len[3 * m + k] = lenv;
+        }
+        __syncwarp();
+    };
 
     // P = Pl * Pr
     {
-        uint64_t* dst = out.X[0] + m * out.cap[0];
-        int l = (n[0] && n[3]) ? product(0, 3, s_res[warp][0]) : 0;
-        for (int t = lane; t < (int)out.cap[0]; t += 32) dst[t] = t < l ? s_res[warp][0][t] : 0;
-        if (lane == 0) out.len[3 * m + 0] = l;
-        __syncwarp();
+        const int l = product(0, 3, s_res[g][0]);
+        store(0, s_res[g][0], l, l);
     }
     // Q = Ql * Qr
     {
-        uint64_t* dst = out.X[1] + m * out.cap[1];
-        int l = product(1, 4, s_res[warp][0]);
-        for (int t = lane; t < (int)out.cap[1]; t += 32) dst[t] = t < l ? s_res[warp][0][t] : 0;
-        if (lane == 0) out.len[3 * m + 1] = l;
-        __syncwarp();
+        const int l = product(1, 4, s_res[g][0]);
+        store(1, s_res[g][0], l, l);
     }
     // R = Qr * Rl + s * Pl * Rr
     {
-        const int lx = product(4, 2, s_res[warp][0]);
-        const int ly = product(0, 5, s_res[warp][1]);
+        const int lx = product(4, 2, s_res[g][0]);
+        const int ly = product(0, 5, s_res[g][1]);
         // |R| < 2 max(|Qr Rl|, |Pl Rr|): max(lx, ly) + 1 limbs; limb i = x_i + sgn y_i before carries
         const int nr = (lx > ly ? lx : ly) + 1;
-        const uint64_t* x = s_res[warp][0];
-        const uint64_t* y = s_res[warp][1];
-        uint64_t* r = s_res[warp][0];  // in place over x: every lane reads its limbs before any writes
-        const int lr = warp_resolve<KR>(
+        const uint64_t* x = s_res[g][0];
+        const uint64_t* y = s_res[g][1];
+        uint64_t* r = s_res[g][0];  // in place over x: every lane reads its limbs before any writes
+        const int lr = group_resolve<KR, G>(
             [&](int i) {
                 const __int128 xi = i < lx ? x[i] : 0, yi = i < ly ? y[i] : 0;
                 return sgn > 0 ? xi + yi : xi - yi;
             },
             nr, r);
         __syncwarp();
-        uint64_t* dst = out.X[2] + m * out.cap[2];
-        for (int t = lane; t < (int)out.cap[2]; t += 32) dst[t] = t < nr ? s_res[warp][0][t] : 0;
-        if (lane == 0) out.len[3 * m + 2] = lr < (int)out.cap[2] ? lr : out.cap[2];
-        __syncwarp();
+        store(2, r, nr, lr < (int)out.cap[2] ? lr : (int)out.cap[2]);
     }
 }
 
@@ -865,8 +874,9 @@ struct DeviceBS {
             LevelView in = view(slot, C), out = view(oslot, P);
             auto tl0 = std::chrono::steady_clock::now();
             if (P.kind == 1) {
-                // children's largest slot decides the kernel: a thread per merge up to 16 limbs,
-                // a warp per merge (shared-memory schoolbook sized to the children) above
+                // children's largest slot decides the kernel: a thread per merge up to 16 limbs
+                // (measured faster there than lane groups, whose carry resolution outweighs such
+                // small products), 16 lanes per merge up to 32, a warp per merge up to 64
                 const uint32_t cmax = std::max({C.cap[0], C.cap[1], C.cap[2]});
                 if (cmax <= 8)
                     bs_thread_merge_kernel<8><<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(in, out, P.nodes, a0,
@@ -875,11 +885,11 @@ struct DeviceBS {
                     bs_thread_merge_kernel<16><<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(in, out, P.nodes,
                                                                                                   a0, b0, d);
                 else if (cmax <= 32)
-                    bs_warp_merge_kernel<32><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes, a0, b0,
-                                                                                            d);
+                    bs_group_merge_kernel<32, 16><<<(unsigned)((P.nodes + 7) / 8), 128, 0, st>>>(in, out, P.nodes, a0,
+                                                                                                 b0, d);
                 else
-                    bs_warp_merge_kernel<kWarpMaxC><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(in, out, P.nodes,
-                                                                                                  a0, b0, d);
+                    bs_group_merge_kernel<kWarpMaxC, 32><<<(unsigned)((P.nodes + 3) / 4), 128, 0, st>>>(
+                        in, out, P.nodes, a0, b0, d);
                 e = cudaGetLastError();
                 if (launches) ++*launches;
             } else {

@@ -53,6 +53,7 @@ struct DevPool {
     uint32_t* seg_ = nullptr;
     size_t seg_cap_ = 0;
     uint64_t* host_word_ = nullptr;           // pinned, 8 words
+    uint32_t add_epoch_ = 0;                  // one-pass sums: the last call's epoch (seg_ words)
     ~DevPool() { trim(); }
     void trim();                              // frees everything (no DevNum may be live)
     // Opens an arena of `bytes` unless the open one has that much room left; false (and nothing

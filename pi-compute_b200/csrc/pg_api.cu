@@ -92,6 +92,7 @@ pg_status check_device_error(pg_ctx* c) {
         cudaStreamSynchronize(c->stream);
         if (err == 1) return fail(c, PG_ERR_TIMEOUT, "carry look-back wait ran out of iterations");
         if (err & 4) return fail(c, PG_ERR_TIMEOUT, "tile load wait ran out of iterations");
+        if (err & 8) return fail(c, PG_ERR_TIMEOUT, "sum look-back wait ran out of iterations");
         return fail(c, PG_ERR_INTERNAL, "carry out of the most significant word");
     }
     return PG_OK;

@@ -38,6 +38,7 @@
 #include <set>
 
 #include "../../include/pi_b200.h"
+#include "bigint.cuh"
 #include "ckpt_io.h"
 #include "devnum.h"
 #include "host_div.h"
@@ -1077,6 +1078,39 @@ bool srt_digits(DevArith& A, SharedProduct& sp, const SrtPlan& P, DevNum& V, cha
 // PG_EXACT_CONVERSION unset).
 bool pi_tree_path(size_t digits) { return srt_fits(srt_plan(digits + 1)) && !std::getenv("PG_EXACT_CONVERSION"); }
 
+// The status and message of a workspace error word (bits set by the kernels: 1 a carry look-back
+// wait ran out, 2 a carry out of the top word, 4 a tile load wait ran out, 8 a sum's look-back
+// wait ran out).
+pg_status workspace_error_status(uint32_t err, const char*& what) {
+    if (err & kErrAddWait) {
+        what = "sum look-back wait ran out of iterations";
+        return PG_ERR_TIMEOUT;
+    }
+    if (err & 4) {
+        what = "tile load wait ran out of iterations";
+        return PG_ERR_TIMEOUT;
+    }
+    if (err == 1) {
+        what = "carry look-back wait ran out of iterations";
+        return PG_ERR_TIMEOUT;
+    }
+    what = "carry out of the top word";
+    return PG_ERR_INTERNAL;
+}
+
+// Throws (after clearing it) when a workspace's error word is set; waits for the stream.
+void throw_workspace_error(const Workspace& W, cudaStream_t st, const char* where) {
+    uint32_t err = 0;
+    if (W.sync) cudaMemcpyAsync(&err, W.sync, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) throw DevError(PG_ERR_DEVICE, std::string(where) + ": device error");
+    if (!err) return;
+    cudaMemsetAsync(W.sync, 0, 4, st);
+    cudaStreamSynchronize(st);
+    const char* what = "";
+    const pg_status s = workspace_error_status(err, what);
+    throw DevError(s, std::string(where) + ": " + what);
+}
+
 // Buffers of a pi run's finish sized before it starts, so that a fresh process does not grow
 // them step by step (each growth a cudaMalloc on the critical path; a process's first run made
 // some 450 of them): the product workspace for the largest product (two k-bit factors, k the
@@ -1144,6 +1178,7 @@ struct PiHelper {
                 }
                 srt_powers(*A, J, pw);
                 A->sync();
+                throw_workspace_error(fs.ws2, fs.st2, "helper stream");
             } catch (...) {
                 err = std::current_exception();
             }
@@ -1176,6 +1211,7 @@ struct PiHelper {
                     over1 = 0;
                 }
                 A->sync();
+                throw_workspace_error(fs.ws2, fs.st2, "helper stream");
             } catch (...) {
                 err = std::current_exception();
             }
@@ -1523,13 +1559,14 @@ pg_status product_errors(pg_ctx* ctx) {
     Workspace& W = ctx_workspace(ctx);
     cudaStream_t st = ctx_stream(ctx);
     uint32_t err = 0;
-    cudaMemcpyAsync(&err, W.sync, 4, cudaMemcpyDeviceToHost, st);
+    if (W.sync) cudaMemcpyAsync(&err, W.sync, 4, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess) return fail(ctx, PG_ERR_DEVICE, "device error");
     if (err) {
         cudaMemsetAsync(W.sync, 0, 4, st);
         cudaStreamSynchronize(st);
-        return fail(ctx, err == 1 ? PG_ERR_TIMEOUT : PG_ERR_INTERNAL,
-                    err == 1 ? "carry look-back wait ran out of iterations" : "carry out of the top word");
+        const char* what = "";
+        const pg_status s = workspace_error_status(err, what);
+        return fail(ctx, s, what);
     }
     return PG_OK;
 }

@@ -72,3 +72,33 @@ def test_pi_1b_digits_matches_reference():
     want = g["1000000000"]
     assert got[:66].decode() == want["head"] and got[-64:].decode() == want["tail"]
     assert hashlib.sha256(got).hexdigest() == want["sha256"]
+
+
+ADD_SCRIPT = r"""
+import math, os, sys
+sys.set_int_max_str_digits(0)
+sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
+from helpers import pkg
+
+with pkg.Engine(0) as eng:
+    # long runs of ones and zeros: sums whose carries cross many 2048-limb segments
+    for k in (3 * (1 << 20) + 17, 1 << 21):
+        for r in ((1 << k) - 1, (1 << (k - 1)) + 1, ((1 << k) - 1) ^ (1 << (k // 2))):
+            assert eng.recip_floor(r) == (1 << (2 * r.bit_length())) // r, (k, r.bit_length())
+    s = 400_001
+    assert eng.sqrt_scaled(10005, s) == math.isqrt(10005 << (2 * s)), s
+    print(eng.pi(1_000_000)[-64:].decode())
+print("ok")
+"""
+
+
+@pytest.mark.parametrize("onepass", ["1", "0"])
+def test_long_sums_one_pass_and_three_launch_forms(onepass):
+    """Plain sums of long numbers run as one launch with a bounded look-back between segments
+    (default) or as three launches (PG_ADD_ONEPASS=0); both give exact quotients and roots where
+    the carries run across many segments, and the same pi digits."""
+    env = dict(os.environ, PG_ADD_ONEPASS=onepass)
+    r = subprocess.run([sys.executable, "-c", ADD_SCRIPT, ROOT], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout[-2000:] + r.stderr[-4000:]
+    golden = json.load(open(os.path.join(GOLDEN, "pi_golden.json")))["1000000"]
+    assert r.stdout.strip().splitlines()[-2] == golden["tail"]
