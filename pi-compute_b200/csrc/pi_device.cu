@@ -253,9 +253,29 @@ struct FinishState {
     DevPool pool2;
     Workspace ws2;
     cudaStream_t st2 = nullptr;
+    // pi's finish after the splitting, at the device's highest stream priority: its chain of
+    // small Newton levels then gets SMs ahead of the helper stream's long kernels (the powers of
+    // ten, the first product) instead of queueing behind them. PG_FINISH_PRIORITY=0: the
+    // context's stream.
+    cudaStream_t st_hi = nullptr;
+    cudaStream_t finish_stream(cudaStream_t fallback) {
+        const char* e = std::getenv("PG_FINISH_PRIORITY");
+        if (e && e[0] == '0' && e[1] == 0) return fallback;
+        if (!st_hi) {
+            int least = 0, greatest = 0;
+            if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+                cudaStreamCreateWithPriority(&st_hi, cudaStreamNonBlocking, greatest) != cudaSuccess) {
+                cudaGetLastError();
+                st_hi = nullptr;
+                return fallback;
+            }
+        }
+        return st_hi;
+    }
     ~FinishState() {
         ws2.release();
         if (st2) cudaStreamDestroy(st2);
+        if (st_hi) cudaStreamDestroy(st_hi);
     }
 };
 // The trace's high-water marks of the finish's buffers (bytes held at the end of a call).
@@ -427,10 +447,36 @@ void recip_floor(DevArith& A, DevNum& Z, const DevNum& R, bool exact = true) {
     const size_t h = k / 2 + 32;
     Num Rh(A), Zh(A), Z0(A), T(A), E(A), D(A);
     A.tdiv_q_2exp(Rh, R, k - h);
+    // the trace times each level of at least 2^16 bits apart from the ones below it (waiting for
+    // the stream around them)
+    const bool tr = trace_on() && k >= (1u << 16);
+    std::chrono::steady_clock::time_point tl0, tl1;
+    if (tr) {
+        A.sync();
+        tl0 = std::chrono::steady_clock::now();
+    }
     // The half-precision reciprocal without its exact correction: within c <= 2 units of
     // 2^(2h)/Rh (the bound this step keeps, below), which saves a product and its host waits at
     // every level of the recursion.
     recip_floor(A, Zh, Rh, false);
+    if (tr) {
+        A.sync();
+        tl1 = std::chrono::steady_clock::now();
+    }
+    struct LevelTrace {
+        DevArith& A;
+        bool on;
+        size_t k;
+        std::chrono::steady_clock::time_point t0, t1;
+        ~LevelTrace() {
+            if (!on) return;
+            cudaStreamSynchronize(A.stream());  // no throw from a destructor
+            const auto t2 = std::chrono::steady_clock::now();
+            std::fprintf(stderr, "[pi_device]   reciprocal level %zu bits: %.3f ms (levels below %.3f ms)\n", k,
+                         std::chrono::duration<double, std::milli>(t2 - t1).count(),
+                         std::chrono::duration<double, std::milli>(t1 - t0).count());
+        }
+    } ltrace{A, tr, k, tl0, tl1};
     A.shl(Z0, Zh, k - h);
     // E = 2^(2k) - R Z0. With R = 2^(k-h) (Rh + f), 0 <= f < 1, and Rh >= 2^(h-1):
     // |2^(2k)/R - Z0| <= (c + 4) 2^(k-h), so |E| < (c + 4) 2^(2k-h) < 2^(2k-h+3): E follows from
@@ -1746,7 +1792,11 @@ pg_status pg_pi(pg_ctx* ctx, size_t digits, char* out, double* seconds) {
     auto t1 = std::chrono::steady_clock::now();
     s = pg::guarded(ctx, [&] {
         pg::FinishState& fs = *pg::ctx_finish(ctx);
-        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), pg::ctx_stream(ctx), pg::ctx_launches(ctx), fs.pool);
+        // the finish's stream: the high-priority one after a splitting in one piece (the splitting
+        // has finished: bs_run_locked waited for it); the context's own when subtrees are merged
+        // here, since their splittings reuse the level buffers between merges on that stream
+        cudaStream_t fst = big ? pg::ctx_stream(ctx) : fs.finish_stream(pg::ctx_stream(ctx));
+        pg::DevArith A(pg::ctx_tables(ctx), pg::ctx_workspace(ctx), fst, pg::ctx_launches(ctx), fs.pool);
         // Q, R of the root (both positive for a = 0)
         pg::Num Q(A), R(A);
         if (big) {
