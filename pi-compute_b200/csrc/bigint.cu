@@ -227,7 +227,9 @@ __global__ void __launch_bounds__(kBigThreads) add_onepass_kernel(AddArgs A, uin
         for (int w = 0; w < kBigThreads / 32; ++w) agg = gp_compose(s_w[w], agg);
         volatile uint32_t* stw = A.seg + (blockIdx.x - seg);  // the job's status words
         const uint32_t tag = epoch << 8;
-        if (lane == 0 && seg > 0) stw[seg] = tag | 8u | agg;
+        const bool withheld = A.withhold1 && seg + 1 == A.withhold1;
+        const uint32_t limit = A.spin_limit ? A.spin_limit : kAddSpinLimit;
+        if (lane == 0 && seg > 0 && !withheld) stw[seg] = tag | 8u | agg;
         // look back 32 segments at a time: lane l reads segment j - l (j the window's nearest);
         // once every word of the window is valid, the nearest lane holding a carry out ends the
         // walk, and the window's function is the composition of the aggregates nearer than it
@@ -243,7 +245,7 @@ __global__ void __launch_bounds__(kBigThreads) add_onepass_kernel(AddArgs A, uin
                 uint32_t w = idx < 0 ? (tag | 16u | (A.cin << 2)) : stw[idx];
                 bool valid = (w >> 8) == epoch && (w & 24u);
                 while (!__all_sync(0xffffffffu, valid)) {
-                    if (++polls > kAddSpinLimit) {
+                    if (++polls > limit) {
                         timed_out = true;
                         break;
                     }
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(kBigThreads) add_onepass_kernel(AddArgs A, uin
         }
         if (lane == 0) {
             const uint32_t cout = gp_apply(agg, cin);
-            stw[seg] = tag | 16u | 8u | (cout << 2) | agg;
+            if (!withheld) stw[seg] = tag | 16u | 8u | (cout << 2) | agg;
             if (seg == nseg - 1 && A.carry_out) A.carry_out[job] = cout;
             s_cin = cin;
         }
@@ -669,6 +671,12 @@ void DevArith::run_add(const AddArgs& a0, int form) {
     if (form == 0 && add_onepass()) {
         if (!W_.sync) check(W_.ensure_sync(1), "error word");
         a.err = W_.sync;
+        // test hooks, read on every call so that a test can set and clear them around one
+        // operation: PG_TEST_ADD_SPIN_LIMIT=n ends each wait after n polls, PG_TEST_ADD_WITHHOLD=s
+        // keeps segment s from publishing its status, so that the later segments' waits run out
+        // (kErrAddWait; no GPU fault). Unset: the built-in limit, no hook.
+        if (const char* e = std::getenv("PG_TEST_ADD_SPIN_LIMIT")) a.spin_limit = (uint32_t)std::strtoul(e, nullptr, 10);
+        if (const char* e = std::getenv("PG_TEST_ADD_WITHHOLD")) a.withhold1 = (uint32_t)std::strtoul(e, nullptr, 10) + 1;
         if (++P_.add_epoch_ > 0xffffffu) {  // the epoch field wraps: clear the words, start again
             check(cudaMemsetAsync(seg_, 0, seg_cap_ * 4, st_), "DevArith segments");
             P_.add_epoch_ = 1;

@@ -47,6 +47,8 @@ struct AddArgs {
     uint32_t* seg;           // long form: per (job, segment) transfer / status words
     uint64_t njobs;
     uint32_t* err;           // one-pass form: error word (kErrAddWait)
+    uint32_t spin_limit;     // one-pass form: polls per wait (0: kAddSpinLimit)
+    uint32_t withhold1;      // test hook: segment withhold1 - 1 never publishes its status (0: none)
 };
 
 }  // namespace pg

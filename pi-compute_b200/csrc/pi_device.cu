@@ -1595,14 +1595,20 @@ pg_status product_errors(pg_ctx* ctx) {
     return PG_OK;
 }
 
+// Runs f, then reports the kernels' error word; when f throws, an error the kernels recorded
+// (a wait that ran out, say) is reported first: it is the cause, the throw its consequence.
 template <class F>
 pg_status guarded(pg_ctx* ctx, F&& f) {
     try {
         f();
     } catch (const DevError& e) {
-        return fail(ctx, e.status, e.what());
+        const std::string what = e.what();
+        const pg_status k = product_errors(ctx);
+        return k != PG_OK ? k : fail(ctx, e.status, what);
     } catch (const std::exception& e) {
-        return fail(ctx, PG_ERR_INTERNAL, e.what());
+        const std::string what = e.what();
+        const pg_status k = product_errors(ctx);
+        return k != PG_OK ? k : fail(ctx, PG_ERR_INTERNAL, what);
     }
     return product_errors(ctx);
 }

@@ -5,6 +5,9 @@ that fails. Both failures are made on the host, without faulting, trapping or ha
   from publishing its carry (PG_TEST_CRT_SPIN_LIMIT / PG_TEST_CRT_WITHHOLD, read by the library
   at every launch), so that the next block's wait runs out: the product must report
   PG_ERR_TIMEOUT, and the same context must then compute the product correctly;
+* the look-back wait of the one-launch long sums (add_onepass_kernel) the same way
+  (PG_TEST_ADD_SPIN_LIMIT / PG_TEST_ADD_WITHHOLD): a reciprocal whose sums span many segments must
+  report PG_ERR_TIMEOUT, and then be exact;
 * every library device allocation fails while PG_TEST_FAIL_DEVICE_ALLOC is set: a product that
   needs a larger workspace, and a device buffer, must report PG_ERR_OOM, and the context must
   work once the variable is cleared.
@@ -56,6 +59,18 @@ def test_lookback_wait_runs_out_and_context_recovers(eng):
     exp = oracle.mul_gmp(a, b)
     assert np.array_equal(_with_env(narrow, lambda: eng.mul_limbs(a, b)), exp)
     assert np.array_equal(eng.mul_limbs(a, b), exp)
+
+
+def test_sum_lookback_wait_runs_out_and_context_recovers(eng):
+    # a 2^21-bit reciprocal: its top Newton level sums numbers of 2^15 - 2^16 limbs (16-32
+    # segments of 2048); segment 2 never publishes its status, so the later segments' waits run out
+    k = 1 << 21
+    r = pkg.limbs_to_int(pkg.random_operand(k // 64, 21)) | (1 << (k - 1))
+    with pytest.raises(pkg.PgError) as err:
+        _with_env({"PG_TEST_ADD_SPIN_LIMIT": "2000", "PG_TEST_ADD_WITHHOLD": "2"}, lambda: eng.recip_floor(r))
+    assert err.value.status == pkg.PG_ERR_TIMEOUT
+    assert "sum look-back" in eng.last_error()
+    assert eng.recip_floor(r) == (1 << (2 * k)) // r
 
 
 def test_device_allocation_failure_is_oom_and_context_recovers(eng):
