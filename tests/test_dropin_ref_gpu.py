@@ -1,5 +1,5 @@
 """The drop-in inside the reference's own code: the reference's UNCHANGED BinarySplitting and
-PiEngine (compiled from its sources into oracle/_ref/libpiref_b200.so) run with this build's
+PiEngine (compiled from its sources into oracle/_ref/libpiref_b200.so) run with the library's
 pi::B200Multiplier behind their `Multiplier&` (binary_splitting.h:39, pi_engine.h:34), the way the
 reference's main.cpp:128-176 hands them its own GPU multipliers. P/Q/R must equal the reference's
 golden values (written by its GmpMultiplier run, tests/golden/bs_golden.json) and the digits its
