@@ -111,9 +111,12 @@ inline cudaError_t dev_malloc(T** p, size_t bytes) {
 }
 
 inline cudaError_t dev_free(void* p) {
-    if (!p) return cudaSuccess;
     FreeList& f = free_list();
     std::lock_guard<std::mutex> lk(f.mu);
+    if (!p) {
+        if (!f.pending.empty() && f.scopes.load() == 0) flush_pending_locked(f);
+        return cudaSuccess;
+    }
     size_t bytes = 0;
     auto it = f.sizes.find(p);
     if (it != f.sizes.end()) {
