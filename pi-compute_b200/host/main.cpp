@@ -137,6 +137,7 @@ int main(int argc, char** argv) {
         std::fprintf(stderr, "Error: --checkpoint needs --batched (the device-resident pipeline)\n");
         return 1;
     }
+    std::string mapped;  // the output file while it holds no digits yet (removed on an error)
     try {
         // The device context (CUDA context, twiddle tables, tuned splits) is made first so that the
         // trace can report it apart from the computation.
@@ -164,11 +165,13 @@ int main(int argc, char** argv) {
         pi::PiEngine eng(*mult);
         if (mapper.joinable()) mapper.join();
         cfg.digits_out = om.p;
+        if (om.p) mapped = output;
         const auto t_compute = std::chrono::steady_clock::now();
         pi::PiResult r = eng.compute(cfg);
         const auto t_write = std::chrono::steady_clock::now();
         if (om.p) {
             if (!om.finish()) throw std::runtime_error("cannot write " + output);
+            mapped.clear();
         } else {
             om.finish();
             FILE* f = std::fopen(output.c_str(), "wb");
@@ -204,6 +207,7 @@ int main(int argc, char** argv) {
         std::fflush(stderr);
         _exit(0);
     } catch (const std::exception& e) {
+        if (!mapped.empty()) ::unlink(mapped.c_str());  // no file of zeros left behind
         std::fprintf(stderr, "Error: %s\n", e.what());
         return 1;
     }
