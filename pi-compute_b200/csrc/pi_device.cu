@@ -402,7 +402,9 @@ void residue_diff(DevArith& A, DevNum& e, size_t p, const DevNum& xm, int logL) 
 // dropping E's low bits costs < 1/2 and the floor < 1 (the lower levels stay exact).
 // Reciprocals of up to this many bits are divided on the host (exact): the Newton levels below it
 // (k -> k/2 + 32 down to 64 bits, a dozen of them) would cost more in launches and host waits.
-constexpr size_t kHostRecipBits = 4096;
+// Knuth's division takes ~110 us at 12288 bits on one host core, a device level of 5-10 kbits
+// 0.3-0.7 ms while the helper stream's long kernels share the device.
+constexpr size_t kHostRecipBits = 12288;
 
 void recip_floor(DevArith& A, DevNum& Z, const DevNum& R, bool exact = true) {
     const size_t k = A.bits(R);
