@@ -183,7 +183,12 @@ void pg_graph_destroy(pg_graph* g);
  * pg_pi: the whole computation on one device: level-batched binary splitting over the
  *   reference's term count, then pg_pi_finish's steps, all in HBM. out receives digits + 2
  *   characters; seconds (if not NULL, 4 entries) receives splitting, final formula,
- *   conversion and total wall time. */
+ *   conversion and total wall time.
+ * pg_pi, pg_pi_finish and pg_pi_checkpointed free no device buffer while they run (cudaFree
+ *   waits for the whole device): the buffers they outgrow are freed by the next allocation or
+ *   free the library makes after they return (at the latest by pg_destroy), or at once when an
+ *   allocation fails for want of memory or when more than a quarter of the device's memory
+ *   waits to be freed. */
 pg_status pg_recip_floor(pg_ctx* ctx, const uint64_t* r, size_t nr, uint64_t* z, size_t zcap, size_t* zlen);
 /* out = a * b mod (2^(32 L) - 1), L = 2^logL (6 <= logL <= 26), for na, nb <= L/2 limbs: one
  * L-point transform product (the product wraps around) and a fold of its top words. The result
