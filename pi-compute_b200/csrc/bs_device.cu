@@ -884,6 +884,9 @@ struct DeviceBS {
                 else if (cmax <= 16)
                     bs_thread_merge_kernel<16><<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(in, out, P.nodes,
                                                                                                   a0, b0, d);
+                else if (cmax <= 20)
+                    bs_thread_merge_kernel<20><<<(unsigned)((P.nodes + 127) / 128), 128, 0, st>>>(in, out, P.nodes,
+                                                                                                  a0, b0, d);
                 else if (cmax <= 32)
                     bs_group_merge_kernel<32, 16><<<(unsigned)((P.nodes + 7) / 8), 128, 0, st>>>(in, out, P.nodes, a0,
                                                                                                  b0, d);
